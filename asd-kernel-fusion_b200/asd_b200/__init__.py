@@ -1,0 +1,283 @@
+"""Python binding of libasd_b200.so (ctypes).
+
+This is the host-side mirror of the reference's interface for the hot path:
+the reference's own entry points (``euler``, ``runge_kutta``, ``fused_dgemm``
+with their argument meaning) and the context API that runs whole steps on the
+GPU.  Spin arrays are float64 numpy arrays in the reference layout
+``[nfile][N*N][3]`` (llg_sqt_baseline.c:185, :202).
+
+The library is the product: this module only marshals arguments.  If the
+shared library is missing the import fails; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_ROOT = Path(__file__).resolve().parent.parent
+LIB_PATH = Path(os.environ.get("ASD_B200_LIB", PKG_ROOT / "lib" / "libasd_b200.so"))
+
+ASD_OK = 0
+ASD_ERR_INVALID = -1
+ASD_ERR_CUDA = -2
+ASD_ERR_NOMEM = -3
+ASD_ERR_TIMEOUT = -4
+ASD_ERR_STATE = -5
+ASD_ERR_UNSUPPORTED = -6
+
+SQT_FP64 = 0
+SQT_TF32X3 = 1
+SQT_BF16X3 = 2
+SQT_FP64_FUSED = 3
+MODE_NAMES = {SQT_FP64: "fp64", SQT_TF32X3: "tf32x3", SQT_BF16X3: "bf16x3", SQT_FP64_FUSED: "fp64_fused"}
+MODES = {v: k for k, v in MODE_NAMES.items()}
+
+# every symbol include/asd_b200.h declares
+EXPORTED_SYMBOLS = (
+    "asd_version", "asd_last_error", "asd_params_default", "asd_set_device",
+    "asd_ctx_create", "asd_ctx_destroy", "asd_ctx_set_stream", "asd_ctx_get_params",
+    "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
+    "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
+    "asd_ctx_step_host", "asd_ctx_last_launches", "asd_ctx_check_device_status",
+    "asd_umma_gemm_f32", "asd_set_params", "euler", "runge_kutta", "fused_dgemm",
+)
+
+
+class AsdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"asd error {code}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    """asd_params (include/asd_b200.h)."""
+
+    _fields_ = [
+        ("N", C.c_int),
+        ("nfile", C.c_int),
+        ("J1", C.c_double),
+        ("J2", C.c_double),
+        ("alpha", C.c_double),
+        ("hx", C.c_double),
+        ("hy", C.c_double),
+        ("hz", C.c_double),
+        ("dt", C.c_double),
+        ("spin_len", C.c_double),
+        ("vx", C.c_int),
+        ("vy", C.c_int),
+    ]
+
+    @classmethod
+    def make(cls, N, nfile, J1=1.0, dt=0.02, J2=0.0, alpha=0.0, h=(0.0, 0.0, 0.0),
+             spin_len=1.0, vx=None, vy=None):
+        vx = N // 10 if vx is None else vx
+        vy = N // 10 if vy is None else vy
+        return cls(int(N), int(nfile), float(J1), float(J2), float(alpha), float(h[0]),
+                   float(h[1]), float(h[2]), float(dt), float(spin_len), int(vx), int(vy))
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads libasd_b200.so once; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built; run __graft_entry__.build() or make -C "
+                          f"{PKG_ROOT}")
+    lib = C.CDLL(str(LIB_PATH))
+    vp = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    P = C.POINTER(Params)
+    sig = {
+        "asd_version": ([], C.c_char_p),
+        "asd_last_error": ([], C.c_char_p),
+        "asd_params_default": ([P, C.c_int, C.c_int], C.c_int),
+        "asd_set_device": ([C.c_int], C.c_int),
+        "asd_ctx_create": ([P, C.c_uint, C.POINTER(vp)], C.c_int),
+        "asd_ctx_destroy": ([vp], C.c_int),
+        "asd_ctx_set_stream": ([vp, vp], C.c_int),
+        "asd_ctx_get_params": ([vp, P], C.c_int),
+        "asd_ctx_set_spins": ([vp, vp, C.c_int], C.c_int),
+        "asd_ctx_set_spins_device": ([vp, vp, C.c_int], C.c_int),
+        "asd_ctx_get_spins": ([vp, vp], C.c_int),
+        "asd_ctx_get_spins_device": ([vp, vp], C.c_int),
+        "asd_ctx_step": ([vp, C.c_int], C.c_int),
+        "asd_ctx_sqt": ([vp, C.c_int, dp], C.c_int),
+        "asd_ctx_sqt_async": ([vp, C.c_int, vp], C.c_int),
+        "asd_ctx_step_host": ([vp, vp, vp, C.c_int, dp], C.c_int),
+        "asd_ctx_last_launches": ([vp], C.c_int),
+        "asd_ctx_check_device_status": ([vp], C.c_int),
+        "asd_umma_gemm_f32": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, C.c_long, vp],
+                              C.c_int),
+        "asd_set_params": ([C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
+        "euler": ([vp, vp], None),
+        "runge_kutta": ([vp] * 6, None),
+        "fused_dgemm": ([C.POINTER(C.c_int)] * 3 + [dp, vp, C.POINTER(C.c_int), vp,
+                                                   C.POINTER(C.c_int), vp, C.POINTER(C.c_int),
+                                                   vp, vp], None),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().asd_last_error().decode(errors="replace")
+
+
+def _check(rc: int) -> None:
+    if rc != ASD_OK:
+        raise AsdError(rc, last_error())
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _as_spins(a, N, nfile) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.size != N * N * nfile * 3:
+        raise ValueError(f"spins have {a.size} values, expected {nfile}x{N * N}x3")
+    return a
+
+
+def random_spins(N: int, nfile: int, seed: int, spin_len: float = 1.0) -> np.ndarray:
+    """Seeded spins uniform on the sphere, [nfile][N*N][3] float64 (test and bench input;
+    the reference's own initialisation is NaN, llg_sqt_baseline.c:196-206)."""
+    rng = np.random.default_rng(seed)
+    z = rng.uniform(-1.0, 1.0, size=(nfile, N * N))
+    phi = rng.uniform(0.0, 2.0 * np.pi, size=(nfile, N * N))
+    r = np.sqrt(1.0 - z * z)
+    s = np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=-1)
+    return np.ascontiguousarray(s * spin_len, dtype=np.float64)
+
+
+class Context:
+    """asd_ctx: one lattice with nfile replicas resident on the GPU."""
+
+    def __init__(self, params: Params, modes=None):
+        lib = load()
+        mask = 0
+        for m in (modes or ()):
+            mask |= 1 << (MODES[m] if isinstance(m, str) else int(m))
+        h = C.c_void_p()
+        _check(lib.asd_ctx_create(C.byref(params), mask, C.byref(h)))
+        self._h = h
+        self.params = params
+        self.N = params.N
+        self.nfile = params.nfile
+        self._out = (C.c_double * 2)()
+
+    def close(self) -> None:
+        if self._h:
+            load().asd_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(load().asd_ctx_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def set_spins(self, spins: np.ndarray, as_origin: bool = False) -> None:
+        s = _as_spins(spins, self.N, self.nfile)
+        _check(load().asd_ctx_set_spins(self._h, _ptr(s), int(as_origin)))
+
+    def set_spins_device(self, dptr: int, as_origin: bool = False) -> None:
+        _check(load().asd_ctx_set_spins_device(self._h, C.c_void_p(dptr), int(as_origin)))
+
+    def get_spins(self) -> np.ndarray:
+        out = np.empty((self.nfile, self.N * self.N, 3), dtype=np.float64)
+        _check(load().asd_ctx_get_spins(self._h, _ptr(out)))
+        return out
+
+    def get_spins_device(self, dptr: int) -> None:
+        _check(load().asd_ctx_get_spins_device(self._h, C.c_void_p(dptr)))
+
+    def step(self, nsteps: int = 1) -> None:
+        _check(load().asd_ctx_step(self._h, int(nsteps)))
+
+    def sqt(self, mode=SQT_TF32X3) -> complex:
+        mode = MODES[mode] if isinstance(mode, str) else int(mode)
+        _check(load().asd_ctx_sqt(self._h, mode, self._out))
+        return complex(self._out[0], self._out[1])
+
+    def sqt_async(self, mode, d_out_ptr: int) -> None:
+        mode = MODES[mode] if isinstance(mode, str) else int(mode)
+        _check(load().asd_ctx_sqt_async(self._h, mode, C.c_void_p(d_out_ptr)))
+
+    def step_host(self, spin_in_ptr: int, spin_out_ptr: int, mode=SQT_TF32X3) -> complex:
+        mode = MODES[mode] if isinstance(mode, str) else int(mode)
+        _check(load().asd_ctx_step_host(self._h, C.c_void_p(spin_in_ptr),
+                                        C.c_void_p(spin_out_ptr), mode, self._out))
+        return complex(self._out[0], self._out[1])
+
+    def last_launches(self) -> int:
+        return int(load().asd_ctx_last_launches(self._h))
+
+    def check_device_status(self) -> None:
+        _check(load().asd_ctx_check_device_status(self._h))
+
+
+# ------------------------------------------------------------ drop-in layer
+def set_params(N: int, nfile: int, J1: float = 1.0, dt: float = 0.02) -> None:
+    """asd_set_params: the globals the reference's functions read."""
+    _check(load().asd_set_params(int(N), int(nfile), float(J1), float(dt)))
+
+
+def euler(spin: np.ndarray) -> np.ndarray:
+    """The reference's euler(spin0, derivative) (llg_sqt_baseline.c:29)."""
+    s = np.ascontiguousarray(spin, dtype=np.float64)
+    d = np.full_like(s, np.nan)
+    load().euler(_ptr(s), _ptr(d))
+    return d
+
+
+def runge_kutta(spin: np.ndarray):
+    """The reference's runge_kutta (llg_sqt_baseline.c:95); returns cur, k1..k4."""
+    s = np.ascontiguousarray(spin, dtype=np.float64)
+    outs = [np.full_like(s, np.nan) for _ in range(5)]
+    load().runge_kutta(_ptr(s), *[_ptr(o) for o in outs])
+    return tuple(outs)
+
+
+def fused_dgemm(m, n, k, alpha, a, lda, b, ldb, c, ldc, q, sum_):
+    """The reference's fused_dgemm (kernel_fusion/gemm_kernel.h:355); updates c and sum_
+    in place."""
+    ci = lambda v: C.byref(C.c_int(int(v)))
+    al = C.c_double(float(alpha))
+    for arr in (a, b, c, q, sum_):
+        if not (arr.dtype == np.float64 and arr.flags.c_contiguous):
+            raise ValueError("fused_dgemm arrays must be C-contiguous float64")
+    load().fused_dgemm(ci(m), ci(n), ci(k), C.byref(al), _ptr(a), ci(lda), _ptr(b), ci(ldb),
+                       _ptr(c), ci(ldc), _ptr(q), _ptr(sum_))
+
+
+def umma_gemm_f32(kind: int, rows: int, Kp: int, a_hi: int, a_lo: int, b_hi: int, b_lo: int,
+                  c: int, ldc: int, stream: int = 0) -> None:
+    """asd_umma_gemm_f32 on device pointers (diagnostic)."""
+    _check(load().asd_umma_gemm_f32(int(kind), int(rows), int(Kp), C.c_void_p(a_hi),
+                                    C.c_void_p(a_lo), C.c_void_p(b_hi), C.c_void_p(b_lo),
+                                    C.c_void_p(c), int(ldc), C.c_void_p(stream)))

@@ -1,0 +1,111 @@
+// asd_internal.h -- declarations shared by the translation units of
+// libasd_b200.so (not part of the public ABI; see include/asd_b200.h).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/asd_b200.h"
+
+namespace asd {
+
+// Parameters of the LLG right-hand side, passed by value to the kernels.
+struct LLGArgs {
+    int N;        // lattice side
+    int nfile;    // replicas
+    long M;       // N*N
+    double J1, J2;
+    double hx, hy, hz;
+    double alpha;
+    double g;     // 1 / (1 + alpha^2), formed once on the host
+    double dt;
+    double spin_len;
+    int use_j2, use_h, use_damp;
+};
+
+LLGArgs make_llg_args(const asd_params &p);
+
+// ------------------------------------------------------------ error state
+void set_error(const char *fmt, ...);
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+#define ASD_CUDA_TRY(expr)                                   \
+    do {                                                     \
+        cudaError_t _e = (expr);                             \
+        if (_e != cudaSuccess) return ::asd::cuda_fail(_e, #expr); \
+    } while (0)
+
+// Device status word bits (written by kernels, read by the host).
+enum : unsigned { kStatusTimeout = 1u, kStatusBadLaunch = 2u };
+
+// ------------------------------------------------------------ LLG kernels
+// Spins live in the "site-major" layout double[M][nfile][3]: for site i the
+// 3*nfile values of all replicas are contiguous, which is both the stencil's
+// coalescing axis and the K axis of the correlation GEMM (the reference's
+// spin_zero layout, llg_sqt_baseline.c:227-236).
+// Launches one fused RK4 stage (1..4) over all sites and replicas.
+//   stage 1: ys_out = y + k/2,  acc = y + k/6          (k = dt * f(y))
+//   stage 2: ys_out = y + k/2,  acc = acc + k/3        (k = dt * f(ys_in))
+//   stage 3: ys_out = y + k,    acc = acc + k/3
+//   stage 4: y_new  = spin_len * o / |o|, o = acc + k/6 (written to ys_out)
+cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const double *ys_in,
+                             double *acc, double *ys_out, cudaStream_t st);
+
+// AoS [nfile][M][3] <-> site-major [M][nfile][3]
+cudaError_t launch_aos_to_sitemajor(const double *aos, double *sm, long M, int nfile,
+                                    cudaStream_t st);
+cudaError_t launch_sitemajor_to_aos(const double *sm, double *aos, long M, int nfile,
+                                    cudaStream_t st);
+
+// Drop-in kernels on the reference layout (AoS), reference arithmetic only.
+cudaError_t launch_euler_aos(const LLGArgs &a, const double *spin, double *deriv,
+                             cudaStream_t st);
+// pass 1..4 of runge_kutta's element-wise loops (llg_sqt_baseline.c:104-139)
+cudaError_t launch_rk_pass(int pass, long n, double dt, const double *spin, double *cur,
+                           double *k, const double *k1, const double *k2, const double *k3,
+                           cudaStream_t st);
+
+// --------------------------------------------------------- S(q,t) kernels
+// Per-site replica mean (FP64) plus the FP32 epilogue vectors
+// vec4[i] = (mx, my, mz, phase.re), vec1[i] = phase.im for i < M.
+cudaError_t launch_site_mean(const double *state, long M, int nfile, const double2 *phase,
+                             double *mean, float4 *vec4, float *vec1, cudaStream_t st);
+
+// FP64 state [M][K] -> split operands hi/lo [M][Kp] (zero for k >= K).
+// kind 1 = TF32 (stored as fp32 bit patterns), 2 = BF16.
+cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, void *hi,
+                         void *lo, cudaStream_t st);
+
+// Plain FP64 epilogue over a band of C (rows [i0, i0+mb), all n columns,
+// column-major, ldc = mb), C already scaled by 1/nfile: partial sums of
+// u_i w_j (C_ij - m_i . z_j) per block into part[2*block].
+cudaError_t launch_plain_epilogue(const double *C, long i0, long mb, long n, const double *mrow,
+                                  const double *zcol, const double2 *uphase,
+                                  const double2 *wphase, double2 *part, int nblocks_x,
+                                  int nblocks_y, cudaStream_t st);
+
+// out[0..1] = (sum of nparts partials) * scale, deterministic order.
+cudaError_t launch_finalize(const double2 *part, int nparts, double scale, double *out,
+                            cudaStream_t st);
+
+// ------------------------------------------------ tcgen05 split GEMM S(q,t)
+struct UmmaSqtArgs {
+    int kind;             // 1 = TF32x3, 2 = BF16x3
+    long M;               // rows (sites at t)   -- also the column count
+    int Kp;               // padded K (multiple of the 128-byte k block)
+    const void *a_hi, *a_lo;   // [M][Kp]
+    const void *b_hi, *b_lo;   // [M][Kp]
+    const float4 *row4; const float *row1;   // padded to the tile multiple
+    const float4 *col4; const float *col1;
+    float alpha;          // 1/nfile
+    double2 *part;        // one partial per CTA
+    unsigned *status;     // device status word
+    int num_sms;
+    float *dbg_c = nullptr;   // diagnostic: store the accumulator instead
+    long dbg_ldc = 0;
+};
+// Returns the number of CTAs launched (partials written) or a negative error.
+int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st);
+long umma_row_pad(long M);   // rows/cols padded to the tile multiple
+
+}  // namespace asd

@@ -1,0 +1,575 @@
+// ctx.cu -- the context API of libasd_b200.so (include/asd_b200.h): device
+// state, the per-step schedule and the S(q,t) dispatch.
+//
+// One context = one lattice with nfile replicas on one device and one CUDA
+// stream.  Device memory (site-major FP64 spins, M = N*N sites,
+// K = 3*nfile values per site):
+//   y, ys_a, ys_b, acc   RK4 state, stage inputs, running combination  4*M*K
+//   origin               the t = 0 snapshot (B of the GEMM)               M*K
+//   a/b hi/lo            split operands, [Mp][Kp] per enabled split kind
+//   band                 C band of the plain FP64 path (<= 2 GiB)
+// The AoS <-> site-major transposes stage through ys_b.
+#include <cublas_v2.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "asd_internal.h"
+#include "fp64_gemm.h"
+
+namespace asd {
+
+static thread_local char g_err[512] = "";
+static thread_local int g_device = 0;
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+int fail(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    snprintf(g_err, sizeof g_err, "%s: %s", what, cudaGetErrorString(e));
+    return ASD_ERR_CUDA;
+}
+
+int current_device() { return g_device; }
+
+}  // namespace asd
+
+using namespace asd;
+
+struct asd_ctx {
+    asd_params p{};
+    LLGArgs a{};
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    long M = 0, Mp = 0;
+    int K = 0;
+    unsigned modes = 0;
+    double *y = nullptr, *ys_a = nullptr, *ys_b = nullptr, *acc = nullptr, *origin = nullptr;
+    double *mean_t = nullptr, *mean_0 = nullptr;
+    double2 *uphase = nullptr, *wphase = nullptr;
+    float4 *row4 = nullptr, *col4 = nullptr;
+    float *row1 = nullptr, *col1 = nullptr;
+    // split operands per kind (index 1 = TF32, 2 = BF16)
+    void *a_hi[3] = {}, *a_lo[3] = {}, *b_hi[3] = {}, *b_lo[3] = {};
+    int Kp[3] = {};
+    long a_version[3] = {-1, -1, -1};
+    long b_version[3] = {-1, -1, -1};
+    double *band = nullptr;
+    long band_rows = 0;
+    double2 *part = nullptr;
+    long part_cap = 0;
+    double *d_out = nullptr;
+    double *h_out = nullptr;  // pinned
+    unsigned *status = nullptr;
+    cublasHandle_t blas = nullptr;
+    long state_version = 0, origin_version = -1;
+    bool has_state = false, has_origin = false;
+    int last_launches = 0;
+};
+
+namespace {
+
+template <class T>
+int dalloc(T **p, size_t bytes) {
+    cudaError_t e = cudaMalloc((void **)p, bytes < 16 ? 16 : bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(ASD_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    return ASD_OK;
+}
+
+int check_params(const asd_params *p) {
+    if (!p) return fail(ASD_ERR_INVALID, "params is NULL");
+    if (p->N < 3 || p->N > 4096) return fail(ASD_ERR_INVALID, "N=%d out of range [3, 4096]", p->N);
+    if (p->nfile < 1 || p->nfile > 1000000)
+        return fail(ASD_ERR_INVALID, "nfile=%d out of range", p->nfile);
+    if (!(p->spin_len > 0.0)) return fail(ASD_ERR_INVALID, "spin_len must be > 0");
+    if (!(p->dt == p->dt)) return fail(ASD_ERR_INVALID, "dt is NaN");
+    const double lim = 1e300;
+    const double v[] = {p->J1, p->J2, p->alpha, p->hx, p->hy, p->hz, p->dt};
+    for (double x : v)
+        if (!(x > -lim && x < lim)) return fail(ASD_ERR_INVALID, "non-finite parameter");
+    const double M = (double)p->N * p->N;
+    if (M * 3.0 * p->nfile > 4.0e9) return fail(ASD_ERR_INVALID, "N*N*3*nfile too large");
+    return ASD_OK;
+}
+
+int ensure_part(asd_ctx *c, long n) {
+    if (n <= c->part_cap) return ASD_OK;
+    if (c->part) cudaFree(c->part);
+    c->part = nullptr;
+    c->part_cap = 0;
+    int rc = dalloc(&c->part, (size_t)n * sizeof(double2));
+    if (rc == ASD_OK) c->part_cap = n;
+    return rc;
+}
+
+int kp_for(int kind, int K) {
+    const int ke = (kind == 2) ? 64 : 32;
+    return (K + ke - 1) / ke * ke;
+}
+
+int refresh_origin(asd_ctx *c) {
+    // origin mean and the column epilogue vectors
+    ASD_CUDA_TRY(launch_site_mean(c->origin, c->M, c->p.nfile, c->wphase, c->mean_0, c->col4,
+                                  c->col1, c->stream));
+    c->last_launches += 1;
+    c->origin_version = c->state_version;
+    for (int k = 1; k <= 2; ++k) c->b_version[k] = -1;
+    return ASD_OK;
+}
+
+int set_spins_common(asd_ctx *c, const double *aos, bool host, int as_origin) {
+    const size_t bytes = (size_t)c->M * c->K * sizeof(double);
+    if (!aos) return fail(ASD_ERR_INVALID, "spins pointer is NULL");
+    ASD_CUDA_TRY(cudaMemcpyAsync(c->ys_b, aos, bytes,
+                                 host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                 c->stream));
+    ASD_CUDA_TRY(launch_aos_to_sitemajor(c->ys_b, c->y, c->M, c->p.nfile, c->stream));
+    c->last_launches += 1;
+    c->state_version++;
+    c->has_state = true;
+    if (as_origin) {
+        ASD_CUDA_TRY(cudaMemcpyAsync(c->origin, c->y, bytes, cudaMemcpyDeviceToDevice, c->stream));
+        int rc = refresh_origin(c);
+        if (rc != ASD_OK) return rc;
+        c->has_origin = true;
+    }
+    return ASD_OK;
+}
+
+int run_steps(asd_ctx *c, int nsteps) {
+    for (int s = 0; s < nsteps; ++s) {
+        ASD_CUDA_TRY(launch_llg_stage(1, c->a, c->y, c->y, c->acc, c->ys_a, c->stream));
+        ASD_CUDA_TRY(launch_llg_stage(2, c->a, c->y, c->ys_a, c->acc, c->ys_b, c->stream));
+        ASD_CUDA_TRY(launch_llg_stage(3, c->a, c->y, c->ys_b, c->acc, c->ys_a, c->stream));
+        ASD_CUDA_TRY(launch_llg_stage(4, c->a, nullptr, c->ys_a, c->acc, c->y, c->stream));
+        c->last_launches += 4;
+        c->state_version++;
+    }
+    return ASD_OK;
+}
+
+int sqt_plain(asd_ctx *c, double *d_out) {
+    const long M = c->M;
+    const int K = c->K;
+    const double alpha = 1.0 / (double)c->p.nfile;
+    const double beta = 0.0;
+    const long mb = c->band_rows;
+    const int nby = 64;
+    long nparts = 0;
+    for (long i0 = 0; i0 < M; i0 += mb) {
+        const long rows = (M - i0 < mb) ? M - i0 : mb;
+        nparts += ((rows + 127) / 128) * nby;
+    }
+    int rc = ensure_part(c, nparts);
+    if (rc != ASD_OK) return rc;
+    long off = 0;
+    for (long i0 = 0; i0 < M; i0 += mb) {
+        const long rows = (M - i0 < mb) ? M - i0 : mb;
+        cublasStatus_t bs =
+            cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)rows, (int)M, K, &alpha,
+                        c->y + i0 * K, K, c->origin, K, &beta, c->band, (int)rows);
+        if (bs != CUBLAS_STATUS_SUCCESS) return fail(ASD_ERR_CUDA, "cublasDgemm failed (%d)", (int)bs);
+        const int nbx = (int)((rows + 127) / 128);
+        ASD_CUDA_TRY(launch_plain_epilogue(c->band, i0, rows, M, c->mean_t, c->mean_0, c->uphase,
+                                           c->wphase, c->part + off, nbx, nby, c->stream));
+        off += (long)nbx * nby;
+        c->last_launches += 1;  // the epilogue; the DGEMM is cuBLAS's
+    }
+    ASD_CUDA_TRY(launch_finalize(c->part, (int)off, 1.0 / (double)M, d_out, c->stream));
+    c->last_launches += 1;
+    return ASD_OK;
+}
+
+int sqt_fp64_fused(asd_ctx *c, double *d_out) {
+    Fp64GemmArgs g{};
+    g.dropin = 0;
+    g.m = c->M;
+    g.n = c->M;
+    g.k = c->K;
+    g.a = c->y;
+    g.sai = c->K;
+    g.sak = 1;
+    g.a_k_fast = 1;
+    g.b = c->origin;
+    g.sbk = 1;
+    g.sbj = c->K;
+    g.b_k_fast = 1;
+    g.alpha = 1.0 / (double)c->p.nfile;
+    g.mrow = c->mean_t;
+    g.zcol = c->mean_0;
+    g.uphase = c->uphase;
+    g.wphase = c->wphase;
+    const long np = fp64_gemm_num_parts(g);
+    int rc = ensure_part(c, np);
+    if (rc != ASD_OK) return rc;
+    g.part = c->part;
+    ASD_CUDA_TRY(launch_fp64_gemm(g, c->stream));
+    ASD_CUDA_TRY(launch_finalize(c->part, (int)np, 1.0 / (double)c->M, d_out, c->stream));
+    c->last_launches += 2;
+    return ASD_OK;
+}
+
+int sqt_split(asd_ctx *c, int kind, double *d_out) {
+    if (!c->a_hi[kind]) return fail(ASD_ERR_STATE, "split mode %d not enabled at create", kind);
+    if (c->a_version[kind] != c->state_version) {
+        ASD_CUDA_TRY(launch_split(kind, c->y, c->M, c->K, c->Kp[kind], c->a_hi[kind],
+                                  c->a_lo[kind], c->stream));
+        c->a_version[kind] = c->state_version;
+        c->last_launches += 1;
+    }
+    if (c->b_version[kind] != c->origin_version) {
+        ASD_CUDA_TRY(launch_split(kind, c->origin, c->M, c->K, c->Kp[kind], c->b_hi[kind],
+                                  c->b_lo[kind], c->stream));
+        c->b_version[kind] = c->origin_version;
+        c->last_launches += 1;
+    }
+    int rc = ensure_part(c, c->num_sms);
+    if (rc != ASD_OK) return rc;
+    UmmaSqtArgs u{};
+    u.kind = kind;
+    u.M = c->M;
+    u.Kp = c->Kp[kind];
+    u.a_hi = c->a_hi[kind];
+    u.a_lo = c->a_lo[kind];
+    u.b_hi = c->b_hi[kind];
+    u.b_lo = c->b_lo[kind];
+    u.row4 = c->row4;
+    u.row1 = c->row1;
+    u.col4 = c->col4;
+    u.col1 = c->col1;
+    u.alpha = (float)(1.0 / (double)c->p.nfile);
+    u.part = c->part;
+    u.status = c->status;
+    u.num_sms = c->num_sms;
+    const int grid = launch_umma_sqt(u, c->stream);
+    if (grid < 0) return grid;
+    ASD_CUDA_TRY(launch_finalize(c->part, grid, 1.0 / (double)c->M, d_out, c->stream));
+    c->last_launches += 2;
+    return ASD_OK;
+}
+
+int sqt_async(asd_ctx *c, int mode, double *d_out) {
+    if (!c->has_state || !c->has_origin)
+        return fail(ASD_ERR_STATE, "set the spins and the origin before S(q,t)");
+    if (mode < 0 || mode > 3) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
+    if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
+    ASD_CUDA_TRY(launch_site_mean(c->y, c->M, c->p.nfile, c->uphase, c->mean_t, c->row4, c->row1,
+                                  c->stream));
+    c->last_launches += 1;
+    switch (mode) {
+        case ASD_SQT_FP64: return sqt_plain(c, d_out);
+        case ASD_SQT_FP64_FUSED: return sqt_fp64_fused(c, d_out);
+        case ASD_SQT_TF32X3: return sqt_split(c, 1, d_out);
+        case ASD_SQT_BF16X3: return sqt_split(c, 2, d_out);
+    }
+    return ASD_ERR_INVALID;
+}
+
+int read_status(asd_ctx *c) {
+    unsigned st = 0;
+    ASD_CUDA_TRY(cudaMemcpyAsync(&st, c->status, sizeof st, cudaMemcpyDeviceToHost, c->stream));
+    ASD_CUDA_TRY(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream));
+    ASD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (st & kStatusTimeout) return fail(ASD_ERR_TIMEOUT, "a device-side wait gave up (status %u)", st);
+    if (st) return fail(ASD_ERR_CUDA, "device status %u", st);
+    return ASD_OK;
+}
+
+void destroy(asd_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    void *ptrs[] = {c->y, c->ys_a, c->ys_b, c->acc, c->origin, c->mean_t, c->mean_0, c->uphase,
+                    c->wphase, c->row4, c->col4, c->row1, c->col1, c->band, c->part, c->d_out,
+                    c->status};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    for (int k = 1; k <= 2; ++k) {
+        void *ops[] = {c->a_hi[k], c->a_lo[k], c->b_hi[k], c->b_lo[k]};
+        for (void *q : ops)
+            if (q) cudaFree(q);
+    }
+    if (c->h_out) cudaFreeHost(c->h_out);
+    if (c->blas) cublasDestroy(c->blas);
+    delete c;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *asd_version(void) { return "asd_b200 0.1 (sm_100a)"; }
+
+const char *asd_last_error(void) { return g_err; }
+
+int asd_params_default(asd_params *p, int N, int nfile) {
+    if (!p) return fail(ASD_ERR_INVALID, "params is NULL");
+    std::memset(p, 0, sizeof *p);
+    p->N = N;
+    p->nfile = nfile;
+    p->J1 = 1.0;
+    p->dt = 0.02;
+    p->spin_len = 1.0;
+    p->vx = N / 10;
+    p->vy = N / 10;
+    return ASD_OK;
+}
+
+int asd_set_device(int device) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= n) return fail(ASD_ERR_INVALID, "device %d of %d", device, n);
+    g_device = device;
+    return ASD_OK;
+}
+
+int asd_ctx_create(const asd_params *p, unsigned mode_mask, asd_ctx **out) {
+    if (!out) return fail(ASD_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int rc = check_params(p);
+    if (rc != ASD_OK) return rc;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(ASD_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(e));
+    ASD_CUDA_TRY(cudaSetDevice(g_device));
+    cudaDeviceProp prop;
+    ASD_CUDA_TRY(cudaGetDeviceProperties(&prop, g_device));
+    if (prop.major != 10)
+        return fail(ASD_ERR_UNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a",
+                    g_device, prop.major, prop.minor);
+
+    asd_ctx *c = new asd_ctx();
+    c->p = *p;
+    c->a = make_llg_args(*p);
+    c->device = g_device;
+    c->num_sms = prop.multiProcessorCount;
+    c->M = (long)p->N * p->N;
+    c->Mp = umma_row_pad(c->M);
+    c->K = 3 * p->nfile;
+    c->modes = mode_mask ? mode_mask : 0xFu;
+    const size_t sbytes = (size_t)c->M * c->K * sizeof(double);
+#define ASD_ALLOC(ptr, bytes)                 \
+    do {                                      \
+        rc = dalloc(&(ptr), (bytes));         \
+        if (rc != ASD_OK) { destroy(c); return rc; } \
+    } while (0)
+    ASD_ALLOC(c->y, sbytes);
+    ASD_ALLOC(c->ys_a, sbytes);
+    ASD_ALLOC(c->ys_b, sbytes);
+    ASD_ALLOC(c->acc, sbytes);
+    ASD_ALLOC(c->origin, sbytes);
+    ASD_ALLOC(c->mean_t, (size_t)c->M * 3 * sizeof(double));
+    ASD_ALLOC(c->mean_0, (size_t)c->M * 3 * sizeof(double));
+    ASD_ALLOC(c->uphase, (size_t)c->M * sizeof(double2));
+    ASD_ALLOC(c->wphase, (size_t)c->M * sizeof(double2));
+    ASD_ALLOC(c->row4, (size_t)c->Mp * sizeof(float4));
+    ASD_ALLOC(c->col4, (size_t)c->Mp * sizeof(float4));
+    ASD_ALLOC(c->row1, (size_t)c->Mp * sizeof(float));
+    ASD_ALLOC(c->col1, (size_t)c->Mp * sizeof(float));
+    ASD_ALLOC(c->d_out, 2 * sizeof(double));
+    ASD_ALLOC(c->status, sizeof(unsigned));
+    for (int kind = 1; kind <= 2; ++kind) {
+        const int mode = (kind == 1) ? ASD_SQT_TF32X3 : ASD_SQT_BF16X3;
+        if (!(c->modes & (1u << mode))) continue;
+        c->Kp[kind] = kp_for(kind, c->K);
+        const size_t ob = (size_t)c->Mp * c->Kp[kind] * (kind == 2 ? 2 : 4);
+        ASD_ALLOC(c->a_hi[kind], ob);
+        ASD_ALLOC(c->a_lo[kind], ob);
+        ASD_ALLOC(c->b_hi[kind], ob);
+        ASD_ALLOC(c->b_lo[kind], ob);
+        // padding rows stay zero for the lifetime of the context
+        ASD_CUDA_TRY(cudaMemset(c->a_hi[kind], 0, ob));
+        ASD_CUDA_TRY(cudaMemset(c->a_lo[kind], 0, ob));
+        ASD_CUDA_TRY(cudaMemset(c->b_hi[kind], 0, ob));
+        ASD_CUDA_TRY(cudaMemset(c->b_lo[kind], 0, ob));
+    }
+    if (c->modes & (1u << ASD_SQT_FP64)) {
+        long mb = (long)((2048.0 * 1024 * 1024) / (8.0 * c->M));
+        mb = mb / 128 * 128;
+        if (mb < 128) mb = 128;
+        if (mb > c->M) mb = c->M;
+        c->band_rows = mb;
+        ASD_ALLOC(c->band, (size_t)mb * c->M * sizeof(double));
+        if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) {
+            destroy(c);
+            return fail(ASD_ERR_CUDA, "cublasCreate failed");
+        }
+    }
+#undef ASD_ALLOC
+    ASD_CUDA_TRY(cudaMemset(c->row4, 0, (size_t)c->Mp * sizeof(float4)));
+    ASD_CUDA_TRY(cudaMemset(c->col4, 0, (size_t)c->Mp * sizeof(float4)));
+    ASD_CUDA_TRY(cudaMemset(c->row1, 0, (size_t)c->Mp * sizeof(float)));
+    ASD_CUDA_TRY(cudaMemset(c->col1, 0, (size_t)c->Mp * sizeof(float)));
+    ASD_CUDA_TRY(cudaMemset(c->status, 0, sizeof(unsigned)));
+    e = cudaMallocHost((void **)&c->h_out, 2 * sizeof(double));
+    if (e != cudaSuccess) {
+        destroy(c);
+        return cuda_fail(e, "cudaMallocHost");
+    }
+    // Phases u_i = e^{-i q.r_i} and w_j = e^{+i q.r_j}, q = 2 pi (vx, vy) / N
+    // (llg_sqt_baseline.c:267-268), so that u_i w_j = e^{-i q.(r_i - r_j)}.
+    {
+        const double qx = 2.0 * M_PI * p->vx / (double)p->N;
+        const double qy = 2.0 * M_PI * p->vy / (double)p->N;
+        std::vector<double2> u((size_t)c->M), w((size_t)c->M);
+        for (long i = 0; i < c->M; ++i) {
+            const double th = qx * (double)(i / p->N) + qy * (double)(i % p->N);
+            const double cs = std::cos(th), sn = std::sin(th);
+            u[i] = make_double2(cs, -sn);
+            w[i] = make_double2(cs, sn);
+        }
+        ASD_CUDA_TRY(cudaMemcpy(c->uphase, u.data(), (size_t)c->M * sizeof(double2),
+                                cudaMemcpyHostToDevice));
+        ASD_CUDA_TRY(cudaMemcpy(c->wphase, w.data(), (size_t)c->M * sizeof(double2),
+                                cudaMemcpyHostToDevice));
+    }
+    rc = ensure_part(c, c->num_sms);
+    if (rc != ASD_OK) {
+        destroy(c);
+        return rc;
+    }
+    *out = c;
+    return ASD_OK;
+}
+
+int asd_ctx_destroy(asd_ctx *ctx) {
+    destroy(ctx);
+    return ASD_OK;
+}
+
+int asd_ctx_set_stream(asd_ctx *c, void *stream) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    c->stream = (cudaStream_t)stream;
+    if (c->blas) cublasSetStream(c->blas, c->stream);
+    return ASD_OK;
+}
+
+int asd_ctx_get_params(const asd_ctx *c, asd_params *p) {
+    if (!c || !p) return fail(ASD_ERR_INVALID, "NULL argument");
+    *p = c->p;
+    return ASD_OK;
+}
+
+int asd_ctx_set_spins(asd_ctx *c, const double *spin_aos, int as_origin) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    c->last_launches = 0;
+    int rc = set_spins_common(c, spin_aos, true, as_origin);
+    if (rc != ASD_OK) return rc;
+    ASD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return ASD_OK;
+}
+
+int asd_ctx_set_spins_device(asd_ctx *c, const double *d_spin_aos, int as_origin) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    c->last_launches = 0;
+    return set_spins_common(c, d_spin_aos, false, as_origin);
+}
+
+int asd_ctx_get_spins(asd_ctx *c, double *spin_aos) {
+    if (!c || !spin_aos) return fail(ASD_ERR_INVALID, "NULL argument");
+    if (!c->has_state) return fail(ASD_ERR_STATE, "no spins set");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(launch_sitemajor_to_aos(c->y, c->ys_b, c->M, c->p.nfile, c->stream));
+    ASD_CUDA_TRY(cudaMemcpyAsync(spin_aos, c->ys_b, (size_t)c->M * c->K * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->stream));
+    ASD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return ASD_OK;
+}
+
+int asd_ctx_get_spins_device(asd_ctx *c, double *d_spin_aos) {
+    if (!c || !d_spin_aos) return fail(ASD_ERR_INVALID, "NULL argument");
+    if (!c->has_state) return fail(ASD_ERR_STATE, "no spins set");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(launch_sitemajor_to_aos(c->y, d_spin_aos, c->M, c->p.nfile, c->stream));
+    return ASD_OK;
+}
+
+int asd_ctx_step(asd_ctx *c, int nsteps) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    if (nsteps < 0) return fail(ASD_ERR_INVALID, "nsteps < 0");
+    if (!c->has_state) return fail(ASD_ERR_STATE, "no spins set");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    c->last_launches = 0;
+    return run_steps(c, nsteps);
+}
+
+int asd_ctx_sqt_async(asd_ctx *c, asd_sqt_mode mode, double *d_out) {
+    if (!c || !d_out) return fail(ASD_ERR_INVALID, "NULL argument");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    c->last_launches = 0;
+    return sqt_async(c, (int)mode, d_out);
+}
+
+int asd_ctx_sqt(asd_ctx *c, asd_sqt_mode mode, double out[2]) {
+    if (!c || !out) return fail(ASD_ERR_INVALID, "NULL argument");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    c->last_launches = 0;
+    int rc = sqt_async(c, (int)mode, c->d_out);
+    if (rc != ASD_OK) return rc;
+    ASD_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    rc = read_status(c);  // synchronises
+    if (rc != ASD_OK) return rc;
+    out[0] = c->h_out[0];
+    out[1] = c->h_out[1];
+    return ASD_OK;
+}
+
+int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_sqt_mode mode,
+                      double sqt_out[2]) {
+    if (!c || !spin_in || !spin_out || !sqt_out) return fail(ASD_ERR_INVALID, "NULL argument");
+    if (!c->has_origin) return fail(ASD_ERR_STATE, "set the origin (t = 0 spins) first");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    c->last_launches = 0;
+    int rc = set_spins_common(c, spin_in, true, 0);
+    if (rc != ASD_OK) return rc;
+    rc = run_steps(c, 1);
+    if (rc != ASD_OK) return rc;
+    rc = sqt_async(c, (int)mode, c->d_out);
+    if (rc != ASD_OK) return rc;
+    ASD_CUDA_TRY(launch_sitemajor_to_aos(c->y, c->ys_b, c->M, c->p.nfile, c->stream));
+    ASD_CUDA_TRY(cudaMemcpyAsync(spin_out, c->ys_b, (size_t)c->M * c->K * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->stream));
+    ASD_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    c->last_launches += 1;
+    rc = read_status(c);
+    if (rc != ASD_OK) return rc;
+    sqt_out[0] = c->h_out[0];
+    sqt_out[1] = c->h_out[1];
+    return ASD_OK;
+}
+
+int asd_ctx_last_launches(const asd_ctx *c) { return c ? c->last_launches : 0; }
+
+int asd_ctx_check_device_status(asd_ctx *c) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    return read_status(c);
+}
+
+}  // extern "C"

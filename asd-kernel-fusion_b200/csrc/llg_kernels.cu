@@ -1,0 +1,301 @@
+// llg_kernels.cu -- RK4 time stepping of the LLG equation on the GPU, FP64.
+//
+// Arithmetic contract: every operation is an explicitly rounded FP64
+// intrinsic (__dmul_rn, __dadd_rn, __dsub_rn, __ddiv_rn, __dsqrt_rn), in the
+// order the reference writes it, so the compiler cannot contract a*b+c into
+// an FMA.  With alpha = J2 = h = 0 the trajectory is therefore bit-identical
+// to the reference's euler / runge_kutta / renormalisation built with
+// -ffp-contract=off (llg_sqt_baseline.c:29-142, :298-309).
+#include "asd_internal.h"
+
+namespace asd {
+namespace {
+
+__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dq(double a, double b) { return __ddiv_rn(a, b); }
+
+struct V3 {
+    double x, y, z;
+};
+
+// dS/dt at one (site, replica).  y is indexed as y[site*sstride + off + c].
+// Neighbour order and periodic wrap follow llg_sqt_baseline.c:59-77 with
+// nn = {(1,0), (-1,0), (0,-1), (0,1)} (:175-178); the exchange field starts
+// at 0 and accumulates t*J1 per neighbour (:52, :73-75); tau = H x S
+// (v3d_cross, v3d.h:48-53).  Extensions, each skipped when zero: J2 over the
+// diagonal neighbours (1,1), (1,-1), (-1,1), (-1,-1); the Zeeman field; and
+// Gilbert damping g * (tau + alpha * (S x tau)).
+template <bool J2, bool H, bool DAMP>
+__device__ __forceinline__ V3 llg_rhs(const double *__restrict__ y, long sstride, long off,
+                                      int N, int row, int col, const LLGArgs &a) {
+    const int rp = (row + 1 == N) ? 0 : row + 1;
+    const int rm = (row == 0) ? N - 1 : row - 1;
+    const int cp = (col + 1 == N) ? 0 : col + 1;
+    const int cm = (col == 0) ? N - 1 : col - 1;
+    const long site = (long)row * N + col;
+    const double *c0 = y + site * sstride + off;
+    const double sx = c0[0], sy = c0[1], sz = c0[2];
+    const long nb[4] = {(long)rp * N + col, (long)rm * N + col, (long)row * N + cm,
+                        (long)row * N + cp};
+    double ex = 0.0, ey = 0.0, ez = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double *t = y + nb[j] * sstride + off;
+        ex = da(ex, dm(t[0], a.J1));
+        ey = da(ey, dm(t[1], a.J1));
+        ez = da(ez, dm(t[2], a.J1));
+    }
+    if (J2) {
+        const long nn2[4] = {(long)rp * N + cp, (long)rp * N + cm, (long)rm * N + cp,
+                             (long)rm * N + cm};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double *t = y + nn2[j] * sstride + off;
+            ex = da(ex, dm(t[0], a.J2));
+            ey = da(ey, dm(t[1], a.J2));
+            ez = da(ez, dm(t[2], a.J2));
+        }
+    }
+    if (H) {
+        ex = da(ex, a.hx);
+        ey = da(ey, a.hy);
+        ez = da(ez, a.hz);
+    }
+    V3 tau;
+    tau.x = ds(dm(ey, sz), dm(ez, sy));
+    tau.y = ds(dm(ez, sx), dm(ex, sz));
+    tau.z = ds(dm(ex, sy), dm(ey, sx));
+    if (!DAMP) return tau;
+    const double ux = ds(dm(sy, tau.z), dm(sz, tau.y));
+    const double uy = ds(dm(sz, tau.x), dm(sx, tau.z));
+    const double uz = ds(dm(sx, tau.y), dm(sy, tau.x));
+    V3 d;
+    d.x = dm(a.g, da(tau.x, dm(a.alpha, ux)));
+    d.y = dm(a.g, da(tau.y, dm(a.alpha, uy)));
+    d.z = dm(a.g, da(tau.z, dm(a.alpha, uz)));
+    return d;
+}
+
+// One fused RK4 stage, site-major layout.  Thread t handles replica
+// f = t % nfile of site t / nfile, so a warp touches 32 consecutive 24-byte
+// records (768 contiguous bytes) of each operand.  The combination order
+// reproduces runge_kutta's final sum spin + k1/6 + k2/3 + k3/3 + k4/6
+// evaluated left to right (llg_sqt_baseline.c:138), carried in acc.
+template <int STAGE, bool J2, bool H, bool DAMP>
+__global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double *__restrict__ y,
+                                                        const double *__restrict__ ys,
+                                                        double *__restrict__ acc,
+                                                        double *__restrict__ out) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long total = a.M * a.nfile;
+    if (t >= total) return;
+    const long site = t / a.nfile;
+    const int f = (int)(t - site * a.nfile);
+    const int row = (int)(site / a.N), col = (int)(site - (long)row * a.N);
+    const long sstride = 3L * a.nfile;
+    const long off = 3L * f;
+    const V3 d = llg_rhs<J2, H, DAMP>(ys, sstride, off, a.N, row, col, a);
+    const long e = site * sstride + off;
+    const double k0 = dm(d.x, a.dt), k1 = dm(d.y, a.dt), k2 = dm(d.z, a.dt);
+    if (STAGE == 1) {
+        const double y0 = y[e], y1 = y[e + 1], y2 = y[e + 2];
+        out[e] = da(y0, dq(k0, 2.0));
+        out[e + 1] = da(y1, dq(k1, 2.0));
+        out[e + 2] = da(y2, dq(k2, 2.0));
+        acc[e] = da(y0, dq(k0, 6.0));
+        acc[e + 1] = da(y1, dq(k1, 6.0));
+        acc[e + 2] = da(y2, dq(k2, 6.0));
+    } else if (STAGE == 2 || STAGE == 3) {
+        const double y0 = y[e], y1 = y[e + 1], y2 = y[e + 2];
+        if (STAGE == 2) {
+            out[e] = da(y0, dq(k0, 2.0));
+            out[e + 1] = da(y1, dq(k1, 2.0));
+            out[e + 2] = da(y2, dq(k2, 2.0));
+        } else {
+            out[e] = da(y0, k0);
+            out[e + 1] = da(y1, k1);
+            out[e + 2] = da(y2, k2);
+        }
+        acc[e] = da(acc[e], dq(k0, 3.0));
+        acc[e + 1] = da(acc[e + 1], dq(k1, 3.0));
+        acc[e + 2] = da(acc[e + 2], dq(k2, 3.0));
+    } else {
+        const double o0 = da(acc[e], dq(k0, 6.0));
+        const double o1 = da(acc[e + 1], dq(k1, 6.0));
+        const double o2 = da(acc[e + 2], dq(k2, 6.0));
+        // llg_sqt_baseline.c:301-308 / llg_sqt_fusion.c:353-360
+        const double nrm = __dsqrt_rn(da(da(dm(o0, o0), dm(o1, o1)), dm(o2, o2)));
+        out[e] = dq(dm(a.spin_len, o0), nrm);
+        out[e + 1] = dq(dm(a.spin_len, o1), nrm);
+        out[e + 2] = dq(dm(a.spin_len, o2), nrm);
+    }
+}
+
+template <int STAGE>
+cudaError_t launch_stage_t(const LLGArgs &a, const double *y, const double *ys, double *acc,
+                           double *out, cudaStream_t st) {
+    const long total = a.M * a.nfile;
+    const int threads = 256;
+    const unsigned blocks = (unsigned)((total + threads - 1) / threads);
+    const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
+#define ASD_STAGE_CASE(S, J, Hh, D)                                                            \
+    case S:                                                                                    \
+        llg_stage_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(a, y, ys, acc, out);     \
+        break;
+    switch (sel) {
+        ASD_STAGE_CASE(0, false, false, false)
+        ASD_STAGE_CASE(1, false, false, true)
+        ASD_STAGE_CASE(2, false, true, false)
+        ASD_STAGE_CASE(3, false, true, true)
+        ASD_STAGE_CASE(4, true, false, false)
+        ASD_STAGE_CASE(5, true, false, true)
+        ASD_STAGE_CASE(6, true, true, false)
+        ASD_STAGE_CASE(7, true, true, true)
+    }
+#undef ASD_STAGE_CASE
+    return cudaGetLastError();
+}
+
+// Tiled transpose between [nfile][M][3] and [M][nfile][3] through shared
+// memory: 32 sites x 32 replicas x 3 doubles per block.
+template <bool TO_SITEMAJOR>
+__global__ void __launch_bounds__(256) transpose_kernel(const double *__restrict__ src,
+                                                        double *__restrict__ dst, long M,
+                                                        int nfile) {
+    __shared__ double tile[32][32 * 3 + 1];
+    const long s0 = (long)blockIdx.x * 32;
+    const int f0 = blockIdx.y * 32;
+    // read
+    for (int idx = threadIdx.x; idx < 32 * 96; idx += blockDim.x) {
+        if (TO_SITEMAJOR) {
+            // AoS: for replica f0+r, 96 contiguous doubles of sites s0..s0+31
+            const int r = idx / 96, w = idx % 96;
+            const int f = f0 + r;
+            const long s = s0 + w / 3;
+            if (f < nfile && s < M) tile[r][w] = src[((long)f * M + s0) * 3 + w];
+        } else {
+            // site-major: for site s0+r, 96 contiguous doubles of replicas f0..f0+31
+            const int r = idx / 96, w = idx % 96;
+            const long s = s0 + r;
+            const int f = f0 + w / 3;
+            if (f < nfile && s < M) tile[r][w] = src[(s * nfile + f0) * 3 + w];
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 32 * 96; idx += blockDim.x) {
+        const int r = idx / 96, w = idx % 96;
+        const int c = w % 3, q = w / 3;
+        if (TO_SITEMAJOR) {
+            // write site s0+r, replicas f0..: value from tile[f-f0][(s-s0)*3+c]
+            const long s = s0 + r;
+            const int f = f0 + q;
+            if (f < nfile && s < M) dst[(s * nfile + f) * 3 + c] = tile[q][r * 3 + c];
+        } else {
+            const int f = f0 + r;
+            const long s = s0 + q;
+            if (f < nfile && s < M) dst[((long)f * M + s) * 3 + c] = tile[q][r * 3 + c];
+        }
+    }
+}
+
+// euler on the reference layout: thread t -> site t % M of replica t / M
+// (the reference's loop order, llg_sqt_baseline.c:44-48), reference physics.
+__global__ void __launch_bounds__(256) euler_aos_kernel(LLGArgs a, const double *__restrict__ y,
+                                                        double *__restrict__ d) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.M * a.nfile) return;
+    const long f = t / a.M;
+    const long site = t - f * a.M;
+    const int row = (int)(site / a.N), col = (int)(site - (long)row * a.N);
+    const V3 r = llg_rhs<false, false, false>(y, 3, f * a.M * 3, a.N, row, col, a);
+    d[t * 3] = r.x;
+    d[t * 3 + 1] = r.y;
+    d[t * 3 + 2] = r.z;
+}
+
+// runge_kutta's element-wise loops (llg_sqt_baseline.c:104-139).
+__global__ void rk_pass_kernel(int pass, long n, double dt, const double *__restrict__ spin,
+                               double *__restrict__ cur, double *__restrict__ k,
+                               const double *__restrict__ k1, const double *__restrict__ k2,
+                               const double *__restrict__ k3) {
+    const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double kk = dm(k[j], dt);
+    k[j] = kk;
+    if (pass == 1 || pass == 2) {
+        cur[j] = da(spin[j], dq(kk, 2.0));
+    } else if (pass == 3) {
+        cur[j] = da(spin[j], kk);
+    } else {
+        double v = da(spin[j], dq(k1[j], 6.0));
+        v = da(v, dq(k2[j], 3.0));
+        v = da(v, dq(k3[j], 3.0));
+        cur[j] = da(v, dq(kk, 6.0));
+    }
+}
+
+}  // namespace
+
+LLGArgs make_llg_args(const asd_params &p) {
+    LLGArgs a;
+    a.N = p.N;
+    a.nfile = p.nfile;
+    a.M = (long)p.N * p.N;
+    a.J1 = p.J1;
+    a.J2 = p.J2;
+    a.hx = p.hx;
+    a.hy = p.hy;
+    a.hz = p.hz;
+    a.alpha = p.alpha;
+    a.g = 1.0 / (1.0 + p.alpha * p.alpha);
+    a.dt = p.dt;
+    a.spin_len = p.spin_len;
+    a.use_j2 = p.J2 != 0.0;
+    a.use_h = (p.hx != 0.0 || p.hy != 0.0 || p.hz != 0.0);
+    a.use_damp = p.alpha != 0.0;
+    return a;
+}
+
+cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const double *ys_in,
+                             double *acc, double *ys_out, cudaStream_t st) {
+    switch (stage) {
+        case 1: return launch_stage_t<1>(a, y, ys_in, acc, ys_out, st);
+        case 2: return launch_stage_t<2>(a, y, ys_in, acc, ys_out, st);
+        case 3: return launch_stage_t<3>(a, y, ys_in, acc, ys_out, st);
+        case 4: return launch_stage_t<4>(a, y, ys_in, acc, ys_out, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_aos_to_sitemajor(const double *aos, double *sm, long M, int nfile,
+                                    cudaStream_t st) {
+    dim3 grid((unsigned)((M + 31) / 32), (unsigned)((nfile + 31) / 32));
+    transpose_kernel<true><<<grid, 256, 0, st>>>(aos, sm, M, nfile);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sitemajor_to_aos(const double *sm, double *aos, long M, int nfile,
+                                    cudaStream_t st) {
+    dim3 grid((unsigned)((M + 31) / 32), (unsigned)((nfile + 31) / 32));
+    transpose_kernel<false><<<grid, 256, 0, st>>>(sm, aos, M, nfile);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_euler_aos(const LLGArgs &a, const double *spin, double *deriv,
+                             cudaStream_t st) {
+    const long total = a.M * a.nfile;
+    euler_aos_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a, spin, deriv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rk_pass(int pass, long n, double dt, const double *spin, double *cur,
+                           double *k, const double *k1, const double *k2, const double *k3,
+                           cudaStream_t st) {
+    rk_pass_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(pass, n, dt, spin, cur, k, k1,
+                                                                 k2, k3);
+    return cudaGetLastError();
+}
+
+}  // namespace asd

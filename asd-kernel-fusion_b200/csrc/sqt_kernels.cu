@@ -1,0 +1,202 @@
+// sqt_kernels.cu -- the memory-bound pieces around the S(q,t) correlation
+// GEMM: replica means, operand splitting, the FP64 phase epilogue of the
+// plain path, and the deterministic final reduction.
+//
+// S(q,t) = (1/M) sum_ij u_i w_j (C_ij - m_i . z_j),  C = (1/nfile) A B^T,
+// with u_i = e^{-i q.r_i}, w_j = e^{+i q.r_j} (so u_i w_j is the reference's
+// qmat entry e^{-i q.(r_i - r_j)}, gemm/llg_sqt_mkl.c:290-300), m_i the
+// replica mean at t (fint_avg, :349-366) and z_j the mean at t = 0
+// (zerot_avg, llg_sqt_baseline.c:240-259).
+#include <cuda_bf16.h>
+
+#include "asd_internal.h"
+
+namespace asd {
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One warp per site: mean over replicas of the 3 components.
+__global__ void __launch_bounds__(256) site_mean_kernel(const double *__restrict__ state, long M,
+                                                        int nfile,
+                                                        const double2 *__restrict__ phase,
+                                                        double *__restrict__ mean,
+                                                        float4 *__restrict__ vec4,
+                                                        float *__restrict__ vec1) {
+    const long site = (long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    if (site >= M) return;
+    const double *p = state + site * 3L * nfile;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int f = lane; f < nfile; f += 32) {
+        sx += p[3 * f];
+        sy += p[3 * f + 1];
+        sz += p[3 * f + 2];
+    }
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    sz = warp_sum(sz);
+    if (lane == 0) {
+        const double mx = sx / nfile, my = sy / nfile, mz = sz / nfile;
+        mean[site * 3] = mx;
+        mean[site * 3 + 1] = my;
+        mean[site * 3 + 2] = mz;
+        const double2 ph = phase[site];
+        vec4[site] = make_float4((float)mx, (float)my, (float)mz, (float)ph.x);
+        vec1[site] = (float)ph.y;
+    }
+}
+
+// hi = round(x), lo = round(x - hi), each to the operand format.
+__device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
+    uint32_t h, l;
+    const float xf = (float)x;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(xf));
+    hi = __uint_as_float(h);
+    const float rf = (float)(x - (double)hi);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rf));
+    lo = __uint_as_float(l);
+}
+
+__global__ void __launch_bounds__(256) split_tf32_kernel(const double *__restrict__ s, long M,
+                                                         int K, int Kp, float2 *__restrict__ hi,
+                                                         float2 *__restrict__ lo) {
+    // one thread per pair of consecutive k (Kp is even)
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int half = Kp / 2;
+    if (t >= M * half) return;
+    const long row = t / half;
+    const int k = (int)(t - row * half) * 2;
+    float2 h = make_float2(0.f, 0.f), l = make_float2(0.f, 0.f);
+    if (k < K) split_tf32(s[row * K + k], h.x, l.x);
+    if (k + 1 < K) split_tf32(s[row * K + k + 1], h.y, l.y);
+    hi[t] = h;
+    lo[t] = l;
+}
+
+__global__ void __launch_bounds__(256) split_bf16_kernel(const double *__restrict__ s, long M,
+                                                         int K, int Kp,
+                                                         __nv_bfloat162 *__restrict__ hi,
+                                                         __nv_bfloat162 *__restrict__ lo) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int half = Kp / 2;
+    if (t >= M * half) return;
+    const long row = t / half;
+    const int k = (int)(t - row * half) * 2;
+    double x0 = 0.0, x1 = 0.0;
+    if (k < K) x0 = s[row * K + k];
+    if (k + 1 < K) x1 = s[row * K + k + 1];
+    const __nv_bfloat16 h0 = __double2bfloat16(x0), h1 = __double2bfloat16(x1);
+    const __nv_bfloat16 l0 = __double2bfloat16(x0 - (double)__bfloat162float(h0));
+    const __nv_bfloat16 l1 = __double2bfloat16(x1 - (double)__bfloat162float(h1));
+    hi[t] = __halves2bfloat162(h0, h1);
+    lo[t] = __halves2bfloat162(l0, l1);
+}
+
+// Plain FP64 epilogue.  Block (bx, by): rows [i0 + 128*bx, +128) of the band,
+// columns j = by, by + gridDim.y, ...  Thread = one row; a warp reads 32
+// consecutive rows of one column (coalesced, column-major C).
+__global__ void __launch_bounds__(128) plain_epilogue_kernel(
+    const double *__restrict__ C, long i0, long mb, long n, const double *__restrict__ mrow,
+    const double *__restrict__ zcol, const double2 *__restrict__ uphase,
+    const double2 *__restrict__ wphase, double2 *__restrict__ part) {
+    const long li = (long)blockIdx.x * 128 + threadIdx.x;
+    double tre = 0.0, tim = 0.0;
+    if (li < mb) {
+        const long i = i0 + li;
+        const double mx = mrow[i * 3], my = mrow[i * 3 + 1], mz = mrow[i * 3 + 2];
+        double sre = 0.0, sim = 0.0;
+        for (long j = blockIdx.y; j < n; j += gridDim.y) {
+            const double outer = mx * zcol[j * 3] + my * zcol[j * 3 + 1] + mz * zcol[j * 3 + 2];
+            const double v = C[li + j * mb] - outer;
+            const double2 w = wphase[j];
+            sre += w.x * v;
+            sim += w.y * v;
+        }
+        const double2 u = uphase[i];
+        tre = u.x * sre - u.y * sim;
+        tim = u.x * sim + u.y * sre;
+    }
+    __shared__ double red[2][4];
+    tre = warp_sum(tre);
+    tim = warp_sum(tim);
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x / 32] = tre;
+        red[1][threadIdx.x / 32] = tim;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double a = (red[0][0] + red[0][1]) + (red[0][2] + red[0][3]);
+        const double b = (red[1][0] + red[1][1]) + (red[1][2] + red[1][3]);
+        part[(long)blockIdx.y * gridDim.x + blockIdx.x] = make_double2(a, b);
+    }
+}
+
+// Single block, fixed summation order: thread t sums t, t+256, ... then a
+// shared-memory tree.
+__global__ void __launch_bounds__(256) finalize_kernel(const double2 *__restrict__ part,
+                                                       int nparts, double scale,
+                                                       double *__restrict__ out) {
+    __shared__ double sre[256], sim[256];
+    double a = 0.0, b = 0.0;
+    for (int k = threadIdx.x; k < nparts; k += 256) {
+        a += part[k].x;
+        b += part[k].y;
+    }
+    sre[threadIdx.x] = a;
+    sim[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            sre[threadIdx.x] += sre[threadIdx.x + s];
+            sim[threadIdx.x] += sim[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sre[0] * scale;
+        out[1] = sim[0] * scale;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_site_mean(const double *state, long M, int nfile, const double2 *phase,
+                             double *mean, float4 *vec4, float *vec1, cudaStream_t st) {
+    const unsigned blocks = (unsigned)((M + 7) / 8);
+    site_mean_kernel<<<blocks, 256, 0, st>>>(state, M, nfile, phase, mean, vec4, vec1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, void *hi, void *lo,
+                         cudaStream_t st) {
+    const long total = M * (Kp / 2);
+    const unsigned blocks = (unsigned)((total + 255) / 256);
+    if (kind == 1)
+        split_tf32_kernel<<<blocks, 256, 0, st>>>(state, M, K, Kp, (float2 *)hi, (float2 *)lo);
+    else
+        split_bf16_kernel<<<blocks, 256, 0, st>>>(state, M, K, Kp, (__nv_bfloat162 *)hi,
+                                                  (__nv_bfloat162 *)lo);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plain_epilogue(const double *C, long i0, long mb, long n, const double *mrow,
+                                  const double *zcol, const double2 *uphase,
+                                  const double2 *wphase, double2 *part, int nblocks_x,
+                                  int nblocks_y, cudaStream_t st) {
+    dim3 grid((unsigned)nblocks_x, (unsigned)nblocks_y);
+    plain_epilogue_kernel<<<grid, 128, 0, st>>>(C, i0, mb, n, mrow, zcol, uphase, wphase, part);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const double2 *part, int nparts, double scale, double *out,
+                            cudaStream_t st) {
+    finalize_kernel<<<1, 256, 0, st>>>(part, nparts, scale, out);
+    return cudaGetLastError();
+}
+
+}  // namespace asd

@@ -1,0 +1,414 @@
+// umma_sqt.cu -- S(q,t) as one persistent tcgen05 GEMM with the phase, the
+// connected-part subtraction and the reduction fused into its epilogue.
+//
+// This is the B200 counterpart of the reference's fused_dgemm + KERNEL
+// (kernel_fusion/gemm_kernel.h:1-224, :355-422), which streams the full C
+// and qmat matrices (2 N^4 + 2 N^4 doubles) through its store epilogue.
+// Here neither C nor qmat exists: the phase factorises as u_i * w_j and the
+// outer term as m_i . z_j, so the epilogue needs only per-row and per-column
+// vectors, and each CTA leaves one complex partial sum.
+//
+// Precision (3-term split): A = Ah + Al, B = Bh + Bl in TF32 or BF16, the
+// tensor cores accumulate Ah Bh + Ah Bl + Al Bh in FP32 in TMEM; the epilogue
+// works in FP32 per 32-column chunk and accumulates in FP64 across chunks,
+// tiles and CTAs.
+//
+// Roles (192 threads, one CTA per SM, persistent over 128 x 256 tiles):
+//   warp 0      TMA producer (one thread): 4 tiles per k block (Ah, Al, Bh, Bl)
+//   warp 1      MMA issuer (one thread): 3 x 4 tcgen05.mma per k block
+//   warps 2..5  epilogue: TMEM -> registers, phase/outer/reduction
+// TMEM holds two 128 x 256 FP32 accumulators (all 512 columns), so the
+// epilogue of one tile overlaps the MMAs of the next.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "asd_internal.h"
+#include "ptx_sm100.cuh"
+
+namespace asd {
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 256;
+constexpr int STAGES = 2;
+constexpr int ROW_BYTES = 128;                  // one swizzle row per k block
+constexpr int A_TILE = BM * ROW_BYTES;          // 16 KB
+constexpr int B_TILE = BN * ROW_BYTES;          // 32 KB
+constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;  // 96 KB
+constexpr int NUM_THREADS = 192;
+constexpr int TMEM_COLS = 512;
+constexpr uint32_t WAIT_LIMIT = 1u << 24;
+constexpr int GROUP_M = 8;
+
+struct SmemTail {
+    uint64_t full[STAGES];
+    uint64_t empty[STAGES];
+    uint64_t tfull[2];
+    uint64_t tempty[2];
+    uint64_t drain;
+    uint32_t tmem_base;
+    int abort_flag;
+    double red[2][4];
+};
+constexpr int SMEM_BYTES = 1024 /*alignment slack*/ + STAGES * STAGE_BYTES + sizeof(SmemTail);
+
+__device__ __forceinline__ void tile_coords(int tile, int num_m, int num_n, int &mb, int &nb) {
+    const int per_group = GROUP_M * num_n;
+    const int group = tile / per_group;
+    const int first_m = group * GROUP_M;
+    const int gsz = min(GROUP_M, num_m - first_m);
+    const int r = tile - group * per_group;
+    mb = first_m + r % gsz;
+    nb = r / gsz;
+}
+
+__device__ __forceinline__ void raise_abort(SmemTail *t, unsigned *status) {
+    t->abort_flag = 1;
+    if (status) atomicOr(status, (unsigned)kStatusTimeout);
+}
+
+// KIND: 1 = TF32x3, 2 = BF16x3.  STORE: instead of the S(q,t) epilogue,
+// write the raw FP32 accumulator to dbg_c[i * dbg_ldc + j] (diagnostic).
+template <int KIND, bool STORE>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    umma_sqt_kernel(const __grid_constant__ CUtensorMap tm_ah,
+                    const __grid_constant__ CUtensorMap tm_al,
+                    const __grid_constant__ CUtensorMap tm_bh,
+                    const __grid_constant__ CUtensorMap tm_bl, int num_m, int num_n, int num_kb,
+                    const float4 *__restrict__ row4, const float *__restrict__ row1,
+                    const float4 *__restrict__ col4, const float *__restrict__ col1, float alpha,
+                    double2 *__restrict__ part, unsigned *__restrict__ status,
+                    float *__restrict__ dbg_c, long dbg_ldc) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    SmemTail *tail = reinterpret_cast<SmemTail *>(smem + STAGES * STAGE_BYTES);
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    const int num_tiles = num_m * num_n;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            ptx::mbar_init(&tail->full[s], 1);
+            ptx::mbar_init(&tail->empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            ptx::mbar_init(&tail->tfull[b], 1);
+            ptx::mbar_init(&tail->tempty[b], 4);
+        }
+        ptx::mbar_init(&tail->drain, 1);
+        tail->abort_flag = 0;
+        ptx::fence_mbar_init();
+    }
+    if (warp == 0) {
+        ptx::tmem_alloc(&tail->tmem_base, TMEM_COLS);
+        ptx::tmem_relinquish();
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const uint32_t tmem_base = tail->tmem_base;
+    volatile int *abort_flag = &tail->abort_flag;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            ptx::tma_prefetch_desc(&tm_ah);
+            ptx::tma_prefetch_desc(&tm_al);
+            ptx::tma_prefetch_desc(&tm_bh);
+            ptx::tma_prefetch_desc(&tm_bl);
+            constexpr int KE = (KIND == 2) ? 64 : 32;  // elements per 128-byte row
+            int stage = 0;
+            uint32_t phase = 0;
+            bool issued[STAGES] = {};
+            uint32_t issued_parity[STAGES] = {};
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+                int mb, nb;
+                tile_coords(tile, num_m, num_n, mb, nb);
+                for (int kb = 0; kb < num_kb; ++kb) {
+                    if (!ptx::mbar_wait_bounded(&tail->empty[stage], phase ^ 1u, abort_flag,
+                                                WAIT_LIMIT)) {
+                        raise_abort(tail, status);
+                        ok = false;
+                        break;
+                    }
+                    uint8_t *st = smem + stage * STAGE_BYTES;
+                    ptx::mbar_arrive_expect_tx(&tail->full[stage], STAGE_BYTES);
+                    const int x = kb * KE;
+                    ptx::tma_load_2d(st, &tm_ah, &tail->full[stage], x, mb * BM);
+                    ptx::tma_load_2d(st + A_TILE, &tm_al, &tail->full[stage], x, mb * BM);
+                    ptx::tma_load_2d(st + 2 * A_TILE, &tm_bh, &tail->full[stage], x, nb * BN);
+                    ptx::tma_load_2d(st + 2 * A_TILE + B_TILE, &tm_bl, &tail->full[stage], x,
+                                     nb * BN);
+                    issued[stage] = true;
+                    issued_parity[stage] = phase;
+                    if (++stage == STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            // Never leave the CTA with bulk copies still landing in shared
+            // memory: wait (bounded, ignoring the abort flag) for the last
+            // fill of every stage.
+            for (int s = 0; s < STAGES; ++s) {
+                if (!issued[s]) continue;
+                uint32_t i = 0;
+                while (!ptx::mbar_try_wait(&tail->full[s], issued_parity[s]) && i < WAIT_LIMIT) {
+                    ++i;
+                    __nanosleep(64);
+                }
+                if (i >= WAIT_LIMIT && status) atomicOr(status, (unsigned)kStatusTimeout);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t IDESC = ptx::umma_idesc(KIND == 2 ? 1u : 2u, BM, BN);
+            int stage = 0;
+            uint32_t phase = 0;
+            int abuf = 0;
+            uint32_t aphase = 0;
+            bool ok = true;
+            const uint32_t smem_base = ptx::smem_u32(smem);
+            for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+                if (!ptx::mbar_wait_bounded(&tail->tempty[abuf], aphase ^ 1u, abort_flag,
+                                            WAIT_LIMIT)) {
+                    raise_abort(tail, status);
+                    break;
+                }
+                ptx::tc_fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)(abuf * BN);
+                for (int kb = 0; kb < num_kb; ++kb) {
+                    if (!ptx::mbar_wait_bounded(&tail->full[stage], phase, abort_flag,
+                                                WAIT_LIMIT)) {
+                        raise_abort(tail, status);
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
+                    const uint32_t s0 = smem_base + stage * STAGE_BYTES;
+                    const uint64_t dah = ptx::umma_desc_kmajor_sw128(s0);
+                    const uint64_t dal = ptx::umma_desc_kmajor_sw128(s0 + A_TILE);
+                    const uint64_t dbh = ptx::umma_desc_kmajor_sw128(s0 + 2 * A_TILE);
+                    const uint64_t dbl = ptx::umma_desc_kmajor_sw128(s0 + 2 * A_TILE + B_TILE);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const uint64_t adv = (uint64_t)(2 * kk);  // 32 bytes per MMA k step
+                        const uint32_t accum = (kb > 0 || kk > 0) ? 1u : 0u;
+                        if (KIND == 2) {
+                            ptx::umma_f16(d_tmem, dah + adv, dbh + adv, IDESC, accum);
+                            ptx::umma_f16(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
+                            ptx::umma_f16(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
+                        } else {
+                            ptx::umma_tf32(d_tmem, dah + adv, dbh + adv, IDESC, accum);
+                            ptx::umma_tf32(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
+                            ptx::umma_tf32(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
+                        }
+                    }
+                    ptx::umma_commit(&tail->empty[stage]);
+                    if (++stage == STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                ptx::umma_commit(&tail->tfull[abuf]);
+                if (++abuf == 2) {
+                    abuf = 0;
+                    aphase ^= 1u;
+                }
+            }
+            // Wait for every issued MMA before TMEM can be released.
+            ptx::umma_commit(&tail->drain);
+            uint32_t i = 0;
+            while (!ptx::mbar_try_wait(&tail->drain, 0u) && i < WAIT_LIMIT) {
+                ++i;
+                __nanosleep(64);
+            }
+            if (i >= WAIT_LIMIT && status) atomicOr(status, (unsigned)kStatusTimeout);
+        }
+    } else {
+        // Epilogue warps 2..5 own TMEM lane quarters (warp % 4) * 32.
+        const int quarter = warp & 3;
+        const int rloc = quarter * 32 + lane;
+        int abuf = 0;
+        uint32_t aphase = 0;
+        double tot_re = 0.0, tot_im = 0.0;
+        for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+            int mb, nb;
+            tile_coords(tile, num_m, num_n, mb, nb);
+            const long i = (long)mb * BM + rloc;
+            const float4 r4 = STORE ? make_float4(0.f, 0.f, 0.f, 0.f) : row4[i];
+            const float ui = STORE ? 0.f : row1[i];
+            if (!ptx::mbar_wait_bounded(&tail->tfull[abuf], aphase, abort_flag, WAIT_LIMIT)) {
+                raise_abort(tail, status);
+                break;
+            }
+            ptx::tc_fence_after();
+            double s_re = 0.0, s_im = 0.0;
+            const long j0 = (long)nb * BN;
+#pragma unroll 1
+            for (int c = 0; c < BN / 32; ++c) {
+                uint32_t v[32];
+                const uint32_t taddr =
+                    tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(abuf * BN + c * 32);
+                ptx::tmem_ld_32x32b_x32(taddr, v);
+                ptx::tmem_ld_wait();
+                if (STORE) {
+                    float *dst = dbg_c + i * dbg_ldc + j0 + c * 32;
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) dst[jj] = __uint_as_float(v[jj]);
+                    continue;
+                }
+                float cre = 0.f, cim = 0.f;
+#pragma unroll
+                for (int jj = 0; jj < 32; ++jj) {
+                    const long j = j0 + c * 32 + jj;
+                    const float4 z = __ldg(&col4[j]);
+                    const float wim = __ldg(&col1[j]);
+                    float o = r4.x * z.x;
+                    o = fmaf(r4.y, z.y, o);
+                    o = fmaf(r4.z, z.z, o);
+                    const float val = fmaf(alpha, __uint_as_float(v[jj]), -o);
+                    cre = fmaf(z.w, val, cre);
+                    cim = fmaf(wim, val, cim);
+                }
+                s_re += (double)cre;
+                s_im += (double)cim;
+            }
+            ptx::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&tail->tempty[abuf]);
+            // u_i * s_i with u_i = (r4.w, ui)
+            tot_re += (double)r4.w * s_re - (double)ui * s_im;
+            tot_im += (double)r4.w * s_im + (double)ui * s_re;
+            if (++abuf == 2) {
+                abuf = 0;
+                aphase ^= 1u;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            tot_re += __shfl_xor_sync(0xffffffffu, tot_re, o);
+            tot_im += __shfl_xor_sync(0xffffffffu, tot_im, o);
+        }
+        if (lane == 0) {
+            tail->red[0][warp - 2] = tot_re;
+            tail->red[1][warp - 2] = tot_im;
+        }
+    }
+
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    if (threadIdx.x == 0 && !STORE) {
+        const double re = (tail->red[0][0] + tail->red[0][1]) + (tail->red[0][2] + tail->red[0][3]);
+        const double im = (tail->red[1][0] + tail->red[1][1]) + (tail->red[1][2] + tail->red[1][3]);
+        part[blockIdx.x] = make_double2(re, im);
+    }
+    if (warp == 0) ptx::tmem_dealloc(tmem_base, TMEM_COLS);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// Row-major [rows][Kp] operand, box = 128 bytes of K x box_rows rows, 128B swizzle.
+int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int box_rows) {
+    auto enc = get_encode_fn();
+    if (!enc) return fail(ASD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const int esize = (kind == 2) ? 2 : 4;
+    const CUtensorMapDataType dt =
+        (kind == 2) ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    cuuint64_t gdim[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+    cuuint64_t gstride[1] = {(cuuint64_t)Kp * esize};
+    cuuint32_t box[2] = {(cuuint32_t)(128 / esize), (cuuint32_t)box_rows};
+    cuuint32_t estride[2] = {1, 1};
+    CUresult r = enc(m, dt, 2, const_cast<void *>(base), gdim, gstride, box, estride,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(ASD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return ASD_OK;
+}
+
+}  // namespace
+
+long umma_row_pad(long M) { return (M + BN - 1) / BN * BN; }
+
+int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
+    const long Mp = umma_row_pad(a.M);
+    const int ke = (a.kind == 2) ? 64 : 32;
+    if (a.Kp % ke != 0 || a.Kp <= 0) return fail(ASD_ERR_INVALID, "Kp=%d not a multiple of %d", a.Kp, ke);
+    if (((uintptr_t)a.a_hi | (uintptr_t)a.a_lo | (uintptr_t)a.b_hi | (uintptr_t)a.b_lo) & 15)
+        return fail(ASD_ERR_INVALID, "operand base not 16-byte aligned");
+    CUtensorMap tah, tal, tbh, tbl;
+    int rc;
+    if ((rc = make_tmap(&tah, a.a_hi, a.kind, Mp, a.Kp, BM)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tal, a.a_lo, a.kind, Mp, a.Kp, BM)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tbh, a.b_hi, a.kind, Mp, a.Kp, BN)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tbl, a.b_lo, a.kind, Mp, a.Kp, BN)) != ASD_OK) return rc;
+    const int num_m = (int)(Mp / BM), num_n = (int)(Mp / BN), num_kb = a.Kp / ke;
+    const int tiles = num_m * num_n;
+    const int grid = tiles < a.num_sms ? tiles : a.num_sms;
+    cudaError_t e;
+    auto go = [&](auto kern) {
+        cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             SMEM_BYTES);
+        if (r == cudaSuccess)
+            kern<<<grid, NUM_THREADS, SMEM_BYTES, st>>>(tah, tal, tbh, tbl, num_m, num_n, num_kb,
+                                                        a.row4, a.row1, a.col4, a.col1, a.alpha,
+                                                        a.part, a.status, a.dbg_c, a.dbg_ldc);
+        return r;
+    };
+    if (a.kind == 2)
+        e = a.dbg_c ? go(umma_sqt_kernel<2, true>) : go(umma_sqt_kernel<2, false>);
+    else
+        e = a.dbg_c ? go(umma_sqt_kernel<1, true>) : go(umma_sqt_kernel<1, false>);
+    if (e != cudaSuccess) return cuda_fail(e, "umma_sqt setup");
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "umma_sqt launch");
+    return grid;
+}
+
+}  // namespace asd
+
+// Diagnostic entry point (declared in include/asd_b200.h): the bare
+// split-precision tensor-core product C = Ah Bh^T + Ah Bl^T + Al Bh^T, FP32,
+// device pointers, rows a multiple of 256.
+extern "C" int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, const void *a_lo,
+                                 const void *b_hi, const void *b_lo, float *c, long ldc,
+                                 void *stream) {
+    using namespace asd;
+    if (kind != 1 && kind != 2) return fail(ASD_ERR_INVALID, "kind must be 1 (TF32) or 2 (BF16)");
+    if (rows <= 0 || rows % 256 != 0) return fail(ASD_ERR_INVALID, "rows must be a multiple of 256");
+    if (!a_hi || !a_lo || !b_hi || !b_lo || !c || ldc < rows)
+        return fail(ASD_ERR_INVALID, "bad pointer or ldc");
+    int dev = 0, sms = 0;
+    ASD_CUDA_TRY(cudaGetDevice(&dev));
+    ASD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    UmmaSqtArgs u{};
+    u.kind = kind;
+    u.M = rows;
+    u.Kp = Kp;
+    u.a_hi = a_hi;
+    u.a_lo = a_lo;
+    u.b_hi = b_hi;
+    u.b_lo = b_lo;
+    u.num_sms = sms;
+    u.dbg_c = c;
+    u.dbg_ldc = ldc;
+    const int g = launch_umma_sqt(u, (cudaStream_t)stream);
+    return g < 0 ? g : ASD_OK;
+}

@@ -1,0 +1,169 @@
+/*
+ * asd_b200.h -- C ABI of libasd_b200.so, a B200 (sm_100a) implementation of
+ * the hot path of hwchen2017/ASD-kernel-fusion: RK4 time stepping of the
+ * Landau-Lifshitz(-Gilbert) equation for classical spins on a periodic
+ * N x N lattice, and the GEMM-formulated real-space spin-spin correlation
+ * that gives the dynamical structure factor S(q,t).
+ *
+ * Two layers:
+ *
+ *  1. Drop-in symbols with the reference's names, signatures and semantics
+ *     (host pointers, synchronous, parameters taken from the caller's globals
+ *     or from asd_set_params):
+ *        euler            <- baseline/llg_sqt_baseline.c:29
+ *        runge_kutta      <- baseline/llg_sqt_baseline.c:95
+ *        fused_dgemm      <- kernel_fusion/gemm_kernel.h:355
+ *     A C program of the reference links libasd_b200.so instead of defining
+ *     these functions itself.
+ *
+ *  2. A context API (asd_ctx_*) that keeps the replicas' spins resident in
+ *     HBM and runs a whole step on one CUDA stream: four fused RK4 stage
+ *     kernels (the last one renormalises), then S(q,t) through a tcgen05
+ *     tensor-core GEMM in split precision (TF32x3 or BF16x3) whose epilogue
+ *     applies the phase, the connected-part subtraction and the reduction,
+ *     or through the FP64 path.  It replaces the per-step body of main()
+ *     (llg_sqt_baseline.c:289-426, llg_sqt_fusion.c:340-449).
+ *
+ * Spin arrays crossing the ABI use the reference's layout, "AoS":
+ * double[nfile][N*N][3] (llg_sqt_baseline.c:185, :202), site index
+ * i = row*N + col.  All functions returning int return ASD_OK (0) or a
+ * negative ASD_ERR_* code; asd_last_error() describes the last failure on the
+ * calling thread.  There is no CPU fallback: without a usable sm_100 device
+ * every call that computes returns ASD_ERR_CUDA.
+ */
+#ifndef ASD_B200_H
+#define ASD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ASD_OK 0
+#define ASD_ERR_INVALID (-1)     /* a parameter is out of range            */
+#define ASD_ERR_CUDA (-2)        /* a CUDA runtime or cuBLAS call failed     */
+#define ASD_ERR_NOMEM (-3)       /* device or host allocation failed         */
+#define ASD_ERR_TIMEOUT (-4)     /* a bounded device-side wait gave up       */
+#define ASD_ERR_STATE (-5)       /* call order (e.g. no spins set yet)       */
+#define ASD_ERR_UNSUPPORTED (-6) /* the device is not sm_100                 */
+
+/* Arithmetic of the S(q,t) correlation GEMM. */
+typedef enum {
+    ASD_SQT_FP64 = 0,   /* FP64 GEMM (cuBLAS DGEMM) + FP64 phase epilogue: the plain path */
+    ASD_SQT_TF32X3 = 1, /* tcgen05 kind::tf32, hi*hi + hi*lo + lo*hi, FP32 accumulate   */
+    ASD_SQT_BF16X3 = 2, /* tcgen05 kind::f16 (bf16), hi*hi + hi*lo + lo*hi, FP32 accum. */
+    ASD_SQT_FP64_FUSED = 3 /* FP64 CUDA-core GEMM with the phase epilogue fused          */
+} asd_sqt_mode;
+
+/* Model parameters.  The reference hard-wires alpha = J2 = h = 0,
+ * spin_len = 1 (1.5 in its fusion program) and vx = vy = N/10
+ * (llg_sqt_baseline.c:12-20, :172-173). */
+typedef struct {
+    int N;           /* lattice side (>= 3); M = N*N sites                        */
+    int nfile;       /* independent replicas ("snapshots", Nfile)                */
+    double J1;       /* nearest-neighbour exchange (J1, :14)                     */
+    double J2;       /* next-nearest (diagonal) exchange                          */
+    double alpha;    /* Gilbert damping                                           */
+    double hx, hy, hz; /* Zeeman field, added to H_eff.  The reference's commented
+                          term exchg.z += -hz (llg_sqt_baseline.c:79) is h=(0,0,-hz). */
+    double dt;       /* RK4 step (dt, :16)                                        */
+    double spin_len; /* length after renormalisation                              */
+    int vx, vy;      /* q = 2*pi*(vx, vy)/N                                       */
+} asd_params;
+
+/* ----------------------------------------------------------------- common */
+const char *asd_version(void);
+const char *asd_last_error(void);
+/* Reference defaults for N and nfile: J1=1, dt=0.02, spin_len=1, vx=vy=N/10. */
+int asd_params_default(asd_params *p, int N, int nfile);
+/* Selects the CUDA device used by later calls on this thread (default 0). */
+int asd_set_device(int device);
+
+/* ------------------------------------------------------------ context API */
+typedef struct asd_ctx asd_ctx;
+
+/* Allocates the device state for p (about 4 spin arrays in FP64 plus the
+ * split GEMM operands).  mode_mask: bit (1<<asd_sqt_mode) for every S(q,t)
+ * mode the context must be able to run (0 = all).  Replaces the set-up in
+ * main(), llg_sqt_baseline.c:146-287. */
+int asd_ctx_create(const asd_params *p, unsigned mode_mask, asd_ctx **out);
+int asd_ctx_destroy(asd_ctx *ctx);
+/* Runs all later work of ctx on this CUDA stream (a cudaStream_t). */
+int asd_ctx_set_stream(asd_ctx *ctx, void *stream);
+int asd_ctx_get_params(const asd_ctx *ctx, asd_params *p);
+
+/* Copies spins (AoS, host) to the device as the current state.  With
+ * as_origin != 0 they also become the t = 0 snapshot that S(q,t) correlates
+ * against (spin_zero and zerot_avg, llg_sqt_baseline.c:227-259). */
+int asd_ctx_set_spins(asd_ctx *ctx, const double *spin_aos, int as_origin);
+/* Same from a device buffer in the AoS layout. */
+int asd_ctx_set_spins_device(asd_ctx *ctx, const double *d_spin_aos, int as_origin);
+/* Copies the current state back (AoS, host). */
+int asd_ctx_get_spins(asd_ctx *ctx, double *spin_aos);
+int asd_ctx_get_spins_device(asd_ctx *ctx, double *d_spin_aos);
+
+/* nsteps RK4 steps with renormalisation (llg_sqt_baseline.c:296-309),
+ * asynchronous on the context's stream. */
+int asd_ctx_step(asd_ctx *ctx, int nsteps);
+
+/* S(q,t) between the current state and the origin at q = 2*pi*(vx,vy)/N,
+ * into out[0] (real) and out[1] (imaginary); synchronous.  Equals
+ * sqt[num] of the reference (llg_sqt_fusion.c:368-442, gemm/llg_sqt_mkl.c:347-423). */
+int asd_ctx_sqt(asd_ctx *ctx, asd_sqt_mode mode, double out[2]);
+/* Asynchronous form: writes out[0..1] (a device pointer) on the stream. */
+int asd_ctx_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
+
+/* One full step through host buffers, the reference's own contract: spins
+ * (AoS) come from host memory, one RK4 step runs, the new spins go back to
+ * spin_out and S(q,t) into sqt_out.  spin_in may equal spin_out. */
+int asd_ctx_step_host(asd_ctx *ctx, const double *spin_in, double *spin_out,
+                      asd_sqt_mode mode, double sqt_out[2]);
+
+/* Number of kernels the last asd_ctx_step / asd_ctx_sqt* call launched. */
+int asd_ctx_last_launches(const asd_ctx *ctx);
+
+/* Status word set by device code (bounded waits that gave up, etc.);
+ * returns ASD_OK or ASD_ERR_TIMEOUT and clears it. */
+int asd_ctx_check_device_status(asd_ctx *ctx);
+
+/* Diagnostic: the bare tensor-core product of the split S(q,t) GEMM,
+ * C[i*ldc + j] = sum_k Ah[i][k]Bh[j][k] + Ah[i][k]Bl[j][k] + Al[i][k]Bh[j][k]
+ * in FP32, for device operands [rows][Kp] (kind 1: TF32 bit patterns in
+ * float, kind 2: bf16), rows a multiple of 256, Kp a multiple of 32 (TF32)
+ * or 64 (BF16).  Asynchronous on stream.  It has no counterpart in the
+ * reference; tests use it to check the tcgen05 core apart from the epilogue. */
+int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, const void *a_lo,
+                      const void *b_hi, const void *b_lo, float *c, long ldc, void *stream);
+
+/* ------------------------------------------------------- drop-in symbols */
+/* The reference reads N, Nfile, J1, dt, nn and num_neighbor from globals its
+ * program defines (llg_sqt_baseline.c:12-20).  The drop-in functions use the
+ * values set here; without a call they fall back to those globals when the
+ * host program defines them (weak references), else to the reference's
+ * initial values (N=100, Nfile=50, J1=1.0, dt=0.02). */
+int asd_set_params(int N, int Nfile, double J1, double dt);
+
+/* llg_sqt_baseline.c:29 -- derivative[f][i][:] = H x S for every replica and
+ * site, H = J1 * sum of the 4 neighbours; host arrays [Nfile][N*N][3]. */
+void euler(double *spin0, double *derivative);
+
+/* llg_sqt_baseline.c:95 -- one RK4 step: cur_input = spin + k1/6 + k2/3 +
+ * k3/3 + k4/6 with k_s = dt * f(stage input); k1..k4 receive the scaled
+ * increments, as in the reference. */
+void runge_kutta(double *spin, double *cur_input, double *k1, double *k2, double *k3,
+                 double *k4);
+
+/* kernel_fusion/gemm_kernel.h:355 -- C += fuse_C (x) (alpha * A * B) on the
+ * interleaved complex layout (re rows (i/4)*8+i%4, im rows +4, ldc >= 2*m),
+ * and sum[0..1] += the sums of the updated real and imaginary parts, once per
+ * K block of 240 as the reference does.  Column-major A (m x k, lda) and B
+ * (k x n, ldb); all pointers are host memory.  Rows past the last multiple of
+ * 4 and a last odd column are left untouched, as in the reference. */
+void fused_dgemm(int *m, int *n, int *k, double *alpha, double *a, int *lda, double *b,
+                 int *ldb, double *c, int *ldc, double *fuse_C, double *sum);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,116 @@
+"""GPU parity of S(q,t) (through the C ABI) against the oracle and the
+reference fixtures.
+
+Tolerances: FP64 paths 1e-12 relative; the split-precision tensor-core paths
+(TF32x3, BF16x3) 1e-5 relative, the bound the design targets."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import asd_b200 as asd
+import oracle as orc
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-12, "fp64_fused": 1e-12, "tf32x3": 1e-5, "bf16x3": 1e-5}
+
+
+@pytest.mark.parametrize("name", ["llg_n12_f4", "llg_n20_f6"])
+def test_sqt_matches_reference_fixture(golden, name):
+    g = golden(name)
+    N, nf = int(g["N"]), int(g["nfile"])
+    ref = complex(g["sqt_gemm_len1"])
+    with asd.Context(asd.Params.make(N, nf, J1=float(g["J1"]), dt=float(g["dt"]))) as ctx:
+        ctx.set_spins(g["spins0"], as_origin=True)
+        ctx.step(int(g["nsteps"]))
+        assert np.array_equal(ctx.get_spins(), g["steps_len1"])
+        for mode, tol in TOL.items():
+            got = ctx.sqt(mode)
+            assert rel_err(got, ref) < tol, (mode, got, ref)
+
+
+@pytest.mark.parametrize("N,nfile,steps", [(16, 8, 2), (32, 50, 3), (24, 200, 1), (40, 11, 4), (50, 64, 2)])
+def test_sqt_modes_vs_oracle(oracle, N, nfile, steps):
+    s0 = asd.random_spins(N, nfile, seed=N * 3 + nfile)
+    kw = dict(J1=-1.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005)
+    with asd.Context(asd.Params.make(N, nfile, **kw)) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        ctx.step(steps)
+        st = ctx.get_spins()
+        vx = N // 10
+        ref = oracle.sqt_factorized(N, nfile, vx, vx, st, s0)
+        if N <= 32:
+            assert rel_err(oracle.sqt_gemm(N, nfile, vx, vx, st, s0), ref) < 1e-12
+        for mode, tol in TOL.items():
+            got = ctx.sqt(mode)
+            assert rel_err(got, ref) < tol, (mode, got, ref)
+
+
+def test_sqt_at_origin_and_q_zero(oracle):
+    """t = 0 (A = B) and q = 0 (vx = vy = 0, every phase 1)."""
+    N, nf = 32, 40
+    s0 = asd.random_spins(N, nf, seed=2)
+    with asd.Context(asd.Params.make(N, nf, vx=0, vy=0)) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        ref = oracle.sqt_factorized(N, nf, 0, 0, s0, s0)
+        for mode, tol in TOL.items():
+            assert rel_err(ctx.sqt(mode), ref) < tol, mode
+
+
+def test_sqt_repeatable_and_deterministic():
+    N, nf = 48, 30
+    s0 = asd.random_spins(N, nf, seed=7)
+    with asd.Context(asd.Params.make(N, nf)) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        ctx.step(2)
+        for mode in TOL:
+            a = ctx.sqt(mode)
+            b = ctx.sqt(mode)
+            assert a == b, mode
+
+
+@pytest.mark.parametrize("name", ["fused_dgemm_valid", "fused_dgemm_rows", "fused_dgemm_cols"])
+def test_dropin_fused_dgemm_matches_reference(golden, name):
+    g = golden(name)
+    c = g["c_in"].copy()
+    s = np.zeros(2 * 128)
+    asd.fused_dgemm(int(g["m"]), int(g["n"]), int(g["k"]), float(g["alpha"]), g["a"],
+                    int(g["lda"]), g["b"], int(g["ldb"]), c, int(g["ldc"]), g["q"], s)
+    assert np.array_equal(c, g["c_out"])  # the same FMA chain per element
+    total = np.array([s[0::2].sum(), s[1::2].sum()])
+    assert np.allclose(total, g["sum"], rtol=1e-13, atol=1e-12)
+
+
+def test_dropin_fused_dgemm_sqt_glue(oracle):
+    """The reference's fused S(q,t) sequence (llg_sqt_fusion.c:370-441) run
+    with the GPU fused_dgemm equals the oracle's fused form."""
+    N, nf = 12, 6
+    M, K = N * N, 3 * nf
+    s0 = asd.random_spins(N, nf, seed=31)
+    st = oracle.steps(orc.make_params(N, nf), s0, 3)
+    ref = oracle.sqt_fused(N, nf, 1, 1, st, s0)
+    a = np.ascontiguousarray(st.transpose(0, 2, 1).reshape(K, M))   # spint: A(j, 3i+c) at j + (3i+c)M
+    b = np.ascontiguousarray(s0.transpose(1, 0, 2).reshape(M * K))   # spin_zero
+    fint = st.mean(axis=0)
+    zerot = s0.mean(axis=0)
+    qx = 2 * np.pi * 1 / N
+    r = np.arange(M) // N
+    cc = np.arange(M) % N
+    th = qx * (r[:, None] - r[None, :]) + qx * (cc[:, None] - cc[None, :])
+    qm = np.exp(-1j * th)
+    rows = (np.arange(M) // 4) * 8 + np.arange(M) % 4
+    ldc = 2 * M
+    qmat = np.zeros((M, ldc))  # [j][row]
+    cmat = np.zeros((M, ldc))
+    outer = fint @ zerot.T
+    qmat[:, rows] = qm.real.T
+    qmat[:, rows + 4] = qm.imag.T
+    cmat[:, rows] = -(outer * qm.real).T
+    cmat[:, rows + 4] = -(outer * qm.imag).T
+    s = np.zeros(256)
+    qf, cf = qmat.reshape(-1), cmat.reshape(-1).copy()
+    asd.fused_dgemm(M, M, K, 1.0 / nf, a.reshape(-1), M, b, K, cf, ldc, qf, s)
+    got = complex(s[0::2].sum(), s[1::2].sum()) / M
+    assert rel_err(got, ref) < 1e-12

@@ -1,0 +1,56 @@
+"""The tcgen05 core of the split S(q,t) GEMM on its own: the raw FP32
+accumulator (asd_umma_gemm_f32) against an FP64 product of the same split
+operands computed by torch.  This isolates descriptor, swizzle and TMEM
+layout errors from the fused epilogue."""
+from __future__ import annotations
+
+import pytest
+
+import asd_b200 as asd
+
+pytestmark = pytest.mark.gpu
+
+
+def tf32_round(x):
+    import torch
+
+    i = x.float().contiguous().view(torch.int32)
+    i = (i + 0x1000) & ~0x1FFF  # round half away from zero on the magnitude bits
+    return i.view(torch.float32)
+
+
+def split(x, kind):
+    import torch
+
+    if kind == 2:
+        hi = x.to(torch.bfloat16)
+        lo = (x - hi.double()).to(torch.bfloat16)
+    else:
+        hi = tf32_round(x)
+        lo = tf32_round(x - hi.double())
+    return hi.contiguous(), lo.contiguous()
+
+
+@pytest.mark.parametrize("kind,rows,Kp", [(1, 256, 32), (2, 256, 64), (1, 512, 96), (2, 768, 192),
+                                          (1, 1024, 1504), (2, 512, 1536)])
+def test_umma_core_matches_fp64_product(kind, rows, Kp):
+    import torch
+
+    g = torch.Generator(device="cuda").manual_seed(rows + Kp + kind)
+    A = torch.randn(rows, Kp, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(rows, Kp, dtype=torch.float64, device="cuda", generator=g) * 0.5 + 0.1
+    ah, al = split(A, kind)
+    bh, bl = split(B, kind)
+    C = torch.full((rows, rows), float("nan"), dtype=torch.float32, device="cuda")
+    asd.umma_gemm_f32(kind, rows, Kp, ah.data_ptr(), al.data_ptr(), bh.data_ptr(), bl.data_ptr(),
+                      C.data_ptr(), rows, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    Ah, Al, Bh, Bl = (t.double() for t in (ah, al, bh, bl))
+    ref = Ah @ Bh.T + Ah @ Bl.T + Al @ Bh.T
+    err = (C.double() - ref).abs().max().item()
+    scale = (Ah.abs() @ Bh.abs().T).max().item()
+    assert not torch.isnan(C).any()
+    assert err <= 2e-6 * scale, (err, scale)
+    # and the split product is close to the exact FP64 product
+    exact = A @ B.T
+    assert (C.double() - exact).abs().max().item() <= (3e-5 if kind == 2 else 2e-6) * scale
