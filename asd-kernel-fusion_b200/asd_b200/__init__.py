@@ -41,7 +41,8 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_create", "asd_ctx_destroy", "asd_ctx_set_stream", "asd_ctx_get_params",
     "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
-    "asd_ctx_step_host", "asd_ctx_last_launches", "asd_ctx_check_device_status",
+    "asd_ctx_step_host", "asd_ctx_set_chunk_k", "asd_ctx_last_launches",
+    "asd_ctx_check_device_status",
     "asd_umma_gemm_f32", "asd_set_params", "euler", "runge_kutta", "fused_dgemm",
 )
 
@@ -111,9 +112,11 @@ def load() -> C.CDLL:
         "asd_ctx_sqt": ([vp, C.c_int, dp], C.c_int),
         "asd_ctx_sqt_async": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_step_host": ([vp, vp, vp, C.c_int, dp], C.c_int),
+        "asd_ctx_set_chunk_k": ([vp, C.c_int], C.c_int),
         "asd_ctx_last_launches": ([vp], C.c_int),
         "asd_ctx_check_device_status": ([vp], C.c_int),
-        "asd_umma_gemm_f32": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, C.c_long, vp],
+        "asd_umma_gemm_f32": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, C.c_long, C.c_int,
+                               vp],
                               C.c_int),
         "asd_set_params": ([C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
         "euler": ([vp, vp], None),
@@ -234,6 +237,9 @@ class Context:
                                         C.c_void_p(spin_out_ptr), mode, self._out))
         return complex(self._out[0], self._out[1])
 
+    def set_chunk_k(self, chunk_k: int) -> None:
+        _check(load().asd_ctx_set_chunk_k(self._h, int(chunk_k)))
+
     def last_launches(self) -> int:
         return int(load().asd_ctx_last_launches(self._h))
 
@@ -276,8 +282,8 @@ def fused_dgemm(m, n, k, alpha, a, lda, b, ldb, c, ldc, q, sum_):
 
 
 def umma_gemm_f32(kind: int, rows: int, Kp: int, a_hi: int, a_lo: int, b_hi: int, b_lo: int,
-                  c: int, ldc: int, stream: int = 0) -> None:
+                  c: int, ldc: int, chunk_k: int = 0, stream: int = 0) -> None:
     """asd_umma_gemm_f32 on device pointers (diagnostic)."""
     _check(load().asd_umma_gemm_f32(int(kind), int(rows), int(Kp), C.c_void_p(a_hi),
                                     C.c_void_p(a_lo), C.c_void_p(b_hi), C.c_void_p(b_lo),
-                                    C.c_void_p(c), int(ldc), C.c_void_p(stream)))
+                                    C.c_void_p(c), int(ldc), int(chunk_k), C.c_void_p(stream)))

@@ -101,6 +101,7 @@ struct UmmaSqtArgs {
     double2 *part;        // one partial per CTA
     unsigned *status;     // device status word
     int num_sms;
+    int chunk_k = 0;          // K elements per TMEM accumulation chunk (0: all)
     float *dbg_c = nullptr;   // diagnostic: store the accumulator instead
     long dbg_ldc = 0;
 };

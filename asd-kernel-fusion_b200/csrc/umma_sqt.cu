@@ -77,6 +77,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     const __grid_constant__ CUtensorMap tm_al,
                     const __grid_constant__ CUtensorMap tm_bh,
                     const __grid_constant__ CUtensorMap tm_bl, int num_m, int num_n, int num_kb,
+                    int kb_per_chunk,
                     const float4 *__restrict__ row4, const float *__restrict__ row1,
                     const float4 *__restrict__ col4, const float *__restrict__ col1, float alpha,
                     double2 *__restrict__ part, unsigned *__restrict__ status,
@@ -173,51 +174,60 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             bool ok = true;
             const uint32_t smem_base = ptx::smem_u32(smem);
             for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
-                if (!ptx::mbar_wait_bounded(&tail->tempty[abuf], aphase ^ 1u, abort_flag,
-                                            WAIT_LIMIT)) {
-                    raise_abort(tail, status);
-                    break;
-                }
-                ptx::tc_fence_after();
-                const uint32_t d_tmem = tmem_base + (uint32_t)(abuf * BN);
-                for (int kb = 0; kb < num_kb; ++kb) {
-                    if (!ptx::mbar_wait_bounded(&tail->full[stage], phase, abort_flag,
+                // K is accumulated in chunks of kb_per_chunk k blocks, each
+                // into a fresh TMEM buffer: the tensor core's FP32
+                // accumulation loses precision with the number of
+                // accumulation steps, and the epilogue adds the chunks in FP64.
+                for (int kb0 = 0; kb0 < num_kb && ok; kb0 += kb_per_chunk) {
+                    const int kb1 = min(kb0 + kb_per_chunk, num_kb);
+                    if (!ptx::mbar_wait_bounded(&tail->tempty[abuf], aphase ^ 1u, abort_flag,
                                                 WAIT_LIMIT)) {
                         raise_abort(tail, status);
                         ok = false;
                         break;
                     }
                     ptx::tc_fence_after();
-                    const uint32_t s0 = smem_base + stage * STAGE_BYTES;
-                    const uint64_t dah = ptx::umma_desc_kmajor_sw128(s0);
-                    const uint64_t dal = ptx::umma_desc_kmajor_sw128(s0 + A_TILE);
-                    const uint64_t dbh = ptx::umma_desc_kmajor_sw128(s0 + 2 * A_TILE);
-                    const uint64_t dbl = ptx::umma_desc_kmajor_sw128(s0 + 2 * A_TILE + B_TILE);
+                    const uint32_t d_tmem = tmem_base + (uint32_t)(abuf * BN);
+                    for (int kb = kb0; kb < kb1; ++kb) {
+                        if (!ptx::mbar_wait_bounded(&tail->full[stage], phase, abort_flag,
+                                                    WAIT_LIMIT)) {
+                            raise_abort(tail, status);
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                        const uint32_t s0 = smem_base + stage * STAGE_BYTES;
+                        const uint64_t dah = ptx::umma_desc_kmajor_sw128(s0);
+                        const uint64_t dal = ptx::umma_desc_kmajor_sw128(s0 + A_TILE);
+                        const uint64_t dbh = ptx::umma_desc_kmajor_sw128(s0 + 2 * A_TILE);
+                        const uint64_t dbl =
+                            ptx::umma_desc_kmajor_sw128(s0 + 2 * A_TILE + B_TILE);
 #pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) {
-                        const uint64_t adv = (uint64_t)(2 * kk);  // 32 bytes per MMA k step
-                        const uint32_t accum = (kb > 0 || kk > 0) ? 1u : 0u;
-                        if (KIND == 2) {
-                            ptx::umma_f16(d_tmem, dah + adv, dbh + adv, IDESC, accum);
-                            ptx::umma_f16(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
-                            ptx::umma_f16(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
-                        } else {
-                            ptx::umma_tf32(d_tmem, dah + adv, dbh + adv, IDESC, accum);
-                            ptx::umma_tf32(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
-                            ptx::umma_tf32(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
+                        for (int kk = 0; kk < 4; ++kk) {
+                            const uint64_t adv = (uint64_t)(2 * kk);  // 32 bytes per k step
+                            const uint32_t accum = (kb > kb0 || kk > 0) ? 1u : 0u;
+                            if (KIND == 2) {
+                                ptx::umma_f16(d_tmem, dah + adv, dbh + adv, IDESC, accum);
+                                ptx::umma_f16(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
+                                ptx::umma_f16(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
+                            } else {
+                                ptx::umma_tf32(d_tmem, dah + adv, dbh + adv, IDESC, accum);
+                                ptx::umma_tf32(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
+                                ptx::umma_tf32(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
+                            }
+                        }
+                        ptx::umma_commit(&tail->empty[stage]);
+                        if (++stage == STAGES) {
+                            stage = 0;
+                            phase ^= 1u;
                         }
                     }
-                    ptx::umma_commit(&tail->empty[stage]);
-                    if (++stage == STAGES) {
-                        stage = 0;
-                        phase ^= 1u;
+                    if (!ok) break;
+                    ptx::umma_commit(&tail->tfull[abuf]);
+                    if (++abuf == 2) {
+                        abuf = 0;
+                        aphase ^= 1u;
                     }
-                }
-                if (!ok) break;
-                ptx::umma_commit(&tail->tfull[abuf]);
-                if (++abuf == 2) {
-                    abuf = 0;
-                    aphase ^= 1u;
                 }
             }
             // Wait for every issued MMA before TMEM can be released.
@@ -242,52 +252,76 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const long i = (long)mb * BM + rloc;
             const float4 r4 = STORE ? make_float4(0.f, 0.f, 0.f, 0.f) : row4[i];
             const float ui = STORE ? 0.f : row1[i];
-            if (!ptx::mbar_wait_bounded(&tail->tfull[abuf], aphase, abort_flag, WAIT_LIMIT)) {
-                raise_abort(tail, status);
-                break;
-            }
-            ptx::tc_fence_after();
             double s_re = 0.0, s_im = 0.0;
             const long j0 = (long)nb * BN;
+            bool ok = true;
+            for (int kb0 = 0; kb0 < num_kb; kb0 += kb_per_chunk) {
+                const bool first = (kb0 == 0);
+                const bool last = (kb0 + kb_per_chunk >= num_kb);
+                if (!ptx::mbar_wait_bounded(&tail->tfull[abuf], aphase, abort_flag, WAIT_LIMIT)) {
+                    raise_abort(tail, status);
+                    ok = false;
+                    break;
+                }
+                ptx::tc_fence_after();
+                // Per 32-column group, in FP32: a = sum_j w_j acc_ij and, in the
+                // last chunk only, o = sum_j w_j (m_i . z_j); the row sum
+                // s_i = alpha * a - o is carried in FP64.
 #pragma unroll 1
-            for (int c = 0; c < BN / 32; ++c) {
-                uint32_t v[32];
-                const uint32_t taddr =
-                    tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(abuf * BN + c * 32);
-                ptx::tmem_ld_32x32b_x32(taddr, v);
-                ptx::tmem_ld_wait();
-                if (STORE) {
-                    float *dst = dbg_c + i * dbg_ldc + j0 + c * 32;
+                for (int c = 0; c < BN / 32; ++c) {
+                    uint32_t v[32];
+                    const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) +
+                                           (uint32_t)(abuf * BN + c * 32);
+                    ptx::tmem_ld_32x32b_x32(taddr, v);
+                    ptx::tmem_ld_wait();
+                    if (STORE) {
+                        float *dst = dbg_c + i * dbg_ldc + j0 + c * 32;
 #pragma unroll
-                    for (int jj = 0; jj < 32; ++jj) dst[jj] = __uint_as_float(v[jj]);
-                    continue;
-                }
-                float cre = 0.f, cim = 0.f;
+                        for (int jj = 0; jj < 32; ++jj)
+                            dst[jj] = (first ? 0.f : dst[jj]) + __uint_as_float(v[jj]);
+                        continue;
+                    }
+                    float are = 0.f, aim = 0.f, ore = 0.f, oim = 0.f;
+                    if (last) {
 #pragma unroll
-                for (int jj = 0; jj < 32; ++jj) {
-                    const long j = j0 + c * 32 + jj;
-                    const float4 z = __ldg(&col4[j]);
-                    const float wim = __ldg(&col1[j]);
-                    float o = r4.x * z.x;
-                    o = fmaf(r4.y, z.y, o);
-                    o = fmaf(r4.z, z.z, o);
-                    const float val = fmaf(alpha, __uint_as_float(v[jj]), -o);
-                    cre = fmaf(z.w, val, cre);
-                    cim = fmaf(wim, val, cim);
+                        for (int jj = 0; jj < 32; ++jj) {
+                            const long j = j0 + c * 32 + jj;
+                            const float4 z = __ldg(&col4[j]);
+                            const float wim = __ldg(&col1[j]);
+                            const float acc = __uint_as_float(v[jj]);
+                            float o = r4.x * z.x;
+                            o = fmaf(r4.y, z.y, o);
+                            o = fmaf(r4.z, z.z, o);
+                            are = fmaf(z.w, acc, are);
+                            aim = fmaf(wim, acc, aim);
+                            ore = fmaf(z.w, o, ore);
+                            oim = fmaf(wim, o, oim);
+                        }
+                    } else {
+#pragma unroll
+                        for (int jj = 0; jj < 32; ++jj) {
+                            const long j = j0 + c * 32 + jj;
+                            const float wre = __ldg(&col4[j].w);
+                            const float wim = __ldg(&col1[j]);
+                            const float acc = __uint_as_float(v[jj]);
+                            are = fmaf(wre, acc, are);
+                            aim = fmaf(wim, acc, aim);
+                        }
+                    }
+                    s_re += (double)alpha * (double)are - (double)ore;
+                    s_im += (double)alpha * (double)aim - (double)oim;
                 }
-                s_re += (double)cre;
-                s_im += (double)cim;
+                ptx::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive(&tail->tempty[abuf]);
+                if (++abuf == 2) {
+                    abuf = 0;
+                    aphase ^= 1u;
+                }
             }
-            ptx::tc_fence_before();
-            __syncwarp();
-            if (lane == 0) ptx::mbar_arrive(&tail->tempty[abuf]);
             // u_i * s_i with u_i = (r4.w, ui)
             tot_re += (double)r4.w * s_re - (double)ui * s_im;
             tot_im += (double)r4.w * s_im + (double)ui * s_re;
-            if (++abuf == 2) {
-                abuf = 0;
-                aphase ^= 1u;
-            }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -362,13 +396,17 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     const int num_m = (int)(Mp / BM), num_n = (int)(Mp / BN), num_kb = a.Kp / ke;
     const int tiles = num_m * num_n;
     const int grid = tiles < a.num_sms ? tiles : a.num_sms;
+    // k blocks per accumulation chunk: chunk_k elements of K (0 = all of K)
+    int kpc = a.chunk_k > 0 ? (a.chunk_k + ke - 1) / ke : num_kb;
+    if (kpc < 1) kpc = 1;
+    if (kpc > num_kb) kpc = num_kb;
     cudaError_t e;
     auto go = [&](auto kern) {
         cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              SMEM_BYTES);
         if (r == cudaSuccess)
             kern<<<grid, NUM_THREADS, SMEM_BYTES, st>>>(tah, tal, tbh, tbl, num_m, num_n, num_kb,
-                                                        a.row4, a.row1, a.col4, a.col1, a.alpha,
+                                                        kpc, a.row4, a.row1, a.col4, a.col1, a.alpha,
                                                         a.part, a.status, a.dbg_c, a.dbg_ldc);
         return r;
     };
@@ -389,7 +427,7 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
 // device pointers, rows a multiple of 256.
 extern "C" int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, const void *a_lo,
                                  const void *b_hi, const void *b_lo, float *c, long ldc,
-                                 void *stream) {
+                                 int chunk_k, void *stream) {
     using namespace asd;
     if (kind != 1 && kind != 2) return fail(ASD_ERR_INVALID, "kind must be 1 (TF32) or 2 (BF16)");
     if (rows <= 0 || rows % 256 != 0) return fail(ASD_ERR_INVALID, "rows must be a multiple of 256");
@@ -409,6 +447,7 @@ extern "C" int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, 
     u.num_sms = sms;
     u.dbg_c = c;
     u.dbg_ldc = ldc;
+    u.chunk_k = chunk_k;
     const int g = launch_umma_sqt(u, (cudaStream_t)stream);
     return g < 0 ? g : ASD_OK;
 }

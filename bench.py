@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Benchmark of the hot path: one RK4 step of the LLG equation for every
+replica plus one S(q,t) evaluation, on the 128 x 128 lattice with 500
+replicas (antiferromagnetic J = -1, h = (0, 0, 0.5), alpha = 0.05,
+dt = 0.005), the correlation GEMM in TF32x3.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line on rank 0.  ``value`` is the whole job's throughput in
+site-steps/s (a site-step = one spin of one replica advanced one RK4 step,
+with the step's S(q,t) evaluation included), with the spins resident in HBM.
+``e2e`` is the same metric through asd_ctx_step_host: the spins come from
+pinned host memory and go back every step, as the reference's runge_kutta
+contract has them.  Under torchrun every rank runs its own lattice (weak
+scaling, no collective in the data path); the time is the max over ranks.
+
+``--impl reference`` times the reference's own C code (oracle/_ref, compiled
+from its sources) on the host cores: runge_kutta + renormalisation on the full
+lattice and fused_dgemm's S(q,t) on a band of rows, scaled to the full
+lattice.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "asd-kernel-fusion_b200"))
+
+CONFIG = dict(N=128, nfile=500, J1=-1.0, J2=0.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005)
+WORKLOAD = "llg-rk4+sqt 128x128 lattice, 500 replicas, J=-1, h=(0,0,0.5), alpha=0.05, dt=0.005"
+METRIC = "LLG site-steps/s + S(q,t) GEMM TFLOP/s, mixed vs FP64 plain at stated error"
+LLG_BYTES_PER_SITE_STEP = 384  # 4 fused stage kernels: 3+5+5+3 FP64 3-vectors
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {
+        "gpu_idle": 0x1, "applications_clocks_setting": 0x2, "sw_power_cap": 0x4,
+        "hw_slowdown": 0x8, "sync_boost": 0x10, "sw_thermal_slowdown": 0x20,
+        "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80,
+    }
+
+    def __init__(self, device_index: int, period: float = 0.005):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.period = period
+        self._stop = threading.Event()
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                bits = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, b in self.REASONS.items():
+                    if bits & b:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.nv:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self.nv:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        med = statistics.median(self.samples) if self.samples else None
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------- CPU arms
+def cpu_reference_sample(N, nfile, J1, dt, spins, target_s=2.0, llg=True):
+    """Times the reference's own compiled code (oracle/_ref/libref_fusion.so) on
+    the host cores: runge_kutta + renormalisation on the whole lattice, and the
+    fused S(q,t) (llg_sqt_fusion.c:370-441 around fused_dgemm) on a band of
+    rows, scaled to all rows.  Returns seconds per full step and a description.
+    The reference model has no damping or field: its RK4 costs the same
+    regardless of those parameters."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+
+    if not orc.RefLib.available("fusion"):
+        return None
+    r = orc.RefLib("fusion")
+    threads = r.setup(N, nfile, J1=J1, dt=dt, threads=0)
+    M = N * N
+    t_llg = 0.0
+    if llg:
+        s = spins.copy()
+        r.steps(s, 1, 1.0)  # warm
+        t0 = time.perf_counter()
+        s = r.steps(s, 1, 1.0)
+        t_llg = time.perf_counter() - t0
+    # size the band of GEMM rows so one evaluation takes about target_s
+    rows = 256
+    r.fusion_init(spins, rows)
+    t0 = time.perf_counter()
+    r.fusion_sqt(spins)
+    t_small = time.perf_counter() - t0
+    rows = int(min(M, max(256, rows * target_s / max(t_small, 1e-6))))
+    rows -= rows % 256
+    rows = max(rows, 256)
+    r.fusion_init(spins, rows)
+    t0 = time.perf_counter()
+    r.fusion_sqt(spins)
+    t_band = time.perf_counter() - t0
+    r.lib.ref_fusion_free()
+    t_sqt = t_band * M / rows
+    sample = (f"reference runge_kutta+renorm on all {M}x{nfile} site-replicas, fused_dgemm S(q,t) "
+              f"on {rows} of {M} rows scaled by {M / rows:.2f}, {threads} OpenMP threads")
+    return dict(t_llg=t_llg, t_sqt=t_sqt, threads=threads, sample=sample, rows=rows)
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    N, nf = CONFIG["N"], CONFIG["nfile"]
+    import asd_b200 as asd
+
+    spins = asd.random_spins(N, nf, seed=0)
+    vals = []
+    info = None
+    for it in range(args.warmup + args.steps):
+        info = cpu_reference_sample(N, nf, CONFIG["J1"], CONFIG["dt"], spins,
+                                    target_s=args.ref_target_s)
+        if info is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "oracle/_ref/libref_fusion.so not built (make -C oracle ref)"}))
+            return 0
+        if it >= args.warmup:
+            vals.append(info["t_llg"] + info["t_sqt"])
+    t = statistics.median(vals)
+    value = N * N * nf / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "site-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded spins uniform on the sphere",
+        "config": {"workload": WORKLOAD, "sites": N * N, "replicas": nf, "gemm_m": N * N,
+                   "gemm_k": 3 * nf},
+        "cpu_baseline": {"value": value, "unit": "site-steps/s", "cores": info["threads"],
+                         "kind": "reference", "sample": info["sample"]},
+        "e2e": {"value": value, "unit": "site-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "llg_site_steps_per_s": N * N * nf / info["t_llg"],
+        "sqt_tflops": 2.0 * (N * N) ** 2 * 3 * nf / info["t_sqt"] / 1e12,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import asd_b200 as asd
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    N, nf = CONFIG["N"], CONFIG["nfile"]
+    M, K = N * N, 3 * nf
+    mode = args.mode
+    params = asd.Params.make(N, nf, J1=CONFIG["J1"], J2=CONFIG["J2"], alpha=CONFIG["alpha"],
+                             h=CONFIG["h"], dt=CONFIG["dt"])
+    asd.load().asd_set_device(local)
+    ctx = asd.Context(params, modes=["fp64", "tf32x3", "bf16x3"])
+    if args.chunk_k >= 0:
+        ctx.set_chunk_k(args.chunk_k)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    spins0 = asd.random_spins(N, nf, seed=rank)
+    ctx.set_spins(spins0, as_origin=True)
+    total = args.warmup + args.steps
+    d_out = torch.zeros(2 * max(total, 1), dtype=torch.float64, device="cuda")
+
+    def one_step(i):
+        ctx.step(1)
+        n1 = ctx.last_launches()
+        ctx.sqt_async(mode, d_out.data_ptr() + 16 * i)
+        return n1 + ctx.last_launches()
+
+    for i in range(args.warmup):
+        one_step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for i in range(args.warmup, total):
+            launches += one_step(i)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ctx.check_device_status()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+        dist.barrier()
+    value = world * M * nf / (ms / 1e3)
+    sqt_last = complex(*d_out[2 * (total - 1):2 * total].tolist())
+
+    extra = {}
+    if rank == 0:
+        extra = component_measurements(ctx, asd, torch, stream, M, K, nf, args)
+    e2e = e2e_measurement(ctx, asd, torch, spins0, mode, M, nf, args, world)
+    if world > 1:
+        dist.barrier()
+    if rank != 0:
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    hbm, bf16, src = measured_peaks()
+    gemm_flops = 2.0 * M * M * K
+    gemm_ms = extra["sqt_ms"][mode]
+    achieved = gemm_flops / (gemm_ms / 1e3) / 1e12
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(f"umma_sqt_{mode}")
+    line = {
+        "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": f"f64 RK4 + {mode} GEMM (fp32 accumulate, f64 reduction)",
+        "data": "synthetic: seeded spins uniform on the sphere",
+        "config": {"workload": WORKLOAD, "sites": M, "replicas": nf, "gemm_m": M, "gemm_n": M,
+                   "gemm_k": K, "sqt_mode": mode, "chunk_k": args.chunk_k if args.chunk_k >= 0 else 512,
+                   "l2": "inputs larger than L2 (spin state 197 MB per array, operands 197 MB)"},
+        "roofline": {"bound": "tensor", "kernel": f"umma_sqt_kernel ({mode})",
+                     "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+                     "frac": achieved / bf16, "traffic": traffic,
+                     "peak_source": f"{src} dense bf16 burst (MEASURED_PEAKS.json)",
+                     "achieved_counts": "useful 2*M*M*K per evaluation; the 3-term split issues 3x that on the tensor pipe"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": e2e,
+        "sqt_last": [sqt_last.real, sqt_last.imag],
+    }
+    line.update(extra["report"])
+    if world == 1 and not args.no_cpu_baseline:
+        info = cpu_reference_sample(N, nf, CONFIG["J1"], CONFIG["dt"], spins0, target_s=1.5)
+        if info is not None:
+            v = M * nf / (info["t_llg"] + info["t_sqt"])
+            line["cpu_baseline"] = {"value": v, "unit": "site-steps/s", "cores": info["threads"],
+                                    "kind": "reference", "sample": info["sample"]}
+    print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
+    """LLG alone, every S(q,t) mode alone, and the split modes' error against
+    the FP64 path, on the current state (rank 0)."""
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    d = torch.zeros(2, dtype=torch.float64, device="cuda")
+    reps = 10
+    ctx.step(2)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    ctx.step(reps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    llg_ms = ev0.elapsed_time(ev1) / reps
+    llg_gbs = LLG_BYTES_PER_SITE_STEP * M * nf / (llg_ms / 1e3) / 1e9
+    hbm, bf16, src = measured_peaks()
+    sqt_ms, vals = {}, {}
+    for mode in ("fp64", "tf32x3", "bf16x3"):
+        n = 2 if mode == "fp64" else 5
+        ctx.sqt_async(mode, d.data_ptr())  # operands split, warm
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(n):
+            ctx.sqt_async(mode, d.data_ptr())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        sqt_ms[mode] = ev0.elapsed_time(ev1) / n
+        vals[mode] = complex(*d.tolist())
+    ref = vals["fp64"]
+    flops = 2.0 * M * M * K
+    report = {
+        "llg": {"site_steps_per_s": M * nf / (llg_ms / 1e3), "ms": llg_ms, "achieved_gbs": llg_gbs,
+                "hbm_peak_gbs": hbm, "frac": llg_gbs / hbm,
+                "bytes_per_site_step": LLG_BYTES_PER_SITE_STEP},
+        "sqt": {m: {"ms": sqt_ms[m], "tflops": flops / (sqt_ms[m] / 1e3) / 1e12,
+                    "value": [vals[m].real, vals[m].imag],
+                    "rel_err_vs_fp64": abs(vals[m] - ref) / abs(ref)} for m in sqt_ms},
+        "sqt_speedup_vs_fp64": {m: sqt_ms["fp64"] / sqt_ms[m] for m in ("tf32x3", "bf16x3")},
+    }
+    return {"sqt_ms": sqt_ms, "report": report}
+
+
+def e2e_measurement(ctx, asd, torch, spins0, mode, M, nf, args, world):
+    """asd_ctx_step_host: per step, pinned host spins in, RK4 + S(q,t), spins and
+    S(q,t) back to pinned host memory."""
+    n = M * nf * 3
+    h_in = torch.from_numpy(spins0.reshape(-1).copy()).pin_memory()
+    h_out = torch.empty(n, dtype=torch.float64).pin_memory()
+    steps = max(2, min(args.steps, 10))
+    ctx.step_host(h_in.data_ptr(), h_out.data_ptr(), mode)  # warm
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.step_host(h_out.data_ptr(), h_out.data_ptr(), mode)
+    dt = (time.perf_counter() - t0) / steps
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([dt], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = t.item()
+    return {"value": world * M * nf / dt, "unit": "site-steps/s", "h2d_bytes_per_step": n * 8,
+            "d2h_bytes_per_step": n * 8 + 16, "ms_per_step": dt * 1e3,
+            "api": "asd_ctx_step_host (pinned host buffers)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["tf32x3", "bf16x3", "fp64", "fp64_fused"], default="tf32x3")
+    ap.add_argument("--chunk-k", type=int, default=-1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-target-s", type=float, default=2.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -120,6 +120,13 @@ int asd_ctx_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
 int asd_ctx_step_host(asd_ctx *ctx, const double *spin_in, double *spin_out,
                       asd_sqt_mode mode, double sqt_out[2]);
 
+/* K elements accumulated per TMEM chunk by the split S(q,t) modes (rounded
+ * up to the 128-byte k block; 0 = all of K in one accumulator).  The tensor
+ * cores' FP32 accumulation loses precision with every accumulation step, so
+ * K is cut into chunks whose partial products the epilogue adds in FP64.
+ * Default 512. */
+int asd_ctx_set_chunk_k(asd_ctx *ctx, int chunk_k);
+
 /* Number of kernels the last asd_ctx_step / asd_ctx_sqt* call launched. */
 int asd_ctx_last_launches(const asd_ctx *ctx);
 
@@ -131,10 +138,12 @@ int asd_ctx_check_device_status(asd_ctx *ctx);
  * C[i*ldc + j] = sum_k Ah[i][k]Bh[j][k] + Ah[i][k]Bl[j][k] + Al[i][k]Bh[j][k]
  * in FP32, for device operands [rows][Kp] (kind 1: TF32 bit patterns in
  * float, kind 2: bf16), rows a multiple of 256, Kp a multiple of 32 (TF32)
- * or 64 (BF16).  Asynchronous on stream.  It has no counterpart in the
+ * or 64 (BF16); chunk_k as for asd_ctx_set_chunk_k (the chunk partials are
+ * added in FP32 here).  Asynchronous on stream.  It has no counterpart in the
  * reference; tests use it to check the tcgen05 core apart from the epilogue. */
 int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, const void *a_lo,
-                      const void *b_hi, const void *b_lo, float *c, long ldc, void *stream);
+                      const void *b_hi, const void *b_lo, float *c, long ldc, int chunk_k,
+                      void *stream);
 
 /* ------------------------------------------------------- drop-in symbols */
 /* The reference reads N, Nfile, J1, dt, nn and num_neighbor from globals its
