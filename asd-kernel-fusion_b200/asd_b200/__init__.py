@@ -43,7 +43,8 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
     "asd_ctx_step_host", "asd_ctx_set_chunk_k", "asd_ctx_last_launches",
     "asd_ctx_check_device_status",
-    "asd_umma_gemm_f32", "asd_set_params", "euler", "runge_kutta", "fused_dgemm",
+    "asd_umma_gemm_f32", "asd_sqt_split_noalloc", "asd_set_params", "euler", "runge_kutta",
+    "fused_dgemm",
 )
 
 
@@ -118,6 +119,8 @@ def load() -> C.CDLL:
         "asd_umma_gemm_f32": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, C.c_long, C.c_int,
                                vp],
                               C.c_int),
+        "asd_sqt_split_noalloc": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp,
+                                   C.c_double, C.c_double, C.c_int, vp, vp], C.c_int),
         "asd_set_params": ([C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
         "euler": ([vp, vp], None),
         "runge_kutta": ([vp] * 6, None),
@@ -287,3 +290,14 @@ def umma_gemm_f32(kind: int, rows: int, Kp: int, a_hi: int, a_lo: int, b_hi: int
     _check(load().asd_umma_gemm_f32(int(kind), int(rows), int(Kp), C.c_void_p(a_hi),
                                     C.c_void_p(a_lo), C.c_void_p(b_hi), C.c_void_p(b_lo),
                                     C.c_void_p(c), int(ldc), int(chunk_k), C.c_void_p(stream)))
+
+
+def sqt_split_noalloc(kind: int, rows: int, Kp: int, a_hi: int, a_lo: int, b_hi: int, b_lo: int,
+                      row4: int, row1: int, col4: int, col1: int, alpha: float, scale: float,
+                      chunk_k: int, d_out: int, stream: int = 0) -> None:
+    """asd_sqt_split_noalloc on device pointers: S(q,t) without any allocation."""
+    v = C.c_void_p
+    _check(load().asd_sqt_split_noalloc(int(kind), int(rows), int(Kp), v(a_hi), v(a_lo), v(b_hi),
+                                        v(b_lo), v(row4), v(row1), v(col4), v(col1),
+                                        float(alpha), float(scale), int(chunk_k), v(d_out),
+                                        v(stream)))

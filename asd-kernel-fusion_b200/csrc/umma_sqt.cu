@@ -451,3 +451,130 @@ extern "C" int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, 
     const int g = launch_umma_sqt(u, (cudaStream_t)stream);
     return g < 0 ? g : ASD_OK;
 }
+
+// ------------------------------------------------ allocation-free variant
+// Some hosts cannot call cudaMalloc from the code that evaluates S(q,t):
+// applications that hand all device memory to their own pool or caching
+// allocator at start-up and keep a fixed budget, and time-step loops that
+// must not call cudaMalloc/cudaFree because those calls can synchronise the
+// device and stall the other streams.  asd_sqt_split_noalloc serves them: the
+// caller passes every input and output buffer, and the only scratch the
+// kernels need -- one partial sum per CTA and a status word -- lives in the
+// fixed array below, which every GPU that loads this library holds until the
+// process exits.
+namespace asd {
+namespace {
+
+constexpr int kNoAllocMaxCtas = 1024;  // partials: at most one per CTA
+constexpr size_t kNoAllocPartBytes = kNoAllocMaxCtas * sizeof(double2);
+constexpr size_t kNoAllocScratchBytes = kNoAllocPartBytes + 256;  // + status word
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  The symbol's
+// name in host code is only a host-side stand-in; the device address is
+// looked up once per device, with that device current.
+int noalloc_scratch(unsigned char **out) {
+    int dev = 0;
+    ASD_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(ASD_ERR_UNSUPPORTED, "device index %d", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_addr[dev] = p;
+    }
+    *out = static_cast<unsigned char *>(g_noalloc_addr[dev]);
+    return ASD_OK;
+}
+
+// Sum of the per-CTA partials in a fixed order, times scale; NaN when a
+// bounded wait in the GEMM gave up (status word non-zero).
+__global__ void __launch_bounds__(256) noalloc_finalize_kernel(const double2 *__restrict__ part,
+                                                               int nparts, double scale,
+                                                               const unsigned *__restrict__ status,
+                                                               double *__restrict__ out) {
+    __shared__ double sre[256], sim[256];
+    double a = 0.0, b = 0.0;
+    for (int k = threadIdx.x; k < nparts; k += 256) {
+        a += part[k].x;
+        b += part[k].y;
+    }
+    sre[threadIdx.x] = a;
+    sim[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            sre[threadIdx.x] += sre[threadIdx.x + s];
+            sim[threadIdx.x] += sim[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const bool bad = (*status != 0u);
+        out[0] = bad ? __longlong_as_double(0x7ff8000000000000ll) : sre[0] * scale;
+        out[1] = bad ? __longlong_as_double(0x7ff8000000000000ll) : sim[0] * scale;
+    }
+}
+
+}  // namespace
+}  // namespace asd
+
+extern "C" int asd_sqt_split_noalloc(int kind, long rows, int Kp, const void *a_hi,
+                                     const void *a_lo, const void *b_hi, const void *b_lo,
+                                     const void *row4, const float *row1, const void *col4,
+                                     const float *col1, double alpha, double scale, int chunk_k,
+                                     double *d_out, void *stream) {
+    using namespace asd;
+    if (kind != 1 && kind != 2) return fail(ASD_ERR_INVALID, "kind must be 1 (TF32x3) or 2 (BF16x3)");
+    if (rows <= 0 || rows % 256 != 0) return fail(ASD_ERR_INVALID, "rows must be a positive multiple of 256");
+    if (!a_hi || !a_lo || !b_hi || !b_lo || !row4 || !row1 || !col4 || !col1 || !d_out)
+        return fail(ASD_ERR_INVALID, "NULL buffer");
+    if (((uintptr_t)row4 | (uintptr_t)col4) & 15)
+        return fail(ASD_ERR_INVALID, "row4/col4 must be 16-byte aligned");
+    if (chunk_k < 0) return fail(ASD_ERR_INVALID, "chunk_k < 0");
+    int dev = 0, sms = 0;
+    ASD_CUDA_TRY(cudaGetDevice(&dev));
+    ASD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long tiles = (rows / 128) * (rows / 256);
+    const long ctas = tiles < sms ? tiles : sms;
+    if (ctas > kNoAllocMaxCtas)
+        return fail(ASD_ERR_UNSUPPORTED,
+                    "the fixed scratch holds %d CTA partials; this launch needs %ld", kNoAllocMaxCtas,
+                    ctas);
+    unsigned char *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc != ASD_OK) return rc;
+    double2 *part = reinterpret_cast<double2 *>(scratch);
+    unsigned *status = reinterpret_cast<unsigned *>(scratch + kNoAllocPartBytes);
+    cudaStream_t st = (cudaStream_t)stream;
+    // the status word keeps the last call's value: clear it
+    ASD_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned), st));
+    UmmaSqtArgs u{};
+    u.kind = kind;
+    u.M = rows;
+    u.Kp = Kp;
+    u.a_hi = a_hi;
+    u.a_lo = a_lo;
+    u.b_hi = b_hi;
+    u.b_lo = b_lo;
+    u.row4 = static_cast<const float4 *>(row4);
+    u.row1 = row1;
+    u.col4 = static_cast<const float4 *>(col4);
+    u.col1 = col1;
+    u.alpha = (float)alpha;
+    u.part = part;
+    u.status = status;
+    u.num_sms = sms;
+    u.chunk_k = chunk_k;
+    const int grid = launch_umma_sqt(u, st);
+    if (grid < 0) return grid;
+    noalloc_finalize_kernel<<<1, 256, 0, st>>>(part, grid, scale, status, d_out);
+    ASD_CUDA_TRY(cudaGetLastError());
+    return ASD_OK;
+}

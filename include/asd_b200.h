@@ -145,6 +145,39 @@ int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, const void 
                       const void *b_hi, const void *b_lo, float *c, long ldc, int chunk_k,
                       void *stream);
 
+/* S(q,t) through the split tensor-core GEMM without allocating anything.
+ * No counterpart in the reference.  For callers that may not call cudaMalloc
+ * or cudaFree while they step a simulation: hosts that give all device memory
+ * to their own pool or caching allocator at start-up and run on a fixed
+ * budget, and step loops where an allocation call would synchronise the
+ * device and stall other streams.  The caller passes every input and output
+ * buffer (device pointers, stream-ordered on `stream`):
+ *   a_hi, a_lo, b_hi, b_lo  split operands [rows][Kp] (kind 1: TF32 bit
+ *                           patterns in float; kind 2: bf16), rows a multiple
+ *                           of 256 with zero padding rows, Kp a multiple of 32
+ *                           (TF32) or 64 (BF16) with zero padding columns;
+ *   row4, row1, col4, col1  epilogue vectors, `rows` entries each, zero past
+ *                           the last site: row4[i] = (m_i, Re u_i) as float4,
+ *                           row1[i] = Im u_i, col4[j] = (z_j, Re w_j),
+ *                           col1[j] = Im w_j, with m, z the replica means at t
+ *                           and 0 and u_i w_j = e^{-i q.(r_i - r_j)};
+ *   d_out                   2 doubles: S = scale * sum_ij u_i w_j
+ *                           (alpha C_ij - m_i . z_j).
+ * Its only scratch (one partial per CTA, at most 1024 CTAs = 16 KiB, plus a
+ * status word) is a fixed array in the library's device memory that every GPU
+ * which loads the library keeps until the process exits.  Limit: at most 1024
+ * CTAs, i.e. devices with up to 1024 SMs; larger launches are rejected with
+ * ASD_ERR_UNSUPPORTED.  The first call on a device looks up that array's
+ * device address (once per device); make that first call before any stream
+ * capture.  All calls share the one array, so calls whose work overlaps on
+ * the GPU (different streams, or different host threads) race and must be
+ * ordered by the caller.  If a bounded wait in the kernel gives up, d_out
+ * receives NaN. */
+int asd_sqt_split_noalloc(int kind, long rows, int Kp, const void *a_hi, const void *a_lo,
+                          const void *b_hi, const void *b_lo, const void *row4, const float *row1,
+                          const void *col4, const float *col1, double alpha, double scale,
+                          int chunk_k, double *d_out, void *stream);
+
 /* ------------------------------------------------------- drop-in symbols */
 /* The reference reads N, Nfile, J1, dt, nn and num_neighbor from globals its
  * program defines (llg_sqt_baseline.c:12-20).  The drop-in functions use the
