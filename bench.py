@@ -246,10 +246,11 @@ def run_ours(args):
     value = world * M * nf / (ms / 1e3)
     sqt_last = complex(*d_out[2 * (total - 1):2 * total].tolist())
 
-    extra = {}
-    if rank == 0:
+    extra = {"sqt_ms": {}, "report": {}}
+    if rank == 0 and not args.no_extras:
         extra = component_measurements(ctx, asd, torch, stream, M, K, nf, args)
-    e2e = e2e_measurement(ctx, asd, torch, spins0, mode, M, nf, args, world)
+    e2e = None if args.no_extras else e2e_measurement(ctx, asd, torch, spins0, mode, M, nf,
+                                                      args, world)
     if world > 1:
         dist.barrier()
     if rank != 0:
@@ -260,7 +261,7 @@ def run_ours(args):
 
     hbm, bf16, src = measured_peaks()
     gemm_flops = 2.0 * M * M * K
-    gemm_ms = extra["sqt_ms"][mode]
+    gemm_ms = extra["sqt_ms"].get(mode, float("nan"))
     achieved = gemm_flops / (gemm_ms / 1e3) / 1e12
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
@@ -285,7 +286,7 @@ def run_ours(args):
         "sqt_last": [sqt_last.real, sqt_last.imag],
     }
     line.update(extra["report"])
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and not args.no_extras:
         info = cpu_reference_sample(N, nf, CONFIG["J1"], CONFIG["dt"], spins0, target_s=1.5)
         if info is not None:
             v = M * nf / (info["t_llg"] + info["t_sqt"])
@@ -371,6 +372,9 @@ def main():
     ap.add_argument("--mode", choices=["tf32x3", "bf16x3", "fp64", "fp64_fused"], default="tf32x3")
     ap.add_argument("--chunk-k", type=int, default=-1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="only the timed steps (for profiling): no per-component timings, e2e "
+                         "or CPU baseline after the timed region")
     ap.add_argument("--ref-target-s", type=float, default=2.0)
     args = ap.parse_args()
     if args.impl == "reference":
