@@ -144,19 +144,21 @@ __device__ __forceinline__ void tmem_ld_wait() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Shared-memory matrix descriptor for a K-major operand tile stored with the
-// 128-byte swizzle: rows of 128 bytes, 8-row (1024-byte) swizzle atoms laid
-// out contiguously, so the stride between 8-row groups is 1024 bytes (64 in
-// 16-byte units) and the leading offset is unused (1).  Bits: start address
-// >> 4 [0,14), LBO [16,30), SBO [32,46), version 1 [46,48), swizzle mode 2
-// (128B) [61,64).  The tile base must be 1024-byte aligned.
-__device__ __forceinline__ uint64_t umma_desc_kmajor_sw128(uint32_t smem_addr) {
+// Shared-memory matrix descriptor for a K-major operand tile stored with a
+// ROWB-byte swizzle (ROWB = 128 or 64): rows of ROWB bytes, 8-row swizzle
+// atoms laid out contiguously, so the stride between 8-row groups (SBO) is
+// 8 * ROWB bytes and the leading offset is unused (1).  Bits: start address
+// >> 4 [0,14), LBO [16,30), SBO >> 4 [32,46), version 1 [46,48), swizzle
+// mode [61,64) (2 = 128B, 4 = 64B).  The tile base must be 1024-byte aligned.
+template <int ROWB>
+__device__ __forceinline__ uint64_t umma_desc_kmajor(uint32_t smem_addr) {
+    static_assert(ROWB == 64 || ROWB == 128, "swizzle width");
     uint64_t d = 0;
     d |= static_cast<uint64_t>((smem_addr & 0x3FFFFu) >> 4);
     d |= static_cast<uint64_t>(1u) << 16;
-    d |= static_cast<uint64_t>(64u) << 32;
+    d |= static_cast<uint64_t>((8u * ROWB) >> 4) << 32;
     d |= static_cast<uint64_t>(1u) << 46;
-    d |= static_cast<uint64_t>(2u) << 61;
+    d |= static_cast<uint64_t>(ROWB == 128 ? 2u : 4u) << 61;
     return d;
 }
 

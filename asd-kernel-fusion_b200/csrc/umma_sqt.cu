@@ -22,6 +22,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cstdlib>
 #include <mutex>
 
 #include "asd_internal.h"
@@ -32,19 +33,29 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BN = 256;
-constexpr int STAGES = 2;
-constexpr int ROW_BYTES = 128;                  // one swizzle row per k block
-constexpr int A_TILE = BM * ROW_BYTES;          // 16 KB
-constexpr int B_TILE = BN * ROW_BYTES;          // 32 KB
-constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;  // 96 KB
 constexpr int NUM_THREADS = 192;
 constexpr int TMEM_COLS = 512;
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
-constexpr int GROUP_M = 8;
+constexpr int GROUP_M = 16;
+
+// Pipeline geometry.  ROWB = bytes of K per operand row in one pipeline
+// stage (= the swizzle width): 64 -> 4 stages of 48 KB, 128 -> 2 stages of
+// 96 KB.  Smaller stages let a refill start earlier and hide more latency.
+template <int ROWB>
+struct Geo {
+    static constexpr int STAGES = (ROWB == 64) ? 4 : 2;
+    static constexpr int A_TILE = BM * ROWB;
+    static constexpr int B_TILE = BN * ROWB;
+    static constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
+    static constexpr int KSTEPS = ROWB / 32;  // 32-byte MMA k steps per stage
+    static constexpr int PIPE_BYTES = STAGES * STAGE_BYTES;
+    // epilogue column table: w_j = (Re, Im) and z_j, double-buffered by tile
+    static constexpr int TABLE_BYTES = 2 * BN * (int)(sizeof(float2) + sizeof(float4));
+};
 
 struct SmemTail {
-    uint64_t full[STAGES];
-    uint64_t empty[STAGES];
+    uint64_t full[4];
+    uint64_t empty[4];
     uint64_t tfull[2];
     uint64_t tempty[2];
     uint64_t drain;
@@ -52,7 +63,12 @@ struct SmemTail {
     int abort_flag;
     double red[2][4];
 };
-constexpr int SMEM_BYTES = 1024 /*alignment slack*/ + STAGES * STAGE_BYTES + sizeof(SmemTail);
+
+template <int ROWB>
+constexpr int smem_bytes() {
+    return 1024 /*alignment slack*/ + Geo<ROWB>::PIPE_BYTES + Geo<ROWB>::TABLE_BYTES +
+           (int)sizeof(SmemTail);
+}
 
 __device__ __forceinline__ void tile_coords(int tile, int num_m, int num_n, int &mb, int &nb) {
     const int per_group = GROUP_M * num_n;
@@ -69,29 +85,35 @@ __device__ __forceinline__ void raise_abort(SmemTail *t, unsigned *status) {
     if (status) atomicOr(status, (unsigned)kStatusTimeout);
 }
 
+__device__ __forceinline__ void epilogue_bar() {
+    asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
+}
+
 // KIND: 1 = TF32x3, 2 = BF16x3.  STORE: instead of the S(q,t) epilogue,
 // write the raw FP32 accumulator to dbg_c[i * dbg_ldc + j] (diagnostic).
-template <int KIND, bool STORE>
+template <int KIND, bool STORE, int ROWB>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     umma_sqt_kernel(const __grid_constant__ CUtensorMap tm_ah,
                     const __grid_constant__ CUtensorMap tm_al,
                     const __grid_constant__ CUtensorMap tm_bh,
                     const __grid_constant__ CUtensorMap tm_bl, int num_m, int num_n, int num_kb,
-                    int kb_per_chunk,
-                    const float4 *__restrict__ row4, const float *__restrict__ row1,
-                    const float4 *__restrict__ col4, const float *__restrict__ col1, float alpha,
-                    double2 *__restrict__ part, unsigned *__restrict__ status,
-                    float *__restrict__ dbg_c, long dbg_ldc) {
+                    int kb_per_chunk, const float4 *__restrict__ row4,
+                    const float *__restrict__ row1, const float4 *__restrict__ col4,
+                    const float *__restrict__ col1, float alpha, double2 *__restrict__ part,
+                    unsigned *__restrict__ status, float *__restrict__ dbg_c, long dbg_ldc) {
+    using G = Geo<ROWB>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-    SmemTail *tail = reinterpret_cast<SmemTail *>(smem + STAGES * STAGE_BYTES);
+    float2 *tab_w = reinterpret_cast<float2 *>(smem + G::PIPE_BYTES);           // [2][BN]
+    float4 *tab_z = reinterpret_cast<float4 *>(smem + G::PIPE_BYTES + 2 * BN * sizeof(float2));
+    SmemTail *tail = reinterpret_cast<SmemTail *>(smem + G::PIPE_BYTES + G::TABLE_BYTES);
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
     const int num_tiles = num_m * num_n;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) {
+        for (int s = 0; s < G::STAGES; ++s) {
             ptx::mbar_init(&tail->full[s], 1);
             ptx::mbar_init(&tail->empty[s], 1);
         }
@@ -119,11 +141,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             ptx::tma_prefetch_desc(&tm_al);
             ptx::tma_prefetch_desc(&tm_bh);
             ptx::tma_prefetch_desc(&tm_bl);
-            constexpr int KE = (KIND == 2) ? 64 : 32;  // elements per 128-byte row
+            constexpr int KE = ROWB / ((KIND == 2) ? 2 : 4);  // elements per stage row
             int stage = 0;
             uint32_t phase = 0;
-            bool issued[STAGES] = {};
-            uint32_t issued_parity[STAGES] = {};
+            bool issued[G::STAGES] = {};
+            uint32_t issued_parity[G::STAGES] = {};
             bool ok = true;
             for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
                 int mb, nb;
@@ -135,17 +157,17 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         ok = false;
                         break;
                     }
-                    uint8_t *st = smem + stage * STAGE_BYTES;
-                    ptx::mbar_arrive_expect_tx(&tail->full[stage], STAGE_BYTES);
+                    uint8_t *st = smem + stage * G::STAGE_BYTES;
+                    ptx::mbar_arrive_expect_tx(&tail->full[stage], G::STAGE_BYTES);
                     const int x = kb * KE;
                     ptx::tma_load_2d(st, &tm_ah, &tail->full[stage], x, mb * BM);
-                    ptx::tma_load_2d(st + A_TILE, &tm_al, &tail->full[stage], x, mb * BM);
-                    ptx::tma_load_2d(st + 2 * A_TILE, &tm_bh, &tail->full[stage], x, nb * BN);
-                    ptx::tma_load_2d(st + 2 * A_TILE + B_TILE, &tm_bl, &tail->full[stage], x,
-                                     nb * BN);
+                    ptx::tma_load_2d(st + G::A_TILE, &tm_al, &tail->full[stage], x, mb * BM);
+                    ptx::tma_load_2d(st + 2 * G::A_TILE, &tm_bh, &tail->full[stage], x, nb * BN);
+                    ptx::tma_load_2d(st + 2 * G::A_TILE + G::B_TILE, &tm_bl, &tail->full[stage],
+                                     x, nb * BN);
                     issued[stage] = true;
                     issued_parity[stage] = phase;
-                    if (++stage == STAGES) {
+                    if (++stage == G::STAGES) {
                         stage = 0;
                         phase ^= 1u;
                     }
@@ -154,7 +176,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             // Never leave the CTA with bulk copies still landing in shared
             // memory: wait (bounded, ignoring the abort flag) for the last
             // fill of every stage.
-            for (int s = 0; s < STAGES; ++s) {
+            for (int s = 0; s < G::STAGES; ++s) {
                 if (!issued[s]) continue;
                 uint32_t i = 0;
                 while (!ptx::mbar_try_wait(&tail->full[s], issued_parity[s]) && i < WAIT_LIMIT) {
@@ -196,14 +218,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                             break;
                         }
                         ptx::tc_fence_after();
-                        const uint32_t s0 = smem_base + stage * STAGE_BYTES;
-                        const uint64_t dah = ptx::umma_desc_kmajor_sw128(s0);
-                        const uint64_t dal = ptx::umma_desc_kmajor_sw128(s0 + A_TILE);
-                        const uint64_t dbh = ptx::umma_desc_kmajor_sw128(s0 + 2 * A_TILE);
+                        const uint32_t s0 = smem_base + stage * G::STAGE_BYTES;
+                        const uint64_t dah = ptx::umma_desc_kmajor<ROWB>(s0);
+                        const uint64_t dal = ptx::umma_desc_kmajor<ROWB>(s0 + G::A_TILE);
+                        const uint64_t dbh = ptx::umma_desc_kmajor<ROWB>(s0 + 2 * G::A_TILE);
                         const uint64_t dbl =
-                            ptx::umma_desc_kmajor_sw128(s0 + 2 * A_TILE + B_TILE);
+                            ptx::umma_desc_kmajor<ROWB>(s0 + 2 * G::A_TILE + G::B_TILE);
 #pragma unroll
-                        for (int kk = 0; kk < 4; ++kk) {
+                        for (int kk = 0; kk < G::KSTEPS; ++kk) {
                             const uint64_t adv = (uint64_t)(2 * kk);  // 32 bytes per k step
                             const uint32_t accum = (kb > kb0 || kk > 0) ? 1u : 0u;
                             if (KIND == 2) {
@@ -217,7 +239,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                             }
                         }
                         ptx::umma_commit(&tail->empty[stage]);
-                        if (++stage == STAGES) {
+                        if (++stage == G::STAGES) {
                             stage = 0;
                             phase ^= 1u;
                         }
@@ -243,17 +265,35 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         // Epilogue warps 2..5 own TMEM lane quarters (warp % 4) * 32.
         const int quarter = warp & 3;
         const int rloc = quarter * 32 + lane;
+        const int etid = threadIdx.x - 64;  // 0..127 among the epilogue threads
         int abuf = 0;
         uint32_t aphase = 0;
         double tot_re = 0.0, tot_im = 0.0;
-        for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+        int tcount = 0;
+        for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++tcount) {
             int mb, nb;
             tile_coords(tile, num_m, num_n, mb, nb);
             const long i = (long)mb * BM + rloc;
+            const long j0 = (long)nb * BN;
+            const int tb = tcount & 1;
+            float2 *w_tab = tab_w + tb * BN;
+            float4 *z_tab = tab_z + tb * BN;
+            if (!STORE) {
+                // Column table of this tile (double-buffered by tile: every
+                // epilogue warp finished tile - 2 before it passed the
+                // barrier of tile - 1).
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int jl = etid + 128 * h;
+                    const float4 cz = __ldg(&col4[j0 + jl]);
+                    w_tab[jl] = make_float2(cz.w, __ldg(&col1[j0 + jl]));
+                    z_tab[jl] = make_float4(cz.x, cz.y, cz.z, 0.f);
+                }
+                epilogue_bar();
+            }
             const float4 r4 = STORE ? make_float4(0.f, 0.f, 0.f, 0.f) : row4[i];
             const float ui = STORE ? 0.f : row1[i];
             double s_re = 0.0, s_im = 0.0;
-            const long j0 = (long)nb * BN;
             bool ok = true;
             for (int kb0 = 0; kb0 < num_kb; kb0 += kb_per_chunk) {
                 const bool first = (kb0 == 0);
@@ -281,35 +321,35 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                             dst[jj] = (first ? 0.f : dst[jj]) + __uint_as_float(v[jj]);
                         continue;
                     }
-                    float are = 0.f, aim = 0.f, ore = 0.f, oim = 0.f;
-                    if (last) {
+                    const float4 *wq = reinterpret_cast<const float4 *>(w_tab + c * 32);
+                    float are0 = 0.f, aim0 = 0.f, are1 = 0.f, aim1 = 0.f;
 #pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const float4 w = wq[q];  // (Re w, Im w) of columns 2q, 2q+1
+                        const float a0 = __uint_as_float(v[2 * q]);
+                        const float a1 = __uint_as_float(v[2 * q + 1]);
+                        are0 = fmaf(w.x, a0, are0);
+                        aim0 = fmaf(w.y, a0, aim0);
+                        are1 = fmaf(w.z, a1, are1);
+                        aim1 = fmaf(w.w, a1, aim1);
+                    }
+                    float ore = 0.f, oim = 0.f;
+                    if (last) {
+                        const float4 *zq = z_tab + c * 32;
+                        const float2 *wv = w_tab + c * 32;
+#pragma unroll 8
                         for (int jj = 0; jj < 32; ++jj) {
-                            const long j = j0 + c * 32 + jj;
-                            const float4 z = __ldg(&col4[j]);
-                            const float wim = __ldg(&col1[j]);
-                            const float acc = __uint_as_float(v[jj]);
+                            const float4 z = zq[jj];
+                            const float2 w = wv[jj];
                             float o = r4.x * z.x;
                             o = fmaf(r4.y, z.y, o);
                             o = fmaf(r4.z, z.z, o);
-                            are = fmaf(z.w, acc, are);
-                            aim = fmaf(wim, acc, aim);
-                            ore = fmaf(z.w, o, ore);
-                            oim = fmaf(wim, o, oim);
-                        }
-                    } else {
-#pragma unroll
-                        for (int jj = 0; jj < 32; ++jj) {
-                            const long j = j0 + c * 32 + jj;
-                            const float wre = __ldg(&col4[j].w);
-                            const float wim = __ldg(&col1[j]);
-                            const float acc = __uint_as_float(v[jj]);
-                            are = fmaf(wre, acc, are);
-                            aim = fmaf(wim, acc, aim);
+                            ore = fmaf(w.x, o, ore);
+                            oim = fmaf(w.y, o, oim);
                         }
                     }
-                    s_re += (double)alpha * (double)are - (double)ore;
-                    s_im += (double)alpha * (double)aim - (double)oim;
+                    s_re += (double)alpha * (double)(are0 + are1) - (double)ore;
+                    s_im += (double)alpha * (double)(aim0 + aim1) - (double)oim;
                 }
                 ptx::tc_fence_before();
                 __syncwarp();
@@ -319,6 +359,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     aphase ^= 1u;
                 }
             }
+            if (!ok) break;
             // u_i * s_i with u_i = (r4.w, ui)
             tot_re += (double)r4.w * s_re - (double)ui * s_im;
             tot_im += (double)r4.w * s_im + (double)ui * s_re;
@@ -360,7 +401,8 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
 }
 
 // Row-major [rows][Kp] operand, box = 128 bytes of K x box_rows rows, 128B swizzle.
-int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int box_rows) {
+int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int box_rows,
+              int rowb) {
     auto enc = get_encode_fn();
     if (!enc) return fail(ASD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
     const int esize = (kind == 2) ? 2 : 4;
@@ -368,10 +410,11 @@ int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int
         (kind == 2) ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     cuuint64_t gdim[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
     cuuint64_t gstride[1] = {(cuuint64_t)Kp * esize};
-    cuuint32_t box[2] = {(cuuint32_t)(128 / esize), (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)(rowb / esize), (cuuint32_t)box_rows};
     cuuint32_t estride[2] = {1, 1};
     CUresult r = enc(m, dt, 2, const_cast<void *>(base), gdim, gstride, box, estride,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     rowb == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(ASD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return ASD_OK;
@@ -381,18 +424,30 @@ int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int
 
 long umma_row_pad(long M) { return (M + BN - 1) / BN * BN; }
 
+int umma_row_bytes() {
+    // Pipeline stage width (64: 4 x 48 KB stages, the default; 128: 2 x 96 KB).
+    static int rowb = [] {
+        const char *e = getenv("ASD_UMMA_ROWB");
+        return (e && atoi(e) == 128) ? 128 : 64;
+    }();
+    return rowb;
+}
+
 int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     const long Mp = umma_row_pad(a.M);
-    const int ke = (a.kind == 2) ? 64 : 32;
-    if (a.Kp % ke != 0 || a.Kp <= 0) return fail(ASD_ERR_INVALID, "Kp=%d not a multiple of %d", a.Kp, ke);
+    const int esize = (a.kind == 2) ? 2 : 4;
+    if (a.Kp <= 0 || (a.Kp * esize) % 128 != 0)
+        return fail(ASD_ERR_INVALID, "Kp=%d: rows must be a multiple of 128 bytes", a.Kp);
     if (((uintptr_t)a.a_hi | (uintptr_t)a.a_lo | (uintptr_t)a.b_hi | (uintptr_t)a.b_lo) & 15)
         return fail(ASD_ERR_INVALID, "operand base not 16-byte aligned");
+    const int rowb = umma_row_bytes();
+    const int ke = rowb / esize;  // K elements per pipeline stage
     CUtensorMap tah, tal, tbh, tbl;
     int rc;
-    if ((rc = make_tmap(&tah, a.a_hi, a.kind, Mp, a.Kp, BM)) != ASD_OK) return rc;
-    if ((rc = make_tmap(&tal, a.a_lo, a.kind, Mp, a.Kp, BM)) != ASD_OK) return rc;
-    if ((rc = make_tmap(&tbh, a.b_hi, a.kind, Mp, a.Kp, BN)) != ASD_OK) return rc;
-    if ((rc = make_tmap(&tbl, a.b_lo, a.kind, Mp, a.Kp, BN)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tah, a.a_hi, a.kind, Mp, a.Kp, BM, rowb)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tal, a.a_lo, a.kind, Mp, a.Kp, BM, rowb)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tbh, a.b_hi, a.kind, Mp, a.Kp, BN, rowb)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tbl, a.b_lo, a.kind, Mp, a.Kp, BN, rowb)) != ASD_OK) return rc;
     const int num_m = (int)(Mp / BM), num_n = (int)(Mp / BN), num_kb = a.Kp / ke;
     const int tiles = num_m * num_n;
     const int grid = tiles < a.num_sms ? tiles : a.num_sms;
@@ -401,19 +456,29 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     if (kpc < 1) kpc = 1;
     if (kpc > num_kb) kpc = num_kb;
     cudaError_t e;
-    auto go = [&](auto kern) {
-        cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             SMEM_BYTES);
+    auto go = [&](auto kern, int smem) {
+        cudaError_t r =
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (r == cudaSuccess)
-            kern<<<grid, NUM_THREADS, SMEM_BYTES, st>>>(tah, tal, tbh, tbl, num_m, num_n, num_kb,
-                                                        kpc, a.row4, a.row1, a.col4, a.col1, a.alpha,
-                                                        a.part, a.status, a.dbg_c, a.dbg_ldc);
+            kern<<<grid, NUM_THREADS, smem, st>>>(tah, tal, tbh, tbl, num_m, num_n, num_kb, kpc,
+                                                  a.row4, a.row1, a.col4, a.col1, a.alpha, a.part,
+                                                  a.status, a.dbg_c, a.dbg_ldc);
         return r;
     };
-    if (a.kind == 2)
-        e = a.dbg_c ? go(umma_sqt_kernel<2, true>) : go(umma_sqt_kernel<2, false>);
-    else
-        e = a.dbg_c ? go(umma_sqt_kernel<1, true>) : go(umma_sqt_kernel<1, false>);
+    const bool dbg = a.dbg_c != nullptr;
+    if (rowb == 64) {
+        constexpr int S = smem_bytes<64>();
+        if (a.kind == 2)
+            e = dbg ? go(umma_sqt_kernel<2, true, 64>, S) : go(umma_sqt_kernel<2, false, 64>, S);
+        else
+            e = dbg ? go(umma_sqt_kernel<1, true, 64>, S) : go(umma_sqt_kernel<1, false, 64>, S);
+    } else {
+        constexpr int S = smem_bytes<128>();
+        if (a.kind == 2)
+            e = dbg ? go(umma_sqt_kernel<2, true, 128>, S) : go(umma_sqt_kernel<2, false, 128>, S);
+        else
+            e = dbg ? go(umma_sqt_kernel<1, true, 128>, S) : go(umma_sqt_kernel<1, false, 128>, S);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "umma_sqt setup");
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "umma_sqt launch");
