@@ -81,7 +81,7 @@ struct asd_ctx {
     long state_version = 0, origin_version = -1;
     bool has_state = false, has_origin = false;
     int last_launches = 0;
-    int chunk_k = 512;
+    int chunk_k = -1;  // < 0: per mode, 512 for TF32x3 and 1024 for BF16x3
 };
 
 namespace {
@@ -262,7 +262,9 @@ int sqt_split(asd_ctx *c, int kind, double *d_out) {
     u.part = c->part;
     u.status = c->status;
     u.num_sms = c->num_sms;
-    u.chunk_k = c->chunk_k;
+    // Same number of tensor-core accumulation steps per chunk for both kinds
+    // (TF32 MMAs take 8 K elements per step, BF16 ones 16).
+    u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
     const int grid = launch_umma_sqt(u, c->stream);
     if (grid < 0) return grid;
     ASD_CUDA_TRY(launch_finalize(c->part, grid, 1.0 / (double)c->M, d_out, c->stream));
@@ -568,8 +570,7 @@ int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_s
 
 int asd_ctx_set_chunk_k(asd_ctx *c, int chunk_k) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
-    if (chunk_k < 0) return fail(ASD_ERR_INVALID, "chunk_k < 0");
-    c->chunk_k = chunk_k;
+    c->chunk_k = chunk_k < 0 ? -1 : chunk_k;
     return ASD_OK;
 }
 

@@ -425,10 +425,12 @@ int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int
 long umma_row_pad(long M) { return (M + BN - 1) / BN * BN; }
 
 int umma_row_bytes() {
-    // Pipeline stage width (64: 4 x 48 KB stages, the default; 128: 2 x 96 KB).
+    // Pipeline stage width: 128 (2 x 96 KB stages, the default) or 64
+    // (4 x 48 KB stages, ASD_UMMA_ROWB=64).  Measured on B200, the two-stage
+    // form is as fast or faster (fewer barrier round trips per flop).
     static int rowb = [] {
         const char *e = getenv("ASD_UMMA_ROWB");
-        return (e && atoi(e) == 128) ? 128 : 64;
+        return (e && atoi(e) == 64) ? 64 : 128;
     }();
     return rowb;
 }

@@ -273,7 +273,8 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": f"f64 RK4 + {mode} GEMM (fp32 accumulate, f64 reduction)",
         "data": "synthetic: seeded spins uniform on the sphere",
         "config": {"workload": WORKLOAD, "sites": M, "replicas": nf, "gemm_m": M, "gemm_n": M,
-                   "gemm_k": K, "sqt_mode": mode, "chunk_k": args.chunk_k if args.chunk_k >= 0 else 512,
+                   "gemm_k": K, "sqt_mode": mode,
+                   "chunk_k": args.chunk_k if args.chunk_k >= 0 else (512 if mode == "tf32x3" else 1024),
                    "l2": "inputs larger than L2 (spin state 197 MB per array, operands 197 MB)"},
         "roofline": {"bound": "tensor", "kernel": f"umma_sqt_kernel ({mode})",
                      "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",

@@ -121,10 +121,13 @@ int asd_ctx_step_host(asd_ctx *ctx, const double *spin_in, double *spin_out,
                       asd_sqt_mode mode, double sqt_out[2]);
 
 /* K elements accumulated per TMEM chunk by the split S(q,t) modes (rounded
- * up to the 128-byte k block; 0 = all of K in one accumulator).  The tensor
- * cores' FP32 accumulation loses precision with every accumulation step, so
- * K is cut into chunks whose partial products the epilogue adds in FP64.
- * Default 512. */
+ * up to the pipeline's k block; 0 = all of K in one accumulator; negative =
+ * the default).  The tensor cores' FP32 accumulation loses precision with
+ * every accumulation step, so K is cut into chunks whose partial products the
+ * epilogue adds in FP64.  Default: 512 for TF32x3 and 1024 for BF16x3, the
+ * same number of accumulation steps (TF32 MMAs take 8 K elements per step,
+ * BF16 ones 16); measured relative error of S(q,t) about 5e-6 and 4e-6 at
+ * K = 3000. */
 int asd_ctx_set_chunk_k(asd_ctx *ctx, int chunk_k);
 
 /* Number of kernels the last asd_ctx_step / asd_ctx_sqt* call launched. */
