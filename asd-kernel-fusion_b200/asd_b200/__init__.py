@@ -28,6 +28,9 @@ ASD_ERR_TIMEOUT = -4
 ASD_ERR_STATE = -5
 ASD_ERR_UNSUPPORTED = -6
 
+LLG_FUSED_STEP = 0
+LLG_STAGES = 1
+
 SQT_FP64 = 0
 SQT_TF32X3 = 1
 SQT_BF16X3 = 2
@@ -41,7 +44,8 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_create", "asd_ctx_destroy", "asd_ctx_set_stream", "asd_ctx_get_params",
     "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
-    "asd_ctx_step_host", "asd_ctx_set_chunk_k", "asd_ctx_last_launches",
+    "asd_ctx_step_host", "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
+    "asd_ctx_last_launches",
     "asd_ctx_check_device_status",
     "asd_umma_gemm_f32", "asd_sqt_split_noalloc", "asd_set_params", "euler", "runge_kutta",
     "fused_dgemm",
@@ -113,6 +117,7 @@ def load() -> C.CDLL:
         "asd_ctx_sqt": ([vp, C.c_int, dp], C.c_int),
         "asd_ctx_sqt_async": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_step_host": ([vp, vp, vp, C.c_int, dp], C.c_int),
+        "asd_ctx_set_llg_kernel": ([vp, C.c_int], C.c_int),
         "asd_ctx_set_chunk_k": ([vp, C.c_int], C.c_int),
         "asd_ctx_last_launches": ([vp], C.c_int),
         "asd_ctx_check_device_status": ([vp], C.c_int),
@@ -239,6 +244,11 @@ class Context:
         _check(load().asd_ctx_step_host(self._h, C.c_void_p(spin_in_ptr),
                                         C.c_void_p(spin_out_ptr), mode, self._out))
         return complex(self._out[0], self._out[1])
+
+    def set_llg_kernel(self, kernel) -> None:
+        """"fused" (one launch per step, default) or "stages" (four launches)."""
+        k = {"fused": LLG_FUSED_STEP, "stages": LLG_STAGES}.get(kernel, kernel)
+        _check(load().asd_ctx_set_llg_kernel(self._h, int(k)))
 
     def set_chunk_k(self, chunk_k: int) -> None:
         _check(load().asd_ctx_set_chunk_k(self._h, int(chunk_k)))

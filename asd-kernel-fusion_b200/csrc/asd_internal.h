@@ -51,6 +51,11 @@ enum : unsigned { kStatusTimeout = 1u, kStatusBadLaunch = 2u };
 cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const double *ys_in,
                              double *acc, double *ys_out, cudaStream_t st);
 
+// One whole RK4 step (all four stages + renormalisation) in one launch,
+// temporally blocked in shared memory: y -> yout (distinct buffers).
+cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *yout,
+                                  cudaStream_t st);
+
 // AoS [nfile][M][3] <-> site-major [M][nfile][3]
 cudaError_t launch_aos_to_sitemajor(const double *aos, double *sm, long M, int nfile,
                                     cudaStream_t st);

@@ -82,6 +82,7 @@ struct asd_ctx {
     bool has_state = false, has_origin = false;
     int last_launches = 0;
     int chunk_k = -1;  // < 0: per mode, 512 for TF32x3 and 1024 for BF16x3
+    int llg_kernel = ASD_LLG_FUSED_STEP;
 };
 
 namespace {
@@ -158,6 +159,17 @@ int set_spins_common(asd_ctx *c, const double *aos, bool host, int as_origin) {
 }
 
 int run_steps(asd_ctx *c, int nsteps) {
+    if (c->llg_kernel == ASD_LLG_FUSED_STEP) {
+        for (int s = 0; s < nsteps; ++s) {
+            ASD_CUDA_TRY(launch_llg_step_fused(c->a, c->y, c->ys_a, c->stream));
+            double *t = c->y;  // ping-pong: the new state becomes y
+            c->y = c->ys_a;
+            c->ys_a = t;
+            c->last_launches += 1;
+            c->state_version++;
+        }
+        return ASD_OK;
+    }
     for (int s = 0; s < nsteps; ++s) {
         ASD_CUDA_TRY(launch_llg_stage(1, c->a, c->y, c->y, c->acc, c->ys_a, c->stream));
         ASD_CUDA_TRY(launch_llg_stage(2, c->a, c->y, c->ys_a, c->acc, c->ys_b, c->stream));
@@ -565,6 +577,14 @@ int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_s
     if (rc != ASD_OK) return rc;
     sqt_out[0] = c->h_out[0];
     sqt_out[1] = c->h_out[1];
+    return ASD_OK;
+}
+
+int asd_ctx_set_llg_kernel(asd_ctx *c, int kernel) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    if (kernel != ASD_LLG_FUSED_STEP && kernel != ASD_LLG_STAGES)
+        return fail(ASD_ERR_INVALID, "unknown LLG kernel %d", kernel);
+    c->llg_kernel = kernel;
     return ASD_OK;
 }
 

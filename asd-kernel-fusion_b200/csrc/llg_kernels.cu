@@ -6,6 +6,8 @@
 // an FMA.  With alpha = J2 = h = 0 the trajectory is therefore bit-identical
 // to the reference's euler / runge_kutta / renormalisation built with
 // -ffp-contract=off (llg_sqt_baseline.c:29-142, :298-309).
+#include <cstdlib>
+
 #include "asd_internal.h"
 
 namespace asd {
@@ -15,6 +17,9 @@ __device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b
 __device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double dq(double a, double b) { return __ddiv_rn(a, b); }
+// x / 2: the product by 0.5 is the same correctly rounded value (2 is a power
+// of the radix), without a division.
+__device__ __forceinline__ double half(double x) { return __dmul_rn(x, 0.5); }
 
 struct V3 {
     double x, y, z;
@@ -101,18 +106,18 @@ __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double 
     const double k0 = dm(d.x, a.dt), k1 = dm(d.y, a.dt), k2 = dm(d.z, a.dt);
     if (STAGE == 1) {
         const double y0 = y[e], y1 = y[e + 1], y2 = y[e + 2];
-        out[e] = da(y0, dq(k0, 2.0));
-        out[e + 1] = da(y1, dq(k1, 2.0));
-        out[e + 2] = da(y2, dq(k2, 2.0));
+        out[e] = da(y0, half(k0));
+        out[e + 1] = da(y1, half(k1));
+        out[e + 2] = da(y2, half(k2));
         acc[e] = da(y0, dq(k0, 6.0));
         acc[e + 1] = da(y1, dq(k1, 6.0));
         acc[e + 2] = da(y2, dq(k2, 6.0));
     } else if (STAGE == 2 || STAGE == 3) {
         const double y0 = y[e], y1 = y[e + 1], y2 = y[e + 2];
         if (STAGE == 2) {
-            out[e] = da(y0, dq(k0, 2.0));
-            out[e + 1] = da(y1, dq(k1, 2.0));
-            out[e + 2] = da(y2, dq(k2, 2.0));
+            out[e] = da(y0, half(k0));
+            out[e + 1] = da(y1, half(k1));
+            out[e + 2] = da(y2, half(k2));
         } else {
             out[e] = da(y0, k0);
             out[e + 1] = da(y1, k1);
@@ -155,6 +160,183 @@ cudaError_t launch_stage_t(const LLGArgs &a, const double *y, const double *ys, 
         ASD_STAGE_CASE(7, true, true, true)
     }
 #undef ASD_STAGE_CASE
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------ temporally blocked step
+// One RK4 step per launch.  A CTA owns a 16 x 16 core of sites for F
+// replicas and loads the 24 x 24 patch around it (a halo of 4 sites, one per
+// stage) into shared memory.  Stage s then runs on the region within
+// distance 4 - s of the core (Chebyshev distance, which also covers the
+// diagonal J2 neighbours), so stage 4 produces exactly the core.  Stage
+// inputs ping-pong between two shared buffers; the base state and the
+// running combination of each (site, replica) stay in the registers of the
+// thread that owns it.  Only y is read and only the renormalised core is
+// written: 48 bytes of DRAM traffic per site-step instead of 384.  The
+// arithmetic per (site, replica) is the stage kernels' (bit-identical).
+constexpr int FT = 16;              // core side
+constexpr int FH = 4;               // halo = number of stages
+constexpr int FP = FT + 2 * FH;     // patch side
+constexpr int FR1 = (FT + 6) * (FT + 6);  // sites of the stage-1 region
+
+// Site of the patch for the idx-th entry of the region list: the core in
+// row-major order first, then the rings at distance 1, 2, 3.  So the first
+// 256, 324, 400, 484 entries are the regions of stages 4, 3, 2, 1.
+__device__ __forceinline__ void region_site(int idx, int &r, int &c) {
+    if (idx < FT * FT) {
+        r = FH + idx / FT;
+        c = FH + idx % FT;
+        return;
+    }
+    idx -= FT * FT;
+    int d = 1;
+    for (; d < 3; ++d) {
+        const int cnt = 4 * (FT + 2 * d) - 4;
+        if (idx < cnt) break;
+        idx -= cnt;
+    }
+    const int L = FT + 2 * d;
+    if (idx < L) { r = FH - d; c = FH - d + idx; return; }
+    idx -= L;
+    if (idx < L) { r = FH + FT - 1 + d; c = FH - d + idx; return; }
+    idx -= L;
+    if (idx < L - 2) { r = FH - d + 1 + idx; c = FH - d; return; }
+    idx -= L - 2;
+    r = FH - d + 1 + idx;
+    c = FH + FT - 1 + d;
+}
+
+template <int F, int NT, bool J2, bool H, bool DAMP>
+__global__ void __launch_bounds__(NT) llg_step_fused_kernel(LLGArgs a, int tiles_x,
+                                                            const double *__restrict__ y,
+                                                            double *__restrict__ yout) {
+    extern __shared__ double fsm[];
+    constexpr int SLOT = 3 * F;                      // doubles per patch site
+    constexpr int NITEM = (FR1 * F + NT - 1) / NT;   // items owned per thread
+    double *bufA = fsm;
+    double *bufB = fsm + FP * FP * SLOT;
+    const int tile = blockIdx.x;
+    const int R0 = (tile / tiles_x) * FT, C0 = (tile % tiles_x) * FT;
+    const int f0 = blockIdx.y * F;
+    const int N = a.N;
+    const long K = 3L * a.nfile;
+    const int nf = min(F, a.nfile - f0);  // replicas present in this chunk
+
+    // load the patch (periodic wrap), zero for replicas past nfile
+    for (int e = threadIdx.x; e < FP * FP * SLOT; e += NT) {
+        const int slot = e / SLOT, w = e - slot * SLOT;
+        const int pr = slot / FP, pc = slot - pr * FP;
+        const int gr = ((R0 + pr - FH) % N + N) % N;
+        const int gc = ((C0 + pc - FH) % N + N) % N;
+        double v = 0.0;
+        if (w < 3 * nf) v = y[((long)gr * N + gc) * K + 3L * f0 + w];
+        bufA[e] = v;
+    }
+    __syncthreads();
+
+    double yb[NITEM][3], acc[NITEM][3];
+    int slot_of[NITEM];
+#pragma unroll
+    for (int j = 0; j < NITEM; ++j) {
+        const int it = threadIdx.x + j * NT;
+        slot_of[j] = -1;
+        if (it < FR1 * F) {
+            int r, c;
+            region_site(it / F, r, c);
+            slot_of[j] = r * FP + c;
+            const double *p = bufA + slot_of[j] * SLOT + (it % F) * 3;
+            yb[j][0] = p[0];
+            yb[j][1] = p[1];
+            yb[j][2] = p[2];
+        }
+    }
+    // The region list covers each stage's sites first (see region_site).
+    const int stage_items[4] = {FR1 * F, (FT + 4) * (FT + 4) * F, (FT + 2) * (FT + 2) * F,
+                                FT * FT * F};
+    double *in = bufA, *out = bufB;
+#pragma unroll
+    for (int s = 1; s <= 4; ++s) {
+        const int lim = stage_items[s - 1];
+#pragma unroll
+        for (int j = 0; j < NITEM; ++j) {
+            const int it = threadIdx.x + j * NT;
+            const int f = it % F;
+            if (it >= lim || f >= nf) continue;
+            const int slot = slot_of[j];
+            const V3 d = llg_rhs<J2, H, DAMP>(in, SLOT, 3L * f, FP, slot / FP, slot % FP, a);
+            const double k0 = dm(d.x, a.dt), k1 = dm(d.y, a.dt), k2 = dm(d.z, a.dt);
+            double *o = out + slot * SLOT + 3 * f;
+            if (s == 1) {
+                o[0] = da(yb[j][0], half(k0));
+                o[1] = da(yb[j][1], half(k1));
+                o[2] = da(yb[j][2], half(k2));
+                acc[j][0] = da(yb[j][0], dq(k0, 6.0));
+                acc[j][1] = da(yb[j][1], dq(k1, 6.0));
+                acc[j][2] = da(yb[j][2], dq(k2, 6.0));
+            } else if (s == 2) {
+                o[0] = da(yb[j][0], half(k0));
+                o[1] = da(yb[j][1], half(k1));
+                o[2] = da(yb[j][2], half(k2));
+                acc[j][0] = da(acc[j][0], dq(k0, 3.0));
+                acc[j][1] = da(acc[j][1], dq(k1, 3.0));
+                acc[j][2] = da(acc[j][2], dq(k2, 3.0));
+            } else if (s == 3) {
+                o[0] = da(yb[j][0], k0);
+                o[1] = da(yb[j][1], k1);
+                o[2] = da(yb[j][2], k2);
+                acc[j][0] = da(acc[j][0], dq(k0, 3.0));
+                acc[j][1] = da(acc[j][1], dq(k1, 3.0));
+                acc[j][2] = da(acc[j][2], dq(k2, 3.0));
+            } else {
+                const double o0 = da(acc[j][0], dq(k0, 6.0));
+                const double o1 = da(acc[j][1], dq(k1, 6.0));
+                const double o2 = da(acc[j][2], dq(k2, 6.0));
+                const double nrm = __dsqrt_rn(da(da(dm(o0, o0), dm(o1, o1)), dm(o2, o2)));
+                const int gr = R0 + slot / FP - FH, gc = C0 + slot % FP - FH;
+                if (gr < N && gc < N) {
+                    double *g = yout + ((long)gr * N + gc) * K + 3L * (f0 + f);
+                    g[0] = dq(dm(a.spin_len, o0), nrm);
+                    g[1] = dq(dm(a.spin_len, o1), nrm);
+                    g[2] = dq(dm(a.spin_len, o2), nrm);
+                }
+            }
+        }
+        if (s < 4) {
+            __syncthreads();
+            double *t = in;
+            in = out;
+            out = t;
+        }
+    }
+}
+
+template <int F, int NT>
+cudaError_t launch_fused_t(const LLGArgs &a, const double *y, double *yout, cudaStream_t st) {
+    const int tiles_x = (a.N + FT - 1) / FT;
+    dim3 grid((unsigned)(tiles_x * tiles_x), (unsigned)((a.nfile + F - 1) / F));
+    if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+    const size_t smem = 2ull * FP * FP * 3 * F * sizeof(double);
+    const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
+    cudaError_t e = cudaSuccess;
+#define ASD_FUSED_CASE(S, J, Hh, D)                                                         \
+    case S: {                                                                               \
+        auto k = llg_step_fused_kernel<F, NT, J, Hh, D>;                                    \
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        if (e == cudaSuccess) k<<<grid, NT, smem, st>>>(a, tiles_x, y, yout);               \
+        break;                                                                              \
+    }
+    switch (sel) {
+        ASD_FUSED_CASE(0, false, false, false)
+        ASD_FUSED_CASE(1, false, false, true)
+        ASD_FUSED_CASE(2, false, true, false)
+        ASD_FUSED_CASE(3, false, true, true)
+        ASD_FUSED_CASE(4, true, false, false)
+        ASD_FUSED_CASE(5, true, false, true)
+        ASD_FUSED_CASE(6, true, true, false)
+        ASD_FUSED_CASE(7, true, true, true)
+    }
+#undef ASD_FUSED_CASE
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
@@ -225,7 +407,7 @@ __global__ void rk_pass_kernel(int pass, long n, double dt, const double *__rest
     const double kk = dm(k[j], dt);
     k[j] = kk;
     if (pass == 1 || pass == 2) {
-        cur[j] = da(spin[j], dq(kk, 2.0));
+        cur[j] = da(spin[j], half(kk));
     } else if (pass == 3) {
         cur[j] = da(spin[j], kk);
     } else {
@@ -267,6 +449,17 @@ cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const
         case 4: return launch_stage_t<4>(a, y, ys_in, acc, ys_out, st);
     }
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *yout,
+                                  cudaStream_t st) {
+    // 2 replicas per CTA, 256 threads (55 KB of shared memory, 4 CTAs per SM);
+    // ASD_LLG_REPLICAS=4 selects 4 replicas and 512 threads.
+    static const int f4 = [] {
+        const char *e = getenv("ASD_LLG_REPLICAS");
+        return (e && atoi(e) == 4) ? 1 : 0;
+    }();
+    return f4 ? launch_fused_t<4, 512>(a, y, yout, st) : launch_fused_t<2, 256>(a, y, yout, st);
 }
 
 cudaError_t launch_aos_to_sitemajor(const double *aos, double *sm, long M, int nfile,

@@ -39,6 +39,7 @@ CONFIG = dict(N=128, nfile=500, J1=-1.0, J2=0.0, alpha=0.05, h=(0.0, 0.0, 0.5), 
 WORKLOAD = "llg-rk4+sqt 128x128 lattice, 500 replicas, J=-1, h=(0,0,0.5), alpha=0.05, dt=0.005"
 METRIC = "LLG site-steps/s + S(q,t) GEMM TFLOP/s, mixed vs FP64 plain at stated error"
 LLG_BYTES_PER_SITE_STEP = 384  # 4 fused stage kernels: 3+5+5+3 FP64 3-vectors
+LLG_FUSED_BYTES_PER_SITE_STEP = 48  # one temporally blocked step: read y, write y
 
 
 def env_rank():
@@ -306,14 +307,18 @@ def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     d = torch.zeros(2, dtype=torch.float64, device="cuda")
     reps = 10
-    ctx.step(2)
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    ctx.step(reps)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    llg_ms = ev0.elapsed_time(ev1) / reps
-    llg_gbs = LLG_BYTES_PER_SITE_STEP * M * nf / (llg_ms / 1e3) / 1e9
+    llg = {}
+    for kern, bps in (("stages", LLG_BYTES_PER_SITE_STEP), ("fused", LLG_FUSED_BYTES_PER_SITE_STEP)):
+        ctx.set_llg_kernel(kern)
+        ctx.step(2)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        ctx.step(reps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / reps
+        llg[kern] = (ms, bps * M * nf / (ms / 1e3) / 1e9, bps)
+    ctx.set_llg_kernel("fused")
     hbm, bf16, src = measured_peaks()
     sqt_ms, vals = {}, {}
     for mode in ("fp64", "tf32x3", "bf16x3"):
@@ -330,9 +335,9 @@ def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
     ref = vals["fp64"]
     flops = 2.0 * M * M * K
     report = {
-        "llg": {"site_steps_per_s": M * nf / (llg_ms / 1e3), "ms": llg_ms, "achieved_gbs": llg_gbs,
-                "hbm_peak_gbs": hbm, "frac": llg_gbs / hbm,
-                "bytes_per_site_step": LLG_BYTES_PER_SITE_STEP},
+        "llg": {k: {"site_steps_per_s": M * nf / (v[0] / 1e3), "ms": v[0], "achieved_gbs": v[1],
+                    "hbm_peak_gbs": hbm, "frac": v[1] / hbm, "bytes_per_site_step": v[2]}
+                for k, v in llg.items()},
         "sqt": {m: {"ms": sqt_ms[m], "tflops": flops / (sqt_ms[m] / 1e3) / 1e12,
                     "value": [vals[m].real, vals[m].imag],
                     "rel_err_vs_fp64": abs(vals[m] - ref) / abs(ref)} for m in sqt_ms},

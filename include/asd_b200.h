@@ -120,6 +120,14 @@ int asd_ctx_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
 int asd_ctx_step_host(asd_ctx *ctx, const double *spin_in, double *spin_out,
                       asd_sqt_mode mode, double sqt_out[2]);
 
+/* How asd_ctx_step runs one RK4 step.  Both give bit-identical spins. */
+#define ASD_LLG_FUSED_STEP 0 /* default: one launch per step, the four stages
+                                temporally blocked in shared memory (48 B of
+                                DRAM traffic per site-step)                  */
+#define ASD_LLG_STAGES 1     /* four launches, one fused kernel per RK4 stage
+                                (384 B of DRAM traffic per site-step)        */
+int asd_ctx_set_llg_kernel(asd_ctx *ctx, int kernel);
+
 /* K elements accumulated per TMEM chunk by the split S(q,t) modes (rounded
  * up to the pipeline's k block; 0 = all of K in one accumulator; negative =
  * the default).  The tensor cores' FP32 accumulation loses precision with

@@ -22,13 +22,17 @@ CASES = [
     (16, 7, dict(J1=1.0, J2=-0.3, alpha=0.02, dt=0.005)),
     (10, 2, dict(J1=1.0, alpha=0.1, dt=0.01)),
     (3, 1, dict(J1=1.0, J2=0.5, h=(0.1, 0.2, 0.3), alpha=0.3, dt=0.02)),   # smallest lattice
+    (37, 9, dict(J1=-0.8, J2=0.2, h=(0.0, 0.3, 0.1), alpha=0.07, dt=0.01)),  # ragged tiles
+    (48, 4, dict(J1=1.0, dt=0.02)),                      # several whole tiles
 ]
 
 
+@pytest.mark.parametrize("kernel", ["fused", "stages"])
 @pytest.mark.parametrize("N,nfile,kw", CASES)
-def test_ctx_steps_bit_exact(oracle, N, nfile, kw):
+def test_ctx_steps_bit_exact(oracle, N, nfile, kw, kernel):
     s0 = asd.random_spins(N, nfile, seed=N + nfile, spin_len=kw.get("spin_len", 1.0))
     with asd.Context(asd.Params.make(N, nfile, **kw), modes=["fp64"]) as ctx:
+        ctx.set_llg_kernel(kernel)
         ctx.set_spins(s0, as_origin=True)
         assert np.array_equal(ctx.get_spins(), s0)  # layout round trip
         ctx.step(5)
@@ -37,13 +41,15 @@ def test_ctx_steps_bit_exact(oracle, N, nfile, kw):
     assert np.array_equal(got, want), np.abs(got - want).max()
 
 
+@pytest.mark.parametrize("kernel", ["fused", "stages"])
 @pytest.mark.parametrize("name", ["llg_n12_f4", "llg_n20_f6"])
-def test_ctx_matches_reference_fixture(golden, name):
+def test_ctx_matches_reference_fixture(golden, name, kernel):
     g = golden(name)
     N, nf, n = int(g["N"]), int(g["nfile"]), int(g["nsteps"])
     for length, key in ((1.0, "steps_len1"), (1.5, "steps_len15")):
         p = asd.Params.make(N, nf, J1=float(g["J1"]), dt=float(g["dt"]), spin_len=length)
         with asd.Context(p, modes=["fp64"]) as ctx:
+            ctx.set_llg_kernel(kernel)
             ctx.set_spins(g["spins0"], as_origin=True)
             ctx.step(n)
             assert np.array_equal(ctx.get_spins(), g[key])
