@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_step_host", "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
     "asd_ctx_last_launches",
     "asd_ctx_check_device_status",
-    "asd_umma_gemm_f32", "asd_sqt_split_noalloc", "asd_set_params", "euler", "runge_kutta",
+    "asd_check_const_division", "asd_umma_gemm_f32", "asd_sqt_split_noalloc", "asd_set_params", "euler", "runge_kutta",
     "fused_dgemm",
 )
 
@@ -121,6 +121,7 @@ def load() -> C.CDLL:
         "asd_ctx_set_chunk_k": ([vp, C.c_int], C.c_int),
         "asd_ctx_last_launches": ([vp], C.c_int),
         "asd_ctx_check_device_status": ([vp], C.c_int),
+        "asd_check_const_division": ([vp, C.c_long, vp, vp], C.c_int),
         "asd_umma_gemm_f32": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, C.c_long, C.c_int,
                                vp],
                               C.c_int),
@@ -311,3 +312,9 @@ def sqt_split_noalloc(kind: int, rows: int, Kp: int, a_hi: int, a_lo: int, b_hi:
                                         v(b_lo), v(row4), v(row1), v(col4), v(col1),
                                         float(alpha), float(scale), int(chunk_k), v(d_out),
                                         v(stream)))
+
+
+def check_const_division(x_ptr: int, n: int, bad_ptr: int, stream: int = 0) -> None:
+    """asd_check_const_division on device pointers (diagnostic)."""
+    _check(load().asd_check_const_division(C.c_void_p(x_ptr), int(n), C.c_void_p(bad_ptr),
+                                           C.c_void_p(stream)))

@@ -56,6 +56,10 @@ cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const
 cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *yout,
                                   cudaStream_t st);
 
+// Counts the x[i] for which the constant divisions by 3 and 6 of the LLG
+// kernels differ from __ddiv_rn in any bit (diagnostic).
+cudaError_t launch_div_check(const double *x, long n, unsigned long long *bad, cudaStream_t st);
+
 // AoS [nfile][M][3] <-> site-major [M][nfile][3]
 cudaError_t launch_aos_to_sitemajor(const double *aos, double *sm, long M, int nfile,
                                     cudaStream_t st);

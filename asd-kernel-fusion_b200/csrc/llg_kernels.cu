@@ -21,6 +21,26 @@ __device__ __forceinline__ double dq(double a, double b) { return __ddiv_rn(a, b
 // of the radix), without a division.
 __device__ __forceinline__ double half(double x) { return __dmul_rn(x, 0.5); }
 
+// x / d for the constants d = 3 and 6, correctly rounded, by Markstein's
+// correction step (P. Markstein, IBM J. Res. Dev. 34(1), 1990): with
+// yinv = RN(1/d), q = RN(x * yinv) is within one ulp of x/d, the remainder
+// r = x - q d is exact in one FMA, and RN(q + r * yinv) is RN(x/d).  Valid
+// away from overflow and the subnormal range, which the RK4 increments never
+// reach; zeros keep their sign.  Three FP64 operations instead of a
+// division routine; tests compare it with __ddiv_rn bit for bit.
+__device__ __forceinline__ double div3(double x) {
+    constexpr double yinv = 1.0 / 3.0;  // RN(1/3), folded at compile time
+    const double q = __dmul_rn(x, yinv);
+    const double r = __fma_rn(-q, 3.0, x);
+    return x == 0.0 ? x : __fma_rn(r, yinv, q);
+}
+__device__ __forceinline__ double div6(double x) {
+    constexpr double yinv = 1.0 / 6.0;  // RN(1/6)
+    const double q = __dmul_rn(x, yinv);
+    const double r = __fma_rn(-q, 6.0, x);
+    return x == 0.0 ? x : __fma_rn(r, yinv, q);
+}
+
 struct V3 {
     double x, y, z;
 };
@@ -109,9 +129,9 @@ __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double 
         out[e] = da(y0, half(k0));
         out[e + 1] = da(y1, half(k1));
         out[e + 2] = da(y2, half(k2));
-        acc[e] = da(y0, dq(k0, 6.0));
-        acc[e + 1] = da(y1, dq(k1, 6.0));
-        acc[e + 2] = da(y2, dq(k2, 6.0));
+        acc[e] = da(y0, div6(k0));
+        acc[e + 1] = da(y1, div6(k1));
+        acc[e + 2] = da(y2, div6(k2));
     } else if (STAGE == 2 || STAGE == 3) {
         const double y0 = y[e], y1 = y[e + 1], y2 = y[e + 2];
         if (STAGE == 2) {
@@ -123,13 +143,13 @@ __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double 
             out[e + 1] = da(y1, k1);
             out[e + 2] = da(y2, k2);
         }
-        acc[e] = da(acc[e], dq(k0, 3.0));
-        acc[e + 1] = da(acc[e + 1], dq(k1, 3.0));
-        acc[e + 2] = da(acc[e + 2], dq(k2, 3.0));
+        acc[e] = da(acc[e], div3(k0));
+        acc[e + 1] = da(acc[e + 1], div3(k1));
+        acc[e + 2] = da(acc[e + 2], div3(k2));
     } else {
-        const double o0 = da(acc[e], dq(k0, 6.0));
-        const double o1 = da(acc[e + 1], dq(k1, 6.0));
-        const double o2 = da(acc[e + 2], dq(k2, 6.0));
+        const double o0 = da(acc[e], div6(k0));
+        const double o1 = da(acc[e + 1], div6(k1));
+        const double o2 = da(acc[e + 2], div6(k2));
         // llg_sqt_baseline.c:301-308 / llg_sqt_fusion.c:353-360
         const double nrm = __dsqrt_rn(da(da(dm(o0, o0), dm(o1, o1)), dm(o2, o2)));
         out[e] = dq(dm(a.spin_len, o0), nrm);
@@ -257,40 +277,55 @@ __global__ void __launch_bounds__(NT) llg_step_fused_kernel(LLGArgs a, int tiles
 #pragma unroll
     for (int s = 1; s <= 4; ++s) {
         const int lim = stage_items[s - 1];
+        // phase 1: every owned item's increment k = dt * f(stage input), all
+        // loads from `in` before any store to `out`
+        double kv[NITEM][3];
+#pragma unroll
+        for (int j = 0; j < NITEM; ++j) {
+            const int it = threadIdx.x + j * NT;
+            const int f = it % F;
+            kv[j][0] = kv[j][1] = kv[j][2] = 0.0;
+            if (it >= lim || f >= nf) continue;
+            const int slot = slot_of[j];
+            const V3 d = llg_rhs<J2, H, DAMP>(in, SLOT, 3L * f, FP, slot / FP, slot % FP, a);
+            kv[j][0] = dm(d.x, a.dt);
+            kv[j][1] = dm(d.y, a.dt);
+            kv[j][2] = dm(d.z, a.dt);
+        }
+        // phase 2: stage combination
 #pragma unroll
         for (int j = 0; j < NITEM; ++j) {
             const int it = threadIdx.x + j * NT;
             const int f = it % F;
             if (it >= lim || f >= nf) continue;
             const int slot = slot_of[j];
-            const V3 d = llg_rhs<J2, H, DAMP>(in, SLOT, 3L * f, FP, slot / FP, slot % FP, a);
-            const double k0 = dm(d.x, a.dt), k1 = dm(d.y, a.dt), k2 = dm(d.z, a.dt);
+            const double k0 = kv[j][0], k1 = kv[j][1], k2 = kv[j][2];
             double *o = out + slot * SLOT + 3 * f;
             if (s == 1) {
                 o[0] = da(yb[j][0], half(k0));
                 o[1] = da(yb[j][1], half(k1));
                 o[2] = da(yb[j][2], half(k2));
-                acc[j][0] = da(yb[j][0], dq(k0, 6.0));
-                acc[j][1] = da(yb[j][1], dq(k1, 6.0));
-                acc[j][2] = da(yb[j][2], dq(k2, 6.0));
+                acc[j][0] = da(yb[j][0], div6(k0));
+                acc[j][1] = da(yb[j][1], div6(k1));
+                acc[j][2] = da(yb[j][2], div6(k2));
             } else if (s == 2) {
                 o[0] = da(yb[j][0], half(k0));
                 o[1] = da(yb[j][1], half(k1));
                 o[2] = da(yb[j][2], half(k2));
-                acc[j][0] = da(acc[j][0], dq(k0, 3.0));
-                acc[j][1] = da(acc[j][1], dq(k1, 3.0));
-                acc[j][2] = da(acc[j][2], dq(k2, 3.0));
+                acc[j][0] = da(acc[j][0], div3(k0));
+                acc[j][1] = da(acc[j][1], div3(k1));
+                acc[j][2] = da(acc[j][2], div3(k2));
             } else if (s == 3) {
                 o[0] = da(yb[j][0], k0);
                 o[1] = da(yb[j][1], k1);
                 o[2] = da(yb[j][2], k2);
-                acc[j][0] = da(acc[j][0], dq(k0, 3.0));
-                acc[j][1] = da(acc[j][1], dq(k1, 3.0));
-                acc[j][2] = da(acc[j][2], dq(k2, 3.0));
+                acc[j][0] = da(acc[j][0], div3(k0));
+                acc[j][1] = da(acc[j][1], div3(k1));
+                acc[j][2] = da(acc[j][2], div3(k2));
             } else {
-                const double o0 = da(acc[j][0], dq(k0, 6.0));
-                const double o1 = da(acc[j][1], dq(k1, 6.0));
-                const double o2 = da(acc[j][2], dq(k2, 6.0));
+                const double o0 = da(acc[j][0], div6(k0));
+                const double o1 = da(acc[j][1], div6(k1));
+                const double o2 = da(acc[j][2], div6(k2));
                 const double nrm = __dsqrt_rn(da(da(dm(o0, o0), dm(o1, o1)), dm(o2, o2)));
                 const int gr = R0 + slot / FP - FH, gc = C0 + slot % FP - FH;
                 if (gr < N && gc < N) {
@@ -418,7 +453,21 @@ __global__ void rk_pass_kernel(int pass, long n, double dt, const double *__rest
     }
 }
 
+__global__ void div_check_kernel(const double *__restrict__ x, long n, unsigned long long *bad) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double v = x[i];
+        const bool ok3 = __double_as_longlong(div3(v)) == __double_as_longlong(__ddiv_rn(v, 3.0));
+        const bool ok6 = __double_as_longlong(div6(v)) == __double_as_longlong(__ddiv_rn(v, 6.0));
+        if (!ok3 || !ok6) atomicAdd(bad, 1ull);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_div_check(const double *x, long n, unsigned long long *bad, cudaStream_t st) {
+    div_check_kernel<<<1184, 256, 0, st>>>(x, n, bad);
+    return cudaGetLastError();
+}
 
 LLGArgs make_llg_args(const asd_params &p) {
     LLGArgs a;
@@ -492,3 +541,11 @@ cudaError_t launch_rk_pass(int pass, long n, double dt, const double *spin, doub
 }
 
 }  // namespace asd
+
+extern "C" int asd_check_const_division(const double *x, long n, unsigned long long *bad,
+                                        void *stream) {
+    using namespace asd;
+    if (!x || !bad || n < 0) return fail(ASD_ERR_INVALID, "bad argument");
+    ASD_CUDA_TRY(launch_div_check(x, n, bad, (cudaStream_t)stream));
+    return ASD_OK;
+}

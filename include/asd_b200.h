@@ -145,6 +145,12 @@ int asd_ctx_last_launches(const asd_ctx *ctx);
  * returns ASD_OK or ASD_ERR_TIMEOUT and clears it. */
 int asd_ctx_check_device_status(asd_ctx *ctx);
 
+/* Diagnostic: adds to *bad (device counter) the number of x[i] (device array)
+ * for which the LLG kernels' divisions by the constants 3 and 6 (Markstein's
+ * correction step) differ in any bit from the correctly rounded division.
+ * No counterpart in the reference; tests use it.  Asynchronous on stream. */
+int asd_check_const_division(const double *x, long n, unsigned long long *bad, void *stream);
+
 /* Diagnostic: the bare tensor-core product of the split S(q,t) GEMM,
  * C[i*ldc + j] = sum_k Ah[i][k]Bh[j][k] + Ah[i][k]Bl[j][k] + Al[i][k]Bh[j][k]
  * in FP32, for device operands [rows][Kp] (kind 1: TF32 bit patterns in

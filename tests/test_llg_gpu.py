@@ -84,3 +84,28 @@ def test_long_run_stays_on_sphere():
         ctx.step(200)
         out = ctx.get_spins()
     assert np.allclose(np.linalg.norm(out, axis=-1), 1.0, atol=1e-15)
+
+
+def test_constant_division_is_correctly_rounded():
+    """The stage kernels divide by 3 and 6 with Markstein's correction step;
+    it must equal the correctly rounded division bit for bit over the range
+    the RK4 increments use and well beyond it."""
+    import torch
+
+    g = torch.Generator(device="cuda").manual_seed(5)
+    n = 1 << 24
+    mant = torch.rand(n, dtype=torch.float64, device="cuda", generator=g) + 1.0
+    expo = torch.randint(-300, 300, (n,), device="cuda", generator=g).double()
+    sign = torch.where(torch.rand(n, device="cuda", generator=g) < 0.5, -1.0, 1.0).double()
+    x = (sign * mant * torch.exp2(expo)).contiguous()
+    # plus dense samples around typical increments and exact multiples of 3
+    y = (torch.rand(n, dtype=torch.float64, device="cuda", generator=g) - 0.5) * 0.1
+    z = torch.arange(-(1 << 20), 1 << 20, dtype=torch.float64, device="cuda") * 3.0 * 2.0 ** -30
+    special = torch.tensor([0.0, -0.0, 1.0, -1.0, 3.0, 6.0, 1e-300, -1e-300, 2.0 ** -1000],
+                           dtype=torch.float64, device="cuda")
+    bad = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for arr in (x, y, z, special):
+        asd.check_const_division(arr.data_ptr(), arr.numel(), bad.data_ptr(),
+                                 torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert int(bad.item()) == 0
