@@ -28,8 +28,8 @@ ASD_ERR_TIMEOUT = -4
 ASD_ERR_STATE = -5
 ASD_ERR_UNSUPPORTED = -6
 
-LLG_FUSED_STEP = 0
-LLG_STAGES = 1
+LLG_STAGES = 0
+LLG_FUSED_STEP = 1
 
 SQT_FP64 = 0
 SQT_TF32X3 = 1
@@ -247,7 +247,7 @@ class Context:
         return complex(self._out[0], self._out[1])
 
     def set_llg_kernel(self, kernel) -> None:
-        """"fused" (one launch per step, default) or "stages" (four launches)."""
+        """"stages" (four launches, the default) or "fused" (one launch per step)."""
         k = {"fused": LLG_FUSED_STEP, "stages": LLG_STAGES}.get(kernel, kernel)
         _check(load().asd_ctx_set_llg_kernel(self._h, int(k)))
 

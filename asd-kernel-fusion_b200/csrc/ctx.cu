@@ -82,7 +82,7 @@ struct asd_ctx {
     bool has_state = false, has_origin = false;
     int last_launches = 0;
     int chunk_k = -1;  // < 0: per mode, 512 for TF32x3 and 1024 for BF16x3
-    int llg_kernel = ASD_LLG_FUSED_STEP;
+    int llg_kernel = ASD_LLG_STAGES;
 };
 
 namespace {

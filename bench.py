@@ -318,7 +318,7 @@ def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1) / reps
         llg[kern] = (ms, bps * M * nf / (ms / 1e3) / 1e9, bps)
-    ctx.set_llg_kernel("fused")
+    ctx.set_llg_kernel("stages")
     hbm, bf16, src = measured_peaks()
     sqt_ms, vals = {}, {}
     for mode in ("fp64", "tf32x3", "bf16x3"):

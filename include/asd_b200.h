@@ -121,11 +121,13 @@ int asd_ctx_step_host(asd_ctx *ctx, const double *spin_in, double *spin_out,
                       asd_sqt_mode mode, double sqt_out[2]);
 
 /* How asd_ctx_step runs one RK4 step.  Both give bit-identical spins. */
-#define ASD_LLG_FUSED_STEP 0 /* default: one launch per step, the four stages
+#define ASD_LLG_STAGES 0     /* default: four launches, one fused kernel per RK4
+                                stage, HBM-bound (384 B of DRAM traffic per
+                                site-step; 83% of HBM bandwidth on B200)      */
+#define ASD_LLG_FUSED_STEP 1 /* one launch per step, the four stages
                                 temporally blocked in shared memory (48 B of
-                                DRAM traffic per site-step)                  */
-#define ASD_LLG_STAGES 1     /* four launches, one fused kernel per RK4 stage
-                                (384 B of DRAM traffic per site-step)        */
+                                DRAM traffic per site-step, but FP64- and
+                                latency-bound: slightly slower on B200)       */
 int asd_ctx_set_llg_kernel(asd_ctx *ctx, int kernel);
 
 /* K elements accumulated per TMEM chunk by the split S(q,t) modes (rounded
