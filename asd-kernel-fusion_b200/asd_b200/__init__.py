@@ -44,6 +44,7 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_create", "asd_ctx_destroy", "asd_ctx_set_stream", "asd_ctx_get_params",
     "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
+    "asd_ctx_sqt_grid_async",
     "asd_ctx_step_host", "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
     "asd_ctx_last_launches",
     "asd_ctx_check_device_status",
@@ -116,6 +117,7 @@ def load() -> C.CDLL:
         "asd_ctx_step": ([vp, C.c_int], C.c_int),
         "asd_ctx_sqt": ([vp, C.c_int, dp], C.c_int),
         "asd_ctx_sqt_async": ([vp, C.c_int, vp], C.c_int),
+        "asd_ctx_sqt_grid_async": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_step_host": ([vp, vp, vp, C.c_int, dp], C.c_int),
         "asd_ctx_set_llg_kernel": ([vp, C.c_int], C.c_int),
         "asd_ctx_set_chunk_k": ([vp, C.c_int], C.c_int),
@@ -239,6 +241,21 @@ class Context:
     def sqt_async(self, mode, d_out_ptr: int) -> None:
         mode = MODES[mode] if isinstance(mode, str) else int(mode)
         _check(load().asd_ctx_sqt_async(self._h, mode, C.c_void_p(d_out_ptr)))
+
+    def sqt_grid_async(self, mode, d_out_ptr: int) -> None:
+        mode = MODES[mode] if isinstance(mode, str) else int(mode)
+        _check(load().asd_ctx_sqt_grid_async(self._h, mode, C.c_void_p(d_out_ptr)))
+
+    def sqt_grid(self, mode=SQT_FP64) -> np.ndarray:
+        """S(q,t) on the whole q grid as an N x N complex array [a, b] (q = 2 pi (a, b)/N)."""
+        import torch
+
+        out = torch.zeros(2 * self.N * self.N, dtype=torch.float64, device="cuda")
+        self.sqt_grid_async(mode, out.data_ptr())
+        torch.cuda.synchronize()
+        self.check_device_status()
+        v = out.cpu().numpy()
+        return (v[0::2] + 1j * v[1::2]).reshape(self.N, self.N)
 
     def step_host(self, spin_in_ptr: int, spin_out_ptr: int, mode=SQT_TF32X3) -> complex:
         mode = MODES[mode] if isinstance(mode, str) else int(mode)

@@ -93,6 +93,18 @@ cudaError_t launch_plain_epilogue(const double *C, long i0, long mb, long n, con
                                   const double2 *wphase, double2 *part, int nblocks_x,
                                   int nblocks_y, cudaStream_t st);
 
+// q grid, FP64 path: bins alpha-scaled C band elements minus m_i . z_j by
+// displacement into per-block FP64 histograms gpart[block][N*N].
+cudaError_t launch_bin_band(const double *C, long i0, long mb, long n, int lat_n,
+                            const double *mrow, const double *zcol, double *gpart, int nblocks_x,
+                            int nblocks_y, cudaStream_t st);
+// G[b] = sum over p < nparts of gpart[p][b], fixed order.
+cudaError_t launch_hist_reduce(const double *gpart, int nparts, int nbins, double *G,
+                               cudaStream_t st);
+// out[2*(a*N+b)+{0,1}] = scale * sum_d G[d] e^{-2 pi i (a dr + b dc)/N}; tmp holds N*N double2.
+cudaError_t launch_grid_dft(const double *G, int lat_n, double scale, double2 *tmp, double *out,
+                            cudaStream_t st);
+
 // out[0..1] = (sum of nparts partials) * scale, deterministic order.
 cudaError_t launch_finalize(const double2 *part, int nparts, double scale, double *out,
                             cudaStream_t st);
@@ -113,6 +125,8 @@ struct UmmaSqtArgs {
     int chunk_k = 0;          // K elements per TMEM accumulation chunk (0: all)
     float *dbg_c = nullptr;   // diagnostic: store the accumulator instead
     long dbg_ldc = 0;
+    double *gpart = nullptr;  // q grid: per-CTA FP64 histograms [grid][N*N]
+    int lat_n = 0;            // lattice side (q grid)
 };
 // Returns the number of CTAs launched (partials written) or a negative error.
 int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st);

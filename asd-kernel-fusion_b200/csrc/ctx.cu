@@ -82,6 +82,8 @@ struct asd_ctx {
     bool has_state = false, has_origin = false;
     int last_launches = 0;
     int chunk_k = -1;  // < 0: per mode, 512 for TF32x3 and 1024 for BF16x3
+    double *grid_g = nullptr;     // q grid: N*N displacement bins (FP64)
+    double2 *grid_t = nullptr;    // q grid: DFT intermediate
     int llg_kernel = ASD_LLG_STAGES;
 };
 
@@ -301,6 +303,97 @@ int sqt_async(asd_ctx *c, int mode, double *d_out) {
     return ASD_ERR_INVALID;
 }
 
+constexpr int kGridMaxSites = 4096;
+
+int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
+    if (!c->has_state || !c->has_origin)
+        return fail(ASD_ERR_STATE, "set the spins and the origin before S(q,t)");
+    const int N = c->p.N;
+    const long M = c->M;
+    if (M > kGridMaxSites)
+        return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t) supports N*N <= %d sites (N=%d)",
+                    kGridMaxSites, N);
+    if (mode != ASD_SQT_FP64 && mode != ASD_SQT_TF32X3 && mode != ASD_SQT_BF16X3)
+        return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t): mode %d not supported", mode);
+    if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
+    int rc;
+    if (!c->grid_g) {
+        if ((rc = dalloc(&c->grid_g, (size_t)M * sizeof(double))) != ASD_OK) return rc;
+        if ((rc = dalloc(&c->grid_t, (size_t)M * sizeof(double2))) != ASD_OK) return rc;
+    }
+    ASD_CUDA_TRY(launch_site_mean(c->y, c->M, c->p.nfile, c->uphase, c->mean_t, c->row4, c->row1,
+                                  c->stream));
+    c->last_launches += 1;
+    int nparts = 0;
+    if (mode == ASD_SQT_FP64) {
+        const double alpha = 1.0 / (double)c->p.nfile, beta = 0.0;
+        const long mb = c->band_rows;
+        const int nby = 8;
+        long total = 0;
+        for (long i0 = 0; i0 < M; i0 += mb) total += ((((M - i0 < mb) ? M - i0 : mb) + 127) / 128) * nby;
+        if ((rc = ensure_part(c, (total * M + 1) / 2)) != ASD_OK) return rc;
+        double *gpart = reinterpret_cast<double *>(c->part);
+        long off = 0;
+        for (long i0 = 0; i0 < M; i0 += mb) {
+            const long rows = (M - i0 < mb) ? M - i0 : mb;
+            cublasStatus_t bs =
+                cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)rows, (int)M, c->K, &alpha,
+                            c->y + i0 * c->K, c->K, c->origin, c->K, &beta, c->band, (int)rows);
+            if (bs != CUBLAS_STATUS_SUCCESS) return fail(ASD_ERR_CUDA, "cublasDgemm failed (%d)", (int)bs);
+            const int nbx = (int)((rows + 127) / 128);
+            ASD_CUDA_TRY(launch_bin_band(c->band, i0, rows, M, N, c->mean_t, c->mean_0,
+                                         gpart + off * M, nbx, nby, c->stream));
+            off += (long)nbx * nby;
+            c->last_launches += 1;
+        }
+        nparts = (int)off;
+    } else {
+        const int kind = (mode == ASD_SQT_TF32X3) ? 1 : 2;
+        if (!c->a_hi[kind]) return fail(ASD_ERR_STATE, "split mode %d not enabled at create", kind);
+        if (c->a_version[kind] != c->state_version) {
+            ASD_CUDA_TRY(launch_split(kind, c->y, c->M, c->K, c->Kp[kind], c->a_hi[kind],
+                                      c->a_lo[kind], c->stream));
+            c->a_version[kind] = c->state_version;
+            c->last_launches += 1;
+        }
+        if (c->b_version[kind] != c->origin_version) {
+            ASD_CUDA_TRY(launch_split(kind, c->origin, c->M, c->K, c->Kp[kind], c->b_hi[kind],
+                                      c->b_lo[kind], c->stream));
+            c->b_version[kind] = c->origin_version;
+            c->last_launches += 1;
+        }
+        if ((rc = ensure_part(c, ((long)c->num_sms * M + 1) / 2)) != ASD_OK) return rc;
+        UmmaSqtArgs u{};
+        u.kind = kind;
+        u.M = c->M;
+        u.Kp = c->Kp[kind];
+        u.a_hi = c->a_hi[kind];
+        u.a_lo = c->a_lo[kind];
+        u.b_hi = c->b_hi[kind];
+        u.b_lo = c->b_lo[kind];
+        u.row4 = c->row4;
+        u.row1 = c->row1;
+        u.col4 = c->col4;
+        u.col1 = c->col1;
+        u.alpha = (float)(1.0 / (double)c->p.nfile);
+        u.part = c->part;
+        u.status = c->status;
+        u.num_sms = c->num_sms;
+        u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
+        u.gpart = reinterpret_cast<double *>(c->part);
+        u.lat_n = N;
+        const int grid = launch_umma_sqt(u, c->stream);
+        if (grid < 0) return grid;
+        c->last_launches += 1;
+        nparts = grid;
+    }
+    ASD_CUDA_TRY(launch_hist_reduce(reinterpret_cast<double *>(c->part), nparts, (int)M, c->grid_g,
+                                    c->stream));
+    ASD_CUDA_TRY(launch_grid_dft(c->grid_g, N, 1.0 / (double)M, c->grid_t, d_out, c->stream));
+    c->last_launches += 3;
+    return ASD_OK;
+}
+
 int read_status(asd_ctx *c) {
     unsigned st = 0;
     ASD_CUDA_TRY(cudaMemcpyAsync(&st, c->status, sizeof st, cudaMemcpyDeviceToHost, c->stream));
@@ -317,7 +410,7 @@ void destroy(asd_ctx *c) {
     cudaStreamSynchronize(c->stream);
     void *ptrs[] = {c->y, c->ys_a, c->ys_b, c->acc, c->origin, c->mean_t, c->mean_0, c->uphase,
                     c->wphase, c->row4, c->col4, c->row1, c->col1, c->band, c->part, c->d_out,
-                    c->status};
+                    c->status, c->grid_g, c->grid_t};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (int k = 1; k <= 2; ++k) {
@@ -538,6 +631,13 @@ int asd_ctx_sqt_async(asd_ctx *c, asd_sqt_mode mode, double *d_out) {
     ASD_CUDA_TRY(cudaSetDevice(c->device));
     c->last_launches = 0;
     return sqt_async(c, (int)mode, d_out);
+}
+
+int asd_ctx_sqt_grid_async(asd_ctx *c, asd_sqt_mode mode, double *d_out) {
+    if (!c || !d_out) return fail(ASD_ERR_INVALID, "NULL argument");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    c->last_launches = 0;
+    return sqt_grid_async(c, (int)mode, d_out);
 }
 
 int asd_ctx_sqt(asd_ctx *c, asd_sqt_mode mode, double out[2]) {

@@ -505,13 +505,8 @@ cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const
 
 cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *yout,
                                   cudaStream_t st) {
-    // 2 replicas per CTA, 256 threads (55 KB of shared memory, 4 CTAs per SM);
-    // ASD_LLG_REPLICAS=4 selects 4 replicas and 512 threads.
-    static const int f4 = [] {
-        const char *e = getenv("ASD_LLG_REPLICAS");
-        return (e && atoi(e) == 4) ? 1 : 0;
-    }();
-    return f4 ? launch_fused_t<4, 512>(a, y, yout, st) : launch_fused_t<2, 256>(a, y, yout, st);
+    // 2 replicas per CTA, 256 threads (55 KB of shared memory, 4 CTAs per SM)
+    return launch_fused_t<2, 256>(a, y, yout, st);
 }
 
 cudaError_t launch_aos_to_sitemajor(const double *aos, double *sm, long M, int nfile,

@@ -136,6 +136,83 @@ __global__ void __launch_bounds__(128) plain_epilogue_kernel(
     }
 }
 
+// q grid, FP64 path.  Block (bx, by): rows [i0 + 128 bx, +128) of the band,
+// columns by, by + gridDim.y, ...; each element C_ij - m_i . z_j goes to bin
+// (r_i - r_j, c_i - c_j) mod N of a shared FP64 histogram, which the block
+// then writes to its own slice of gpart.
+__global__ void __launch_bounds__(128) bin_band_kernel(const double *__restrict__ C, long i0,
+                                                       long mb, long n, int N,
+                                                       const double *__restrict__ mrow,
+                                                       const double *__restrict__ zcol,
+                                                       double *__restrict__ gpart) {
+    extern __shared__ double hist[];
+    const int nbins = N * N;
+    for (int b = threadIdx.x; b < nbins; b += 128) hist[b] = 0.0;
+    __syncthreads();
+    const long li = (long)blockIdx.x * 128 + threadIdx.x;
+    if (li < mb) {
+        const long i = i0 + li;
+        const int ri = (int)(i / N), ci = (int)(i % N);
+        const double mx = mrow[i * 3], my = mrow[i * 3 + 1], mz = mrow[i * 3 + 2];
+        for (long j = blockIdx.y; j < n; j += gridDim.y) {
+            const double outer = mx * zcol[j * 3] + my * zcol[j * 3 + 1] + mz * zcol[j * 3 + 2];
+            const double v = C[li + j * mb] - outer;
+            int dr = ri - (int)(j / N), dc = ci - (int)(j % N);
+            dr += (dr < 0) ? N : 0;
+            dc += (dc < 0) ? N : 0;
+            atomicAdd(&hist[dr * N + dc], v);
+        }
+    }
+    __syncthreads();
+    double *g = gpart + ((long)blockIdx.y * gridDim.x + blockIdx.x) * nbins;
+    for (int b = threadIdx.x; b < nbins; b += 128) g[b] = hist[b];
+}
+
+__global__ void hist_reduce_kernel(const double *__restrict__ gpart, int nparts, int nbins,
+                                   double *__restrict__ G) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nbins) return;
+    double s = 0.0;
+    for (int p = 0; p < nparts; ++p) s += gpart[(long)p * nbins + b];
+    G[b] = s;
+}
+
+// Separable 2-D DFT of the displacement histogram: T[dr][b] = sum_dc G[dr][dc]
+// e^{-2 pi i b dc / N}, then S[a][b] = scale * sum_dr T[dr][b] e^{-2 pi i a dr / N}.
+__global__ void grid_dft_rows_kernel(const double *__restrict__ G, int N,
+                                     double2 *__restrict__ T) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * N) return;
+    const int dr = t / N, b = t % N;
+    double re = 0.0, im = 0.0;
+    for (int dc = 0; dc < N; ++dc) {
+        double sn, cs;
+        sincospi(2.0 * (double)((b * dc) % N) / (double)N, &sn, &cs);
+        const double g = G[dr * N + dc];
+        re += g * cs;
+        im -= g * sn;
+    }
+    T[t] = make_double2(re, im);
+}
+
+__global__ void grid_dft_cols_kernel(const double2 *__restrict__ T, int N, double scale,
+                                     double *__restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * N) return;
+    const int a = t / N, b = t % N;
+    double re = 0.0, im = 0.0;
+    for (int dr = 0; dr < N; ++dr) {
+        double sn, cs;
+        sincospi(2.0 * (double)((a * dr) % N) / (double)N, &sn, &cs);
+        const double2 v = T[dr * N + b];
+        // (v.x + i v.y) (cs - i sn)
+        re += v.x * cs + v.y * sn;
+        im += v.y * cs - v.x * sn;
+    }
+    out[2 * t] = re * scale;
+    out[2 * t + 1] = im * scale;
+}
+
 // Single block, fixed summation order: thread t sums t, t+256, ... then a
 // shared-memory tree.
 __global__ void __launch_bounds__(256) finalize_kernel(const double2 *__restrict__ part,
@@ -190,6 +267,29 @@ cudaError_t launch_plain_epilogue(const double *C, long i0, long mb, long n, con
                                   int nblocks_y, cudaStream_t st) {
     dim3 grid((unsigned)nblocks_x, (unsigned)nblocks_y);
     plain_epilogue_kernel<<<grid, 128, 0, st>>>(C, i0, mb, n, mrow, zcol, uphase, wphase, part);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_band(const double *C, long i0, long mb, long n, int lat_n,
+                            const double *mrow, const double *zcol, double *gpart, int nblocks_x,
+                            int nblocks_y, cudaStream_t st) {
+    dim3 grid((unsigned)nblocks_x, (unsigned)nblocks_y);
+    const size_t smem = (size_t)lat_n * lat_n * sizeof(double);
+    bin_band_kernel<<<grid, 128, smem, st>>>(C, i0, mb, n, lat_n, mrow, zcol, gpart);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hist_reduce(const double *gpart, int nparts, int nbins, double *G,
+                               cudaStream_t st) {
+    hist_reduce_kernel<<<(nbins + 255) / 256, 256, 0, st>>>(gpart, nparts, nbins, G);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grid_dft(const double *G, int lat_n, double scale, double2 *tmp, double *out,
+                            cudaStream_t st) {
+    const int n = lat_n * lat_n;
+    grid_dft_rows_kernel<<<(n + 127) / 128, 128, 0, st>>>(G, lat_n, tmp);
+    grid_dft_cols_kernel<<<(n + 127) / 128, 128, 0, st>>>(tmp, lat_n, scale, out);
     return cudaGetLastError();
 }
 

@@ -37,6 +37,7 @@ constexpr int NUM_THREADS = 192;
 constexpr int TMEM_COLS = 512;
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
 constexpr int GROUP_M = 16;
+constexpr int kGridMaxBins = 4096;  // q-grid histogram: N*N FP32 bins in shared memory
 
 // Pipeline geometry.  ROWB = bytes of K per operand row in one pipeline
 // stage (= the swizzle width): 64 -> 4 stages of 48 KB, 128 -> 2 stages of
@@ -67,7 +68,7 @@ struct SmemTail {
 template <int ROWB>
 constexpr int smem_bytes() {
     return 1024 /*alignment slack*/ + Geo<ROWB>::PIPE_BYTES + Geo<ROWB>::TABLE_BYTES +
-           (int)sizeof(SmemTail);
+           (int)((sizeof(SmemTail) + 15) & ~size_t(15));
 }
 
 __device__ __forceinline__ void tile_coords(int tile, int num_m, int num_n, int &mb, int &nb) {
@@ -89,9 +90,15 @@ __device__ __forceinline__ void epilogue_bar() {
     asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
 }
 
-// KIND: 1 = TF32x3, 2 = BF16x3.  STORE: instead of the S(q,t) epilogue,
-// write the raw FP32 accumulator to dbg_c[i * dbg_ldc + j] (diagnostic).
-template <int KIND, bool STORE, int ROWB>
+// KIND: 1 = TF32x3, 2 = BF16x3.  EPI selects the epilogue:
+//   EPI_PHASE  S(q,t) at one q: per-CTA partial sum of u_i w_j (alpha C - m.z)
+//   EPI_STORE  the raw FP32 accumulator to dbg_c[i * dbg_ldc + j] (diagnostic)
+//   EPI_GRID   displacement bins for the whole q grid: every element
+//              alpha C_ij - m_i.z_j goes to bin (r_i - r_j) mod N of a
+//              per-tile FP32 shared histogram, flushed after each tile into
+//              this CTA's FP64 histogram gpart[blockIdx.x][N*N]
+constexpr int EPI_PHASE = 0, EPI_STORE = 1, EPI_GRID = 2;
+template <int KIND, int EPI, int ROWB>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     umma_sqt_kernel(const __grid_constant__ CUtensorMap tm_ah,
                     const __grid_constant__ CUtensorMap tm_al,
@@ -100,14 +107,19 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     int kb_per_chunk, const float4 *__restrict__ row4,
                     const float *__restrict__ row1, const float4 *__restrict__ col4,
                     const float *__restrict__ col1, float alpha, double2 *__restrict__ part,
-                    unsigned *__restrict__ status, float *__restrict__ dbg_c, long dbg_ldc) {
+                    unsigned *__restrict__ status, float *__restrict__ dbg_c, long dbg_ldc,
+                    int lat_n, long n_sites, double *__restrict__ gpart) {
     using G = Geo<ROWB>;
+    constexpr bool STORE = (EPI == EPI_STORE);
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
     float2 *tab_w = reinterpret_cast<float2 *>(smem + G::PIPE_BYTES);           // [2][BN]
     float4 *tab_z = reinterpret_cast<float4 *>(smem + G::PIPE_BYTES + 2 * BN * sizeof(float2));
     SmemTail *tail = reinterpret_cast<SmemTail *>(smem + G::PIPE_BYTES + G::TABLE_BYTES);
+    float *hist = reinterpret_cast<float *>(smem + G::PIPE_BYTES + G::TABLE_BYTES +
+                                            ((sizeof(SmemTail) + 15) & ~size_t(15)));
+    const int nbins = lat_n * lat_n;
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
     const int num_tiles = num_m * num_n;
@@ -270,6 +282,13 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         uint32_t aphase = 0;
         double tot_re = 0.0, tot_im = 0.0;
         int tcount = 0;
+        double *gp = (EPI == EPI_GRID) ? gpart + (long)blockIdx.x * nbins : nullptr;
+        if (EPI == EPI_GRID) {
+            for (int b = etid; b < nbins; b += 128) {
+                hist[b] = 0.f;
+                gp[b] = 0.0;
+            }
+        }
         for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++tcount) {
             int mb, nb;
             tile_coords(tile, num_m, num_n, mb, nb);
@@ -321,6 +340,35 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                             dst[jj] = (first ? 0.f : dst[jj]) + __uint_as_float(v[jj]);
                         continue;
                     }
+                    if (EPI == EPI_GRID) {
+                        if (i >= n_sites) continue;  // padding row
+                        const int r_i = (int)(i / lat_n), c_i = (int)(i - (long)r_i * lat_n);
+                        const long js = j0 + c * 32;
+                        int rj = (int)(js / lat_n), cj = (int)(js - (long)rj * lat_n);
+                        const float4 *zq = z_tab + c * 32;
+#pragma unroll 4
+                        for (int jj = 0; jj < 32; ++jj) {
+                            if (js + jj < n_sites) {
+                                float val = alpha * __uint_as_float(v[jj]);
+                                if (last) {
+                                    const float4 z = zq[jj];
+                                    float o = r4.x * z.x;
+                                    o = fmaf(r4.y, z.y, o);
+                                    o = fmaf(r4.z, z.z, o);
+                                    val -= o;
+                                }
+                                int dr = r_i - rj, dc = c_i - cj;
+                                dr += (dr < 0) ? lat_n : 0;
+                                dc += (dc < 0) ? lat_n : 0;
+                                atomicAdd(&hist[dr * lat_n + dc], val);
+                            }
+                            if (++cj == lat_n) {
+                                cj = 0;
+                                ++rj;
+                            }
+                        }
+                        continue;
+                    }
                     const float4 *wq = reinterpret_cast<const float4 *>(w_tab + c * 32);
                     float are0 = 0.f, aim0 = 0.f, are1 = 0.f, aim1 = 0.f;
 #pragma unroll
@@ -360,6 +408,15 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 }
             }
             if (!ok) break;
+            if (EPI == EPI_GRID) {
+                // tile histogram -> this CTA's FP64 histogram, then clear it
+                epilogue_bar();
+                for (int b = etid; b < nbins; b += 128) {
+                    gp[b] += (double)hist[b];
+                    hist[b] = 0.f;
+                }
+                epilogue_bar();
+            }
             // u_i * s_i with u_i = (r4.w, ui)
             tot_re += (double)r4.w * s_re - (double)ui * s_im;
             tot_im += (double)r4.w * s_im + (double)ui * s_re;
@@ -378,7 +435,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     ptx::tc_fence_before();
     __syncthreads();
     ptx::tc_fence_after();
-    if (threadIdx.x == 0 && !STORE) {
+    if (threadIdx.x == 0 && EPI == EPI_PHASE) {
         const double re = (tail->red[0][0] + tail->red[0][1]) + (tail->red[0][2] + tail->red[0][3]);
         const double im = (tail->red[1][0] + tail->red[1][1]) + (tail->red[1][2] + tail->red[1][3]);
         part[blockIdx.x] = make_double2(re, im);
@@ -464,23 +521,32 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
         if (r == cudaSuccess)
             kern<<<grid, NUM_THREADS, smem, st>>>(tah, tal, tbh, tbl, num_m, num_n, num_kb, kpc,
                                                   a.row4, a.row1, a.col4, a.col1, a.alpha, a.part,
-                                                  a.status, a.dbg_c, a.dbg_ldc);
+                                                  a.status, a.dbg_c, a.dbg_ldc, a.lat_n, a.M,
+                                                  a.gpart);
         return r;
     };
-    const bool dbg = a.dbg_c != nullptr;
+    const int epi = a.dbg_c ? EPI_STORE : (a.gpart ? EPI_GRID : EPI_PHASE);
+    if (epi == EPI_GRID && (a.lat_n < 1 || (long)a.lat_n * a.lat_n != a.M ||
+                            a.lat_n * a.lat_n > kGridMaxBins))
+        return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t) supports N*N <= %d sites", kGridMaxBins);
+    const int hist_bytes = (epi == EPI_GRID) ? 4 * a.lat_n * a.lat_n + 16 : 0;
+#define ASD_UMMA_GO(K, E, R) go(umma_sqt_kernel<K, E, R>, smem_bytes<R>() + hist_bytes)
     if (rowb == 64) {
-        constexpr int S = smem_bytes<64>();
         if (a.kind == 2)
-            e = dbg ? go(umma_sqt_kernel<2, true, 64>, S) : go(umma_sqt_kernel<2, false, 64>, S);
+            e = epi == EPI_STORE ? ASD_UMMA_GO(2, EPI_STORE, 64)
+              : epi == EPI_GRID  ? ASD_UMMA_GO(2, EPI_GRID, 64) : ASD_UMMA_GO(2, EPI_PHASE, 64);
         else
-            e = dbg ? go(umma_sqt_kernel<1, true, 64>, S) : go(umma_sqt_kernel<1, false, 64>, S);
+            e = epi == EPI_STORE ? ASD_UMMA_GO(1, EPI_STORE, 64)
+              : epi == EPI_GRID  ? ASD_UMMA_GO(1, EPI_GRID, 64) : ASD_UMMA_GO(1, EPI_PHASE, 64);
     } else {
-        constexpr int S = smem_bytes<128>();
         if (a.kind == 2)
-            e = dbg ? go(umma_sqt_kernel<2, true, 128>, S) : go(umma_sqt_kernel<2, false, 128>, S);
+            e = epi == EPI_STORE ? ASD_UMMA_GO(2, EPI_STORE, 128)
+              : epi == EPI_GRID  ? ASD_UMMA_GO(2, EPI_GRID, 128) : ASD_UMMA_GO(2, EPI_PHASE, 128);
         else
-            e = dbg ? go(umma_sqt_kernel<1, true, 128>, S) : go(umma_sqt_kernel<1, false, 128>, S);
+            e = epi == EPI_STORE ? ASD_UMMA_GO(1, EPI_STORE, 128)
+              : epi == EPI_GRID  ? ASD_UMMA_GO(1, EPI_GRID, 128) : ASD_UMMA_GO(1, EPI_PHASE, 128);
     }
+#undef ASD_UMMA_GO
     if (e != cudaSuccess) return cuda_fail(e, "umma_sqt setup");
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "umma_sqt launch");

@@ -114,6 +114,17 @@ int asd_ctx_sqt(asd_ctx *ctx, asd_sqt_mode mode, double out[2]);
 /* Asynchronous form: writes out[0..1] (a device pointer) on the stream. */
 int asd_ctx_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
 
+/* S(q,t) for every q = 2*pi*(a, b)/N of the N x N grid, into d_out[2*(a*N+b)]
+ * (real) and d_out[2*(a*N+b)+1] (imaginary), a device buffer of 2*N*N
+ * doubles; asynchronous.  The same correlation GEMM, with an epilogue that
+ * bins every connected C_ij by the displacement r_i - r_j (mod N), followed by
+ * a 2-D DFT of the N*N bins; d_out[2*(vx*N+vy)] equals asd_ctx_sqt's value.
+ * Modes ASD_SQT_FP64, ASD_SQT_TF32X3 and ASD_SQT_BF16X3; lattices with
+ * N*N <= 4096 (the bins live in shared memory).  The split modes sum in FP32
+ * shared-memory atomics, so their last bits vary from run to run.
+ * No counterpart in the reference (its programs evaluate one q). */
+int asd_ctx_sqt_grid_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
+
 /* One full step through host buffers, the reference's own contract: spins
  * (AoS) come from host memory, one RK4 step runs, the new spins go back to
  * spin_out and S(q,t) into sqt_out.  spin_in may equal spin_out. */
