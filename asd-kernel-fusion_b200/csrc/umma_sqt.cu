@@ -60,6 +60,7 @@ struct SmemTail {
     uint64_t tfull[2];
     uint64_t tempty[2];
     uint64_t drain;
+    uint64_t ebar;  // epilogue warps' barrier
     uint32_t tmem_base;
     int abort_flag;
     double red[2][4];
@@ -86,8 +87,16 @@ __device__ __forceinline__ void raise_abort(SmemTail *t, unsigned *status) {
     if (status) atomicOr(status, (unsigned)kStatusTimeout);
 }
 
-__device__ __forceinline__ void epilogue_bar() {
-    asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
+// Barrier among the four epilogue warps on an mbarrier (count 4, one arrival
+// per warp), so that the wait is bounded like every other wait here: a warp
+// that gives up, or sees the abort flag, leaves instead of hanging.
+__device__ __forceinline__ bool epilogue_sync(uint64_t *bar, uint32_t &phase,
+                                              volatile int *abort) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) ptx::mbar_arrive(bar);
+    const bool ok = ptx::mbar_wait_bounded(bar, phase, abort, WAIT_LIMIT);
+    phase ^= 1u;
+    return ok;
 }
 
 // KIND: 1 = TF32x3, 2 = BF16x3.  EPI selects the epilogue:
@@ -134,6 +143,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             ptx::mbar_init(&tail->tempty[b], 4);
         }
         ptx::mbar_init(&tail->drain, 1);
+        ptx::mbar_init(&tail->ebar, 4);
         tail->abort_flag = 0;
         ptx::fence_mbar_init();
     }
@@ -282,6 +292,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         uint32_t aphase = 0;
         double tot_re = 0.0, tot_im = 0.0;
         int tcount = 0;
+        uint32_t ephase = 0;
         double *gp = (EPI == EPI_GRID) ? gpart + (long)blockIdx.x * nbins : nullptr;
         if (EPI == EPI_GRID) {
             for (int b = etid; b < nbins; b += 128) {
@@ -308,7 +319,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     w_tab[jl] = make_float2(cz.w, __ldg(&col1[j0 + jl]));
                     z_tab[jl] = make_float4(cz.x, cz.y, cz.z, 0.f);
                 }
-                epilogue_bar();
+                if (!epilogue_sync(&tail->ebar, ephase, abort_flag)) {
+                    raise_abort(tail, status);
+                    break;
+                }
             }
             const float4 r4 = STORE ? make_float4(0.f, 0.f, 0.f, 0.f) : row4[i];
             const float ui = STORE ? 0.f : row1[i];
@@ -410,12 +424,18 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             if (!ok) break;
             if (EPI == EPI_GRID) {
                 // tile histogram -> this CTA's FP64 histogram, then clear it
-                epilogue_bar();
+                if (!epilogue_sync(&tail->ebar, ephase, abort_flag)) {
+                    raise_abort(tail, status);
+                    break;
+                }
                 for (int b = etid; b < nbins; b += 128) {
                     gp[b] += (double)hist[b];
                     hist[b] = 0.f;
                 }
-                epilogue_bar();
+                if (!epilogue_sync(&tail->ebar, ephase, abort_flag)) {
+                    raise_abort(tail, status);
+                    break;
+                }
             }
             // u_i * s_i with u_i = (r4.w, ui)
             tot_re += (double)r4.w * s_re - (double)ui * s_im;
