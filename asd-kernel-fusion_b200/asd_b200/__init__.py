@@ -44,11 +44,12 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_create", "asd_ctx_destroy", "asd_ctx_set_stream", "asd_ctx_get_params",
     "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
-    "asd_ctx_sqt_grid_async",
+    "asd_ctx_sqt_grid_async", "asd_ctx_sqt_grid",
     "asd_ctx_step_host", "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
     "asd_ctx_last_launches",
     "asd_ctx_check_device_status",
-    "asd_check_const_division", "asd_umma_gemm_f32", "asd_sqt_split_noalloc", "asd_set_params", "euler", "runge_kutta",
+    "asd_check_const_division", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
+    "asd_spins_save", "asd_spins_load", "asd_set_params", "euler", "runge_kutta",
     "fused_dgemm",
 )
 
@@ -118,6 +119,7 @@ def load() -> C.CDLL:
         "asd_ctx_sqt": ([vp, C.c_int, dp], C.c_int),
         "asd_ctx_sqt_async": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_sqt_grid_async": ([vp, C.c_int, vp], C.c_int),
+        "asd_ctx_sqt_grid": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_step_host": ([vp, vp, vp, C.c_int, dp], C.c_int),
         "asd_ctx_set_llg_kernel": ([vp, C.c_int], C.c_int),
         "asd_ctx_set_chunk_k": ([vp, C.c_int], C.c_int),
@@ -129,6 +131,9 @@ def load() -> C.CDLL:
                               C.c_int),
         "asd_sqt_split_noalloc": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp,
                                    C.c_double, C.c_double, C.c_int, vp, vp], C.c_int),
+        "asd_spins_save": ([C.c_char_p, C.c_int, C.c_int, C.c_long, C.c_double, vp], C.c_int),
+        "asd_spins_load": ([C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                            C.POINTER(C.c_long), C.POINTER(C.c_double), vp, C.c_size_t], C.c_int),
         "asd_set_params": ([C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
         "euler": ([vp, vp], None),
         "runge_kutta": ([vp] * 6, None),
@@ -248,13 +253,9 @@ class Context:
 
     def sqt_grid(self, mode=SQT_FP64) -> np.ndarray:
         """S(q,t) on the whole q grid as an N x N complex array [a, b] (q = 2 pi (a, b)/N)."""
-        import torch
-
-        out = torch.zeros(2 * self.N * self.N, dtype=torch.float64, device="cuda")
-        self.sqt_grid_async(mode, out.data_ptr())
-        torch.cuda.synchronize()
-        self.check_device_status()
-        v = out.cpu().numpy()
+        mode = MODES[mode] if isinstance(mode, str) else int(mode)
+        v = np.empty(2 * self.N * self.N, dtype=np.float64)
+        _check(load().asd_ctx_sqt_grid(self._h, mode, _ptr(v)))
         return (v[0::2] + 1j * v[1::2]).reshape(self.N, self.N)
 
     def step_host(self, spin_in_ptr: int, spin_out_ptr: int, mode=SQT_TF32X3) -> complex:
@@ -335,3 +336,24 @@ def check_const_division(x_ptr: int, n: int, bad_ptr: int, stream: int = 0) -> N
     """asd_check_const_division on device pointers (diagnostic)."""
     _check(load().asd_check_const_division(C.c_void_p(x_ptr), int(n), C.c_void_p(bad_ptr),
                                            C.c_void_p(stream)))
+
+
+def save_spins(path, spins: np.ndarray, step: int = 0, spin_len: float = 1.0) -> None:
+    """asd_spins_save: spins [nfile][N*N][3] float64 to a checkpoint file."""
+    s = np.ascontiguousarray(spins, dtype=np.float64)
+    nfile, M, _ = s.shape
+    N = int(round(M ** 0.5))
+    _check(load().asd_spins_save(str(path).encode(), N, nfile, int(step), float(spin_len),
+                                 _ptr(s)))
+
+
+def load_spins(path):
+    """asd_spins_load: returns (spins [nfile][N*N][3], step, spin_len)."""
+    N, nf, st, sl = C.c_int(), C.c_int(), C.c_long(), C.c_double()
+    lib = load()
+    _check(lib.asd_spins_load(str(path).encode(), C.byref(N), C.byref(nf), C.byref(st),
+                              C.byref(sl), None, 0))
+    out = np.empty((nf.value, N.value * N.value, 3), dtype=np.float64)
+    _check(lib.asd_spins_load(str(path).encode(), C.byref(N), C.byref(nf), C.byref(st),
+                              C.byref(sl), C.c_void_p(_ptr(out)), out.size))
+    return out, st.value, sl.value

@@ -84,6 +84,7 @@ struct asd_ctx {
     int chunk_k = -1;  // < 0: per mode, 512 for TF32x3 and 1024 for BF16x3
     double *grid_g = nullptr;     // q grid: N*N displacement bins (FP64)
     double2 *grid_t = nullptr;    // q grid: DFT intermediate
+    double *grid_out = nullptr;   // q grid: device result for the host-buffer form
     int llg_kernel = ASD_LLG_STAGES;
 };
 
@@ -410,7 +411,7 @@ void destroy(asd_ctx *c) {
     cudaStreamSynchronize(c->stream);
     void *ptrs[] = {c->y, c->ys_a, c->ys_b, c->acc, c->origin, c->mean_t, c->mean_0, c->uphase,
                     c->wphase, c->row4, c->col4, c->row1, c->col1, c->band, c->part, c->d_out,
-                    c->status, c->grid_g, c->grid_t};
+                    c->status, c->grid_g, c->grid_t, c->grid_out};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (int k = 1; k <= 2; ++k) {
@@ -638,6 +639,18 @@ int asd_ctx_sqt_grid_async(asd_ctx *c, asd_sqt_mode mode, double *d_out) {
     ASD_CUDA_TRY(cudaSetDevice(c->device));
     c->last_launches = 0;
     return sqt_grid_async(c, (int)mode, d_out);
+}
+
+int asd_ctx_sqt_grid(asd_ctx *c, asd_sqt_mode mode, double *out) {
+    if (!c || !out) return fail(ASD_ERR_INVALID, "NULL argument");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    c->last_launches = 0;
+    const size_t bytes = (size_t)c->M * 2 * sizeof(double);
+    int rc;
+    if (!c->grid_out && (rc = dalloc(&c->grid_out, bytes)) != ASD_OK) return rc;
+    if ((rc = sqt_grid_async(c, (int)mode, c->grid_out)) != ASD_OK) return rc;
+    ASD_CUDA_TRY(cudaMemcpyAsync(out, c->grid_out, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return read_status(c);  // synchronises
 }
 
 int asd_ctx_sqt(asd_ctx *c, asd_sqt_mode mode, double out[2]) {

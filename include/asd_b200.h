@@ -124,6 +124,8 @@ int asd_ctx_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
  * shared-memory atomics, so their last bits vary from run to run.
  * No counterpart in the reference (its programs evaluate one q). */
 int asd_ctx_sqt_grid_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
+/* Same into host memory (2*N*N doubles); synchronous. */
+int asd_ctx_sqt_grid(asd_ctx *ctx, asd_sqt_mode mode, double *out);
 
 /* One full step through host buffers, the reference's own contract: spins
  * (AoS) come from host memory, one RK4 step runs, the new spins go back to
@@ -207,6 +209,19 @@ int asd_sqt_split_noalloc(int kind, long rows, int Kp, const void *a_hi, const v
                           const void *b_hi, const void *b_lo, const void *row4, const float *row1,
                           const void *col4, const float *col1, double alpha, double scale,
                           int chunk_k, double *d_out, void *stream);
+
+/* --------------------------------------------------------- spin-state I/O */
+/* The reference keeps spins only in memory; these define a file format for
+ * checkpoints: a 64-byte header (magic "ASDSPIN1", int32 N, int32 nfile,
+ * int64 step, double spin_len, 32 reserved bytes) followed by the spins in
+ * the reference's AoS layout, little-endian doubles.  Host only; no GPU. */
+int asd_spins_save(const char *path, int N, int nfile, long step, double spin_len,
+                   const double *spin_aos);
+/* Reads the header into N, nfile (and step, spin_len when not NULL); with
+ * spin_aos == NULL only the header is read (size query), else the spins are
+ * read into spin_aos, which must hold `capacity` >= nfile*N*N*3 doubles. */
+int asd_spins_load(const char *path, int *N, int *nfile, long *step, double *spin_len,
+                   double *spin_aos, size_t capacity);
 
 /* ------------------------------------------------------- drop-in symbols */
 /* The reference reads N, Nfile, J1, dt, nn and num_neighbor from globals its
