@@ -42,6 +42,7 @@ MODES = {v: k for k, v in MODE_NAMES.items()}
 EXPORTED_SYMBOLS = (
     "asd_version", "asd_last_error", "asd_params_default", "asd_set_device",
     "asd_ctx_create", "asd_ctx_destroy", "asd_ctx_set_stream", "asd_ctx_get_params",
+    "asd_ctx_set_params", "asd_ctx_loss_grad",
     "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
     "asd_ctx_sqt_grid_async", "asd_ctx_sqt_grid",
@@ -111,6 +112,8 @@ def load() -> C.CDLL:
         "asd_ctx_destroy": ([vp], C.c_int),
         "asd_ctx_set_stream": ([vp, vp], C.c_int),
         "asd_ctx_get_params": ([vp, P], C.c_int),
+        "asd_ctx_set_params": ([vp, P], C.c_int),
+        "asd_ctx_loss_grad": ([vp, C.c_int, C.c_int, C.c_int, vp, dp, vp, vp], C.c_int),
         "asd_ctx_set_spins": ([vp, vp, C.c_int], C.c_int),
         "asd_ctx_set_spins_device": ([vp, vp, C.c_int], C.c_int),
         "asd_ctx_get_spins": ([vp, vp], C.c_int),
@@ -216,6 +219,30 @@ class Context:
     @property
     def handle(self) -> C.c_void_p:
         return self._h
+
+    def set_params(self, params: Params) -> None:
+        _check(load().asd_ctx_set_params(self._h, C.byref(params)))
+        self.params = params
+
+    def loss_grad(self, nsteps: int, stride: int, checkpoint: int = 50, target=None):
+        """asd_ctx_loss_grad: returns (loss, grad[6] = dL/d(J1, J2, alpha, hx, hy, hz),
+        S(q,t_e) for e = 1..nsteps // stride as a complex array)."""
+        E = nsteps // stride
+        sq = np.zeros(2 * E)
+        grad = np.zeros(6)
+        loss = C.c_double(0.0)
+        tgt = None
+        if target is not None:
+            t = np.asarray(target)
+            tgt = np.ascontiguousarray(np.stack([t.real, t.imag], axis=-1).reshape(-1)
+                                       if np.iscomplexobj(t) else t, dtype=np.float64)
+            if tgt.size != 2 * E:
+                raise ValueError(f"target has {tgt.size} values, expected {2 * E}")
+        _check(load().asd_ctx_loss_grad(self._h, int(nsteps), int(stride), int(checkpoint),
+                                        None if tgt is None else C.c_void_p(_ptr(tgt)),
+                                        C.byref(loss), C.c_void_p(_ptr(grad)),
+                                        C.c_void_p(_ptr(sq))))
+        return loss.value, grad, sq[0::2] + 1j * sq[1::2]
 
     def set_stream(self, stream_ptr: int) -> None:
         _check(load().asd_ctx_set_stream(self._h, C.c_void_p(stream_ptr)))

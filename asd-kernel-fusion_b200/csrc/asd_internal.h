@@ -109,6 +109,27 @@ cudaError_t launch_grid_dft(const double *G, int lat_n, double scale, double2 *t
 cudaError_t launch_finalize(const double2 *part, int nparts, double scale, double *out,
                             cudaStream_t st);
 
+// ------------------------------------------------ adjoint (adjoint.cu)
+int adjoint_blocks(const LLGArgs &a);
+cudaError_t launch_vjp_p(const LLGArgs &a, const double *S, const double *mu, double *P,
+                         double *loc, double *bacc, cudaStream_t st);
+cudaError_t launch_vjp_gather(const LLGArgs &a, const double *P, const double *loc,
+                              const double *lam_v, const double *lam_y_in, double *lam_y_out,
+                              double *mu_out, double cv, double cs, int has_next,
+                              cudaStream_t st);
+cudaError_t launch_adj_renorm(const LLGArgs &a, const double *s4, const double *acc,
+                              const double *lam, double *lam_v, double *mu, cudaStream_t st);
+int fsum_chunks(long M);
+cudaError_t launch_fsum(const double *A, long M, int K, const double2 *ph, double2 *Fpart,
+                        cudaStream_t st);
+cudaError_t launch_gz(const double2 *Fpart, long M, int K, int nfile, double2 *G, double2 *Z,
+                      cudaStream_t st);
+cudaError_t launch_sqt_value(const double2 *Fpart, long M, int K, int nfile, const double2 *G,
+                             const double2 *Z, double2 *out, cudaStream_t st);
+cudaError_t launch_loss_grad(double *lam, long M, int K, const double2 *u, const double2 *G,
+                             const double2 *Z, double cre, double cim, cudaStream_t st);
+cudaError_t launch_param_reduce(const double *bacc, int nblocks, double *grad, cudaStream_t st);
+
 // ------------------------------------------------ tcgen05 split GEMM S(q,t)
 struct UmmaSqtArgs {
     int kind;             // 1 = TF32x3, 2 = BF16x3

@@ -85,6 +85,9 @@ struct asd_ctx {
     double *grid_g = nullptr;     // q grid: N*N displacement bins (FP64)
     double2 *grid_t = nullptr;    // q grid: DFT intermediate
     double *grid_out = nullptr;   // q grid: device result for the host-buffer form
+    // adjoint work space (allocated on the first asd_ctx_loss_grad)
+    std::vector<double *> adj_bufs;
+    long adj_states = 0;
     int llg_kernel = ASD_LLG_STAGES;
 };
 
@@ -304,6 +307,140 @@ int sqt_async(asd_ctx *c, int mode, double *d_out) {
     return ASD_ERR_INVALID;
 }
 
+// One RK4 step y_in -> y_out on caller-chosen buffers (the four stage kernels;
+// s2, s3, s4 and acc receive the stage states and the running combination).
+int step_into(asd_ctx *c, const double *y_in, double *s2, double *s3, double *s4, double *acc,
+              double *y_out) {
+    ASD_CUDA_TRY(launch_llg_stage(1, c->a, y_in, y_in, acc, s2, c->stream));
+    ASD_CUDA_TRY(launch_llg_stage(2, c->a, y_in, s2, acc, s3, c->stream));
+    ASD_CUDA_TRY(launch_llg_stage(3, c->a, y_in, s3, acc, s4, c->stream));
+    if (y_out) ASD_CUDA_TRY(launch_llg_stage(4, c->a, nullptr, s4, acc, y_out, c->stream));
+    return ASD_OK;
+}
+
+int loss_grad(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target, double *loss,
+              double *grad, double *sqt_out) {
+    if (!c->has_origin) return fail(ASD_ERR_STATE, "set the origin (t = 0 spins) first");
+    if (nsteps < 1 || stride < 1 || stride > nsteps || ckpt < 1)
+        return fail(ASD_ERR_INVALID, "nsteps=%d stride=%d checkpoint=%d", nsteps, stride, ckpt);
+    const long M = c->M;
+    const int K = c->K, E = nsteps / stride;
+    const size_t sb = (size_t)M * K * sizeof(double);
+    const int nck = (nsteps + ckpt - 1) / ckpt;  // checkpoints at 0, ckpt, 2 ckpt, ...
+    const long need = 10 + nck + (ckpt + 1);
+    int rc;
+    if (c->adj_states < need) {
+        for (double *q : c->adj_bufs)
+            if (q) cudaFree(q);
+        c->adj_bufs.assign(need + 2, nullptr);
+        c->adj_states = 0;
+        for (long i = 0; i < need; ++i)
+            if ((rc = dalloc(&c->adj_bufs[i], sb)) != ASD_OK) return rc;
+        const int nb = adjoint_blocks(c->a);
+        const size_t small = (size_t)nb * 6 * sizeof(double) +
+                             ((size_t)fsum_chunks(M) * K + 2 * K + 8 + 2) * sizeof(double2);
+        if ((rc = dalloc(&c->adj_bufs[need], small)) != ASD_OK) return rc;
+        if ((rc = dalloc(&c->adj_bufs[need + 1], (size_t)(E + 8) * sizeof(double2))) != ASD_OK)
+            return rc;
+        c->adj_states = need;
+    } else {
+        // the S(q,t) buffer depends on E
+        if (c->adj_bufs[c->adj_states + 1]) cudaFree(c->adj_bufs[c->adj_states + 1]);
+        c->adj_bufs[c->adj_states + 1] = nullptr;
+        if ((rc = dalloc(&c->adj_bufs[c->adj_states + 1], (size_t)(E + 8) * sizeof(double2))) !=
+            ASD_OK)
+            return rc;
+    }
+    double **B = c->adj_bufs.data();
+    double *s2 = B[0], *s3 = B[1], *s4 = B[2], *acc = B[3], *lam = B[4], *lam_v = B[5],
+           *lam_y = B[6], *mu = B[7], *P = B[8], *loc = B[9];
+    double **ck = B + 10;               // nck checkpoints
+    double **seg = B + 10 + nck;        // ckpt + 1 recomputed states
+    const int nb = adjoint_blocks(c->a);
+    double *bacc = B[c->adj_states];
+    double2 *Fpart = reinterpret_cast<double2 *>(bacc + (size_t)nb * 6);
+    double2 *G = Fpart + (size_t)fsum_chunks(M) * K;
+    double2 *Z = G + K;
+    double *dgrad = reinterpret_cast<double *>(Z + 4);
+    double2 *Sv = reinterpret_cast<double2 *>(B[c->adj_states + 1]);
+    cudaStream_t st = c->stream;
+    c->last_launches = 0;
+
+    // G_k and Z_c of the origin
+    ASD_CUDA_TRY(launch_fsum(c->origin, M, K, c->wphase, Fpart, st));
+    ASD_CUDA_TRY(launch_gz(Fpart, M, K, c->p.nfile, G, Z, st));
+    // forward: checkpoints and S(q,t) at every stride-th step
+    ASD_CUDA_TRY(cudaMemcpyAsync(ck[0], c->origin, sb, cudaMemcpyDeviceToDevice, st));
+    double *cur = seg[0], *nxt = seg[1];
+    ASD_CUDA_TRY(cudaMemcpyAsync(cur, c->origin, sb, cudaMemcpyDeviceToDevice, st));
+    for (int n = 1; n <= nsteps; ++n) {
+        if ((rc = step_into(c, cur, s2, s3, s4, acc, nxt)) != ASD_OK) return rc;
+        double *t = cur;
+        cur = nxt;
+        nxt = t;
+        if (n % ckpt == 0 && n / ckpt < nck)
+            ASD_CUDA_TRY(cudaMemcpyAsync(ck[n / ckpt], cur, sb, cudaMemcpyDeviceToDevice, st));
+        if (n % stride == 0 && n / stride <= E) {
+            ASD_CUDA_TRY(launch_fsum(cur, M, K, c->uphase, Fpart, st));
+            ASD_CUDA_TRY(launch_sqt_value(Fpart, M, K, c->p.nfile, G, Z, Sv + (n / stride - 1), st));
+        }
+    }
+    std::vector<double2> S((size_t)E);
+    ASD_CUDA_TRY(cudaMemcpyAsync(S.data(), Sv, (size_t)E * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    ASD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (sqt_out)
+        for (int e = 0; e < E; ++e) sqt_out[2 * e] = S[e].x, sqt_out[2 * e + 1] = S[e].y;
+    double L = 0.0;
+    std::vector<double2> coef((size_t)E, make_double2(0.0, 0.0));
+    if (target) {
+        const double scale = 2.0 / ((double)E * (double)M * c->p.nfile);
+        for (int e = 0; e < E; ++e) {
+            const double dr = S[e].x - target[2 * e], di = S[e].y - target[2 * e + 1];
+            L += dr * dr + di * di;
+            coef[e] = make_double2(scale * dr, -scale * di);  // 2 conj(S - T) / (E M nfile)
+        }
+        L /= E;
+    }
+    if (loss) *loss = L;
+    if (!grad) return ASD_OK;
+    for (int q = 0; q < 6; ++q) grad[q] = 0.0;
+    if (!target) return ASD_OK;
+
+    // backward through the segments, last first
+    ASD_CUDA_TRY(cudaMemsetAsync(lam, 0, sb, st));
+    ASD_CUDA_TRY(cudaMemsetAsync(bacc, 0, (size_t)nb * 6 * sizeof(double), st));
+    for (int cidx = nck - 1; cidx >= 0; --cidx) {
+        const int base = cidx * ckpt;
+        const int len = (nsteps - base < ckpt) ? nsteps - base : ckpt;
+        ASD_CUDA_TRY(cudaMemcpyAsync(seg[0], ck[cidx], sb, cudaMemcpyDeviceToDevice, st));
+        for (int j = 1; j <= len; ++j)
+            if ((rc = step_into(c, seg[j - 1], s2, s3, s4, acc, seg[j])) != ASD_OK) return rc;
+        for (int n = base + len; n > base; --n) {
+            const int j = n - base;
+            if (n % stride == 0 && n / stride <= E) {
+                const double2 cf = coef[n / stride - 1];
+                ASD_CUDA_TRY(launch_loss_grad(lam, M, K, c->uphase, G, Z, cf.x, cf.y, st));
+            }
+            // y_{n-1} = seg[j-1]: recompute the stage states, then the adjoint
+            if ((rc = step_into(c, seg[j - 1], s2, s3, s4, acc, nullptr)) != ASD_OK) return rc;
+            const LLGArgs &a = c->a;
+            ASD_CUDA_TRY(launch_adj_renorm(a, s4, acc, lam, lam_v, mu, st));
+            ASD_CUDA_TRY(launch_vjp_p(a, s4, mu, P, loc, bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, P, loc, lam_v, lam_v, lam_y, mu, 1.0 / 3.0, 1.0, 1, st));
+            ASD_CUDA_TRY(launch_vjp_p(a, s3, mu, P, loc, bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, P, loc, lam_v, lam_y, lam_y, mu, 1.0 / 3.0, 0.5, 1, st));
+            ASD_CUDA_TRY(launch_vjp_p(a, s2, mu, P, loc, bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, P, loc, lam_v, lam_y, lam_y, mu, 1.0 / 6.0, 0.5, 1, st));
+            ASD_CUDA_TRY(launch_vjp_p(a, seg[j - 1], mu, P, loc, bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, P, loc, lam_v, lam_y, lam, mu, 0.0, 0.0, 0, st));
+        }
+    }
+    ASD_CUDA_TRY(launch_param_reduce(bacc, nb, dgrad, st));
+    ASD_CUDA_TRY(cudaMemcpyAsync(grad, dgrad, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ASD_CUDA_TRY(cudaStreamSynchronize(st));
+    return ASD_OK;
+}
+
 constexpr int kGridMaxSites = 4096;
 
 int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
@@ -419,6 +556,8 @@ void destroy(asd_ctx *c) {
         for (void *q : ops)
             if (q) cudaFree(q);
     }
+    for (double *q : c->adj_bufs)
+        if (q) cudaFree(q);
     if (c->h_out) cudaFreeHost(c->h_out);
     if (c->blas) cublasDestroy(c->blas);
     delete c;
@@ -639,6 +778,38 @@ int asd_ctx_sqt_grid_async(asd_ctx *c, asd_sqt_mode mode, double *d_out) {
     ASD_CUDA_TRY(cudaSetDevice(c->device));
     c->last_launches = 0;
     return sqt_grid_async(c, (int)mode, d_out);
+}
+
+int asd_ctx_loss_grad(asd_ctx *c, int nsteps, int stride, int checkpoint, const double *target,
+                      double *loss, double *grad, double *sqt_out) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    return loss_grad(c, nsteps, stride, checkpoint, target, loss, grad, sqt_out);
+}
+
+int asd_ctx_set_params(asd_ctx *c, const asd_params *p) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    int rc = check_params(p);
+    if (rc != ASD_OK) return rc;
+    if (p->N != c->p.N || p->nfile != c->p.nfile)
+        return fail(ASD_ERR_INVALID, "N and nfile are fixed at create");
+    const bool q_changed = (p->vx != c->p.vx || p->vy != c->p.vy);
+    c->p = *p;
+    c->a = make_llg_args(*p);
+    if (q_changed) {
+        const double qx = 2.0 * M_PI * p->vx / (double)p->N, qy = 2.0 * M_PI * p->vy / (double)p->N;
+        std::vector<double2> u((size_t)c->M), w((size_t)c->M);
+        for (long i = 0; i < c->M; ++i) {
+            const double th = qx * (double)(i / p->N) + qy * (double)(i % p->N);
+            u[i] = make_double2(std::cos(th), -std::sin(th));
+            w[i] = make_double2(std::cos(th), std::sin(th));
+        }
+        ASD_CUDA_TRY(cudaSetDevice(c->device));
+        ASD_CUDA_TRY(cudaMemcpy(c->uphase, u.data(), (size_t)c->M * sizeof(double2), cudaMemcpyHostToDevice));
+        ASD_CUDA_TRY(cudaMemcpy(c->wphase, w.data(), (size_t)c->M * sizeof(double2), cudaMemcpyHostToDevice));
+        if (c->has_origin) return refresh_origin(c);
+    }
+    return ASD_OK;
 }
 
 int asd_ctx_sqt_grid(asd_ctx *c, asd_sqt_mode mode, double *out) {

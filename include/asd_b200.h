@@ -93,6 +93,9 @@ int asd_ctx_destroy(asd_ctx *ctx);
 int asd_ctx_set_stream(asd_ctx *ctx, void *stream);
 int asd_ctx_get_params(const asd_ctx *ctx, asd_params *p);
 
+/* Changes the model parameters of an existing context (N and nfile stay). */
+int asd_ctx_set_params(asd_ctx *ctx, const asd_params *p);
+
 /* Copies spins (AoS, host) to the device as the current state.  With
  * as_origin != 0 they also become the t = 0 snapshot that S(q,t) correlates
  * against (spin_zero and zerot_avg, llg_sqt_baseline.c:227-259). */
@@ -126,6 +129,19 @@ int asd_ctx_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
 int asd_ctx_sqt_grid_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
 /* Same into host memory (2*N*N doubles); synchronous. */
 int asd_ctx_sqt_grid(asd_ctx *ctx, asd_sqt_mode mode, double *out);
+
+/* Loss and gradient for parameter fitting.  Starting from the origin spins,
+ * runs nsteps RK4 steps with the context's parameters and evaluates S(q,t) at
+ * the steps t_e = e * stride, e = 1..E, E = nsteps / stride (in FP64, through
+ * the factorised form of the correlation GEMM); with target (2E doubles,
+ * re/im) the loss is L = (1/E) sum_e |S(q,t_e) - target_e|^2 and grad
+ * (6 doubles) receives dL/d(J1, J2, alpha, hx, hy, hz), computed by the
+ * adjoint of the RK4 step and of the renormalisation, with checkpoints every
+ * `checkpoint` steps and recomputation of each segment.  sqt_out (2E
+ * doubles) receives the S(q,t_e) values.  Host buffers; synchronous.  The
+ * current state is not changed.  No counterpart in the reference. */
+int asd_ctx_loss_grad(asd_ctx *ctx, int nsteps, int stride, int checkpoint, const double *target,
+                      double *loss, double *grad, double *sqt_out);
 
 /* One full step through host buffers, the reference's own contract: spins
  * (AoS) come from host memory, one RK4 step runs, the new spins go back to
