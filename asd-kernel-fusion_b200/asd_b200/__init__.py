@@ -50,7 +50,9 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_last_launches",
     "asd_ctx_check_device_status",
     "asd_check_const_division", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
-    "asd_spins_save", "asd_spins_load", "asd_set_params", "euler", "runge_kutta",
+    "asd_spins_save", "asd_spins_load", "asd_batch_create", "asd_batch_destroy",
+    "asd_batch_set_stream", "asd_batch_set_spins", "asd_batch_get_spins", "asd_batch_run",
+    "asd_batch_configure", "asd_batch_autotune", "asd_set_params", "euler", "runge_kutta",
     "fused_dgemm",
 )
 
@@ -134,6 +136,15 @@ def load() -> C.CDLL:
                               C.c_int),
         "asd_sqt_split_noalloc": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp,
                                    C.c_double, C.c_double, C.c_int, vp, vp], C.c_int),
+        "asd_batch_create": ([vp, C.c_int, C.POINTER(vp)], C.c_int),
+        "asd_batch_destroy": ([vp], C.c_int),
+        "asd_batch_set_stream": ([vp, vp], C.c_int),
+        "asd_batch_set_spins": ([vp, C.c_int, vp], C.c_int),
+        "asd_batch_get_spins": ([vp, C.c_int, vp], C.c_int),
+        "asd_batch_run": ([vp, C.c_int], C.c_int),
+        "asd_batch_configure": ([vp, C.c_int, C.c_int], C.c_int),
+        "asd_batch_autotune": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                C.POINTER(C.c_double)], C.c_int),
         "asd_spins_save": ([C.c_char_p, C.c_int, C.c_int, C.c_long, C.c_double, vp], C.c_int),
         "asd_spins_load": ([C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
                             C.POINTER(C.c_long), C.POINTER(C.c_double), vp, C.c_size_t], C.c_int),
@@ -384,3 +395,78 @@ def load_spins(path):
     _check(lib.asd_spins_load(str(path).encode(), C.byref(N), C.byref(nf), C.byref(st),
                               C.byref(sl), C.c_void_p(_ptr(out)), out.size))
     return out, st.value, sl.value
+
+
+class Lattice(C.Structure):
+    """asd_lattice: one lattice of a batch."""
+
+    _fields_ = [("N", C.c_int), ("J1", C.c_double), ("J2", C.c_double), ("alpha", C.c_double),
+                ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double), ("dt", C.c_double),
+                ("spin_len", C.c_double)]
+
+    @classmethod
+    def make(cls, N, J1=1.0, J2=0.0, alpha=0.0, h=(0.0, 0.0, 0.0), dt=0.01, spin_len=1.0):
+        return cls(int(N), float(J1), float(J2), float(alpha), float(h[0]), float(h[1]),
+                   float(h[2]), float(dt), float(spin_len))
+
+
+class Batch:
+    """asd_batch: independent lattices stepped by one persistent launch."""
+
+    def __init__(self, lattices):
+        self.lattices = list(lattices)
+        arr = (Lattice * len(self.lattices))(*self.lattices)
+        h = C.c_void_p()
+        _check(load().asd_batch_create(arr, len(self.lattices), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            load().asd_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_spins(self, l: int, spins: np.ndarray) -> None:
+        s = np.ascontiguousarray(spins, dtype=np.float32)
+        if s.size != self.lattices[l].N ** 2 * 3:
+            raise ValueError("spins must be float32 [N*N][3]")
+        _check(load().asd_batch_set_spins(self._h, int(l), C.c_void_p(_ptr(s))))
+
+    def get_spins(self, l: int) -> np.ndarray:
+        N = self.lattices[l].N
+        out = np.empty((N * N, 3), dtype=np.float32)
+        _check(load().asd_batch_get_spins(self._h, int(l), C.c_void_p(_ptr(out))))
+        return out
+
+    def run(self, nsteps: int) -> None:
+        _check(load().asd_batch_run(self._h, int(nsteps)))
+
+    def configure(self, tile: int, ctas_per_sm: int) -> None:
+        _check(load().asd_batch_configure(self._h, int(tile), int(ctas_per_sm)))
+
+    def autotune(self, trial_steps: int = 20):
+        t, c, ms = C.c_int(), C.c_int(), C.c_double()
+        _check(load().asd_batch_autotune(self._h, int(trial_steps), C.byref(t), C.byref(c),
+                                         C.byref(ms)))
+        return t.value, c.value, ms.value
+
+
+def noisy_ordered_spins(N: int, eta: float, seed: int) -> np.ndarray:
+    """An ordered state along z with Gaussian noise of amplitude eta, renormalised
+    (the "temperature" of a lattice in an ensemble), float64 [N*N][3]."""
+    rng = np.random.default_rng(seed)
+    s = np.zeros((N * N, 3))
+    s[:, 2] = 1.0
+    s += eta * rng.standard_normal((N * N, 3))
+    return s / np.linalg.norm(s, axis=-1, keepdims=True)

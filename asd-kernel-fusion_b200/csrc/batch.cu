@@ -1,0 +1,476 @@
+// batch.cu -- many independent lattices of different sizes and parameters in
+// one persistent launch.  The reference runs one lattice per program; this is
+// the B200 form of running an ensemble of them (e.g. different temperatures
+// and dampings): all lattices' spins stay resident in L2 (FP32, a few MB),
+// one cooperative kernel runs every RK4 step of every lattice, and a bounded
+// grid barrier separates the four stages of a step.
+//
+// Arithmetic: the RK4 stages in FP32 with explicitly rounded operations in the
+// reference's order (euler / runge_kutta, llg_sqt_baseline.c:29-142), the
+// renormalisation in FP64 (norm and division), rounded to FP32 at the end.
+// The CPU oracle restates the same FP32 arithmetic, so the comparison is bit
+// for bit.
+//
+// Layout: lattice l occupies planes x, y, z of N_l * N_l floats at offset
+// off_l (structure of arrays, one replica per lattice).  Work items are tiles
+// of `tile` consecutive sites of one lattice; CTA b processes items b,
+// b + grid, ...  The tile width and the CTAs per SM come from the autotuner.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <chrono>
+#include <vector>
+
+#include "asd_internal.h"
+
+namespace asd {
+
+struct BatchLattice {
+    int N;
+    long off;  // first float of plane x
+    float J1, J2, alpha, g, hx, hy, hz, dt;
+    double spin_len;
+    int use_j2, use_h, use_damp;
+};
+
+namespace {
+
+constexpr uint32_t BARRIER_LIMIT = 1u << 22;
+
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+
+struct F3 {
+    float x, y, z;
+};
+
+// Reads that follow a grid barrier must not hit stale L1 lines: L2 only.
+__device__ __forceinline__ F3 ld3(const float *p, long M, long i) {
+    return F3{__ldcg(p + i), __ldcg(p + M + i), __ldcg(p + 2 * M + i)};
+}
+
+__device__ __forceinline__ F3 rhs32(const float *ys, const BatchLattice &L, long i) {
+    const int N = L.N;
+    const long M = (long)N * N;
+    const int row = (int)(i / N), col = (int)(i - (long)row * N);
+    const int rp = (row + 1 == N) ? 0 : row + 1, rm = (row == 0) ? N - 1 : row - 1;
+    const int cp = (col + 1 == N) ? 0 : col + 1, cm = (col == 0) ? N - 1 : col - 1;
+    const F3 s = ld3(ys, M, i);
+    const long nb[4] = {(long)rp * N + col, (long)rm * N + col, (long)row * N + cm,
+                        (long)row * N + cp};
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const F3 t = ld3(ys, M, nb[j]);
+        ex = fa(ex, fm(t.x, L.J1));
+        ey = fa(ey, fm(t.y, L.J1));
+        ez = fa(ez, fm(t.z, L.J1));
+    }
+    if (L.use_j2) {
+        const long n2[4] = {(long)rp * N + cp, (long)rp * N + cm, (long)rm * N + cp,
+                            (long)rm * N + cm};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const F3 t = ld3(ys, M, n2[j]);
+            ex = fa(ex, fm(t.x, L.J2));
+            ey = fa(ey, fm(t.y, L.J2));
+            ez = fa(ez, fm(t.z, L.J2));
+        }
+    }
+    if (L.use_h) {
+        ex = fa(ex, L.hx);
+        ey = fa(ey, L.hy);
+        ez = fa(ez, L.hz);
+    }
+    F3 tau{fs(fm(ey, s.z), fm(ez, s.y)), fs(fm(ez, s.x), fm(ex, s.z)), fs(fm(ex, s.y), fm(ey, s.x))};
+    if (!L.use_damp) return tau;
+    const float ux = fs(fm(s.y, tau.z), fm(s.z, tau.y));
+    const float uy = fs(fm(s.z, tau.x), fm(s.x, tau.z));
+    const float uz = fs(fm(s.x, tau.y), fm(s.y, tau.x));
+    return F3{fm(L.g, fa(tau.x, fm(L.alpha, ux))), fm(L.g, fa(tau.y, fm(L.alpha, uy))),
+              fm(L.g, fa(tau.z, fm(L.alpha, uz)))};
+}
+
+struct BarrierState {
+    unsigned count;
+    unsigned gen;
+};
+
+// Grid-wide barrier for a cooperative launch (all CTAs resident).  Bounded:
+// after BARRIER_LIMIT polls the waiting CTA records a timeout in *status and
+// every later barrier returns false at once.
+__device__ bool grid_barrier(BarrierState *bs, unsigned nblocks, unsigned *status,
+                             int *s_fail) {
+    __syncthreads();
+    if (threadIdx.x == 0 && !*s_fail) {
+        volatile unsigned *vgen = &bs->gen;
+        const unsigned g = *vgen;
+        __threadfence();
+        if (atomicAdd(&bs->count, 1u) == nblocks - 1) {
+            atomicExch(&bs->count, 0u);
+            __threadfence();
+            atomicAdd(&bs->gen, 1u);
+        } else {
+            uint32_t i = 0;
+            while (*vgen == g) {
+                if (++i > BARRIER_LIMIT || (*(volatile unsigned *)status) != 0u) {
+                    atomicOr(status, (unsigned)kStatusTimeout);
+                    *s_fail = 1;
+                    break;
+                }
+                if (i > 64) __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return !*s_fail;
+}
+
+struct Item {
+    int lat;
+    int first;  // first site
+    int count;
+};
+
+// One persistent launch for nsteps steps of every lattice.
+__global__ void __launch_bounds__(256) batch_kernel(const BatchLattice *__restrict__ lats,
+                                                    const Item *__restrict__ items, int nitems,
+                                                    float *y, float *ysa, float *ysb, float *acc,
+                                                    int nsteps, BarrierState *bs,
+                                                    unsigned *status) {
+    __shared__ int s_fail;
+    if (threadIdx.x == 0) s_fail = 0;
+    __syncthreads();
+    for (int step = 0; step < nsteps; ++step) {
+        for (int stage = 1; stage <= 4; ++stage) {
+            const float *in = (stage == 1) ? y : (stage == 3 ? ysb : ysa);
+            float *out = (stage == 2) ? ysb : (stage == 4 ? y : ysa);
+            for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+                const Item w = items[it];
+                if ((int)threadIdx.x >= w.count) continue;
+                const BatchLattice L = lats[w.lat];
+                const long M = (long)L.N * L.N;
+                const long i = w.first + threadIdx.x;
+                float *Y = y + L.off, *A = acc + L.off, *O = out + L.off;
+                const float *I = in + L.off;
+                const F3 d = rhs32(I, L, i);
+                const float k0 = fm(d.x, L.dt), k1 = fm(d.y, L.dt), k2 = fm(d.z, L.dt);
+                if (stage == 4) {
+                    const double o0 = (double)fa(__ldcg(A + i), fd(k0, 6.f));
+                    const double o1 = (double)fa(__ldcg(A + M + i), fd(k1, 6.f));
+                    const double o2 = (double)fa(__ldcg(A + 2 * M + i), fd(k2, 6.f));
+                    const double nrm = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(o0, o0),
+                                                                      __dmul_rn(o1, o1)),
+                                                            __dmul_rn(o2, o2)));
+                    O[i] = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o0), nrm));
+                    O[M + i] = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o1), nrm));
+                    O[2 * M + i] = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o2), nrm));
+                } else {
+                    const F3 yb = ld3(Y, M, i);
+                    const F3 kk{k0, k1, k2};
+                    F3 o;
+                    if (stage == 3) o = F3{fa(yb.x, kk.x), fa(yb.y, kk.y), fa(yb.z, kk.z)};
+                    else o = F3{fa(yb.x, fm(kk.x, 0.5f)), fa(yb.y, fm(kk.y, 0.5f)),
+                                fa(yb.z, fm(kk.z, 0.5f))};
+                    O[i] = o.x;
+                    O[M + i] = o.y;
+                    O[2 * M + i] = o.z;
+                    if (stage == 1) {
+                        A[i] = fa(yb.x, fd(kk.x, 6.f));
+                        A[M + i] = fa(yb.y, fd(kk.y, 6.f));
+                        A[2 * M + i] = fa(yb.z, fd(kk.z, 6.f));
+                    } else {
+                        A[i] = fa(__ldcg(A + i), fd(kk.x, 3.f));
+                        A[M + i] = fa(__ldcg(A + M + i), fd(kk.y, 3.f));
+                        A[2 * M + i] = fa(__ldcg(A + 2 * M + i), fd(kk.z, 3.f));
+                    }
+                }
+            }
+            if (!grid_barrier(bs, gridDim.x, status, &s_fail)) return;
+        }
+    }
+}
+
+}  // namespace
+}  // namespace asd
+
+using namespace asd;
+
+struct asd_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<BatchLattice> lat;
+    long total = 0;  // floats per buffer
+    BatchLattice *d_lat = nullptr;
+    float *y = nullptr, *ysa = nullptr, *ysb = nullptr, *acc = nullptr;
+    BarrierState *bs = nullptr;
+    unsigned *status = nullptr;
+    Item *d_items = nullptr;
+    int nitems = 0, tile = 0, ctas_per_sm = 0, grid = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = -1;
+};
+
+namespace {
+
+int build_items(asd_batch *b, int tile) {
+    std::vector<Item> items;
+    for (int l = 0; l < (int)b->lat.size(); ++l) {
+        const int M = b->lat[l].N * b->lat[l].N;
+        for (int f = 0; f < M; f += tile) items.push_back(Item{l, f, std::min(tile, M - f)});
+    }
+    if (b->d_items) cudaFree(b->d_items);
+    b->d_items = nullptr;
+    ASD_CUDA_TRY(cudaMalloc(&b->d_items, items.size() * sizeof(Item)));
+    ASD_CUDA_TRY(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(Item),
+                            cudaMemcpyHostToDevice));
+    b->nitems = (int)items.size();
+    b->tile = tile;
+    return ASD_OK;
+}
+
+int configure(asd_batch *b, int tile, int ctas_per_sm) {
+    if (tile < 32 || tile > 256 || tile % 32) return fail(ASD_ERR_INVALID, "tile %d", tile);
+    int occ = 0, sms = 0;
+    ASD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, 256, 0));
+    ASD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    if (ctas_per_sm < 1 || ctas_per_sm > occ)
+        return fail(ASD_ERR_INVALID, "ctas_per_sm %d (at most %d resident)", ctas_per_sm, occ);
+    int rc = build_items(b, tile);
+    if (rc != ASD_OK) return rc;
+    b->ctas_per_sm = ctas_per_sm;
+    b->grid = std::min(sms * ctas_per_sm, b->nitems);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_steps = -1;
+    return ASD_OK;
+}
+
+int launch(asd_batch *b, int nsteps) {
+    // cooperative: every CTA resident, which the grid barrier relies on
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(b->grid);
+    cfg.blockDim = dim3(256);
+    cfg.stream = b->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    ASD_CUDA_TRY(cudaLaunchKernelEx(&cfg, batch_kernel, (const BatchLattice *)b->d_lat,
+                                    (const Item *)b->d_items, b->nitems, b->y, b->ysa, b->ysb,
+                                    b->acc, nsteps, b->bs, b->status));
+    return ASD_OK;
+}
+
+int run(asd_batch *b, int nsteps) {
+    // one persistent launch, captured once per step count in a CUDA graph
+    if (!b->graph || b->graph_steps != nsteps) {
+        if (b->graph) cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        cudaStream_t cap = b->stream;
+        bool own = false;
+        if (!cap) {  // capture needs a non-default stream
+            ASD_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            own = true;
+        }
+        cudaGraph_t g = nullptr;
+        ASD_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        cudaStream_t saved = b->stream;
+        b->stream = cap;
+        const int rc = launch(b, nsteps);
+        b->stream = saved;
+        const cudaError_t e = cudaStreamEndCapture(cap, &g);
+        if (own) cudaStreamDestroy(cap);
+        if (rc != ASD_OK) return rc;
+        ASD_CUDA_TRY(e);
+        const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        ASD_CUDA_TRY(ei);
+        b->graph_steps = nsteps;
+    }
+    ASD_CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+    return ASD_OK;
+}
+
+int check_status(asd_batch *b) {
+    unsigned st = 0;
+    ASD_CUDA_TRY(cudaMemcpyAsync(&st, b->status, sizeof st, cudaMemcpyDeviceToHost, b->stream));
+    ASD_CUDA_TRY(cudaMemsetAsync(b->status, 0, sizeof(unsigned), b->stream));
+    ASD_CUDA_TRY(cudaMemsetAsync(b->bs, 0, sizeof(BarrierState), b->stream));
+    ASD_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    if (st) return fail(ASD_ERR_TIMEOUT, "the batch kernel's grid barrier gave up (status %u)", st);
+    return ASD_OK;
+}
+
+void destroy(asd_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    void *p[] = {b->d_lat, b->y, b->ysa, b->ysb, b->acc, b->bs, b->status, b->d_items};
+    for (void *q : p)
+        if (q) cudaFree(q);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int asd_batch_create(const asd_lattice *lats, int count, asd_batch **out) {
+    if (!out || !lats || count < 1) return fail(ASD_ERR_INVALID, "bad argument");
+    *out = nullptr;
+    asd_batch *b = new asd_batch();
+    cudaError_t e = cudaGetDevice(&b->device);
+    if (e != cudaSuccess) {
+        delete b;
+        return cuda_fail(e, "cudaGetDevice");
+    }
+    long off = 0;
+    for (int l = 0; l < count; ++l) {
+        const asd_lattice &p = lats[l];
+        if (p.N < 3 || p.N > 4096 || !(p.spin_len > 0)) {
+            delete b;
+            return fail(ASD_ERR_INVALID, "lattice %d: N=%d spin_len=%g", l, p.N, p.spin_len);
+        }
+        BatchLattice L;
+        L.N = p.N;
+        L.off = off;
+        L.J1 = (float)p.J1, L.J2 = (float)p.J2, L.alpha = (float)p.alpha;
+        L.g = (float)(1.0 / (1.0 + (double)(float)p.alpha * (double)(float)p.alpha));
+        L.hx = (float)p.hx, L.hy = (float)p.hy, L.hz = (float)p.hz, L.dt = (float)p.dt;
+        L.spin_len = p.spin_len;
+        L.use_j2 = p.J2 != 0.0;
+        L.use_h = (p.hx != 0.0 || p.hy != 0.0 || p.hz != 0.0);
+        L.use_damp = p.alpha != 0.0;
+        b->lat.push_back(L);
+        off += 3L * p.N * p.N;
+    }
+    b->total = off;
+    const size_t bytes = (size_t)off * sizeof(float);
+    int rc = ASD_OK;
+    if (cudaMalloc(&b->d_lat, count * sizeof(BatchLattice)) != cudaSuccess ||
+        cudaMalloc(&b->y, bytes) != cudaSuccess || cudaMalloc(&b->ysa, bytes) != cudaSuccess ||
+        cudaMalloc(&b->ysb, bytes) != cudaSuccess || cudaMalloc(&b->acc, bytes) != cudaSuccess ||
+        cudaMalloc(&b->bs, sizeof(BarrierState)) != cudaSuccess ||
+        cudaMalloc(&b->status, sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        destroy(b);
+        return fail(ASD_ERR_NOMEM, "cudaMalloc for the batch failed");
+    }
+    cudaMemcpy(b->d_lat, b->lat.data(), count * sizeof(BatchLattice), cudaMemcpyHostToDevice);
+    cudaMemset(b->bs, 0, sizeof(BarrierState));
+    cudaMemset(b->status, 0, sizeof(unsigned));
+    cudaMemset(b->y, 0, bytes);
+    if ((rc = configure(b, 128, 2)) != ASD_OK) {
+        destroy(b);
+        return rc;
+    }
+    *out = b;
+    return ASD_OK;
+}
+
+int asd_batch_destroy(asd_batch *b) {
+    destroy(b);
+    return ASD_OK;
+}
+
+int asd_batch_set_stream(asd_batch *b, void *stream) {
+    if (!b) return fail(ASD_ERR_INVALID, "batch is NULL");
+    b->stream = (cudaStream_t)stream;
+    return ASD_OK;
+}
+
+int asd_batch_set_spins(asd_batch *b, int lattice, const float *spin_aos) {
+    if (!b || !spin_aos || lattice < 0 || lattice >= (int)b->lat.size())
+        return fail(ASD_ERR_INVALID, "bad argument");
+    ASD_CUDA_TRY(cudaSetDevice(b->device));
+    const BatchLattice &L = b->lat[lattice];
+    const long M = (long)L.N * L.N;
+    std::vector<float> soa((size_t)3 * M);
+    for (long i = 0; i < M; ++i)
+        for (int c = 0; c < 3; ++c) soa[c * M + i] = spin_aos[3 * i + c];
+    ASD_CUDA_TRY(cudaMemcpy(b->y + L.off, soa.data(), soa.size() * sizeof(float),
+                            cudaMemcpyHostToDevice));
+    return ASD_OK;
+}
+
+int asd_batch_get_spins(asd_batch *b, int lattice, float *spin_aos) {
+    if (!b || !spin_aos || lattice < 0 || lattice >= (int)b->lat.size())
+        return fail(ASD_ERR_INVALID, "bad argument");
+    ASD_CUDA_TRY(cudaSetDevice(b->device));
+    ASD_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    const BatchLattice &L = b->lat[lattice];
+    const long M = (long)L.N * L.N;
+    std::vector<float> soa((size_t)3 * M);
+    ASD_CUDA_TRY(cudaMemcpy(soa.data(), b->y + L.off, soa.size() * sizeof(float),
+                            cudaMemcpyDeviceToHost));
+    for (long i = 0; i < M; ++i)
+        for (int c = 0; c < 3; ++c) spin_aos[3 * i + c] = soa[c * M + i];
+    return ASD_OK;
+}
+
+int asd_batch_run(asd_batch *b, int nsteps) {
+    if (!b || nsteps < 0) return fail(ASD_ERR_INVALID, "bad argument");
+    if (nsteps == 0) return ASD_OK;
+    ASD_CUDA_TRY(cudaSetDevice(b->device));
+    int rc = run(b, nsteps);
+    if (rc != ASD_OK) return rc;
+    return check_status(b);
+}
+
+int asd_batch_configure(asd_batch *b, int tile, int ctas_per_sm) {
+    if (!b) return fail(ASD_ERR_INVALID, "batch is NULL");
+    ASD_CUDA_TRY(cudaSetDevice(b->device));
+    return configure(b, tile, ctas_per_sm);
+}
+
+int asd_batch_autotune(asd_batch *b, int trial_steps, int *tile, int *ctas_per_sm,
+                       double *ms_per_step) {
+    if (!b || trial_steps < 1) return fail(ASD_ERR_INVALID, "bad argument");
+    ASD_CUDA_TRY(cudaSetDevice(b->device));
+    int occ = 0;
+    ASD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, 256, 0));
+    // the trials advance the spins: keep a copy and restore it afterwards
+    const size_t bytes = (size_t)b->total * sizeof(float);
+    float *save = nullptr;
+    ASD_CUDA_TRY(cudaMalloc(&save, bytes));
+    cudaMemcpyAsync(save, b->y, bytes, cudaMemcpyDeviceToDevice, b->stream);
+    double best = 1e300;
+    int bt = 128, bc = 1;
+    const int tiles[] = {32, 64, 128, 256};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = ASD_OK;
+    for (int t : tiles) {
+        for (int c = 1; c <= std::min(occ, 8); c *= 2) {
+            if ((rc = configure(b, t, c)) != ASD_OK) break;
+            if ((rc = asd_batch_run(b, trial_steps)) != ASD_OK) break;  // captures and warms
+            cudaEventRecord(e0, b->stream);
+            if ((rc = run(b, trial_steps)) != ASD_OK) break;
+            cudaEventRecord(e1, b->stream);
+            if ((rc = check_status(b)) != ASD_OK) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) best = ms, bt = t, bc = c;
+        }
+        if (rc != ASD_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaMemcpyAsync(b->y, save, bytes, cudaMemcpyDeviceToDevice, b->stream);
+    cudaStreamSynchronize(b->stream);
+    cudaFree(save);
+    if (rc != ASD_OK) return rc;
+    if ((rc = configure(b, bt, bc)) != ASD_OK) return rc;
+    if (tile) *tile = bt;
+    if (ctas_per_sm) *ctas_per_sm = bc;
+    if (ms_per_step) *ms_per_step = best / trial_steps;
+    return ASD_OK;
+}
+
+}  // extern "C"

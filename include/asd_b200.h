@@ -226,6 +226,37 @@ int asd_sqt_split_noalloc(int kind, long rows, int Kp, const void *a_hi, const v
                           const void *col4, const float *col1, double alpha, double scale,
                           int chunk_k, double *d_out, void *stream);
 
+/* ------------------------------------------------------ batched lattices */
+/* Many independent lattices (one replica each) of different sizes and
+ * parameters, stepped together by one persistent, graph-captured launch with
+ * all spins resident on the GPU.  RK4 stages in FP32 (explicitly rounded, the
+ * reference's operation order), renormalisation in FP64.  No counterpart in
+ * the reference, which runs one lattice per program. */
+typedef struct {
+    int N;
+    double J1, J2, alpha, hx, hy, hz, dt, spin_len;
+} asd_lattice;
+typedef struct asd_batch asd_batch;
+
+int asd_batch_create(const asd_lattice *lattices, int count, asd_batch **out);
+int asd_batch_destroy(asd_batch *batch);
+int asd_batch_set_stream(asd_batch *batch, void *stream);
+/* Spins of one lattice, float[N*N][3] (host). */
+int asd_batch_set_spins(asd_batch *batch, int lattice, const float *spin_aos);
+int asd_batch_get_spins(asd_batch *batch, int lattice, float *spin_aos);
+/* nsteps RK4 steps of every lattice in one persistent launch (a CUDA graph
+ * per step count); synchronous; ASD_ERR_TIMEOUT if the kernel's bounded grid
+ * barrier gave up. */
+int asd_batch_run(asd_batch *batch, int nsteps);
+/* Work decomposition: `tile` consecutive sites per work item (32..256, a
+ * multiple of 32) and `ctas_per_sm` resident CTAs per SM. */
+int asd_batch_configure(asd_batch *batch, int tile, int ctas_per_sm);
+/* Times trial_steps steps for every tile in {32, 64, 128, 256} and CTAs per SM
+ * in {1, 2, 4, 8} (as far as they fit), keeps the fastest and reports it; the
+ * spins are restored afterwards. */
+int asd_batch_autotune(asd_batch *batch, int trial_steps, int *tile, int *ctas_per_sm,
+                       double *ms_per_step);
+
 /* --------------------------------------------------------- spin-state I/O */
 /* The reference keeps spins only in memory; these define a file format for
  * checkpoints: a 64-byte header (magic "ASDSPIN1", int32 N, int32 nfile,

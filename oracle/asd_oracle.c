@@ -477,3 +477,96 @@ void oracle_sqt_grid(int N, int nfile, const double *spin_t, const double *spin_
     free(zerot);
     free(bins);
 }
+
+/* ------------------------------------------------- FP32 RK4 (batched lattices)
+ * The arithmetic of the batched-lattice GPU path: the same operations as
+ * oracle_llg_deriv / oracle_rk4 (euler / runge_kutta, llg_sqt_baseline.c:29-142)
+ * in FP32, each rounded as written (x86-64 SSE float arithmetic with
+ * -ffp-contract=off); the renormalisation in FP64 and rounded to FP32 at the
+ * end.  One replica; spins float[N*N][3]. */
+static void deriv_f32(const oracle_params *p, const float *s, float *d)
+{
+    const int N = p->N;
+    const long M = (long)N * N;
+    const float J1 = (float)p->J1, J2 = (float)p->J2, al = (float)p->alpha;
+    const float hx = (float)p->hx, hy = (float)p->hy, hz = (float)p->hz;
+    const float g = (float)(1.0 / (1.0 + (double)al * (double)al));
+    const int use_j2 = p->J2 != 0.0, use_h = (p->hx != 0.0 || p->hy != 0.0 || p->hz != 0.0);
+    const int use_damp = p->alpha != 0.0;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < M; i++) {
+        const int row = (int)(i / N), col = (int)(i % N);
+        const float sx = s[i * 3], sy = s[i * 3 + 1], sz = s[i * 3 + 2];
+        float ex = 0.0f, ey = 0.0f, ez = 0.0f;
+        for (int j = 0; j < 4; j++) {
+            const long nb = (long)((row + kNN[j][0] + N) % N) * N + (col + kNN[j][1] + N) % N;
+            ex += s[nb * 3] * J1;
+            ey += s[nb * 3 + 1] * J1;
+            ez += s[nb * 3 + 2] * J1;
+        }
+        if (use_j2)
+            for (int j = 0; j < 4; j++) {
+                const long nb = (long)((row + kNNN[j][0] + N) % N) * N + (col + kNNN[j][1] + N) % N;
+                ex += s[nb * 3] * J2;
+                ey += s[nb * 3 + 1] * J2;
+                ez += s[nb * 3 + 2] * J2;
+            }
+        if (use_h) {
+            ex += hx;
+            ey += hy;
+            ez += hz;
+        }
+        const float tx = ey * sz - ez * sy, ty = ez * sx - ex * sz, tz = ex * sy - ey * sx;
+        if (use_damp) {
+            const float ux = sy * tz - sz * ty, uy = sz * tx - sx * tz, uz = sx * ty - sy * tx;
+            d[i * 3] = g * (tx + al * ux);
+            d[i * 3 + 1] = g * (ty + al * uy);
+            d[i * 3 + 2] = g * (tz + al * uz);
+        } else {
+            d[i * 3] = tx;
+            d[i * 3 + 1] = ty;
+            d[i * 3 + 2] = tz;
+        }
+    }
+}
+
+int oracle_steps_f32(const oracle_params *p, float *spin, int nsteps)
+{
+    const long n = (long)p->N * p->N * 3;
+    float *buf = (float *)malloc((size_t)4 * n * sizeof(float));
+    if (!buf) return -1;
+    float *ys = buf, *acc = buf + n, *d = buf + 2 * n, *ys2 = buf + 3 * n;
+    const float dt = (float)p->dt;
+    for (int step = 0; step < nsteps; step++) {
+        /* stage 1 */
+        deriv_f32(p, spin, d);
+        for (long j = 0; j < n; j++) {
+            const float k = d[j] * dt;
+            ys[j] = spin[j] + k * 0.5f;
+            acc[j] = spin[j] + k / 6.0f;
+        }
+        /* stages 2, 3 */
+        deriv_f32(p, ys, d);
+        for (long j = 0; j < n; j++) {
+            const float k = d[j] * dt;
+            ys2[j] = spin[j] + k * 0.5f;
+            acc[j] = acc[j] + k / 3.0f;
+        }
+        deriv_f32(p, ys2, d);
+        for (long j = 0; j < n; j++) {
+            const float k = d[j] * dt;
+            ys[j] = spin[j] + k;
+            acc[j] = acc[j] + k / 3.0f;
+        }
+        /* stage 4 + FP64 renormalisation */
+        deriv_f32(p, ys, d);
+        for (long j = 0; j < n / 3; j++) {
+            double o[3];
+            for (int c = 0; c < 3; c++) o[c] = (double)(acc[j * 3 + c] + (d[j * 3 + c] * dt) / 6.0f);
+            const double nrm = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+            for (int c = 0; c < 3; c++) spin[j * 3 + c] = (float)(p->spin_len * o[c] / nrm);
+        }
+    }
+    free(buf);
+    return 0;
+}

@@ -11,7 +11,7 @@
  * own layout, "AoS": double[nfile][N*N][3] (llg_sqt_baseline.c:185, :202).
  *
  * Parity pins (see tests/test_oracle_pins.py): when the reference sources are
- * present, oracle/build_ref.sh compiles them into oracle/_ref/ and the tests
+ * present, `make -C oracle ref` compiles them into oracle/_ref/ and the tests
  * check this restatement against the reference's own euler/runge_kutta (bit
  * exact, both built with -ffp-contract=off) and fused_dgemm (C bit exact, the
  * running sums to 1e-13), and tests/golden/ holds fixtures produced by the
@@ -87,6 +87,10 @@ void oracle_sqt_grid(int N, int nfile, const double *spin_t, const double *spin_
 void oracle_fused_dgemm(int m, int n, int k, double alpha, const double *a, int lda,
                         const double *b, int ldb, double *c, int ldc,
                         const double *q, double *sum);
+
+/* nsteps of the FP32 RK4 with FP64 renormalisation of the batched-lattice GPU
+ * path, one replica, spins float[N*N][3] in place. */
+int oracle_steps_f32(const oracle_params *p, float *spin, int nsteps);
 
 /* Interleaved complex layout of the fusion variant (llg_sqt_fusion.c:324-327). */
 static inline long oracle_row_re(long i) { return (i / 4) * 8 + (i % 4); }

@@ -75,6 +75,9 @@ class Oracle:
         lib.oracle_steps.restype = C.c_int
         for name in ("oracle_sqt_gemm", "oracle_sqt_direct", "oracle_sqt_fused", "oracle_sqt_factorized"):
             getattr(lib, name).argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
+        fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+        lib.oracle_steps_f32.argtypes = [P, fp, C.c_int]
+        lib.oracle_steps_f32.restype = C.c_int
         lib.oracle_sqt_grid.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp]
         lib.oracle_fused_dgemm.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, _dp, C.c_int,
                                            _dp, C.c_int, _dp, C.c_int, _dp, _dp]
@@ -101,6 +104,13 @@ class Oracle:
         s = np.array(spin, dtype=np.float64, copy=True, order="C")
         if self.lib.oracle_steps(C.byref(p), s, int(nsteps)) != 0:
             raise MemoryError("oracle_steps")
+        return s
+
+    def steps_f32(self, p: OracleParams, spin: np.ndarray, nsteps: int) -> np.ndarray:
+        """FP32 RK4 + FP64 renormalisation, one replica, float32 [N*N][3]."""
+        s = np.array(spin, dtype=np.float32, copy=True, order="C")
+        if self.lib.oracle_steps_f32(C.byref(p), s, int(nsteps)) != 0:
+            raise MemoryError("oracle_steps_f32")
         return s
 
     # S(q,t) --------------------------------------------------------------
