@@ -49,7 +49,7 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_step_host", "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
     "asd_ctx_last_launches",
     "asd_ctx_check_device_status",
-    "asd_check_const_division", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
+    "asd_check_bounded_wait", "asd_check_const_division", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
     "asd_spins_save", "asd_spins_load", "asd_batch_create", "asd_batch_destroy",
     "asd_batch_set_stream", "asd_batch_set_spins", "asd_batch_get_spins", "asd_batch_run",
     "asd_batch_configure", "asd_batch_autotune", "asd_set_params", "euler", "runge_kutta",
@@ -130,6 +130,7 @@ def load() -> C.CDLL:
         "asd_ctx_set_chunk_k": ([vp, C.c_int], C.c_int),
         "asd_ctx_last_launches": ([vp], C.c_int),
         "asd_ctx_check_device_status": ([vp], C.c_int),
+        "asd_check_bounded_wait": ([C.c_int, C.c_uint, vp], C.c_int),
         "asd_check_const_division": ([vp, C.c_long, vp, vp], C.c_int),
         "asd_umma_gemm_f32": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, C.c_long, C.c_int,
                                vp],

@@ -194,7 +194,22 @@ __global__ void __launch_bounds__(256) batch_kernel(const BatchLattice *__restri
     }
 }
 
+// One CTA waits at a grid barrier sized for two: nothing arrives for the
+// second, so the bounded barrier must give up and record a timeout.
+__global__ void grid_barrier_probe_kernel(BarrierState *bs, unsigned *status) {
+    __shared__ int s_fail;
+    if (threadIdx.x == 0) s_fail = 0;
+    __syncthreads();
+    grid_barrier(bs, 2u, status, &s_fail);
+}
+
 }  // namespace
+
+cudaError_t launch_grid_barrier_probe(void *bs, unsigned *status, cudaStream_t st) {
+    grid_barrier_probe_kernel<<<1, 32, 0, st>>>(static_cast<BarrierState *>(bs), status);
+    return cudaGetLastError();
+}
+
 }  // namespace asd
 
 using namespace asd;
@@ -474,3 +489,22 @@ int asd_batch_autotune(asd_batch *b, int trial_steps, int *tile, int *ctas_per_s
 }
 
 }  // extern "C"
+
+extern "C" int asd_check_bounded_wait(int which, unsigned limit, void *stream) {
+    using namespace asd;
+    if (which != 0 && which != 1) return fail(ASD_ERR_INVALID, "which must be 0 or 1");
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned *d = nullptr;  // status word + a barrier state
+    ASD_CUDA_TRY(cudaMalloc(&d, 4 * sizeof(unsigned)));
+    cudaError_t e = cudaMemsetAsync(d, 0, 4 * sizeof(unsigned), st);
+    if (e == cudaSuccess)
+        e = which == 0 ? launch_mbar_timeout_probe(limit, d, st)
+                       : launch_grid_barrier_probe(d + 2, d, st);
+    unsigned h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "bounded-wait probe");
+    if (h & kStatusTimeout) return fail(ASD_ERR_TIMEOUT, "the probe's wait gave up as designed");
+    return ASD_OK;
+}

@@ -573,6 +573,28 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     return grid;
 }
 
+namespace {
+// Waits on an mbarrier that no thread ever arrives at: the bounded wait must
+// give up after `limit` polls and record a timeout.
+__global__ void mbar_timeout_probe_kernel(uint32_t limit, unsigned *status) {
+    __shared__ uint64_t bar;
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) {
+        ptx::mbar_init(&bar, 1);
+        abort_flag = 0;
+        ptx::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !ptx::mbar_wait_bounded(&bar, 0u, &abort_flag, limit))
+        atomicOr(status, (unsigned)kStatusTimeout);
+}
+}  // namespace
+
+cudaError_t launch_mbar_timeout_probe(uint32_t limit, unsigned *status, cudaStream_t st) {
+    mbar_timeout_probe_kernel<<<1, 32, 0, st>>>(limit, status);
+    return cudaGetLastError();
+}
+
 }  // namespace asd
 
 // Diagnostic entry point (declared in include/asd_b200.h): the bare

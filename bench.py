@@ -369,6 +369,117 @@ def e2e_measurement(ctx, asd, torch, spins0, mode, M, nf, args, world):
             "api": "asd_ctx_step_host (pinned host buffers)"}
 
 
+# ------------------------------------------------------ other configurations
+def timed(torch, fn, reps):
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(reps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_workload(args):
+    """Secondary workloads, one JSON line each (not the headline):
+    sqt256   256x256 lattice, 1000 replicas, J=1, J2=-0.3, alpha=0.02, dt=0.005:
+             one RK4 step + S(q,t) in BF16x3, with the FP64 path's time and error
+    adjoint64  64x64 lattice, 100 replicas, 1000 steps, S(q,t) every 10 steps,
+             checkpoints every 50: loss + gradient wrt (J1, J2, alpha, h)
+    batch48  48 lattices of sizes in {48,64,96,128,160}^2, noise amplitude in
+             [0, 0.5], alpha in [0.01, 0.2]: 2000 steps in one persistent launch"""
+    import torch
+
+    import asd_b200 as asd
+
+    torch.cuda.set_device(0)
+    hbm, bf16, src = measured_peaks()
+    out = {"impl": "ours", "workload": args.workload, "n_gpus": 1, "data": "synthetic"}
+    if args.workload == "sqt256":
+        N, nf = 256, 1000
+        M, K = N * N, 3 * nf
+        ctx = asd.Context(asd.Params.make(N, nf, J1=1.0, J2=-0.3, alpha=0.02, dt=0.005),
+                          modes=["fp64", "bf16x3", "tf32x3"])
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        ctx.set_spins(asd.random_spins(N, nf, seed=0), as_origin=True)
+        d = torch.zeros(2, dtype=torch.float64, device="cuda")
+        ctx.step(3)
+        step_ms = timed(torch, lambda: (ctx.step(1), ctx.sqt_async("bf16x3", d.data_ptr())),
+                        args.steps)
+        llg_ms = timed(torch, lambda: ctx.step(1), 10)
+        vals, ms = {}, {}
+        for mode, reps in (("bf16x3", 5), ("tf32x3", 3), ("fp64", 1)):
+            ctx.sqt_async(mode, d.data_ptr())
+            ms[mode] = timed(torch, lambda: ctx.sqt_async(mode, d.data_ptr()), reps)
+            vals[mode] = complex(*d.tolist())
+        flops = 2.0 * M * M * K
+        out.update({
+            "metric": METRIC, "value": M * nf / (step_ms / 1e3), "unit": "site-steps/s",
+            "ms_per_step": step_ms, "dtype": "f64 RK4 + bf16x3 GEMM",
+            "config": {"workload": "256x256 lattice, 1000 replicas, J=1, J2=-0.3, alpha=0.02, dt=0.005",
+                       "gemm_m": M, "gemm_k": K},
+            "llg": {"ms": llg_ms, "achieved_gbs": LLG_BYTES_PER_SITE_STEP * M * nf / llg_ms / 1e6,
+                    "hbm_peak_gbs": hbm},
+            "sqt": {m: {"ms": ms[m], "tflops": flops / ms[m] / 1e9,
+                        "rel_err_vs_fp64": abs(vals[m] - vals["fp64"]) / abs(vals["fp64"])}
+                    for m in ms},
+            "sqt_speedup_vs_fp64": {m: ms["fp64"] / ms[m] for m in ("bf16x3", "tf32x3")},
+            "roofline": {"bound": "tensor", "kernel": "umma_sqt_kernel (bf16x3)",
+                         "achieved": flops / ms["bf16x3"] / 1e9, "peak": bf16, "unit": "TFLOP/s",
+                         "frac": flops / ms["bf16x3"] / 1e9 / bf16, "traffic": None},
+        })
+        ctx.close()
+    elif args.workload == "adjoint64":
+        N, nf, nsteps, stride, ck = 64, 100, 1000, 10, 50
+        s0 = asd.random_spins(N, nf, seed=0)
+        ctx = asd.Context(asd.Params.make(N, nf, J1=1.0, alpha=0.1, h=(0, 0, 0.2), dt=0.01),
+                          modes=["fp64"])
+        ctx.set_spins(s0, as_origin=True)
+        _, _, target = ctx.loss_grad(nsteps, stride, ck, None)
+        ctx.set_params(asd.Params.make(N, nf, J1=0.8, alpha=0.15, dt=0.01))
+        t0 = time.perf_counter()
+        fwd = ctx.loss_grad(nsteps, stride, ck, None)
+        t_fwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        loss, grad, _ = ctx.loss_grad(nsteps, stride, ck, target)
+        t_grad = time.perf_counter() - t0
+        out.update({
+            "metric": "loss + adjoint gradient wall time", "value": t_grad, "unit": "s",
+            "higher_is_better": False,
+            "config": {"workload": "64x64 lattice, 100 replicas, 1000 steps, S(q,t) every 10 steps, checkpoints every 50"},
+            "forward_only_s": t_fwd, "loss": loss, "grad": list(grad),
+            "site_steps_per_s_forward": N * N * nf * nsteps / t_fwd,
+        })
+        ctx.close()
+    elif args.workload == "batch48":
+        rng = np.random.default_rng(5)
+        sizes = [int(x) for x in rng.choice([48, 64, 96, 128, 160], size=48)]
+        lats = []
+        for k, N in enumerate(sizes):
+            lats.append(asd.Lattice.make(N, J1=1.0, alpha=float(rng.uniform(0.01, 0.2)), dt=0.01))
+        b = asd.Batch(lats)
+        for l, N in enumerate(sizes):
+            b.set_spins(l, asd.noisy_ordered_spins(N, float(rng.uniform(0, 0.5)), l).astype(np.float32))
+        tile, ctas, _ = b.autotune(20)
+        b.run(10)
+        t0 = time.perf_counter()
+        b.run(2000)
+        t = time.perf_counter() - t0
+        sites = sum(N * N for N in sizes)
+        out.update({
+            "metric": "batched site-steps/s (one persistent launch, 2000 steps)",
+            "value": sites * 2000 / t, "unit": "site-steps/s", "ms_per_step": t / 2000 * 1e3,
+            "dtype": "f32 RK4 + f64 renorm",
+            "config": {"workload": "48 lattices, sizes in {48,64,96,128,160}^2", "sites": sites,
+                       "tile": tile, "ctas_per_sm": ctas},
+        })
+        b.close()
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -382,7 +493,11 @@ def main():
                     help="only the timed steps (for profiling): no per-component timings, e2e "
                          "or CPU baseline after the timed region")
     ap.add_argument("--ref-target-s", type=float, default=2.0)
+    ap.add_argument("--workload", choices=["headline", "sqt256", "adjoint64", "batch48"],
+                    default="headline", help="secondary workloads print their own line")
     args = ap.parse_args()
+    if args.workload != "headline":
+        return run_workload(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

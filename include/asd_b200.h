@@ -176,6 +176,14 @@ int asd_ctx_last_launches(const asd_ctx *ctx);
  * returns ASD_OK or ASD_ERR_TIMEOUT and clears it. */
 int asd_ctx_check_device_status(asd_ctx *ctx);
 
+/* Diagnostic: runs one of the library's bounded waits against a condition
+ * that nothing satisfies -- which = 0: the mbarrier wait of the tensor-core
+ * GEMM (`limit` polls); which = 1: the grid barrier of the batched kernel --
+ * and returns ASD_ERR_TIMEOUT when the wait gave up and reported it, as
+ * designed.  No counterpart in the reference; the failure-detection tests use
+ * it (no GPU fault is involved). */
+int asd_check_bounded_wait(int which, unsigned limit, void *stream);
+
 /* Diagnostic: adds to *bad (device counter) the number of x[i] (device array)
  * for which the LLG kernels' divisions by the constants 3 and 6 (Markstein's
  * correction step) differ in any bit from the correctly rounded division.
