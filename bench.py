@@ -42,6 +42,24 @@ LLG_BYTES_PER_SITE_STEP = 384  # 4 fused stage kernels: 3+5+5+3 FP64 3-vectors
 LLG_FUSED_BYTES_PER_SITE_STEP = 48  # one temporally blocked step: read y, write y
 
 
+def aggregate(ms_per_step: float, units_per_rank: float, world: int, dist=None, device=None):
+    """Whole-job throughput of a weak-scaling run: every rank processed
+    units_per_rank units in ms_per_step on its own clock; the job's time is
+    the slowest rank's.  Returns (max ms over ranks, units per second)."""
+    if world > 1 and dist is not None:
+        import torch
+
+        t = torch.tensor([ms_per_step], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_per_step = float(t.item())
+    return ms_per_step, world * units_per_rank / (ms_per_step / 1e3)
+
+
+def rank_seed(rank: int) -> int:
+    """Each rank steps its own lattice (independent ensembles)."""
+    return rank
+
+
 def env_rank():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -212,7 +230,7 @@ def run_ours(args):
         ctx.set_chunk_k(args.chunk_k)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
-    spins0 = asd.random_spins(N, nf, seed=rank)
+    spins0 = asd.random_spins(N, nf, seed=rank_seed(rank))
     ctx.set_spins(spins0, as_origin=True)
     total = args.warmup + args.steps
     d_out = torch.zeros(2 * max(total, 1), dtype=torch.float64, device="cuda")
@@ -239,12 +257,9 @@ def run_ours(args):
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
     ctx.check_device_status()
+    ms, value = aggregate(ms, M * nf, world, dist if world > 1 else None, "cuda")
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
         dist.barrier()
-    value = world * M * nf / (ms / 1e3)
     sqt_last = complex(*d_out[2 * (total - 1):2 * total].tolist())
 
     extra = {"sqt_ms": {}, "report": {}}
@@ -357,15 +372,12 @@ def e2e_measurement(ctx, asd, torch, spins0, mode, M, nf, args, world):
     t0 = time.perf_counter()
     for _ in range(steps):
         ctx.step_host(h_out.data_ptr(), h_out.data_ptr(), mode)
-    dt = (time.perf_counter() - t0) / steps
-    if world > 1:
-        import torch.distributed as dist
+    ms = (time.perf_counter() - t0) / steps * 1e3
+    import torch.distributed as dist
 
-        t = torch.tensor([dt], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dt = t.item()
-    return {"value": world * M * nf / dt, "unit": "site-steps/s", "h2d_bytes_per_step": n * 8,
-            "d2h_bytes_per_step": n * 8 + 16, "ms_per_step": dt * 1e3,
+    ms, value = aggregate(ms, M * nf, world, dist if world > 1 else None, "cuda")
+    return {"value": value, "unit": "site-steps/s", "h2d_bytes_per_step": n * 8,
+            "d2h_bytes_per_step": n * 8 + 16, "ms_per_step": ms,
             "api": "asd_ctx_step_host (pinned host buffers)"}
 
 
