@@ -88,6 +88,9 @@ struct asd_ctx {
     // adjoint work space (allocated on the first asd_ctx_loss_grad)
     std::vector<double *> adj_bufs;
     long adj_states = 0;
+    // asd_ctx_step_host: copy stream and event for the overlapped read-back
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t spins_ready = nullptr;
     int llg_kernel = ASD_LLG_STAGES;
 };
 
@@ -559,6 +562,8 @@ void destroy(asd_ctx *c) {
     for (double *q : c->adj_bufs)
         if (q) cudaFree(q);
     if (c->h_out) cudaFreeHost(c->h_out);
+    if (c->spins_ready) cudaEventDestroy(c->spins_ready);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->blas) cublasDestroy(c->blas);
     delete c;
 }
@@ -849,14 +854,24 @@ int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_s
     if (rc != ASD_OK) return rc;
     rc = run_steps(c, 1);
     if (rc != ASD_OK) return rc;
-    rc = sqt_async(c, (int)mode, c->d_out);
-    if (rc != ASD_OK) return rc;
+    // The new spins go back to the host on a second stream while S(q,t) runs:
+    // the read-back over PCIe overlaps the correlation GEMM.
+    if (!c->copy_stream) {
+        ASD_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        ASD_CUDA_TRY(cudaEventCreateWithFlags(&c->spins_ready, cudaEventDisableTiming));
+    }
     ASD_CUDA_TRY(launch_sitemajor_to_aos(c->y, c->ys_b, c->M, c->p.nfile, c->stream));
+    c->last_launches += 1;
+    ASD_CUDA_TRY(cudaEventRecord(c->spins_ready, c->stream));
+    ASD_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->spins_ready, 0));
     ASD_CUDA_TRY(cudaMemcpyAsync(spin_out, c->ys_b, (size_t)c->M * c->K * sizeof(double),
-                                 cudaMemcpyDeviceToHost, c->stream));
+                                 cudaMemcpyDeviceToHost, c->copy_stream));
+    rc = sqt_async(c, (int)mode, c->d_out);
+    const cudaError_t ec = cudaStreamSynchronize(c->copy_stream);
+    if (rc != ASD_OK) return rc;
+    ASD_CUDA_TRY(ec);
     ASD_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost,
                                  c->stream));
-    c->last_launches += 1;
     rc = read_status(c);
     if (rc != ASD_OK) return rc;
     sqt_out[0] = c->h_out[0];

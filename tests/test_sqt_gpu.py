@@ -114,3 +114,27 @@ def test_dropin_fused_dgemm_sqt_glue(oracle):
     asd.fused_dgemm(M, M, K, 1.0 / nf, a.reshape(-1), M, b, K, cf, ldc, qf, s)
     got = complex(s[0::2].sum(), s[1::2].sum()) / M
     assert rel_err(got, ref) < 1e-12
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_step_host_matches_the_device_path(pinned):
+    """asd_ctx_step_host (host spins in, one step, spins and S(q,t) out, the
+    read-back overlapped with the GEMM) equals set_spins + step + get_spins +
+    sqt, also when the input and output buffers are the same."""
+    import torch
+
+    N, nf = 24, 10
+    s0 = asd.random_spins(N, nf, seed=8)
+    p = asd.Params.make(N, nf, J1=-1.0, alpha=0.05, h=(0, 0, 0.5), dt=0.005)
+    with asd.Context(p) as a, asd.Context(p) as b:
+        a.set_spins(s0, as_origin=True)
+        b.set_spins(s0, as_origin=True)
+        buf = torch.from_numpy(s0.reshape(-1).copy())
+        if pinned:
+            buf = buf.pin_memory()
+        for step in range(3):
+            got = a.step_host(buf.data_ptr(), buf.data_ptr(), "tf32x3")
+            b.step(1)
+            want = b.sqt("tf32x3")
+            assert np.array_equal(buf.numpy().reshape(s0.shape), b.get_spins()), step
+            assert got == want
