@@ -35,42 +35,29 @@ struct V3 {
     double x, y, z;
 };
 
-// dS/dt at one (site, replica).  y is indexed as y[site*sstride + off + c].
-// Neighbour order and periodic wrap follow llg_sqt_baseline.c:59-77 with
-// nn = {(1,0), (-1,0), (0,-1), (0,1)} (:175-178); the exchange field starts
-// at 0 and accumulates t*J1 per neighbour (:52, :73-75); tau = H x S
-// (v3d_cross, v3d.h:48-53).  Extensions, each skipped when zero: J2 over the
-// diagonal neighbours (1,1), (1,-1), (-1,1), (-1,-1); the Zeeman field; and
-// Gilbert damping g * (tau + alpha * (S x tau)).
+// dS/dt from the centre spin s and its neighbours' values nb (nearest, in the
+// reference's order) and n2 (diagonal; read only when J2).  The exchange field
+// starts at 0 and accumulates t*J1 per neighbour (llg_sqt_baseline.c:52,
+// :73-75); tau = H x S (v3d_cross, v3d.h:48-53).  Extensions, each skipped
+// when zero: J2 over the diagonal neighbours, the Zeeman field, and Gilbert
+// damping g * (tau + alpha * (S x tau)).  Every kernel that evaluates the
+// right-hand side goes through this function, so all share one operation order.
 template <bool J2, bool H, bool DAMP>
-__device__ __forceinline__ V3 llg_rhs(const double *__restrict__ y, long sstride, long off,
-                                      int N, int row, int col, const LLGArgs &a) {
-    const int rp = (row + 1 == N) ? 0 : row + 1;
-    const int rm = (row == 0) ? N - 1 : row - 1;
-    const int cp = (col + 1 == N) ? 0 : col + 1;
-    const int cm = (col == 0) ? N - 1 : col - 1;
-    const long site = (long)row * N + col;
-    const double *c0 = y + site * sstride + off;
-    const double sx = c0[0], sy = c0[1], sz = c0[2];
-    const long nb[4] = {(long)rp * N + col, (long)rm * N + col, (long)row * N + cm,
-                        (long)row * N + cp};
+__device__ __forceinline__ V3 llg_rhs_vals(const V3 &s, const V3 (&nb)[4], const V3 (&n2)[4],
+                                           const LLGArgs &a) {
     double ex = 0.0, ey = 0.0, ez = 0.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const double *t = y + nb[j] * sstride + off;
-        ex = da(ex, dm(t[0], a.J1));
-        ey = da(ey, dm(t[1], a.J1));
-        ez = da(ez, dm(t[2], a.J1));
+        ex = da(ex, dm(nb[j].x, a.J1));
+        ey = da(ey, dm(nb[j].y, a.J1));
+        ez = da(ez, dm(nb[j].z, a.J1));
     }
     if (J2) {
-        const long nn2[4] = {(long)rp * N + cp, (long)rp * N + cm, (long)rm * N + cp,
-                             (long)rm * N + cm};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const double *t = y + nn2[j] * sstride + off;
-            ex = da(ex, dm(t[0], a.J2));
-            ey = da(ey, dm(t[1], a.J2));
-            ez = da(ez, dm(t[2], a.J2));
+            ex = da(ex, dm(n2[j].x, a.J2));
+            ey = da(ey, dm(n2[j].y, a.J2));
+            ez = da(ez, dm(n2[j].z, a.J2));
         }
     }
     if (H) {
@@ -79,13 +66,13 @@ __device__ __forceinline__ V3 llg_rhs(const double *__restrict__ y, long sstride
         ez = da(ez, a.hz);
     }
     V3 tau;
-    tau.x = ds(dm(ey, sz), dm(ez, sy));
-    tau.y = ds(dm(ez, sx), dm(ex, sz));
-    tau.z = ds(dm(ex, sy), dm(ey, sx));
+    tau.x = ds(dm(ey, s.z), dm(ez, s.y));
+    tau.y = ds(dm(ez, s.x), dm(ex, s.z));
+    tau.z = ds(dm(ex, s.y), dm(ey, s.x));
     if (!DAMP) return tau;
-    const double ux = ds(dm(sy, tau.z), dm(sz, tau.y));
-    const double uy = ds(dm(sz, tau.x), dm(sx, tau.z));
-    const double uz = ds(dm(sx, tau.y), dm(sy, tau.x));
+    const double ux = ds(dm(s.y, tau.z), dm(s.z, tau.y));
+    const double uy = ds(dm(s.z, tau.x), dm(s.x, tau.z));
+    const double uz = ds(dm(s.x, tau.y), dm(s.y, tau.x));
     V3 d;
     d.x = dm(a.g, da(tau.x, dm(a.alpha, ux)));
     d.y = dm(a.g, da(tau.y, dm(a.alpha, uy)));
@@ -93,3 +80,46 @@ __device__ __forceinline__ V3 llg_rhs(const double *__restrict__ y, long sstride
     return d;
 }
 
+// Periodic neighbour sites of (row, col): nearest in the reference's order
+// (1,0), (-1,0), (0,-1), (0,1) and diagonal (1,1), (1,-1), (-1,1), (-1,-1).
+__device__ __forceinline__ void neighbour_sites(int N, int row, int col, long (&nb)[4],
+                                                long (&n2)[4]) {
+    const int rp = (row + 1 == N) ? 0 : row + 1;
+    const int rm = (row == 0) ? N - 1 : row - 1;
+    const int cp = (col + 1 == N) ? 0 : col + 1;
+    const int cm = (col == 0) ? N - 1 : col - 1;
+    nb[0] = (long)rp * N + col;
+    nb[1] = (long)rm * N + col;
+    nb[2] = (long)row * N + cm;
+    nb[3] = (long)row * N + cp;
+    n2[0] = (long)rp * N + cp;
+    n2[1] = (long)rp * N + cm;
+    n2[2] = (long)rm * N + cp;
+    n2[3] = (long)rm * N + cm;
+}
+
+// dS/dt at one (site, replica).  y is indexed as y[site*sstride + off + c].
+// Neighbour order and periodic wrap follow llg_sqt_baseline.c:59-77 with
+// nn = {(1,0), (-1,0), (0,-1), (0,1)} (:175-178).
+template <bool J2, bool H, bool DAMP>
+__device__ __forceinline__ V3 llg_rhs(const double *__restrict__ y, long sstride, long off,
+                                      int N, int row, int col, const LLGArgs &a) {
+    long nbs[4], n2s[4];
+    neighbour_sites(N, row, col, nbs, n2s);
+    const double *c0 = y + ((long)row * N + col) * sstride + off;
+    const V3 s{c0[0], c0[1], c0[2]};
+    V3 nb[4], n2[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double *t = y + nbs[j] * sstride + off;
+        nb[j] = V3{t[0], t[1], t[2]};
+    }
+    if (J2) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double *t = y + n2s[j] * sstride + off;
+            n2[j] = V3{t[0], t[1], t[2]};
+        }
+    }
+    return llg_rhs_vals<J2, H, DAMP>(s, nb, n2, a);
+}

@@ -24,6 +24,10 @@ CASES = [
     (3, 1, dict(J1=1.0, J2=0.5, h=(0.1, 0.2, 0.3), alpha=0.3, dt=0.02)),   # smallest lattice
     (37, 9, dict(J1=-0.8, J2=0.2, h=(0.0, 0.3, 0.1), alpha=0.07, dt=0.01)),  # ragged tiles
     (48, 4, dict(J1=1.0, dt=0.02)),                      # several whole tiles
+    # even replica counts take the two-replicas-per-thread stage kernels
+    (14, 8, dict(J1=-1.0, J2=0.3, alpha=0.05, h=(0.1, 0.0, 0.4), dt=0.005)),
+    (11, 6, dict(J1=0.9, J2=-0.2, h=(0.0, 0.2, 0.0), dt=0.01)),
+    (7, 2, dict(J1=1.0, h=(0.0, 0.0, 0.5), alpha=0.2, dt=0.02, spin_len=1.5)),
 ]
 
 
