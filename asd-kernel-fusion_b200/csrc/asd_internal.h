@@ -151,6 +151,7 @@ struct UmmaSqtArgs {
 };
 // Returns the number of CTAs launched (partials written) or a negative error.
 int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st);
+bool umma_pairs();         // CTA-pair (cta_group::2) GEMM selected
 long umma_row_pad(long M);   // rows/cols padded to the tile multiple
 cudaError_t launch_mbar_timeout_probe(uint32_t limit, unsigned *status, cudaStream_t st);
 cudaError_t launch_grid_barrier_probe(void *bs, unsigned *status, cudaStream_t st);

@@ -92,6 +92,20 @@ struct asd_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t spins_ready = nullptr;
     int llg_kernel = ASD_LLG_STAGES;
+    // Pipelining of asd_ctx_step behind asd_ctx_sqt_async: once a split-mode
+    // S(q,t) has turned y into its GEMM operands, the GEMM reads none of the
+    // LLG buffers, so the next RK4 step may run beside it on llg_stream.
+    // y_free is recorded on the ctx stream right after the split; armed says
+    // that nothing touching y, ys_a, ys_b or acc has been enqueued since.
+    // The split-mode GEMM and its finalize run on gemm_stream, created with
+    // the greatest priority, so that when the split completes the block
+    // scheduler places the persistent GEMM's CTAs before the LLG blocks (the
+    // GEMM takes one CTA per SM and leaves room for four 256-thread LLG
+    // blocks beside it).  Both side streams are forked from and joined back
+    // into the ctx stream with events, so the ctx stream orders everything.
+    cudaStream_t llg_stream = nullptr, gemm_stream = nullptr;
+    cudaEvent_t y_free = nullptr, llg_done = nullptr, gemm_done = nullptr;
+    bool y_free_armed = false;
 };
 
 namespace {
@@ -136,6 +150,58 @@ int ensure_part(asd_ctx *c, long n) {
 int kp_for(int kind, int K) {
     const int ke = (kind == 2) ? 64 : 32;
     return (K + ke - 1) / ke * ke;
+}
+
+// Prologue of every entry point that may enqueue work: select the device and
+// forget the early y_free point (the caller may touch the LLG buffers next).
+cudaError_t enter(asd_ctx *c) {
+    c->y_free_armed = false;
+    return cudaSetDevice(c->device);
+}
+
+bool stream_capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return true;  // unknown: take the fully ordered path
+    }
+    return cs != cudaStreamCaptureStatusNone;
+}
+
+int ensure_llg_stream(asd_ctx *c) {
+    if (c->llg_stream) return ASD_OK;
+    int least = 0, greatest = 0;
+    ASD_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    ASD_CUDA_TRY(cudaStreamCreateWithPriority(&c->gemm_stream, cudaStreamNonBlocking, greatest));
+    ASD_CUDA_TRY(cudaStreamCreateWithPriority(&c->llg_stream, cudaStreamNonBlocking, least));
+    ASD_CUDA_TRY(cudaEventCreateWithFlags(&c->y_free, cudaEventDisableTiming));
+    ASD_CUDA_TRY(cudaEventCreateWithFlags(&c->llg_done, cudaEventDisableTiming));
+    ASD_CUDA_TRY(cudaEventCreateWithFlags(&c->gemm_done, cudaEventDisableTiming));
+    return ASD_OK;
+}
+
+// Record the point on the ctx stream after which no enqueued work reads or
+// writes the LLG buffers (called between the split and the GEMM) and fork
+// gemm_stream from it.  Returns the stream the GEMM is to be launched on:
+// gemm_stream, or the ctx stream itself while it is being captured.
+int arm_y_free(asd_ctx *c, cudaStream_t *gemm) {
+    *gemm = c->stream;
+    if (stream_capturing(c->stream)) return ASD_OK;
+    int rc = ensure_llg_stream(c);
+    if (rc != ASD_OK) return rc;
+    ASD_CUDA_TRY(cudaEventRecord(c->y_free, c->stream));
+    ASD_CUDA_TRY(cudaStreamWaitEvent(c->gemm_stream, c->y_free, 0));
+    c->y_free_armed = true;
+    *gemm = c->gemm_stream;
+    return ASD_OK;
+}
+
+// Join gemm_stream back into the ctx stream.
+int join_gemm(asd_ctx *c, cudaStream_t gemm) {
+    if (gemm == c->stream) return ASD_OK;
+    ASD_CUDA_TRY(cudaEventRecord(c->gemm_done, gemm));
+    ASD_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->gemm_done, 0));
+    return ASD_OK;
 }
 
 int refresh_origin(asd_ctx *c) {
@@ -267,6 +333,9 @@ int sqt_split(asd_ctx *c, int kind, double *d_out) {
     }
     int rc = ensure_part(c, c->num_sms);
     if (rc != ASD_OK) return rc;
+    cudaStream_t gemm = c->stream;
+    rc = arm_y_free(c, &gemm);
+    if (rc != ASD_OK) return rc;
     UmmaSqtArgs u{};
     u.kind = kind;
     u.M = c->M;
@@ -286,11 +355,16 @@ int sqt_split(asd_ctx *c, int kind, double *d_out) {
     // Same number of tensor-core accumulation steps per chunk for both kinds
     // (TF32 MMAs take 8 K elements per step, BF16 ones 16).
     u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
-    const int grid = launch_umma_sqt(u, c->stream);
-    if (grid < 0) return grid;
-    ASD_CUDA_TRY(launch_finalize(c->part, grid, 1.0 / (double)c->M, d_out, c->stream));
-    c->last_launches += 2;
-    return ASD_OK;
+    const int grid = launch_umma_sqt(u, gemm);
+    if (grid >= 0) {
+        const cudaError_t e = launch_finalize(c->part, grid, 1.0 / (double)c->M, d_out, gemm);
+        if (e != cudaSuccess) rc = cuda_fail(e, "launch_finalize");
+        c->last_launches += 2;
+    } else {
+        rc = grid;
+    }
+    const int jrc = join_gemm(c, gemm);  // joined on the error paths too
+    return rc != ASD_OK ? rc : jrc;
 }
 
 int sqt_async(asd_ctx *c, int mode, double *d_out) {
@@ -564,6 +638,17 @@ void destroy(asd_ctx *c) {
     if (c->h_out) cudaFreeHost(c->h_out);
     if (c->spins_ready) cudaEventDestroy(c->spins_ready);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->llg_stream) {
+        cudaStreamSynchronize(c->llg_stream);
+        cudaStreamDestroy(c->llg_stream);
+    }
+    if (c->gemm_stream) {
+        cudaStreamSynchronize(c->gemm_stream);
+        cudaStreamDestroy(c->gemm_stream);
+    }
+    if (c->gemm_done) cudaEventDestroy(c->gemm_done);
+    if (c->y_free) cudaEventDestroy(c->y_free);
+    if (c->llg_done) cudaEventDestroy(c->llg_done);
     if (c->blas) cublasDestroy(c->blas);
     delete c;
 }
@@ -715,6 +800,7 @@ int asd_ctx_destroy(asd_ctx *ctx) {
 
 int asd_ctx_set_stream(asd_ctx *c, void *stream) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    c->y_free_armed = false;
     c->stream = (cudaStream_t)stream;
     if (c->blas) cublasSetStream(c->blas, c->stream);
     return ASD_OK;
@@ -728,7 +814,7 @@ int asd_ctx_get_params(const asd_ctx *c, asd_params *p) {
 
 int asd_ctx_set_spins(asd_ctx *c, const double *spin_aos, int as_origin) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
     int rc = set_spins_common(c, spin_aos, true, as_origin);
     if (rc != ASD_OK) return rc;
@@ -738,7 +824,7 @@ int asd_ctx_set_spins(asd_ctx *c, const double *spin_aos, int as_origin) {
 
 int asd_ctx_set_spins_device(asd_ctx *c, const double *d_spin_aos, int as_origin) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
     return set_spins_common(c, d_spin_aos, false, as_origin);
 }
@@ -746,7 +832,7 @@ int asd_ctx_set_spins_device(asd_ctx *c, const double *d_spin_aos, int as_origin
 int asd_ctx_get_spins(asd_ctx *c, double *spin_aos) {
     if (!c || !spin_aos) return fail(ASD_ERR_INVALID, "NULL argument");
     if (!c->has_state) return fail(ASD_ERR_STATE, "no spins set");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     ASD_CUDA_TRY(launch_sitemajor_to_aos(c->y, c->ys_b, c->M, c->p.nfile, c->stream));
     ASD_CUDA_TRY(cudaMemcpyAsync(spin_aos, c->ys_b, (size_t)c->M * c->K * sizeof(double),
                                  cudaMemcpyDeviceToHost, c->stream));
@@ -757,7 +843,7 @@ int asd_ctx_get_spins(asd_ctx *c, double *spin_aos) {
 int asd_ctx_get_spins_device(asd_ctx *c, double *d_spin_aos) {
     if (!c || !d_spin_aos) return fail(ASD_ERR_INVALID, "NULL argument");
     if (!c->has_state) return fail(ASD_ERR_STATE, "no spins set");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     ASD_CUDA_TRY(launch_sitemajor_to_aos(c->y, d_spin_aos, c->M, c->p.nfile, c->stream));
     return ASD_OK;
 }
@@ -766,21 +852,32 @@ int asd_ctx_step(asd_ctx *c, int nsteps) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
     if (nsteps < 0) return fail(ASD_ERR_INVALID, "nsteps < 0");
     if (!c->has_state) return fail(ASD_ERR_STATE, "no spins set");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    const bool overlap = c->y_free_armed && nsteps > 0 && !stream_capturing(c->stream);
+    ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
-    return run_steps(c, nsteps);
+    if (!overlap) return run_steps(c, nsteps);
+    // The steps wait only for the split of the last S(q,t), run on llg_stream
+    // beside its GEMM, and the ctx stream joins them before its next work.
+    const cudaStream_t main = c->stream;
+    ASD_CUDA_TRY(cudaStreamWaitEvent(c->llg_stream, c->y_free, 0));
+    c->stream = c->llg_stream;
+    const int rc = run_steps(c, nsteps);
+    c->stream = main;
+    ASD_CUDA_TRY(cudaEventRecord(c->llg_done, c->llg_stream));
+    ASD_CUDA_TRY(cudaStreamWaitEvent(main, c->llg_done, 0));
+    return rc;
 }
 
 int asd_ctx_sqt_async(asd_ctx *c, asd_sqt_mode mode, double *d_out) {
     if (!c || !d_out) return fail(ASD_ERR_INVALID, "NULL argument");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
     return sqt_async(c, (int)mode, d_out);
 }
 
 int asd_ctx_sqt_grid_async(asd_ctx *c, asd_sqt_mode mode, double *d_out) {
     if (!c || !d_out) return fail(ASD_ERR_INVALID, "NULL argument");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
     return sqt_grid_async(c, (int)mode, d_out);
 }
@@ -788,7 +885,7 @@ int asd_ctx_sqt_grid_async(asd_ctx *c, asd_sqt_mode mode, double *d_out) {
 int asd_ctx_loss_grad(asd_ctx *c, int nsteps, int stride, int checkpoint, const double *target,
                       double *loss, double *grad, double *sqt_out) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     return loss_grad(c, nsteps, stride, checkpoint, target, loss, grad, sqt_out);
 }
 
@@ -809,7 +906,7 @@ int asd_ctx_set_params(asd_ctx *c, const asd_params *p) {
             u[i] = make_double2(std::cos(th), -std::sin(th));
             w[i] = make_double2(std::cos(th), std::sin(th));
         }
-        ASD_CUDA_TRY(cudaSetDevice(c->device));
+        ASD_CUDA_TRY(enter(c));
         ASD_CUDA_TRY(cudaMemcpy(c->uphase, u.data(), (size_t)c->M * sizeof(double2), cudaMemcpyHostToDevice));
         ASD_CUDA_TRY(cudaMemcpy(c->wphase, w.data(), (size_t)c->M * sizeof(double2), cudaMemcpyHostToDevice));
         if (c->has_origin) return refresh_origin(c);
@@ -819,7 +916,7 @@ int asd_ctx_set_params(asd_ctx *c, const asd_params *p) {
 
 int asd_ctx_sqt_grid(asd_ctx *c, asd_sqt_mode mode, double *out) {
     if (!c || !out) return fail(ASD_ERR_INVALID, "NULL argument");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
     const size_t bytes = (size_t)c->M * 2 * sizeof(double);
     int rc;
@@ -831,7 +928,7 @@ int asd_ctx_sqt_grid(asd_ctx *c, asd_sqt_mode mode, double *out) {
 
 int asd_ctx_sqt(asd_ctx *c, asd_sqt_mode mode, double out[2]) {
     if (!c || !out) return fail(ASD_ERR_INVALID, "NULL argument");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
     int rc = sqt_async(c, (int)mode, c->d_out);
     if (rc != ASD_OK) return rc;
@@ -848,7 +945,7 @@ int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_s
                       double sqt_out[2]) {
     if (!c || !spin_in || !spin_out || !sqt_out) return fail(ASD_ERR_INVALID, "NULL argument");
     if (!c->has_origin) return fail(ASD_ERR_STATE, "set the origin (t = 0 spins) first");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
     int rc = set_spins_common(c, spin_in, true, 0);
     if (rc != ASD_OK) return rc;
@@ -867,6 +964,7 @@ int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_s
     ASD_CUDA_TRY(cudaMemcpyAsync(spin_out, c->ys_b, (size_t)c->M * c->K * sizeof(double),
                                  cudaMemcpyDeviceToHost, c->copy_stream));
     rc = sqt_async(c, (int)mode, c->d_out);
+    c->y_free_armed = false;  // ys_b is still being read on copy_stream
     const cudaError_t ec = cudaStreamSynchronize(c->copy_stream);
     if (rc != ASD_OK) return rc;
     ASD_CUDA_TRY(ec);
@@ -897,7 +995,7 @@ int asd_ctx_last_launches(const asd_ctx *c) { return c ? c->last_launches : 0; }
 
 int asd_ctx_check_device_status(asd_ctx *c) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
-    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    ASD_CUDA_TRY(enter(c));
     return read_status(c);
 }
 

@@ -40,13 +40,18 @@ constexpr int GROUP_M = 16;
 constexpr int kGridMaxBins = 4096;  // q-grid histogram: N*N FP32 bins in shared memory
 
 // Pipeline geometry.  ROWB = bytes of K per operand row in one pipeline
-// stage (= the swizzle width): 64 -> 4 stages of 48 KB, 128 -> 2 stages of
-// 96 KB.  Smaller stages let a refill start earlier and hide more latency.
-template <int ROWB>
+// stage (= the swizzle width).  Single CTA (PAIR = false): a 128 x 256 tile
+// per CTA, ROWB 64 -> 4 stages of 48 KB, 128 -> 2 stages of 96 KB.  CTA pair
+// (PAIR = true): a 256 x 256 tile per pair of SMs, each CTA loading 128 rows
+// of A and 128 of the 256 B rows, so a stage is 64 KB per SM for the same
+// MMA work per SM as the single-CTA 96 KB stage, and 3 stages fit.
+template <int ROWB, bool PAIR = false>
 struct Geo {
-    static constexpr int STAGES = (ROWB == 64) ? 4 : 2;
+    static constexpr int STAGES = PAIR ? 3 : ((ROWB == 64) ? 4 : 2);
+    static constexpr int BN_LOC = PAIR ? BN / 2 : BN;  // B rows loaded by one CTA
+    static constexpr int TILE_M = PAIR ? 2 * BM : BM;  // accumulator rows per tile
     static constexpr int A_TILE = BM * ROWB;
-    static constexpr int B_TILE = BN * ROWB;
+    static constexpr int B_TILE = BN_LOC * ROWB;
     static constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
     static constexpr int KSTEPS = ROWB / 32;  // 32-byte MMA k steps per stage
     static constexpr int PIPE_BYTES = STAGES * STAGE_BYTES;
@@ -66,9 +71,9 @@ struct SmemTail {
     double red[2][4];
 };
 
-template <int ROWB>
+template <int ROWB, bool PAIR = false>
 constexpr int smem_bytes() {
-    return 1024 /*alignment slack*/ + Geo<ROWB>::PIPE_BYTES + Geo<ROWB>::TABLE_BYTES +
+    return 1024 /*alignment slack*/ + Geo<ROWB, PAIR>::PIPE_BYTES + Geo<ROWB, PAIR>::TABLE_BYTES +
            (int)((sizeof(SmemTail) + 15) & ~size_t(15));
 }
 
@@ -106,8 +111,11 @@ __device__ __forceinline__ bool epilogue_sync(uint64_t *bar, uint32_t &phase,
 //              alpha C_ij - m_i.z_j goes to bin (r_i - r_j) mod N of a
 //              per-tile FP32 shared histogram, flushed after each tile into
 //              this CTA's FP64 histogram gpart[blockIdx.x][N*N]
+// PAIR: launched in clusters of two CTAs that share every tcgen05.mma
+// (cta_group::2, M = 256); tiles are 256 x 256, num_m counts 256-row blocks,
+// and each CTA's epilogue handles its own 128 rows of the tile.
 constexpr int EPI_PHASE = 0, EPI_STORE = 1, EPI_GRID = 2;
-template <int KIND, int EPI, int ROWB>
+template <int KIND, int EPI, int ROWB, bool PAIR>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     umma_sqt_kernel(const __grid_constant__ CUtensorMap tm_ah,
                     const __grid_constant__ CUtensorMap tm_al,
@@ -118,7 +126,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     const float *__restrict__ col1, float alpha, double2 *__restrict__ part,
                     unsigned *__restrict__ status, float *__restrict__ dbg_c, long dbg_ldc,
                     int lat_n, long n_sites, double *__restrict__ gpart) {
-    using G = Geo<ROWB>;
+    using G = Geo<ROWB, PAIR>;
     constexpr bool STORE = (EPI == EPI_STORE);
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -132,6 +140,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
     const int num_tiles = num_m * num_n;
+    // Tile schedule: single CTAs stride over tiles by CTA, pairs by cluster.
+    const uint32_t rank = PAIR ? ptx::cluster_ctarank() : 0u;
+    const bool leader = (rank == 0);
+    const int first_tile = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const int tile_step = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < G::STAGES; ++s) {
@@ -140,7 +153,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             ptx::mbar_init(&tail->tfull[b], 1);
-            ptx::mbar_init(&tail->tempty[b], 4);
+            ptx::mbar_init(&tail->tempty[b], PAIR ? 8 : 4);  // epilogue warps (of both CTAs)
         }
         ptx::mbar_init(&tail->drain, 1);
         ptx::mbar_init(&tail->ebar, 4);
@@ -148,11 +161,22 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         ptx::fence_mbar_init();
     }
     if (warp == 0) {
-        ptx::tmem_alloc(&tail->tmem_base, TMEM_COLS);
-        ptx::tmem_relinquish();
+        if (PAIR) {
+            ptx::tmem_alloc_pair(&tail->tmem_base, TMEM_COLS);
+            ptx::tmem_relinquish_pair();
+        } else {
+            ptx::tmem_alloc(&tail->tmem_base, TMEM_COLS);
+            ptx::tmem_relinquish();
+        }
     }
     ptx::tc_fence_before();
-    __syncthreads();
+    // Pairs: the peer's barriers must be initialised before this CTA's
+    // loads and commits reach them.  Every CTA of a cluster is resident
+    // together, so this barrier cannot wait on a CTA that never starts.
+    if (PAIR)
+        ptx::cluster_sync();
+    else
+        __syncthreads();
     ptx::tc_fence_after();
     const uint32_t tmem_base = tail->tmem_base;
     volatile int *abort_flag = &tail->abort_flag;
@@ -169,9 +193,13 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             bool issued[G::STAGES] = {};
             uint32_t issued_parity[G::STAGES] = {};
             bool ok = true;
-            for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+            // Pairs: both CTAs' bytes complete on the leader's full barrier.
+            const uint32_t full0 = PAIR ? ptx::mapa(ptx::smem_u32(&tail->full[0]), 0u) : 0u;
+            for (int tile = first_tile; tile < num_tiles && ok; tile += tile_step) {
                 int mb, nb;
                 tile_coords(tile, num_m, num_n, mb, nb);
+                const int arow = mb * G::TILE_M + (int)rank * BM;
+                const int brow = nb * BN + (int)rank * G::BN_LOC;
                 for (int kb = 0; kb < num_kb; ++kb) {
                     if (!ptx::mbar_wait_bounded(&tail->empty[stage], phase ^ 1u, abort_flag,
                                                 WAIT_LIMIT)) {
@@ -180,13 +208,23 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         break;
                     }
                     uint8_t *st = smem + stage * G::STAGE_BYTES;
-                    ptx::mbar_arrive_expect_tx(&tail->full[stage], G::STAGE_BYTES);
                     const int x = kb * KE;
-                    ptx::tma_load_2d(st, &tm_ah, &tail->full[stage], x, mb * BM);
-                    ptx::tma_load_2d(st + G::A_TILE, &tm_al, &tail->full[stage], x, mb * BM);
-                    ptx::tma_load_2d(st + 2 * G::A_TILE, &tm_bh, &tail->full[stage], x, nb * BN);
-                    ptx::tma_load_2d(st + 2 * G::A_TILE + G::B_TILE, &tm_bl, &tail->full[stage],
-                                     x, nb * BN);
+                    if (PAIR) {
+                        if (leader)
+                            ptx::mbar_arrive_expect_tx(&tail->full[stage], 2 * G::STAGE_BYTES);
+                        const uint32_t fb = full0 + (uint32_t)(stage * sizeof(uint64_t));
+                        ptx::tma_load_2d_pair(st, &tm_ah, fb, x, arow);
+                        ptx::tma_load_2d_pair(st + G::A_TILE, &tm_al, fb, x, arow);
+                        ptx::tma_load_2d_pair(st + 2 * G::A_TILE, &tm_bh, fb, x, brow);
+                        ptx::tma_load_2d_pair(st + 2 * G::A_TILE + G::B_TILE, &tm_bl, fb, x, brow);
+                    } else {
+                        ptx::mbar_arrive_expect_tx(&tail->full[stage], G::STAGE_BYTES);
+                        ptx::tma_load_2d(st, &tm_ah, &tail->full[stage], x, arow);
+                        ptx::tma_load_2d(st + G::A_TILE, &tm_al, &tail->full[stage], x, arow);
+                        ptx::tma_load_2d(st + 2 * G::A_TILE, &tm_bh, &tail->full[stage], x, brow);
+                        ptx::tma_load_2d(st + 2 * G::A_TILE + G::B_TILE, &tm_bl,
+                                         &tail->full[stage], x, brow);
+                    }
                     issued[stage] = true;
                     issued_parity[stage] = phase;
                     if (++stage == G::STAGES) {
@@ -197,9 +235,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             }
             // Never leave the CTA with bulk copies still landing in shared
             // memory: wait (bounded, ignoring the abort flag) for the last
-            // fill of every stage.
+            // fill of every stage.  In a pair the leader's full barriers
+            // count both CTAs' bytes, so the leader waits for both, and the
+            // closing cluster barrier keeps the peer until then.
             for (int s = 0; s < G::STAGES; ++s) {
-                if (!issued[s]) continue;
+                if (!issued[s] || !leader) continue;
                 uint32_t i = 0;
                 while (!ptx::mbar_try_wait(&tail->full[s], issued_parity[s]) && i < WAIT_LIMIT) {
                     ++i;
@@ -209,15 +249,26 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             }
         }
     } else if (warp == 1) {
-        if (lane == 0) {
-            constexpr uint32_t IDESC = ptx::umma_idesc(KIND == 2 ? 1u : 2u, BM, BN);
+        // Pairs: only the leader issues; its commits arrive on the barriers
+        // of both CTAs (own address, and the peer's through mapa).
+        if (lane == 0 && leader) {
+            constexpr uint32_t IDESC = ptx::umma_idesc(KIND == 2 ? 1u : 2u, G::TILE_M, BN);
+            auto commit_both = [&](uint64_t *bar) {
+                if (PAIR) {
+                    const uint32_t a = ptx::smem_u32(bar);
+                    ptx::umma_commit_pair(a);
+                    ptx::umma_commit_pair(ptx::mapa(a, 1u));
+                } else {
+                    ptx::umma_commit(bar);
+                }
+            };
             int stage = 0;
             uint32_t phase = 0;
             int abuf = 0;
             uint32_t aphase = 0;
             bool ok = true;
             const uint32_t smem_base = ptx::smem_u32(smem);
-            for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+            for (int tile = first_tile; tile < num_tiles && ok; tile += tile_step) {
                 // K is accumulated in chunks of kb_per_chunk k blocks, each
                 // into a fresh TMEM buffer: the tensor core's FP32
                 // accumulation loses precision with the number of
@@ -250,7 +301,15 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         for (int kk = 0; kk < G::KSTEPS; ++kk) {
                             const uint64_t adv = (uint64_t)(2 * kk);  // 32 bytes per k step
                             const uint32_t accum = (kb > kb0 || kk > 0) ? 1u : 0u;
-                            if (KIND == 2) {
+                            if (PAIR && KIND == 2) {
+                                ptx::umma_f16_pair(d_tmem, dah + adv, dbh + adv, IDESC, accum);
+                                ptx::umma_f16_pair(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
+                                ptx::umma_f16_pair(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
+                            } else if (PAIR) {
+                                ptx::umma_tf32_pair(d_tmem, dah + adv, dbh + adv, IDESC, accum);
+                                ptx::umma_tf32_pair(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
+                                ptx::umma_tf32_pair(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
+                            } else if (KIND == 2) {
                                 ptx::umma_f16(d_tmem, dah + adv, dbh + adv, IDESC, accum);
                                 ptx::umma_f16(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
                                 ptx::umma_f16(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
@@ -260,14 +319,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                                 ptx::umma_tf32(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
                             }
                         }
-                        ptx::umma_commit(&tail->empty[stage]);
+                        commit_both(&tail->empty[stage]);
                         if (++stage == G::STAGES) {
                             stage = 0;
                             phase ^= 1u;
                         }
                     }
                     if (!ok) break;
-                    ptx::umma_commit(&tail->tfull[abuf]);
+                    commit_both(&tail->tfull[abuf]);
                     if (++abuf == 2) {
                         abuf = 0;
                         aphase ^= 1u;
@@ -275,7 +334,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 }
             }
             // Wait for every issued MMA before TMEM can be released.
-            ptx::umma_commit(&tail->drain);
+            if (PAIR)
+                ptx::umma_commit_pair(ptx::smem_u32(&tail->drain));
+            else
+                ptx::umma_commit(&tail->drain);
             uint32_t i = 0;
             while (!ptx::mbar_try_wait(&tail->drain, 0u) && i < WAIT_LIMIT) {
                 ++i;
@@ -300,10 +362,12 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 gp[b] = 0.0;
             }
         }
-        for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++tcount) {
+        // Pairs: the accumulator buffers are released on the leader's tempty.
+        const uint32_t tempty0 = PAIR ? ptx::mapa(ptx::smem_u32(&tail->tempty[0]), 0u) : 0u;
+        for (int tile = first_tile; tile < num_tiles; tile += tile_step, ++tcount) {
             int mb, nb;
             tile_coords(tile, num_m, num_n, mb, nb);
-            const long i = (long)mb * BM + rloc;
+            const long i = (long)mb * G::TILE_M + (long)rank * BM + rloc;
             const long j0 = (long)nb * BN;
             const int tb = tcount & 1;
             float2 *w_tab = tab_w + tb * BN;
@@ -415,7 +479,12 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 }
                 ptx::tc_fence_before();
                 __syncwarp();
-                if (lane == 0) ptx::mbar_arrive(&tail->tempty[abuf]);
+                if (lane == 0) {
+                    if (PAIR)
+                        ptx::mbar_arrive_remote(tempty0 + (uint32_t)(abuf * sizeof(uint64_t)));
+                    else
+                        ptx::mbar_arrive(&tail->tempty[abuf]);
+                }
                 if (++abuf == 2) {
                     abuf = 0;
                     aphase ^= 1u;
@@ -453,14 +522,25 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     }
 
     ptx::tc_fence_before();
-    __syncthreads();
+    // Pairs: neither CTA leaves (or frees TMEM) while the leader's MMAs may
+    // still read the peer's shared memory or write its TMEM: the leader's
+    // MMA thread has drained them before it arrives here.
+    if (PAIR)
+        ptx::cluster_sync();
+    else
+        __syncthreads();
     ptx::tc_fence_after();
     if (threadIdx.x == 0 && EPI == EPI_PHASE) {
         const double re = (tail->red[0][0] + tail->red[0][1]) + (tail->red[0][2] + tail->red[0][3]);
         const double im = (tail->red[1][0] + tail->red[1][1]) + (tail->red[1][2] + tail->red[1][3]);
         part[blockIdx.x] = make_double2(re, im);
     }
-    if (warp == 0) ptx::tmem_dealloc(tmem_base, TMEM_COLS);
+    if (warp == 0) {
+        if (PAIR)
+            ptx::tmem_dealloc_pair(tmem_base, TMEM_COLS);
+        else
+            ptx::tmem_dealloc(tmem_base, TMEM_COLS);
+    }
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
@@ -501,6 +581,18 @@ int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int
 
 long umma_row_pad(long M) { return (M + BN - 1) / BN * BN; }
 
+bool umma_pairs() {
+    // ASD_UMMA_PAIR=1 selects the CTA-pair (cta_group::2) kernel.  Measured on
+    // B200 it is within a few per cent of the single-CTA kernel (faster for
+    // TF32x3 at 16384 sites, slower for BF16x3): both already keep the tensor
+    // pipe near its ceiling, so the single-CTA form stays the default.
+    static bool on = [] {
+        const char *e = getenv("ASD_UMMA_PAIR");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
 int umma_row_bytes() {
     // Pipeline stage width: 128 (2 x 96 KB stages, the default) or 64
     // (4 x 48 KB stages, ASD_UMMA_ROWB=64).  Measured on B200, the two-stage
@@ -520,52 +612,72 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     if (((uintptr_t)a.a_hi | (uintptr_t)a.a_lo | (uintptr_t)a.b_hi | (uintptr_t)a.b_lo) & 15)
         return fail(ASD_ERR_INVALID, "operand base not 16-byte aligned");
     const int rowb = umma_row_bytes();
+    const bool pair = umma_pairs() && rowb == 128;
     const int ke = rowb / esize;  // K elements per pipeline stage
+    const int tile_m = pair ? 2 * BM : BM;
+    const int b_rows = pair ? BN / 2 : BN;  // B rows one CTA loads per tile
     CUtensorMap tah, tal, tbh, tbl;
     int rc;
     if ((rc = make_tmap(&tah, a.a_hi, a.kind, Mp, a.Kp, BM, rowb)) != ASD_OK) return rc;
     if ((rc = make_tmap(&tal, a.a_lo, a.kind, Mp, a.Kp, BM, rowb)) != ASD_OK) return rc;
-    if ((rc = make_tmap(&tbh, a.b_hi, a.kind, Mp, a.Kp, BN, rowb)) != ASD_OK) return rc;
-    if ((rc = make_tmap(&tbl, a.b_lo, a.kind, Mp, a.Kp, BN, rowb)) != ASD_OK) return rc;
-    const int num_m = (int)(Mp / BM), num_n = (int)(Mp / BN), num_kb = a.Kp / ke;
+    if ((rc = make_tmap(&tbh, a.b_hi, a.kind, Mp, a.Kp, b_rows, rowb)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tbl, a.b_lo, a.kind, Mp, a.Kp, b_rows, rowb)) != ASD_OK) return rc;
+    const int num_m = (int)(Mp / tile_m), num_n = (int)(Mp / BN), num_kb = a.Kp / ke;
     const int tiles = num_m * num_n;
-    const int grid = tiles < a.num_sms ? tiles : a.num_sms;
     // k blocks per accumulation chunk: chunk_k elements of K (0 = all of K)
     int kpc = a.chunk_k > 0 ? (a.chunk_k + ke - 1) / ke : num_kb;
     if (kpc < 1) kpc = 1;
     if (kpc > num_kb) kpc = num_kb;
+    int grid = 0;
     cudaError_t e;
     auto go = [&](auto kern, int smem) {
         cudaError_t r =
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (r == cudaSuccess)
-            kern<<<grid, NUM_THREADS, smem, st>>>(tah, tal, tbh, tbl, num_m, num_n, num_kb, kpc,
-                                                  a.row4, a.row1, a.col4, a.col1, a.alpha, a.part,
-                                                  a.status, a.dbg_c, a.dbg_ldc, a.lat_n, a.M,
-                                                  a.gpart);
-        return r;
+        if (r != cudaSuccess) return r;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.blockDim = dim3(NUM_THREADS, 1, 1);
+        cfg.dynamicSmemBytes = (size_t)smem;
+        cfg.stream = st;
+        if (pair) {
+            // One cluster of two CTAs per SM pair, as many as fit at once.
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = 2;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            cfg.gridDim = dim3(2, 1, 1);
+            int clusters = 0;
+            r = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
+            if (r != cudaSuccess) return r;
+            if (clusters < 1) return cudaErrorInvalidConfiguration;
+            if (clusters > tiles) clusters = tiles;
+            grid = 2 * clusters;
+        } else {
+            grid = tiles < a.num_sms ? tiles : a.num_sms;
+        }
+        cfg.gridDim = dim3((unsigned)grid, 1, 1);
+        return cudaLaunchKernelEx(&cfg, kern, tah, tal, tbh, tbl, num_m, num_n, num_kb, kpc,
+                                  a.row4, a.row1, a.col4, a.col1, a.alpha, a.part, a.status,
+                                  a.dbg_c, a.dbg_ldc, a.lat_n, a.M, a.gpart);
     };
     const int epi = a.dbg_c ? EPI_STORE : (a.gpart ? EPI_GRID : EPI_PHASE);
     if (epi == EPI_GRID && (a.lat_n < 1 || (long)a.lat_n * a.lat_n != a.M ||
                             a.lat_n * a.lat_n > kGridMaxBins))
         return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t) supports N*N <= %d sites", kGridMaxBins);
     const int hist_bytes = (epi == EPI_GRID) ? 4 * a.lat_n * a.lat_n + 16 : 0;
-#define ASD_UMMA_GO(K, E, R) go(umma_sqt_kernel<K, E, R>, smem_bytes<R>() + hist_bytes)
-    if (rowb == 64) {
-        if (a.kind == 2)
-            e = epi == EPI_STORE ? ASD_UMMA_GO(2, EPI_STORE, 64)
-              : epi == EPI_GRID  ? ASD_UMMA_GO(2, EPI_GRID, 64) : ASD_UMMA_GO(2, EPI_PHASE, 64);
-        else
-            e = epi == EPI_STORE ? ASD_UMMA_GO(1, EPI_STORE, 64)
-              : epi == EPI_GRID  ? ASD_UMMA_GO(1, EPI_GRID, 64) : ASD_UMMA_GO(1, EPI_PHASE, 64);
-    } else {
-        if (a.kind == 2)
-            e = epi == EPI_STORE ? ASD_UMMA_GO(2, EPI_STORE, 128)
-              : epi == EPI_GRID  ? ASD_UMMA_GO(2, EPI_GRID, 128) : ASD_UMMA_GO(2, EPI_PHASE, 128);
-        else
-            e = epi == EPI_STORE ? ASD_UMMA_GO(1, EPI_STORE, 128)
-              : epi == EPI_GRID  ? ASD_UMMA_GO(1, EPI_GRID, 128) : ASD_UMMA_GO(1, EPI_PHASE, 128);
-    }
+#define ASD_UMMA_GO(K, E, R, P) go(umma_sqt_kernel<K, E, R, P>, smem_bytes<R, P>() + hist_bytes)
+#define ASD_UMMA_EPI(K, R, P)                                                                 \
+    (epi == EPI_STORE ? ASD_UMMA_GO(K, EPI_STORE, R, P)                                         \
+     : epi == EPI_GRID ? ASD_UMMA_GO(K, EPI_GRID, R, P) : ASD_UMMA_GO(K, EPI_PHASE, R, P))
+    if (pair)
+        e = (a.kind == 2) ? ASD_UMMA_EPI(2, 128, true) : ASD_UMMA_EPI(1, 128, true);
+    else if (rowb == 64)
+        e = (a.kind == 2) ? ASD_UMMA_EPI(2, 64, false) : ASD_UMMA_EPI(1, 64, false);
+    else
+        e = (a.kind == 2) ? ASD_UMMA_EPI(2, 128, false) : ASD_UMMA_EPI(1, 128, false);
+#undef ASD_UMMA_EPI
 #undef ASD_UMMA_GO
     if (e != cudaSuccess) return cuda_fail(e, "umma_sqt setup");
     e = cudaGetLastError();

@@ -138,3 +138,41 @@ def test_step_host_matches_the_device_path(pinned):
             want = b.sqt("tf32x3")
             assert np.array_equal(buf.numpy().reshape(s0.shape), b.get_spins()), step
             assert got == want
+
+
+@pytest.mark.parametrize("mode", ["tf32x3", "bf16x3"])
+@pytest.mark.parametrize("kernel", ["stages", "fused"])
+def test_step_pipelined_behind_the_split_gemm(oracle, mode, kernel):
+    """asd_ctx_step after a split-mode asd_ctx_sqt_async runs the next RK4 step
+    beside that S(q,t)'s GEMM.  The pipelined sequence must give the same
+    S(q,t) values and spins, bit for bit, as the fully ordered one (any other
+    entry point in between, here asd_ctx_set_stream, orders them), and the
+    spins must equal the oracle's FP64 trajectory."""
+    import torch
+
+    N, nf, n = 64, 48, 6
+    s0 = asd.random_spins(N, nf, seed=21)
+    p = asd.Params.make(N, nf, J1=-1.0, J2=0.1, alpha=0.05, h=(0, 0, 0.5), dt=0.005, vx=3, vy=1)
+    stream = torch.cuda.current_stream()
+    outs = []
+    spins = []
+    for ordered in (False, True):
+        d = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+        with asd.Context(p, modes=[mode]) as ctx:
+            ctx.set_llg_kernel(kernel)
+            ctx.set_stream(stream.cuda_stream)
+            ctx.set_spins(s0, as_origin=True)
+            for i in range(n):
+                if ordered:
+                    ctx.set_stream(stream.cuda_stream)
+                ctx.step(1)
+                ctx.sqt_async(mode, d.data_ptr() + 16 * i)
+            torch.cuda.synchronize()
+            ctx.check_device_status()
+            spins.append(ctx.get_spins())
+        outs.append(d.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(spins[0], spins[1])
+    want = oracle.steps(orc.make_params(N, nf, J1=-1.0, J2=0.1, alpha=0.05, h=(0, 0, 0.5),
+                                        dt=0.005), s0, n)
+    assert np.array_equal(spins[0], want)

@@ -62,3 +62,34 @@ def test_umma_core_matches_fp64_product(kind, rows, Kp, chunk):
     split_eps = 2.0 ** -15 if kind == 2 else 2.0 ** -20
     bound = (split_eps + max(2e-6, steps * 2.0 ** -24)) * scale
     assert (C.double() - exact).abs().max().item() <= bound
+
+
+def test_cta_pair_kernel_matches():
+    """The CTA-pair form of the GEMM (cta_group::2, M = 256 over two SMs,
+    selected by ASD_UMMA_PAIR=1, read once per process), checked in a child
+    process: the raw product on several shapes against the same bound as
+    above, and S(q,t) through a context against the FP64 path."""
+    import os
+    import subprocess
+    import sys
+
+    code = (
+        "import sys; sys.path[:0] = {paths!r}\n"
+        "import test_umma_core_gpu as t\n"
+        "for case in ((1, 256, 32, 0), (2, 768, 192, 0), (1, 1024, 1504, 256),\n"
+        "             (2, 512, 1536, 512)):\n"
+        "    t.test_umma_core_matches_fp64_product(*case)\n"
+        "import asd_b200 as asd\n"
+        "p = asd.Params.make(40, 12, J1=-1.0, alpha=0.05, h=(0, 0, 0.5), dt=0.005, vx=2, vy=1)\n"
+        "with asd.Context(p) as c:\n"
+        "    c.set_spins(asd.random_spins(40, 12, seed=3), as_origin=True)\n"
+        "    c.step(4)\n"
+        "    ref = c.sqt('fp64')\n"
+        "    for m in ('tf32x3', 'bf16x3'):\n"
+        "        assert abs(c.sqt(m) - ref) <= 1e-5 * abs(ref), m\n"
+        "print('ok')\n"
+    ).format(paths=[os.path.dirname(__file__)] + sys.path)
+    env = dict(os.environ, ASD_UMMA_PAIR="1")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
