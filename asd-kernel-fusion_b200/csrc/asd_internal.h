@@ -21,6 +21,10 @@ struct LLGArgs {
     double dt;
     double spin_len;
     int use_j2, use_h, use_damp;
+    // Replica range the RK4 stage kernels update: [f0, f0 + nc).  The whole
+    // ensemble (0, nfile) unless a caller pipelines the step by replica chunk
+    // (replicas never interact, so a chunk's step needs no other replica).
+    int f0, nc;
 };
 
 LLGArgs make_llg_args(const asd_params &p);
@@ -61,6 +65,12 @@ cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *you
 cudaError_t launch_div_check(const double *x, long n, unsigned long long *bad, cudaStream_t st);
 
 // AoS [nfile][M][3] <-> site-major [M][nfile][3]
+// Replica-range forms: the AoS side holds replicas [f0, f0 + nc) only
+// ([nc][M][3]); the site-major side is the whole [M][nfile][3] array.
+cudaError_t launch_aos_to_sitemajor_range(const double *aos, double *sm, long M, int nfile,
+                                          int f0, int nc, cudaStream_t st);
+cudaError_t launch_sitemajor_to_aos_range(const double *sm, double *aos, long M, int nfile,
+                                          int f0, int nc, cudaStream_t st);
 cudaError_t launch_aos_to_sitemajor(const double *aos, double *sm, long M, int nfile,
                                     cudaStream_t st);
 cudaError_t launch_sitemajor_to_aos(const double *sm, double *aos, long M, int nfile,
@@ -82,6 +92,9 @@ cudaError_t launch_site_mean(const double *state, long M, int nfile, const doubl
 
 // FP64 state [M][K] -> split operands hi/lo [M][Kp] (zero for k >= K).
 // kind 1 = TF32 (stored as fp32 bit patterns), 2 = BF16.
+// Columns [kbeg, kend) of every row only (both even, kend <= Kp).
+cudaError_t launch_split_range(int kind, const double *state, long M, int K, int Kp, int kbeg,
+                               int kend, void *hi, void *lo, cudaStream_t st);
 cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, void *hi,
                          void *lo, cudaStream_t st);
 
@@ -148,6 +161,12 @@ struct UmmaSqtArgs {
     long dbg_ldc = 0;
     double *gpart = nullptr;  // q grid: per-CTA FP64 histograms [grid][N*N]
     int lat_n = 0;            // lattice side (q grid)
+    // K sub-range [k_begin, k_end) in elements (multiples of the k block;
+    // k_end = 0: to Kp).  The epilogue applies the connected-part term only
+    // when outer != 0, so the partial sums of launches over disjoint K
+    // ranges, one of them with outer set, add up to S(q,t).
+    int k_begin = 0, k_end = 0;
+    int outer = 1;
 };
 // Returns the number of CTAs launched (partials written) or a negative error.
 int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st);

@@ -106,6 +106,16 @@ struct asd_ctx {
     cudaStream_t llg_stream = nullptr, gemm_stream = nullptr;
     cudaEvent_t y_free = nullptr, llg_done = nullptr, gemm_done = nullptr;
     bool y_free_armed = false;
+    // row4.w / row1 (the phase u_i) are written by every site_mean of y;
+    // false until the first one and after q changes.
+    bool rows_ready = false;
+    // asd_ctx_step_host by replica chunk: double-buffered AoS staging for the
+    // chunk coming in and the chunk going out, a stream for the uploads
+    // (copy_stream carries the downloads) and the events that order them.
+    int hp_replicas = 0;  // chunk size the staging was sized for (0: none)
+    double *stage_in[2] = {}, *stage_out[2] = {};
+    cudaStream_t h2d_stream = nullptr;
+    cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
 };
 
 namespace {
@@ -374,6 +384,7 @@ int sqt_async(asd_ctx *c, int mode, double *d_out) {
     if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
     ASD_CUDA_TRY(launch_site_mean(c->y, c->M, c->p.nfile, c->uphase, c->mean_t, c->row4, c->row1,
                                   c->stream));
+    c->rows_ready = true;
     c->last_launches += 1;
     switch (mode) {
         case ASD_SQT_FP64: return sqt_plain(c, d_out);
@@ -538,6 +549,7 @@ int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
     }
     ASD_CUDA_TRY(launch_site_mean(c->y, c->M, c->p.nfile, c->uphase, c->mean_t, c->row4, c->row1,
                                   c->stream));
+    c->rows_ready = true;
     c->last_launches += 1;
     int nparts = 0;
     if (mode == ASD_SQT_FP64) {
@@ -619,6 +631,154 @@ int read_status(asd_ctx *c) {
     return ASD_OK;
 }
 
+// Replicas per chunk of the pipelined host step: about an eighth of the
+// ensemble, rounded up to a multiple of 64 so that every chunk boundary
+// (3 K columns per replica) is a whole k block of both the TF32 (32
+// columns) and the BF16 (64 columns) GEMM.
+int host_chunk_replicas(int nfile) {
+    const int target = (nfile + 7) / 8;
+    return (target + 63) / 64 * 64;
+}
+
+int ensure_host_pipeline(asd_ctx *c, int cr) {
+    if (!c->copy_stream) {
+        ASD_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        ASD_CUDA_TRY(cudaEventCreateWithFlags(&c->spins_ready, cudaEventDisableTiming));
+    }
+    if (!c->h2d_stream) {
+        ASD_CUDA_TRY(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; ++b) {
+            cudaEvent_t *ev[] = {&c->in_ready[b], &c->in_free[b], &c->out_ready[b],
+                                 &c->out_free[b]};
+            for (cudaEvent_t *x : ev)
+                ASD_CUDA_TRY(cudaEventCreateWithFlags(x, cudaEventDisableTiming));
+        }
+    }
+    if (c->hp_replicas == cr) return ASD_OK;
+    for (int b = 0; b < 2; ++b) {
+        if (c->stage_in[b]) cudaFree(c->stage_in[b]);
+        if (c->stage_out[b]) cudaFree(c->stage_out[b]);
+        c->stage_in[b] = c->stage_out[b] = nullptr;
+    }
+    c->hp_replicas = 0;
+    const size_t bytes = (size_t)cr * c->M * 3 * sizeof(double);
+    for (int b = 0; b < 2; ++b) {
+        int rc = dalloc(&c->stage_in[b], bytes);
+        if (rc == ASD_OK) rc = dalloc(&c->stage_out[b], bytes);
+        if (rc != ASD_OK) return rc;
+    }
+    c->hp_replicas = cr;
+    return ASD_OK;
+}
+
+// asd_ctx_step_host in replica chunks.  Replicas never interact, and the
+// correlation GEMM's K axis is the replica axis, so each chunk goes through
+// upload -> site-major transpose -> the four RK4 stages on its replicas ->
+// AoS transpose -> download, and (split modes) the split of its K columns and
+// a GEMM over that K range whose partial S(q,t) joins the others in the
+// final sum.  Only the last chunk's GEMM carries the connected-part term, after
+// the site means of the whole new state.  Uploads, compute and downloads run
+// on three streams, so the PCIe traffic of one chunk overlaps the compute of
+// its neighbours in both directions.  The spins are bit-identical to the
+// one-shot path; S(q,t) differs only in the order of its partial sums.
+int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int mode, int cr) {
+    const int nf = c->p.nfile;
+    const long M = c->M;
+    const int kind = (mode == ASD_SQT_TF32X3) ? 1 : (mode == ASD_SQT_BF16X3) ? 2 : 0;
+    if (mode < 0 || mode > 3) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
+    if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
+    int rc = ensure_host_pipeline(c, cr);
+    if (rc != ASD_OK) return rc;
+    const int nchunks = (nf + cr - 1) / cr;
+    if (kind) {
+        if (c->b_version[kind] != c->origin_version) {
+            ASD_CUDA_TRY(launch_split(kind, c->origin, M, c->K, c->Kp[kind], c->b_hi[kind],
+                                      c->b_lo[kind], c->stream));
+            c->b_version[kind] = c->origin_version;
+            c->last_launches += 1;
+        }
+        if (!c->rows_ready) {  // the early chunks' epilogues read the phase u_i
+            ASD_CUDA_TRY(launch_site_mean(c->y, M, nf, c->uphase, c->mean_t, c->row4, c->row1,
+                                          c->stream));
+            c->rows_ready = true;
+            c->last_launches += 1;
+        }
+        if ((rc = ensure_part(c, (long)nchunks * c->num_sms)) != ASD_OK) return rc;
+    }
+    const cudaStream_t comp = c->stream, up = c->h2d_stream, down = c->copy_stream;
+    LLGArgs a = c->a;
+    long nparts = 0;
+    for (int r = 0; r < nchunks; ++r) {
+        const int f0 = r * cr, nc = (nf - f0 < cr) ? nf - f0 : cr, b = r & 1;
+        const bool last = (f0 + nc == nf);
+        const size_t off = (size_t)f0 * M * 3, bytes = (size_t)nc * M * 3 * sizeof(double);
+        ASD_CUDA_TRY(cudaStreamWaitEvent(up, c->in_free[b], 0));
+        ASD_CUDA_TRY(cudaMemcpyAsync(c->stage_in[b], spin_in + off, bytes,
+                                     cudaMemcpyHostToDevice, up));
+        ASD_CUDA_TRY(cudaEventRecord(c->in_ready[b], up));
+        ASD_CUDA_TRY(cudaStreamWaitEvent(comp, c->in_ready[b], 0));
+        ASD_CUDA_TRY(launch_aos_to_sitemajor_range(c->stage_in[b], c->y, M, nf, f0, nc, comp));
+        ASD_CUDA_TRY(cudaEventRecord(c->in_free[b], comp));
+        a.f0 = f0;
+        a.nc = nc;
+        ASD_CUDA_TRY(launch_llg_stage(1, a, c->y, c->y, c->acc, c->ys_a, comp));
+        ASD_CUDA_TRY(launch_llg_stage(2, a, c->y, c->ys_a, c->acc, c->ys_b, comp));
+        ASD_CUDA_TRY(launch_llg_stage(3, a, c->y, c->ys_b, c->acc, c->ys_a, comp));
+        ASD_CUDA_TRY(launch_llg_stage(4, a, nullptr, c->ys_a, c->acc, c->y, comp));
+        ASD_CUDA_TRY(cudaStreamWaitEvent(comp, c->out_free[b], 0));
+        ASD_CUDA_TRY(launch_sitemajor_to_aos_range(c->y, c->stage_out[b], M, nf, f0, nc, comp));
+        ASD_CUDA_TRY(cudaEventRecord(c->out_ready[b], comp));
+        ASD_CUDA_TRY(cudaStreamWaitEvent(down, c->out_ready[b], 0));
+        ASD_CUDA_TRY(cudaMemcpyAsync(spin_out + off, c->stage_out[b], bytes,
+                                     cudaMemcpyDeviceToHost, down));
+        ASD_CUDA_TRY(cudaEventRecord(c->out_free[b], down));
+        c->last_launches += 6;
+        if (!kind) continue;
+        const int kbeg = 3 * f0, kend = last ? c->Kp[kind] : 3 * (f0 + nc);
+        ASD_CUDA_TRY(launch_split_range(kind, c->y, M, c->K, c->Kp[kind], kbeg, kend,
+                                        c->a_hi[kind], c->a_lo[kind], comp));
+        c->last_launches += 1;
+        if (last) {
+            ASD_CUDA_TRY(launch_site_mean(c->y, M, nf, c->uphase, c->mean_t, c->row4, c->row1,
+                                          comp));
+            c->last_launches += 1;
+        }
+        UmmaSqtArgs u{};
+        u.kind = kind;
+        u.M = M;
+        u.Kp = c->Kp[kind];
+        u.a_hi = c->a_hi[kind];
+        u.a_lo = c->a_lo[kind];
+        u.b_hi = c->b_hi[kind];
+        u.b_lo = c->b_lo[kind];
+        u.row4 = c->row4;
+        u.row1 = c->row1;
+        u.col4 = c->col4;
+        u.col1 = c->col1;
+        u.alpha = (float)(1.0 / (double)nf);
+        u.part = c->part + nparts;
+        u.status = c->status;
+        u.num_sms = c->num_sms;
+        u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
+        u.k_begin = kbeg;
+        u.k_end = kend;
+        u.outer = last ? 1 : 0;
+        const int grid = launch_umma_sqt(u, comp);
+        if (grid < 0) return grid;
+        nparts += grid;
+        c->last_launches += 1;
+    }
+    c->state_version += 2;  // as set_spins + step
+    c->has_state = true;
+    if (kind) {
+        c->a_version[kind] = c->state_version;
+        ASD_CUDA_TRY(launch_finalize(c->part, (int)nparts, 1.0 / (double)M, c->d_out, comp));
+        c->last_launches += 1;
+        return ASD_OK;
+    }
+    return sqt_async(c, mode, c->d_out);
+}
+
 void destroy(asd_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
@@ -638,6 +798,17 @@ void destroy(asd_ctx *c) {
     if (c->h_out) cudaFreeHost(c->h_out);
     if (c->spins_ready) cudaEventDestroy(c->spins_ready);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    for (int b = 0; b < 2; ++b) {
+        if (c->stage_in[b]) cudaFree(c->stage_in[b]);
+        if (c->stage_out[b]) cudaFree(c->stage_out[b]);
+        cudaEvent_t ev[] = {c->in_ready[b], c->in_free[b], c->out_ready[b], c->out_free[b]};
+        for (cudaEvent_t x : ev)
+            if (x) cudaEventDestroy(x);
+    }
+    if (c->h2d_stream) {
+        cudaStreamSynchronize(c->h2d_stream);
+        cudaStreamDestroy(c->h2d_stream);
+    }
     if (c->llg_stream) {
         cudaStreamSynchronize(c->llg_stream);
         cudaStreamDestroy(c->llg_stream);
@@ -907,6 +1078,7 @@ int asd_ctx_set_params(asd_ctx *c, const asd_params *p) {
             w[i] = make_double2(std::cos(th), std::sin(th));
         }
         ASD_CUDA_TRY(enter(c));
+        c->rows_ready = false;
         ASD_CUDA_TRY(cudaMemcpy(c->uphase, u.data(), (size_t)c->M * sizeof(double2), cudaMemcpyHostToDevice));
         ASD_CUDA_TRY(cudaMemcpy(c->wphase, w.data(), (size_t)c->M * sizeof(double2), cudaMemcpyHostToDevice));
         if (c->has_origin) return refresh_origin(c);
@@ -947,27 +1119,42 @@ int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_s
     if (!c->has_origin) return fail(ASD_ERR_STATE, "set the origin (t = 0 spins) first");
     ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
-    int rc = set_spins_common(c, spin_in, true, 0);
-    if (rc != ASD_OK) return rc;
-    rc = run_steps(c, 1);
-    if (rc != ASD_OK) return rc;
-    // The new spins go back to the host on a second stream while S(q,t) runs:
-    // the read-back over PCIe overlaps the correlation GEMM.
-    if (!c->copy_stream) {
-        ASD_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-        ASD_CUDA_TRY(cudaEventCreateWithFlags(&c->spins_ready, cudaEventDisableTiming));
+    int rc;
+    const int cr = host_chunk_replicas(c->p.nfile);
+    if (cr < c->p.nfile) {
+        rc = step_host_chunked(c, spin_in, spin_out, (int)mode, cr);
+        // Never return while a copy may still touch the caller's buffers.
+        const cudaError_t e1 = cudaStreamSynchronize(c->h2d_stream);
+        const cudaError_t e2 = cudaStreamSynchronize(c->copy_stream);
+        if (rc != ASD_OK) {
+            cudaStreamSynchronize(c->stream);
+            return rc;
+        }
+        ASD_CUDA_TRY(e1);
+        ASD_CUDA_TRY(e2);
+    } else {
+        rc = set_spins_common(c, spin_in, true, 0);
+        if (rc != ASD_OK) return rc;
+        rc = run_steps(c, 1);
+        if (rc != ASD_OK) return rc;
+        // The new spins go back to the host on a second stream while S(q,t)
+        // runs: the read-back over PCIe overlaps the correlation GEMM.
+        if (!c->copy_stream) {
+            ASD_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+            ASD_CUDA_TRY(cudaEventCreateWithFlags(&c->spins_ready, cudaEventDisableTiming));
+        }
+        ASD_CUDA_TRY(launch_sitemajor_to_aos(c->y, c->ys_b, c->M, c->p.nfile, c->stream));
+        c->last_launches += 1;
+        ASD_CUDA_TRY(cudaEventRecord(c->spins_ready, c->stream));
+        ASD_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->spins_ready, 0));
+        ASD_CUDA_TRY(cudaMemcpyAsync(spin_out, c->ys_b, (size_t)c->M * c->K * sizeof(double),
+                                     cudaMemcpyDeviceToHost, c->copy_stream));
+        rc = sqt_async(c, (int)mode, c->d_out);
+        const cudaError_t ec = cudaStreamSynchronize(c->copy_stream);
+        if (rc != ASD_OK) return rc;
+        ASD_CUDA_TRY(ec);
     }
-    ASD_CUDA_TRY(launch_sitemajor_to_aos(c->y, c->ys_b, c->M, c->p.nfile, c->stream));
-    c->last_launches += 1;
-    ASD_CUDA_TRY(cudaEventRecord(c->spins_ready, c->stream));
-    ASD_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->spins_ready, 0));
-    ASD_CUDA_TRY(cudaMemcpyAsync(spin_out, c->ys_b, (size_t)c->M * c->K * sizeof(double),
-                                 cudaMemcpyDeviceToHost, c->copy_stream));
-    rc = sqt_async(c, (int)mode, c->d_out);
-    c->y_free_armed = false;  // ys_b is still being read on copy_stream
-    const cudaError_t ec = cudaStreamSynchronize(c->copy_stream);
-    if (rc != ASD_OK) return rc;
-    ASD_CUDA_TRY(ec);
+    c->y_free_armed = false;  // the staging buffers were in use on the copy streams
     ASD_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost,
                                  c->stream));
     rc = read_status(c);

@@ -26,10 +26,10 @@ __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double 
                                                         double *__restrict__ acc,
                                                         double *__restrict__ out) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long total = a.M * a.nfile;
+    const long total = a.M * a.nc;
     if (t >= total) return;
-    const long site = t / a.nfile;
-    const int f = (int)(t - site * a.nfile);
+    const long site = t / a.nc;
+    const int f = a.f0 + (int)(t - site * a.nc);
     const int row = (int)(site / a.N), col = (int)(site - (long)row * a.N);
     const long sstride = 3L * a.nfile;
     const long off = 3L * f;
@@ -73,7 +73,8 @@ __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double 
 template <int STAGE>
 cudaError_t launch_stage_t(const LLGArgs &a, const double *y, const double *ys, double *acc,
                            double *out, cudaStream_t st) {
-    const long total = a.M * a.nfile;
+    if (a.f0 < 0 || a.nc < 1 || a.f0 + a.nc > a.nfile) return cudaErrorInvalidValue;
+    const long total = a.M * a.nc;
     const int threads = 256;
     const unsigned blocks = (unsigned)((total + threads - 1) / threads);
     const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
@@ -295,24 +296,25 @@ cudaError_t launch_fused_t(const LLGArgs &a, const double *y, double *yout, cuda
 template <bool TO_SITEMAJOR>
 __global__ void __launch_bounds__(256) transpose_kernel(const double *__restrict__ src,
                                                         double *__restrict__ dst, long M,
-                                                        int nfile) {
+                                                        int nfile, int fbeg, int nc) {
+    // The AoS side holds replicas [fbeg, fbeg + nc) as [nc][M][3]; the
+    // site-major side is the whole [M][nfile][3] array.  lf = local replica.
     __shared__ double tile[32][32 * 3 + 1];
     const long s0 = (long)blockIdx.x * 32;
-    const int f0 = blockIdx.y * 32;
+    const int l0 = blockIdx.y * 32;
     // read
     for (int idx = threadIdx.x; idx < 32 * 96; idx += blockDim.x) {
+        const int r = idx / 96, w = idx % 96;
         if (TO_SITEMAJOR) {
-            // AoS: for replica f0+r, 96 contiguous doubles of sites s0..s0+31
-            const int r = idx / 96, w = idx % 96;
-            const int f = f0 + r;
+            // AoS: for replica l0+r, 96 contiguous doubles of sites s0..s0+31
+            const int lf = l0 + r;
             const long s = s0 + w / 3;
-            if (f < nfile && s < M) tile[r][w] = src[((long)f * M + s0) * 3 + w];
+            if (lf < nc && s < M) tile[r][w] = src[((long)lf * M + s0) * 3 + w];
         } else {
-            // site-major: for site s0+r, 96 contiguous doubles of replicas f0..f0+31
-            const int r = idx / 96, w = idx % 96;
+            // site-major: for site s0+r, 96 contiguous doubles of replicas l0..l0+31
             const long s = s0 + r;
-            const int f = f0 + w / 3;
-            if (f < nfile && s < M) tile[r][w] = src[(s * nfile + f0) * 3 + w];
+            const int lf = l0 + w / 3;
+            if (lf < nc && s < M) tile[r][w] = src[(s * nfile + fbeg + l0) * 3 + w];
         }
     }
     __syncthreads();
@@ -320,14 +322,14 @@ __global__ void __launch_bounds__(256) transpose_kernel(const double *__restrict
         const int r = idx / 96, w = idx % 96;
         const int c = w % 3, q = w / 3;
         if (TO_SITEMAJOR) {
-            // write site s0+r, replicas f0..: value from tile[f-f0][(s-s0)*3+c]
+            // write site s0+r, replicas l0..: value from tile[lf-l0][(s-s0)*3+c]
             const long s = s0 + r;
-            const int f = f0 + q;
-            if (f < nfile && s < M) dst[(s * nfile + f) * 3 + c] = tile[q][r * 3 + c];
+            const int lf = l0 + q;
+            if (lf < nc && s < M) dst[(s * nfile + fbeg + lf) * 3 + c] = tile[q][r * 3 + c];
         } else {
-            const int f = f0 + r;
+            const int lf = l0 + r;
             const long s = s0 + q;
-            if (f < nfile && s < M) dst[((long)f * M + s) * 3 + c] = tile[q][r * 3 + c];
+            if (lf < nc && s < M) dst[((long)lf * M + s) * 3 + c] = tile[q][r * 3 + c];
         }
     }
 }
@@ -401,6 +403,8 @@ LLGArgs make_llg_args(const asd_params &p) {
     a.use_j2 = p.J2 != 0.0;
     a.use_h = (p.hx != 0.0 || p.hy != 0.0 || p.hz != 0.0);
     a.use_damp = p.alpha != 0.0;
+    a.f0 = 0;
+    a.nc = p.nfile;
     return a;
 }
 
@@ -421,18 +425,30 @@ cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *you
     return launch_fused_t<2, 256>(a, y, yout, st);
 }
 
+cudaError_t launch_aos_to_sitemajor_range(const double *aos, double *sm, long M, int nfile,
+                                          int f0, int nc, cudaStream_t st) {
+    if (f0 < 0 || nc < 1 || f0 + nc > nfile) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)((M + 31) / 32), (unsigned)((nc + 31) / 32));
+    transpose_kernel<true><<<grid, 256, 0, st>>>(aos, sm, M, nfile, f0, nc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sitemajor_to_aos_range(const double *sm, double *aos, long M, int nfile,
+                                          int f0, int nc, cudaStream_t st) {
+    if (f0 < 0 || nc < 1 || f0 + nc > nfile) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)((M + 31) / 32), (unsigned)((nc + 31) / 32));
+    transpose_kernel<false><<<grid, 256, 0, st>>>(sm, aos, M, nfile, f0, nc);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_aos_to_sitemajor(const double *aos, double *sm, long M, int nfile,
                                     cudaStream_t st) {
-    dim3 grid((unsigned)((M + 31) / 32), (unsigned)((nfile + 31) / 32));
-    transpose_kernel<true><<<grid, 256, 0, st>>>(aos, sm, M, nfile);
-    return cudaGetLastError();
+    return launch_aos_to_sitemajor_range(aos, sm, M, nfile, 0, nfile, st);
 }
 
 cudaError_t launch_sitemajor_to_aos(const double *sm, double *aos, long M, int nfile,
                                     cudaStream_t st) {
-    dim3 grid((unsigned)((M + 31) / 32), (unsigned)((nfile + 31) / 32));
-    transpose_kernel<false><<<grid, 256, 0, st>>>(sm, aos, M, nfile);
-    return cudaGetLastError();
+    return launch_sitemajor_to_aos_range(sm, aos, M, nfile, 0, nfile, st);
 }
 
 cudaError_t launch_euler_aos(const LLGArgs &a, const double *spin, double *deriv,

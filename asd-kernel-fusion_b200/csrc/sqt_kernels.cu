@@ -62,39 +62,43 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
     lo = __uint_as_float(l);
 }
 
+// Both split kernels convert columns [kbeg, kend) of every row (kbeg and kend
+// even; columns K..Kp-1 are the zero padding), one thread per column pair.
 __global__ void __launch_bounds__(256) split_tf32_kernel(const double *__restrict__ s, long M,
-                                                         int K, int Kp, float2 *__restrict__ hi,
+                                                         int K, int Kp, int kbeg, int kend,
+                                                         float2 *__restrict__ hi,
                                                          float2 *__restrict__ lo) {
-    // one thread per pair of consecutive k (Kp is even)
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int half = Kp / 2;
-    if (t >= M * half) return;
-    const long row = t / half;
-    const int k = (int)(t - row * half) * 2;
+    const int pairs = (kend - kbeg) / 2;
+    if (t >= M * pairs) return;
+    const long row = t / pairs;
+    const int k = kbeg + (int)(t - row * pairs) * 2;
     float2 h = make_float2(0.f, 0.f), l = make_float2(0.f, 0.f);
     if (k < K) split_tf32(s[row * K + k], h.x, l.x);
     if (k + 1 < K) split_tf32(s[row * K + k + 1], h.y, l.y);
-    hi[t] = h;
-    lo[t] = l;
+    const long o = row * (Kp / 2) + k / 2;
+    hi[o] = h;
+    lo[o] = l;
 }
 
 __global__ void __launch_bounds__(256) split_bf16_kernel(const double *__restrict__ s, long M,
-                                                         int K, int Kp,
+                                                         int K, int Kp, int kbeg, int kend,
                                                          __nv_bfloat162 *__restrict__ hi,
                                                          __nv_bfloat162 *__restrict__ lo) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int half = Kp / 2;
-    if (t >= M * half) return;
-    const long row = t / half;
-    const int k = (int)(t - row * half) * 2;
+    const int pairs = (kend - kbeg) / 2;
+    if (t >= M * pairs) return;
+    const long row = t / pairs;
+    const int k = kbeg + (int)(t - row * pairs) * 2;
     double x0 = 0.0, x1 = 0.0;
     if (k < K) x0 = s[row * K + k];
     if (k + 1 < K) x1 = s[row * K + k + 1];
     const __nv_bfloat16 h0 = __double2bfloat16(x0), h1 = __double2bfloat16(x1);
     const __nv_bfloat16 l0 = __double2bfloat16(x0 - (double)__bfloat162float(h0));
     const __nv_bfloat16 l1 = __double2bfloat16(x1 - (double)__bfloat162float(h1));
-    hi[t] = __halves2bfloat162(h0, h1);
-    lo[t] = __halves2bfloat162(l0, l1);
+    const long o = row * (Kp / 2) + k / 2;
+    hi[o] = __halves2bfloat162(h0, h1);
+    lo[o] = __halves2bfloat162(l0, l1);
 }
 
 // Plain FP64 epilogue.  Block (bx, by): rows [i0 + 128*bx, +128) of the band,
@@ -249,16 +253,24 @@ cudaError_t launch_site_mean(const double *state, long M, int nfile, const doubl
     return cudaGetLastError();
 }
 
-cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, void *hi, void *lo,
-                         cudaStream_t st) {
-    const long total = M * (Kp / 2);
+cudaError_t launch_split_range(int kind, const double *state, long M, int K, int Kp, int kbeg,
+                               int kend, void *hi, void *lo, cudaStream_t st) {
+    if (kbeg < 0 || kend > Kp || kbeg >= kend || (kbeg | kend | Kp) & 1)
+        return cudaErrorInvalidValue;
+    const long total = M * ((kend - kbeg) / 2);
     const unsigned blocks = (unsigned)((total + 255) / 256);
     if (kind == 1)
-        split_tf32_kernel<<<blocks, 256, 0, st>>>(state, M, K, Kp, (float2 *)hi, (float2 *)lo);
+        split_tf32_kernel<<<blocks, 256, 0, st>>>(state, M, K, Kp, kbeg, kend, (float2 *)hi,
+                                                  (float2 *)lo);
     else
-        split_bf16_kernel<<<blocks, 256, 0, st>>>(state, M, K, Kp, (__nv_bfloat162 *)hi,
-                                                  (__nv_bfloat162 *)lo);
+        split_bf16_kernel<<<blocks, 256, 0, st>>>(state, M, K, Kp, kbeg, kend,
+                                                  (__nv_bfloat162 *)hi, (__nv_bfloat162 *)lo);
     return cudaGetLastError();
+}
+
+cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, void *hi, void *lo,
+                         cudaStream_t st) {
+    return launch_split_range(kind, state, M, K, Kp, 0, Kp, hi, lo, st);
 }
 
 cudaError_t launch_plain_epilogue(const double *C, long i0, long mb, long n, const double *mrow,

@@ -120,8 +120,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     umma_sqt_kernel(const __grid_constant__ CUtensorMap tm_ah,
                     const __grid_constant__ CUtensorMap tm_al,
                     const __grid_constant__ CUtensorMap tm_bh,
-                    const __grid_constant__ CUtensorMap tm_bl, int num_m, int num_n, int num_kb,
-                    int kb_per_chunk, const float4 *__restrict__ row4,
+                    const __grid_constant__ CUtensorMap tm_bl, int num_m, int num_n, int kb_begin,
+                    int kb_end, int kb_per_chunk, int outer, const float4 *__restrict__ row4,
                     const float *__restrict__ row1, const float4 *__restrict__ col4,
                     const float *__restrict__ col1, float alpha, double2 *__restrict__ part,
                     unsigned *__restrict__ status, float *__restrict__ dbg_c, long dbg_ldc,
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 tile_coords(tile, num_m, num_n, mb, nb);
                 const int arow = mb * G::TILE_M + (int)rank * BM;
                 const int brow = nb * BN + (int)rank * G::BN_LOC;
-                for (int kb = 0; kb < num_kb; ++kb) {
+                for (int kb = kb_begin; kb < kb_end; ++kb) {
                     if (!ptx::mbar_wait_bounded(&tail->empty[stage], phase ^ 1u, abort_flag,
                                                 WAIT_LIMIT)) {
                         raise_abort(tail, status);
@@ -273,8 +273,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 // into a fresh TMEM buffer: the tensor core's FP32
                 // accumulation loses precision with the number of
                 // accumulation steps, and the epilogue adds the chunks in FP64.
-                for (int kb0 = 0; kb0 < num_kb && ok; kb0 += kb_per_chunk) {
-                    const int kb1 = min(kb0 + kb_per_chunk, num_kb);
+                for (int kb0 = kb_begin; kb0 < kb_end && ok; kb0 += kb_per_chunk) {
+                    const int kb1 = min(kb0 + kb_per_chunk, kb_end);
                     if (!ptx::mbar_wait_bounded(&tail->tempty[abuf], aphase ^ 1u, abort_flag,
                                                 WAIT_LIMIT)) {
                         raise_abort(tail, status);
@@ -392,9 +392,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const float ui = STORE ? 0.f : row1[i];
             double s_re = 0.0, s_im = 0.0;
             bool ok = true;
-            for (int kb0 = 0; kb0 < num_kb; kb0 += kb_per_chunk) {
-                const bool first = (kb0 == 0);
-                const bool last = (kb0 + kb_per_chunk >= num_kb);
+            for (int kb0 = kb_begin; kb0 < kb_end; kb0 += kb_per_chunk) {
+                const bool first = (kb0 == kb_begin);
+                // the connected-part term, once per row: in the last chunk
+                // of the launch that carries it
+                const bool last = outer && (kb0 + kb_per_chunk >= kb_end);
                 if (!ptx::mbar_wait_bounded(&tail->tfull[abuf], aphase, abort_flag, WAIT_LIMIT)) {
                     raise_abort(tail, status);
                     ok = false;
@@ -623,6 +625,12 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     if ((rc = make_tmap(&tbh, a.b_hi, a.kind, Mp, a.Kp, b_rows, rowb)) != ASD_OK) return rc;
     if ((rc = make_tmap(&tbl, a.b_lo, a.kind, Mp, a.Kp, b_rows, rowb)) != ASD_OK) return rc;
     const int num_m = (int)(Mp / tile_m), num_n = (int)(Mp / BN), num_kb = a.Kp / ke;
+    const int k_end = a.k_end > 0 ? a.k_end : a.Kp;
+    if (a.k_begin < 0 || a.k_begin % ke != 0 || k_end % ke != 0 || k_end > a.Kp ||
+        a.k_begin >= k_end)
+        return fail(ASD_ERR_INVALID, "K range [%d, %d) is not whole k blocks of %d in [0, %d)",
+                    a.k_begin, k_end, ke, a.Kp);
+    const int kb_begin = a.k_begin / ke, kb_end = k_end / ke;
     const int tiles = num_m * num_n;
     // k blocks per accumulation chunk: chunk_k elements of K (0 = all of K)
     int kpc = a.chunk_k > 0 ? (a.chunk_k + ke - 1) / ke : num_kb;
@@ -658,8 +666,8 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
             grid = tiles < a.num_sms ? tiles : a.num_sms;
         }
         cfg.gridDim = dim3((unsigned)grid, 1, 1);
-        return cudaLaunchKernelEx(&cfg, kern, tah, tal, tbh, tbl, num_m, num_n, num_kb, kpc,
-                                  a.row4, a.row1, a.col4, a.col1, a.alpha, a.part, a.status,
+        return cudaLaunchKernelEx(&cfg, kern, tah, tal, tbh, tbl, num_m, num_n, kb_begin, kb_end,
+                                  kpc, a.outer, a.row4, a.row1, a.col4, a.col1, a.alpha, a.part, a.status,
                                   a.dbg_c, a.dbg_ldc, a.lat_n, a.M, a.gpart);
     };
     const int epi = a.dbg_c ? EPI_STORE : (a.gpart ? EPI_GRID : EPI_PHASE);

@@ -176,3 +176,41 @@ def test_step_pipelined_behind_the_split_gemm(oracle, mode, kernel):
     want = oracle.steps(orc.make_params(N, nf, J1=-1.0, J2=0.1, alpha=0.05, h=(0, 0, 0.5),
                                         dt=0.005), s0, n)
     assert np.array_equal(spins[0], want)
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_step_host_in_replica_chunks(oracle, pinned):
+    """Ensembles larger than one upload chunk (64 replicas and up) take the
+    pipelined asd_ctx_step_host: per replica chunk, upload, RK4, download and
+    a GEMM over that chunk's K columns.  200 replicas make chunks of 64, 64,
+    64 and a ragged 8.  The spins must equal the device path and the oracle
+    bit for bit; S(q,t) must equal the device path exactly in the FP64 modes
+    and agree to the split-precision tolerance (1e-5 of the FP64 value) in
+    the split modes, whose partial sums are added in another order."""
+    import torch
+
+    N, nf = 16, 200
+    s0 = asd.random_spins(N, nf, seed=12)
+    kw = dict(J1=-1.0, J2=0.2, alpha=0.05, h=(0, 0, 0.5), dt=0.005)
+    p = asd.Params.make(N, nf, vx=3, vy=2, **kw)
+    with asd.Context(p) as a, asd.Context(p) as b:
+        a.set_spins(s0, as_origin=True)
+        b.set_spins(s0, as_origin=True)
+        buf = torch.from_numpy(s0.reshape(-1).copy())
+        if pinned:
+            buf = buf.pin_memory()
+        want_spins = s0
+        for step, mode in enumerate(["tf32x3", "fp64", "bf16x3", "fp64_fused", "tf32x3"]):
+            got = a.step_host(buf.data_ptr(), buf.data_ptr(), mode)
+            b.step(1)
+            ref = b.sqt("fp64")
+            want_spins = oracle.steps(orc.make_params(N, nf, **kw), want_spins, 1)
+            assert np.array_equal(buf.numpy().reshape(s0.shape), b.get_spins()), step
+            assert np.array_equal(b.get_spins(), want_spins), step
+            if mode.startswith("fp64"):
+                assert got == b.sqt(mode), (step, mode)
+            else:
+                # each split result within 1e-5 of FP64; the chunked one sums
+                # shorter K ranges in FP32 and is usually the closer of the two
+                assert abs(got - ref) <= 1e-5 * abs(ref), (step, mode, got, ref)
+                assert abs(b.sqt(mode) - ref) <= 1e-5 * abs(ref), (step, mode)
