@@ -46,7 +46,9 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
     "asd_ctx_sqt_grid_async", "asd_ctx_sqt_grid",
-    "asd_ctx_step_host", "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
+    "asd_ctx_step_host", "asd_ctx_set_ensemble", "asd_ctx_shard_origin_sums",
+    "asd_ctx_shard_set_origin_sums", "asd_ctx_shard_sqt_async", "asd_ctx_shard_sqt_finish",
+    "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
     "asd_ctx_last_launches",
     "asd_ctx_check_device_status",
     "asd_check_bounded_wait", "asd_check_const_division", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
@@ -55,6 +57,11 @@ EXPORTED_SYMBOLS = (
     "asd_batch_configure", "asd_batch_autotune", "asd_set_params", "euler", "runge_kutta",
     "fused_dgemm",
 )
+
+
+def _addr(x) -> int:
+    """A device address: an int, or a tensor's data pointer."""
+    return int(x.data_ptr()) if hasattr(x, "data_ptr") else int(x)
 
 
 class AsdError(RuntimeError):
@@ -126,6 +133,11 @@ def load() -> C.CDLL:
         "asd_ctx_sqt_grid_async": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_sqt_grid": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_step_host": ([vp, vp, vp, C.c_int, dp], C.c_int),
+        "asd_ctx_set_ensemble": ([vp, C.c_int], C.c_int),
+        "asd_ctx_shard_origin_sums": ([vp, vp], C.c_int),
+        "asd_ctx_shard_set_origin_sums": ([vp, vp], C.c_int),
+        "asd_ctx_shard_sqt_async": ([vp, C.c_int, vp, vp], C.c_int),
+        "asd_ctx_shard_sqt_finish": ([vp, vp, vp, vp], C.c_int),
         "asd_ctx_set_llg_kernel": ([vp, C.c_int], C.c_int),
         "asd_ctx_set_chunk_k": ([vp, C.c_int], C.c_int),
         "asd_ctx_last_launches": ([vp], C.c_int),
@@ -302,6 +314,26 @@ class Context:
         _check(load().asd_ctx_step_host(self._h, C.c_void_p(spin_in_ptr),
                                         C.c_void_p(spin_out_ptr), mode, self._out))
         return complex(self._out[0], self._out[1])
+
+    # replica sharding of one ensemble (see asd_b200.shard) ------------------
+    def set_ensemble(self, nfile_total: int) -> None:
+        _check(load().asd_ctx_set_ensemble(self._h, int(nfile_total)))
+
+    def shard_origin_sums(self, d_zsums) -> None:
+        _check(load().asd_ctx_shard_origin_sums(self._h, C.c_void_p(_addr(d_zsums))))
+
+    def shard_set_origin_sums(self, d_zsums) -> None:
+        _check(load().asd_ctx_shard_set_origin_sums(self._h, C.c_void_p(_addr(d_zsums))))
+
+    def shard_sqt_async(self, mode, d_part, d_sums) -> None:
+        mode = MODES[mode] if isinstance(mode, str) else int(mode)
+        _check(load().asd_ctx_shard_sqt_async(self._h, mode, C.c_void_p(_addr(d_part)),
+                                              C.c_void_p(_addr(d_sums))))
+
+    def shard_sqt_finish(self, d_part, d_sums, d_out) -> None:
+        _check(load().asd_ctx_shard_sqt_finish(self._h, C.c_void_p(_addr(d_part)),
+                                               C.c_void_p(_addr(d_sums)),
+                                               C.c_void_p(_addr(d_out))))
 
     def set_llg_kernel(self, kernel) -> None:
         """"stages" (four launches, the default) or "fused" (one launch per step)."""

@@ -92,6 +92,13 @@ cudaError_t launch_site_mean(const double *state, long M, int nfile, const doubl
 
 // FP64 state [M][K] -> split operands hi/lo [M][Kp] (zero for k >= K).
 // kind 1 = TF32 (stored as fp32 bit patterns), 2 = BF16.
+// Per-site sums over the context's replicas ([M][3]), and the S(q,t) of a
+// replica-sharded ensemble from its all-reduced partial and site sums.
+cudaError_t launch_site_sum(const double *state, long M, int nfile, double *sums,
+                            cudaStream_t st);
+cudaError_t launch_shard_finish(long M, int nfile_total, const double *part, const double *sums,
+                                const double *zsums, const double2 *u, const double2 *w,
+                                double *out, cudaStream_t st);
 // Columns [kbeg, kend) of every row only (both even, kend <= Kp).
 cudaError_t launch_split_range(int kind, const double *state, long M, int K, int Kp, int kbeg,
                                int kend, void *hi, void *lo, cudaStream_t st);

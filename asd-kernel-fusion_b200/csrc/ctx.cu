@@ -116,6 +116,12 @@ struct asd_ctx {
     double *stage_in[2] = {}, *stage_out[2] = {};
     cudaStream_t h2d_stream = nullptr;
     cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
+    // Replica sharding: this context holds nfile of the nfile_total replicas
+    // of one ensemble (0: not sharded); zsums = the ensemble's origin site
+    // sums once exchanged; zero3 = zero means for the FP64 partial GEMMs.
+    int nfile_total = 0;
+    double *zsums = nullptr, *zero3 = nullptr;
+    bool has_zsums = false;
 };
 
 namespace {
@@ -239,6 +245,7 @@ int set_spins_common(asd_ctx *c, const double *aos, bool host, int as_origin) {
         int rc = refresh_origin(c);
         if (rc != ASD_OK) return rc;
         c->has_origin = true;
+        c->has_zsums = false;  // the ensemble's origin sums must be exchanged again
     }
     return ASD_OK;
 }
@@ -266,10 +273,31 @@ int run_steps(asd_ctx *c, int nsteps) {
     return ASD_OK;
 }
 
-int sqt_plain(asd_ctx *c, double *d_out) {
+// Zero site means: the FP64 GEMM paths without their connected-part term.
+int ensure_zero3(asd_ctx *c) {
+    if (c->zero3) return ASD_OK;
+    int rc = dalloc(&c->zero3, (size_t)c->M * 3 * sizeof(double));
+    if (rc != ASD_OK) return rc;
+    ASD_CUDA_TRY(cudaMemset(c->zero3, 0, (size_t)c->M * 3 * sizeof(double)));
+    return ASD_OK;
+}
+
+// The scale of the correlation GEMM: 1 / (replicas of the ensemble).  A
+// shard's partial uses the whole ensemble's count and leaves out the
+// connected-part term, which only the ensemble's means can give.
+double gemm_alpha(const asd_ctx *c, bool shard) {
+    return 1.0 / (double)((shard && c->nfile_total > 0) ? c->nfile_total : c->p.nfile);
+}
+
+int sqt_plain(asd_ctx *c, double *d_out, bool shard) {
     const long M = c->M;
     const int K = c->K;
-    const double alpha = 1.0 / (double)c->p.nfile;
+    const double alpha = gemm_alpha(c, shard);
+    if (shard) {
+        int rc = ensure_zero3(c);
+        if (rc != ASD_OK) return rc;
+    }
+    const double *mrow = shard ? c->zero3 : c->mean_t, *zcol = shard ? c->zero3 : c->mean_0;
     const double beta = 0.0;
     const long mb = c->band_rows;
     const int nby = 64;
@@ -288,7 +316,7 @@ int sqt_plain(asd_ctx *c, double *d_out) {
                         c->y + i0 * K, K, c->origin, K, &beta, c->band, (int)rows);
         if (bs != CUBLAS_STATUS_SUCCESS) return fail(ASD_ERR_CUDA, "cublasDgemm failed (%d)", (int)bs);
         const int nbx = (int)((rows + 127) / 128);
-        ASD_CUDA_TRY(launch_plain_epilogue(c->band, i0, rows, M, c->mean_t, c->mean_0, c->uphase,
+        ASD_CUDA_TRY(launch_plain_epilogue(c->band, i0, rows, M, mrow, zcol, c->uphase,
                                            c->wphase, c->part + off, nbx, nby, c->stream));
         off += (long)nbx * nby;
         c->last_launches += 1;  // the epilogue; the DGEMM is cuBLAS's
@@ -298,7 +326,11 @@ int sqt_plain(asd_ctx *c, double *d_out) {
     return ASD_OK;
 }
 
-int sqt_fp64_fused(asd_ctx *c, double *d_out) {
+int sqt_fp64_fused(asd_ctx *c, double *d_out, bool shard) {
+    if (shard) {
+        int rc = ensure_zero3(c);
+        if (rc != ASD_OK) return rc;
+    }
     Fp64GemmArgs g{};
     g.dropin = 0;
     g.m = c->M;
@@ -312,9 +344,9 @@ int sqt_fp64_fused(asd_ctx *c, double *d_out) {
     g.sbk = 1;
     g.sbj = c->K;
     g.b_k_fast = 1;
-    g.alpha = 1.0 / (double)c->p.nfile;
-    g.mrow = c->mean_t;
-    g.zcol = c->mean_0;
+    g.alpha = gemm_alpha(c, shard);
+    g.mrow = shard ? c->zero3 : c->mean_t;
+    g.zcol = shard ? c->zero3 : c->mean_0;
     g.uphase = c->uphase;
     g.wphase = c->wphase;
     const long np = fp64_gemm_num_parts(g);
@@ -327,7 +359,7 @@ int sqt_fp64_fused(asd_ctx *c, double *d_out) {
     return ASD_OK;
 }
 
-int sqt_split(asd_ctx *c, int kind, double *d_out) {
+int sqt_split(asd_ctx *c, int kind, double *d_out, bool shard) {
     if (!c->a_hi[kind]) return fail(ASD_ERR_STATE, "split mode %d not enabled at create", kind);
     if (c->a_version[kind] != c->state_version) {
         ASD_CUDA_TRY(launch_split(kind, c->y, c->M, c->K, c->Kp[kind], c->a_hi[kind],
@@ -358,7 +390,8 @@ int sqt_split(asd_ctx *c, int kind, double *d_out) {
     u.row1 = c->row1;
     u.col4 = c->col4;
     u.col1 = c->col1;
-    u.alpha = (float)(1.0 / (double)c->p.nfile);
+    u.alpha = (float)gemm_alpha(c, shard);
+    u.outer = shard ? 0 : 1;
     u.part = c->part;
     u.status = c->status;
     u.num_sms = c->num_sms;
@@ -377,7 +410,7 @@ int sqt_split(asd_ctx *c, int kind, double *d_out) {
     return rc != ASD_OK ? rc : jrc;
 }
 
-int sqt_async(asd_ctx *c, int mode, double *d_out) {
+int sqt_async(asd_ctx *c, int mode, double *d_out, bool shard = false) {
     if (!c->has_state || !c->has_origin)
         return fail(ASD_ERR_STATE, "set the spins and the origin before S(q,t)");
     if (mode < 0 || mode > 3) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
@@ -387,10 +420,10 @@ int sqt_async(asd_ctx *c, int mode, double *d_out) {
     c->rows_ready = true;
     c->last_launches += 1;
     switch (mode) {
-        case ASD_SQT_FP64: return sqt_plain(c, d_out);
-        case ASD_SQT_FP64_FUSED: return sqt_fp64_fused(c, d_out);
-        case ASD_SQT_TF32X3: return sqt_split(c, 1, d_out);
-        case ASD_SQT_BF16X3: return sqt_split(c, 2, d_out);
+        case ASD_SQT_FP64: return sqt_plain(c, d_out, shard);
+        case ASD_SQT_FP64_FUSED: return sqt_fp64_fused(c, d_out, shard);
+        case ASD_SQT_TF32X3: return sqt_split(c, 1, d_out, shard);
+        case ASD_SQT_BF16X3: return sqt_split(c, 2, d_out, shard);
     }
     return ASD_ERR_INVALID;
 }
@@ -818,6 +851,8 @@ void destroy(asd_ctx *c) {
         cudaStreamDestroy(c->gemm_stream);
     }
     if (c->gemm_done) cudaEventDestroy(c->gemm_done);
+    if (c->zsums) cudaFree(c->zsums);
+    if (c->zero3) cudaFree(c->zero3);
     if (c->y_free) cudaEventDestroy(c->y_free);
     if (c->llg_done) cudaEventDestroy(c->llg_done);
     if (c->blas) cublasDestroy(c->blas);
@@ -1161,6 +1196,63 @@ int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_s
     if (rc != ASD_OK) return rc;
     sqt_out[0] = c->h_out[0];
     sqt_out[1] = c->h_out[1];
+    return ASD_OK;
+}
+
+int asd_ctx_set_ensemble(asd_ctx *c, int nfile_total) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    if (nfile_total < c->p.nfile)
+        return fail(ASD_ERR_INVALID, "nfile_total=%d is below this shard's %d replicas", nfile_total,
+                    c->p.nfile);
+    c->nfile_total = nfile_total;
+    c->has_zsums = false;
+    return ASD_OK;
+}
+
+int asd_ctx_shard_origin_sums(asd_ctx *c, double *d_zsums) {
+    if (!c || !d_zsums) return fail(ASD_ERR_INVALID, "NULL argument");
+    if (!c->has_origin) return fail(ASD_ERR_STATE, "set the origin (t = 0 spins) first");
+    ASD_CUDA_TRY(enter(c));
+    ASD_CUDA_TRY(launch_site_sum(c->origin, c->M, c->p.nfile, d_zsums, c->stream));
+    c->last_launches = 1;
+    return ASD_OK;
+}
+
+int asd_ctx_shard_set_origin_sums(asd_ctx *c, const double *d_zsums) {
+    if (!c || !d_zsums) return fail(ASD_ERR_INVALID, "NULL argument");
+    ASD_CUDA_TRY(enter(c));
+    if (!c->zsums) {
+        int rc = dalloc(&c->zsums, (size_t)c->M * 3 * sizeof(double));
+        if (rc != ASD_OK) return rc;
+    }
+    ASD_CUDA_TRY(cudaMemcpyAsync(c->zsums, d_zsums, (size_t)c->M * 3 * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, c->stream));
+    c->has_zsums = true;
+    return ASD_OK;
+}
+
+int asd_ctx_shard_sqt_async(asd_ctx *c, asd_sqt_mode mode, double *d_part, double *d_sums) {
+    if (!c || !d_part || !d_sums) return fail(ASD_ERR_INVALID, "NULL argument");
+    if (!c->has_state || !c->has_origin)
+        return fail(ASD_ERR_STATE, "set the spins and the origin before S(q,t)");
+    ASD_CUDA_TRY(enter(c));
+    c->last_launches = 0;
+    ASD_CUDA_TRY(launch_site_sum(c->y, c->M, c->p.nfile, d_sums, c->stream));
+    c->last_launches += 1;
+    return sqt_async(c, (int)mode, d_part, true);
+}
+
+int asd_ctx_shard_sqt_finish(asd_ctx *c, const double *d_part, const double *d_sums,
+                             double *d_out) {
+    if (!c || !d_part || !d_sums || !d_out) return fail(ASD_ERR_INVALID, "NULL argument");
+    if (!c->has_zsums)
+        return fail(ASD_ERR_STATE, "exchange the ensemble's origin sums first "
+                                   "(asd_ctx_shard_set_origin_sums)");
+    ASD_CUDA_TRY(enter(c));
+    const int nft = c->nfile_total > 0 ? c->nfile_total : c->p.nfile;
+    ASD_CUDA_TRY(launch_shard_finish(c->M, nft, d_part, d_sums, c->zsums, c->uphase, c->wphase,
+                                     d_out, c->stream));
+    c->last_launches = 1;
     return ASD_OK;
 }
 

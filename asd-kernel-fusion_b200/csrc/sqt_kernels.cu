@@ -51,6 +51,76 @@ __global__ void __launch_bounds__(256) site_mean_kernel(const double *__restrict
     }
 }
 
+// One warp per site: the sum over this context's replicas of the 3
+// components (lane l adds replicas l, l + 32, ..., as site_mean_kernel).
+__global__ void __launch_bounds__(256) site_sum_kernel(const double *__restrict__ state, long M,
+                                                       int nfile, double *__restrict__ sums) {
+    const long site = (long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    if (site >= M) return;
+    const double *p = state + site * 3L * nfile;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int f = lane; f < nfile; f += 32) {
+        sx += p[3 * f];
+        sy += p[3 * f + 1];
+        sz += p[3 * f + 2];
+    }
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    sz = warp_sum(sz);
+    if (lane == 0) {
+        sums[site * 3] = sx;
+        sums[site * 3 + 1] = sy;
+        sums[site * 3 + 2] = sz;
+    }
+}
+
+// S(q,t) of a replica-sharded ensemble from the all-reduced shard values:
+// part = (1/M) sum_ij u_i w_j alpha C_ij over all shards, sums / zsums = the
+// ensemble's site sums at t and at the origin.  The connected-part term
+// (1/M) sum_ij u_i w_j m_i . z_j factorises as (1/M) sum_c U_c W_c with
+// U_c = sum_i u_i m_ic, W_c = sum_j w_j z_jc.  One block, fixed order.
+__global__ void __launch_bounds__(1024) shard_finish_kernel(
+    long M, double inv_nf, const double *__restrict__ part, const double *__restrict__ sums,
+    const double *__restrict__ zsums, const double2 *__restrict__ u,
+    const double2 *__restrict__ w, double *__restrict__ out) {
+    __shared__ double red[12][1024 / 32];
+    double v[12] = {};
+    for (long i = threadIdx.x; i < M; i += 1024) {
+        const double2 ui = u[i], wi = w[i];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double m = sums[i * 3 + c] * inv_nf, z = zsums[i * 3 + c] * inv_nf;
+            v[4 * c] += ui.x * m;
+            v[4 * c + 1] += ui.y * m;
+            v[4 * c + 2] += wi.x * z;
+            v[4 * c + 3] += wi.y * z;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 12; ++q) v[q] = warp_sum(v[q]);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x / 32;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 12; ++q) red[q][wid] = v[q];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[12];
+        for (int q = 0; q < 12; ++q) {
+            t[q] = 0.0;
+            for (int k = 0; k < 1024 / 32; ++k) t[q] += red[q][k];
+        }
+        double ore = 0.0, oim = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            const double ur = t[4 * c], ui = t[4 * c + 1], wr = t[4 * c + 2], wi = t[4 * c + 3];
+            ore += ur * wr - ui * wi;
+            oim += ur * wi + ui * wr;
+        }
+        out[0] = part[0] - ore / (double)M;
+        out[1] = part[1] - oim / (double)M;
+    }
+}
+
 // hi = round(x), lo = round(x - hi), each to the operand format.
 __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
     uint32_t h, l;
@@ -250,6 +320,20 @@ cudaError_t launch_site_mean(const double *state, long M, int nfile, const doubl
                              double *mean, float4 *vec4, float *vec1, cudaStream_t st) {
     const unsigned blocks = (unsigned)((M + 7) / 8);
     site_mean_kernel<<<blocks, 256, 0, st>>>(state, M, nfile, phase, mean, vec4, vec1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_site_sum(const double *state, long M, int nfile, double *sums,
+                            cudaStream_t st) {
+    site_sum_kernel<<<(unsigned)((M + 7) / 8), 256, 0, st>>>(state, M, nfile, sums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shard_finish(long M, int nfile_total, const double *part, const double *sums,
+                                const double *zsums, const double2 *u, const double2 *w,
+                                double *out, cudaStream_t st) {
+    shard_finish_kernel<<<1, 1024, 0, st>>>(M, 1.0 / (double)nfile_total, part, sums, zsums, u, w,
+                                            out);
     return cudaGetLastError();
 }
 

@@ -505,6 +505,86 @@ def run_workload(args):
     return 0
 
 
+def run_sharded(args):
+    """--shard: the headline ensemble (128x128, 500 replicas) split by replicas
+    over the ranks -- strong scaling of one system.  Each rank steps its
+    replicas; every step's S(q,t) is exchanged through asd_b200.shard
+    (all-reduces of 2 and 3*N*N doubles over NCCL) and is the same on every
+    rank.  Device-resident: no e2e leg."""
+    import torch
+    import torch.distributed as dist
+
+    import asd_b200 as asd
+    from asd_b200.shard import ShardedSqt, shard_range
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    N, nf = CONFIG["N"], CONFIG["nfile"]
+    M = N * N
+    b, e = shard_range(nf, rank, world)
+    mode = args.mode
+    params = asd.Params.make(N, e - b, J1=CONFIG["J1"], J2=CONFIG["J2"], alpha=CONFIG["alpha"],
+                             h=CONFIG["h"], dt=CONFIG["dt"])
+    asd.load().asd_set_device(local)
+    ctx = asd.Context(params, modes=[mode])
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_spins(asd.random_spins(N, nf, seed=0)[b:e], as_origin=True)  # one ensemble
+    ens = ShardedSqt(ctx, nf, M)
+    ens.exchange_origin()
+    total = args.warmup + args.steps
+    d_out = torch.zeros(2 * max(total, 1), dtype=torch.float64, device="cuda")
+
+    def one_step(i):
+        ctx.step(1)
+        n = ctx.last_launches()
+        ens.sqt_async(mode, d_out[2 * i:2 * i + 2])
+        return n + ens.launches
+
+    for i in range(args.warmup):
+        one_step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for i in range(args.warmup, total):
+            launches += one_step(i)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ctx.check_device_status()
+    # units per rank = its share of the one ensemble, so the sum over ranks is the ensemble
+    ms, value = aggregate(ms, M * nf / world, world, dist if world > 1 else None, "cuda")
+    sqt_last = complex(*d_out[2 * (total - 1):2 * total].tolist())
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": f"f64 RK4 + {mode} GEMM (fp32 accumulate, f64 reduction)",
+        "data": "synthetic: seeded spins uniform on the sphere",
+        "config": {"workload": WORKLOAD + ", one ensemble split by replicas", "sites": M,
+                   "replicas": nf, "parallelism": f"replicas/{world}", "sqt_mode": mode,
+                   "exchange_doubles_per_step": 2 + 3 * M,
+                   "l2": "inputs larger than L2 at 1 and 2 GPUs"},
+        "gpu_launches": launches, "clocks": clk.summary(), "e2e": None,
+        "sqt_last": [sqt_last.real, sqt_last.imag],
+    }))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -520,9 +600,14 @@ def main():
     ap.add_argument("--ref-target-s", type=float, default=2.0)
     ap.add_argument("--workload", choices=["headline", "sqt256", "adjoint64", "batch48"],
                     default="headline", help="secondary workloads print their own line")
+    ap.add_argument("--shard", action="store_true",
+                    help="strong scaling: split the one headline ensemble by replicas over the "
+                         "ranks (S(q,t) exchanged every step) instead of one ensemble per rank")
     args = ap.parse_args()
     if args.workload != "headline":
         return run_workload(args)
+    if args.shard and args.impl == "ours":
+        return run_sharded(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

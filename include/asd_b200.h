@@ -145,18 +145,52 @@ int asd_ctx_loss_grad(asd_ctx *ctx, int nsteps, int stride, int checkpoint, cons
 
 /* One full step through host buffers, the reference's own contract: spins
  * (AoS) come from host memory, one RK4 step runs, the new spins go back to
- * spin_out and S(q,t) into sqt_out.  spin_in may equal spin_out. */
+ * spin_out and S(q,t) into sqt_out.  spin_in may equal spin_out.  Above 64
+ * replicas the step is pipelined by replica chunk (uploads, RK4, downloads
+ * and K-range S(q,t) GEMMs overlap); pinned host memory lets the copies run
+ * asynchronously.  Synchronous: returns when both buffers are final. */
 int asd_ctx_step_host(asd_ctx *ctx, const double *spin_in, double *spin_out,
                       asd_sqt_mode mode, double sqt_out[2]);
+
+/* Replica sharding of one ensemble over several GPUs, one context per GPU.
+ * Replicas never interact, so each context steps its own nfile replicas; the
+ * correlation GEMM's K axis is the replica axis, so S(q,t) is the sum over
+ * shards of a partial GEMM value plus a connected-part term that needs only
+ * the ensemble's site means.  Per evaluation the shards exchange 2 + 3*N*N
+ * doubles (an all-reduce the caller runs, e.g. over NCCL); the origin's site
+ * sums are exchanged once.  No counterpart in the reference (one process).
+ *
+ *   asd_ctx_set_ensemble(ctx, nfile_total)            replicas of the whole ensemble
+ *   asd_ctx_set_spins(ctx, shard_spins, 1)
+ *   asd_ctx_shard_origin_sums(ctx, d_zsums)           [N*N][3] doubles, this shard
+ *     (all-reduce d_zsums)
+ *   asd_ctx_shard_set_origin_sums(ctx, d_zsums)       the ensemble's
+ *   per step:
+ *     asd_ctx_step(ctx, 1)
+ *     asd_ctx_shard_sqt_async(ctx, mode, d_part, d_sums)   2 + [N*N][3] doubles
+ *     (all-reduce d_part and d_sums)
+ *     asd_ctx_shard_sqt_finish(ctx, d_part, d_sums, d_out) S(q,t) of the ensemble
+ *
+ * d_part is this shard's (1/M) sum_ij u_i w_j C_ij with C scaled by
+ * 1/nfile_total and no connected-part term; the finish adds that term from
+ * the means in FP64.  All pointers are device memory, enqueued on the
+ * context's stream.  Setting new origin spins requires a new exchange. */
+int asd_ctx_set_ensemble(asd_ctx *ctx, int nfile_total);
+int asd_ctx_shard_origin_sums(asd_ctx *ctx, double *d_zsums);
+int asd_ctx_shard_set_origin_sums(asd_ctx *ctx, const double *d_zsums);
+int asd_ctx_shard_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_part, double *d_sums);
+int asd_ctx_shard_sqt_finish(asd_ctx *ctx, const double *d_part, const double *d_sums,
+                             double *d_out);
 
 /* How asd_ctx_step runs one RK4 step.  Both give bit-identical spins. */
 #define ASD_LLG_STAGES 0     /* default: four launches, one fused kernel per RK4
                                 stage, HBM-bound (384 B of DRAM traffic per
-                                site-step; 83% of HBM bandwidth on B200)      */
+                                site-step; about 75% of HBM bandwidth on B200) */
 #define ASD_LLG_FUSED_STEP 1 /* one launch per step, the four stages
                                 temporally blocked in shared memory (48 B of
                                 DRAM traffic per site-step, but FP64- and
-                                latency-bound: slightly slower on B200)       */
+                                latency-bound: within 10% of the stages on
+                                B200, either way depending on the lattice)   */
 int asd_ctx_set_llg_kernel(asd_ctx *ctx, int kernel);
 
 /* K elements accumulated per TMEM chunk by the split S(q,t) modes (rounded

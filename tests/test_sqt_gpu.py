@@ -178,18 +178,19 @@ def test_step_pipelined_behind_the_split_gemm(oracle, mode, kernel):
     assert np.array_equal(spins[0], want)
 
 
-@pytest.mark.parametrize("pinned", [False, True])
-def test_step_host_in_replica_chunks(oracle, pinned):
+@pytest.mark.parametrize("nf,pinned", [(200, False), (200, True), (65, True), (128, True)])
+def test_step_host_in_replica_chunks(oracle, nf, pinned):
     """Ensembles larger than one upload chunk (64 replicas and up) take the
     pipelined asd_ctx_step_host: per replica chunk, upload, RK4, download and
     a GEMM over that chunk's K columns.  200 replicas make chunks of 64, 64,
-    64 and a ragged 8.  The spins must equal the device path and the oracle
+    64 and a ragged 8 (65: 64 + 1; 128: two whole chunks).  The spins must
+    equal the device path and the oracle
     bit for bit; S(q,t) must equal the device path exactly in the FP64 modes
     and agree to the split-precision tolerance (1e-5 of the FP64 value) in
     the split modes, whose partial sums are added in another order."""
     import torch
 
-    N, nf = 16, 200
+    N = 16
     s0 = asd.random_spins(N, nf, seed=12)
     kw = dict(J1=-1.0, J2=0.2, alpha=0.05, h=(0, 0, 0.5), dt=0.005)
     p = asd.Params.make(N, nf, vx=3, vy=2, **kw)
