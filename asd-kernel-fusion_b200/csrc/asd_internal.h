@@ -56,7 +56,8 @@ cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const
                              double *acc, double *ys_out, cudaStream_t st);
 
 // One whole RK4 step (all four stages + renormalisation) in one launch,
-// temporally blocked in shared memory: y -> yout (distinct buffers).
+// streamed down the lattice by column band (llg_kernels.cu): y -> yout
+// (distinct buffers), replicas [a.f0, a.f0 + a.nc) only.
 cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *yout,
                                   cudaStream_t st);
 

@@ -91,7 +91,7 @@ struct asd_ctx {
     // asd_ctx_step_host: copy stream and event for the overlapped read-back
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t spins_ready = nullptr;
-    int llg_kernel = ASD_LLG_STAGES;
+    int llg_kernel = ASD_LLG_FUSED_STEP;
     // Pipelining of asd_ctx_step behind asd_ctx_sqt_async: once a split-mode
     // S(q,t) has turned y into its GEMM operands, the GEMM reads none of the
     // LLG buffers, so the next RK4 step may run beside it on llg_stream.
@@ -741,6 +741,10 @@ int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int m
     const cudaStream_t comp = c->stream, up = c->h2d_stream, down = c->copy_stream;
     LLGArgs a = c->a;
     long nparts = 0;
+    // The one-launch step is out of place: each chunk's new state goes to
+    // ys_a (its replicas only), and y and ys_a swap after the last chunk.
+    const bool fused = c->llg_kernel == ASD_LLG_FUSED_STEP;
+    double *const ynew = fused ? c->ys_a : c->y;
     for (int r = 0; r < nchunks; ++r) {
         const int f0 = r * cr, nc = (nf - f0 < cr) ? nf - f0 : cr, b = r & 1;
         const bool last = (f0 + nc == nf);
@@ -754,25 +758,29 @@ int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int m
         ASD_CUDA_TRY(cudaEventRecord(c->in_free[b], comp));
         a.f0 = f0;
         a.nc = nc;
-        ASD_CUDA_TRY(launch_llg_stage(1, a, c->y, c->y, c->acc, c->ys_a, comp));
-        ASD_CUDA_TRY(launch_llg_stage(2, a, c->y, c->ys_a, c->acc, c->ys_b, comp));
-        ASD_CUDA_TRY(launch_llg_stage(3, a, c->y, c->ys_b, c->acc, c->ys_a, comp));
-        ASD_CUDA_TRY(launch_llg_stage(4, a, nullptr, c->ys_a, c->acc, c->y, comp));
+        if (fused) {
+            ASD_CUDA_TRY(launch_llg_step_fused(a, c->y, ynew, comp));
+        } else {
+            ASD_CUDA_TRY(launch_llg_stage(1, a, c->y, c->y, c->acc, c->ys_a, comp));
+            ASD_CUDA_TRY(launch_llg_stage(2, a, c->y, c->ys_a, c->acc, c->ys_b, comp));
+            ASD_CUDA_TRY(launch_llg_stage(3, a, c->y, c->ys_b, c->acc, c->ys_a, comp));
+            ASD_CUDA_TRY(launch_llg_stage(4, a, nullptr, c->ys_a, c->acc, c->y, comp));
+        }
         ASD_CUDA_TRY(cudaStreamWaitEvent(comp, c->out_free[b], 0));
-        ASD_CUDA_TRY(launch_sitemajor_to_aos_range(c->y, c->stage_out[b], M, nf, f0, nc, comp));
+        ASD_CUDA_TRY(launch_sitemajor_to_aos_range(ynew, c->stage_out[b], M, nf, f0, nc, comp));
         ASD_CUDA_TRY(cudaEventRecord(c->out_ready[b], comp));
         ASD_CUDA_TRY(cudaStreamWaitEvent(down, c->out_ready[b], 0));
         ASD_CUDA_TRY(cudaMemcpyAsync(spin_out + off, c->stage_out[b], bytes,
                                      cudaMemcpyDeviceToHost, down));
         ASD_CUDA_TRY(cudaEventRecord(c->out_free[b], down));
-        c->last_launches += 6;
+        c->last_launches += fused ? 3 : 6;
         if (!kind) continue;
         const int kbeg = 3 * f0, kend = last ? c->Kp[kind] : 3 * (f0 + nc);
-        ASD_CUDA_TRY(launch_split_range(kind, c->y, M, c->K, c->Kp[kind], kbeg, kend,
+        ASD_CUDA_TRY(launch_split_range(kind, ynew, M, c->K, c->Kp[kind], kbeg, kend,
                                         c->a_hi[kind], c->a_lo[kind], comp));
         c->last_launches += 1;
         if (last) {
-            ASD_CUDA_TRY(launch_site_mean(c->y, M, nf, c->uphase, c->mean_t, c->row4, c->row1,
+            ASD_CUDA_TRY(launch_site_mean(ynew, M, nf, c->uphase, c->mean_t, c->row4, c->row1,
                                           comp));
             c->last_launches += 1;
         }
@@ -800,6 +808,10 @@ int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int m
         if (grid < 0) return grid;
         nparts += grid;
         c->last_launches += 1;
+    }
+    if (fused) {  // ys_a holds the new state of every replica
+        c->ys_a = c->y;
+        c->y = ynew;
     }
     c->state_version += 2;  // as set_spins + step
     c->has_state = true;

@@ -7,6 +7,7 @@
 // to the reference's euler / runge_kutta / renormalisation built with
 // -ffp-contract=off (llg_sqt_baseline.c:29-142, :298-309).
 #include <cstdlib>
+#include <type_traits>
 
 #include "asd_internal.h"
 
@@ -96,199 +97,296 @@ cudaError_t launch_stage_t(const LLGArgs &a, const double *y, const double *ys, 
     return cudaGetLastError();
 }
 
-// ------------------------------------------------ temporally blocked step
-// One RK4 step per launch.  A CTA owns a 16 x 16 core of sites for F
-// replicas and loads the 24 x 24 patch around it (a halo of 4 sites, one per
-// stage) into shared memory.  Stage s then runs on the region within
-// distance 4 - s of the core (Chebyshev distance, which also covers the
-// diagonal J2 neighbours), so stage 4 produces exactly the core.  Stage
-// inputs ping-pong between two shared buffers; the base state and the
-// running combination of each (site, replica) stay in the registers of the
-// thread that owns it.  Only y is read and only the renormalised core is
-// written: 48 bytes of DRAM traffic per site-step instead of 384.  The
-// arithmetic per (site, replica) is the stage kernels' (bit-identical).
-constexpr int FT = 16;              // core side
-constexpr int FH = 4;               // halo = number of stages
-constexpr int FP = FT + 2 * FH;     // patch side
-constexpr int FR1 = (FT + 6) * (FT + 6);  // sites of the stage-1 region
+// ------------------------------------------------ row-streaming step
+// One RK4 step per launch, streamed down the lattice.  The work is a set of
+// columns of rows: a band of wc core columns (plus 4 halo columns each side,
+// one per stage) for SF replicas, over all N rows.  A persistent grid of
+// CTAs splits the band x replica-group x row space evenly, each CTA taking
+// one contiguous run of rows that crosses at most a few (band, group)
+// boundaries; every piece of a run is streamed on its own.
+//
+// A piece of rs rows (relative rows 0..rs+7: 4 halo rows above and below)
+// is walked once, two phases per iteration j, separated by barriers:
+//   phase A: stage 1 on row j-1 (y rows j-2..j), stage 3 on row j-4;
+//   phase B: cp.async prefetch of y row j+1, stage 2 on row j-2, stage 4 on
+//            row j-5 (renormalised, stored to DRAM).
+// Each stage reads only rows written in an earlier phase, and the two stages
+// of a phase are independent (twice the instruction-level parallelism of a
+// stage-per-phase schedule, half the barriers).  Stage inputs live in rings
+// of 3 rows, y in a ring of 5 rows, and the running RK4 combination of the
+// five rows in flight in registers.  Halo work is (wc + 8) / wc in columns;
+// DRAM traffic: y read once (the halo columns mostly from L2) and y_new
+// written once, 48 bytes per site-step.  Per (site, replica) the arithmetic
+// is the stage kernels' (bit-identical).
+namespace stream {
+constexpr int SF = 4;                  // replicas per CTA (96 contiguous bytes per site)
+constexpr int WC_MAX = 64;             // core columns per band
+constexpr int WT_MAX = WC_MAX + 8;     // columns held per row
+constexpr int NT_MAX = WT_MAX * SF;    // threads per CTA at most (288)
+constexpr int YR = 5;                  // rows of the y ring
+constexpr int ROWS = YR + 3 * 3;       // row buffers in shared memory
+constexpr int MIN_RUN = 16;            // fewest rows per CTA
+}  // namespace stream
 
-// Site of the patch for the idx-th entry of the region list: the core in
-// row-major order first, then the rings at distance 1, 2, 3.  So the first
-// 256, 324, 400, 484 entries are the regions of stages 4, 3, 2, 1.
-__device__ __forceinline__ void region_site(int idx, int &r, int &c) {
-    if (idx < FT * FT) {
-        r = FH + idx / FT;
-        c = FH + idx % FT;
-        return;
-    }
-    idx -= FT * FT;
-    int d = 1;
-    for (; d < 3; ++d) {
-        const int cnt = 4 * (FT + 2 * d) - 4;
-        if (idx < cnt) break;
-        idx -= cnt;
-    }
-    const int L = FT + 2 * d;
-    if (idx < L) { r = FH - d; c = FH - d + idx; return; }
-    idx -= L;
-    if (idx < L) { r = FH + FT - 1 + d; c = FH - d + idx; return; }
-    idx -= L;
-    if (idx < L - 2) { r = FH - d + 1 + idx; c = FH - d; return; }
-    idx -= L - 2;
-    r = FH - d + 1 + idx;
-    c = FH + FT - 1 + d;
+struct StreamGeom {
+    int wc;   // core columns per band (a multiple of 8)
+    int wt;   // wc + 8 columns held per row
+    int nb;   // bands: ceil(N / wc)
+    int ng;   // replica groups: ceil(nc / SF)
+    int rw;   // doubles per row buffer: wt * SF * 3
+    long run; // rows per CTA of the nb * ng * N rows of work
+};
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-template <int F, int NT, bool J2, bool H, bool DAMP>
-// At most 64 registers per thread so that four CTAs share an SM: the stages
-// are separated by barriers, and more resident CTAs hide them (measured:
-// 0.60 ms per step at 128x128x500 with four CTAs per SM, 0.83 ms with two).
-__global__ void __launch_bounds__(NT, 4 * 256 / NT) llg_step_fused_kernel(LLGArgs a, int tiles_x,
-                                                            const double *__restrict__ y,
-                                                            double *__restrict__ yout) {
-    extern __shared__ double fsm[];
-    constexpr int SLOT = 3 * F;                      // doubles per patch site
-    constexpr int NITEM = (FR1 * F + NT - 1) / NT;   // items owned per thread
-    double *bufA = fsm;
-    double *bufB = fsm + FP * FP * SLOT;
-    const int tile = blockIdx.x;
-    const int R0 = (tile / tiles_x) * FT, C0 = (tile % tiles_x) * FT;
-    const int f0 = blockIdx.y * F;
+__device__ __forceinline__ V3 ld3(const double *p) { return V3{p[0], p[1], p[2]}; }
+
+// Inputs of one stage at one (site, replica): the centre value, its
+// neighbours in llg_rhs's order -- (row+1), (row-1), (col-1), (col+1), then
+// the diagonals (+1,+1), (+1,-1), (-1,+1), (-1,-1) -- and the RK4 base y.
+struct SIn {
+    V3 s, nb[4], n2[4], yb;
+};
+
+// Loads record `me` of row buffer `mid` and its neighbours from the rows
+// above (`up`, row-1) and below (`dn`, row+1); CS = doubles per column.
+template <bool J2>
+__device__ __forceinline__ void load_in(const double *up, const double *mid, const double *dn,
+                                        int me, SIn &in) {
+    constexpr int CS = stream::SF * 3;
+    in.s = ld3(mid + me);
+    in.nb[0] = ld3(dn + me);
+    in.nb[1] = ld3(up + me);
+    in.nb[2] = ld3(mid + me - CS);
+    in.nb[3] = ld3(mid + me + CS);
+    if (J2) {
+        in.n2[0] = ld3(dn + me + CS);
+        in.n2[1] = ld3(dn + me - CS);
+        in.n2[2] = ld3(up + me + CS);
+        in.n2[3] = ld3(up + me - CS);
+    }
+}
+
+template <bool J2, bool H, bool DAMP>
+__global__ void __launch_bounds__(stream::NT_MAX, 2)
+    llg_step_stream_kernel(LLGArgs a, StreamGeom g, const double *__restrict__ y,
+                           double *__restrict__ yout) {
+    using namespace stream;
+    extern __shared__ double ssm[];
+    const int rw = g.rw;
+    double *const ybuf = ssm;
+    double *const s1 = ssm + YR * rw;
+    double *const s2 = s1 + 3 * rw;
+    double *const s3 = s2 + 3 * rw;
     const int N = a.N;
     const long K = 3L * a.nfile;
-    const int nf = min(F, a.nfile - f0);  // replicas present in this chunk
+    const int tid = threadIdx.x;
+    const int cl = tid / SF, fl = tid - cl * SF;
+    const int me = tid * 3;  // == (cl * SF + fl) * 3
+    const bool comp = cl >= 1 && cl <= g.wt - 2;
+    const double dt = a.dt;
 
-    // load the patch (periodic wrap), zero for replicas past nfile
-    for (int e = threadIdx.x; e < FP * FP * SLOT; e += NT) {
-        const int slot = e / SLOT, w = e - slot * SLOT;
-        const int pr = slot / FP, pc = slot - pr * FP;
-        const int gr = ((R0 + pr - FH) % N + N) % N;
-        const int gc = ((C0 + pc - FH) % N + N) % N;
-        double v = 0.0;
-        if (w < 3 * nf) v = y[((long)gr * N + gc) * K + 3L * f0 + w];
-        bufA[e] = v;
-    }
-    __syncthreads();
+    const long total = (long)g.nb * g.ng * N;
+    long b = (long)blockIdx.x * g.run;
+    const long e = min(b + g.run, total);
+    while (b < e) {
+        // piece: rows [R0, R0 + rs) of work column u = band + nb * grp
+        const long u = b / N;
+        const int R0 = (int)(b - u * N);
+        const int rs = (int)min((long)(N - R0), e - b);
+        b += rs;
+        const int band = (int)(u % g.nb), grp = (int)(u / g.nb);
+        const int C0 = band * g.wc;
+        const int fbase = a.f0 + grp * SF;
+        const int nvalid = min(SF, a.f0 + a.nc - fbase);
+        const int gcol = C0 + cl - 4;
+        const bool store = cl >= 4 && cl < 4 + g.wc && gcol < N && fl < nvalid;
+        const int J = rs + 9;  // iterations: stage 4 reaches relative row rs + 3 at j = rs + 8
 
-    double yb[NITEM][3], acc[NITEM][3];
-    int slot_of[NITEM];
-#pragma unroll
-    for (int j = 0; j < NITEM; ++j) {
-        const int it = threadIdx.x + j * NT;
-        slot_of[j] = -1;
-        if (it < FR1 * F) {
-            int r, c;
-            region_site(it / F, r, c);
-            slot_of[j] = r * FP + c;
-            const double *p = bufA + slot_of[j] * SLOT + (it % F) * 3;
-            yb[j][0] = p[0];
-            yb[j][1] = p[1];
-            yb[j][2] = p[2];
-        }
-    }
-    // The region list covers each stage's sites first (see region_site).
-    const int stage_items[4] = {FR1 * F, (FT + 4) * (FT + 4) * F, (FT + 2) * (FT + 2) * F,
-                                FT * FT * F};
-    double *in = bufA, *out = bufB;
-#pragma unroll
-    for (int s = 1; s <= 4; ++s) {
-        const int lim = stage_items[s - 1];
-        // phase 1: every owned item's increment k = dt * f(stage input), all
-        // loads from `in` before any store to `out`
-        double kv[NITEM][3];
-#pragma unroll
-        for (int j = 0; j < NITEM; ++j) {
-            const int it = threadIdx.x + j * NT;
-            const int f = it % F;
-            kv[j][0] = kv[j][1] = kv[j][2] = 0.0;
-            if (it >= lim || f >= nf) continue;
-            const int slot = slot_of[j];
-            const V3 d = llg_rhs<J2, H, DAMP>(in, SLOT, 3L * f, FP, slot / FP, slot % FP, a);
-            kv[j][0] = dm(d.x, a.dt);
-            kv[j][1] = dm(d.y, a.dt);
-            kv[j][2] = dm(d.z, a.dt);
-        }
-        // phase 2: stage combination
-#pragma unroll
-        for (int j = 0; j < NITEM; ++j) {
-            const int it = threadIdx.x + j * NT;
-            const int f = it % F;
-            if (it >= lim || f >= nf) continue;
-            const int slot = slot_of[j];
-            const double k0 = kv[j][0], k1 = kv[j][1], k2 = kv[j][2];
-            double *o = out + slot * SLOT + 3 * f;
-            if (s == 1) {
-                o[0] = da(yb[j][0], half(k0));
-                o[1] = da(yb[j][1], half(k1));
-                o[2] = da(yb[j][2], half(k2));
-                acc[j][0] = da(yb[j][0], div6(k0));
-                acc[j][1] = da(yb[j][1], div6(k1));
-                acc[j][2] = da(yb[j][2], div6(k2));
-            } else if (s == 2) {
-                o[0] = da(yb[j][0], half(k0));
-                o[1] = da(yb[j][1], half(k1));
-                o[2] = da(yb[j][2], half(k2));
-                acc[j][0] = da(acc[j][0], div3(k0));
-                acc[j][1] = da(acc[j][1], div3(k1));
-                acc[j][2] = da(acc[j][2], div3(k2));
-            } else if (s == 3) {
-                o[0] = da(yb[j][0], k0);
-                o[1] = da(yb[j][1], k1);
-                o[2] = da(yb[j][2], k2);
-                acc[j][0] = da(acc[j][0], div3(k0));
-                acc[j][1] = da(acc[j][1], div3(k1));
-                acc[j][2] = da(acc[j][2], div3(k2));
-            } else {
-                const double o0 = da(acc[j][0], div6(k0));
-                const double o1 = da(acc[j][1], div6(k1));
-                const double o2 = da(acc[j][2], div6(k2));
-                const double nrm = __dsqrt_rn(da(da(dm(o0, o0), dm(o1, o1)), dm(o2, o2)));
-                const int gr = R0 + slot / FP - FH, gc = C0 + slot % FP - FH;
-                if (gr < N && gc < N) {
-                    double *g = yout + ((long)gr * N + gc) * K + 3L * (f0 + f);
-                    g[0] = dq(dm(a.spin_len, o0), nrm);
-                    g[1] = dq(dm(a.spin_len, o1), nrm);
-                    g[2] = dq(dm(a.spin_len, o2), nrm);
+        // y row R0 - 4 + j (periodic) of this band and replica group -> y ring
+        auto load_row = [&](int j) {
+            int gr = (R0 - 4 + j) % N;
+            if (gr < 0) gr += N;
+            double *dst = ybuf + (j % YR) * rw;
+            for (int x = tid; x < rw; x += blockDim.x) {
+                const int c = x / (SF * 3), w = x - c * (SF * 3);
+                int gc = (C0 - 4 + c) % N;
+                if (gc < 0) gc += N;
+                if (w < 3 * nvalid)
+                    cp_async8(dst + x, y + ((long)gr * N + gc) * K + 3L * fbase + w);
+                else
+                    dst[x] = 0.0;
+            }
+        };
+        // Stage bodies on relative row r (in y slot r % 5, ring slot r % 3),
+        // each split into its shared-memory loads (ld) and its arithmetic and
+        // stores (st*), so that the two stages of a phase can issue all their
+        // loads before either computes.
+        auto ld = [&](const double *ring, int nrows, int r, bool with_base) {
+            SIn in;
+            const double *up = ring + ((r - 1) % nrows) * rw, *mid = ring + (r % nrows) * rw,
+                         *dn = ring + ((r + 1) % nrows) * rw;
+            load_in<J2>(up, mid, dn, me, in);
+            if (with_base) in.yb = ld3(ybuf + (r % YR) * rw + me);
+            return in;
+        };
+        auto st1 = [&](const SIn &in, int r, double *ac) {  // s1 = y + k/2, acc = y + k/6
+            const V3 d = llg_rhs_vals<J2, H, DAMP>(in.s, in.nb, in.n2, a);
+            const double k0 = dm(d.x, dt), k1 = dm(d.y, dt), k2 = dm(d.z, dt);
+            double *o = s1 + (r % 3) * rw + me;
+            o[0] = da(in.s.x, half(k0));
+            o[1] = da(in.s.y, half(k1));
+            o[2] = da(in.s.z, half(k2));
+            ac[0] = da(in.s.x, div6(k0));
+            ac[1] = da(in.s.y, div6(k1));
+            ac[2] = da(in.s.z, div6(k2));
+        };
+        auto st2 = [&](const SIn &in, int r, double *ac) {  // s2 = y + k/2, acc += k/3
+            const V3 d = llg_rhs_vals<J2, H, DAMP>(in.s, in.nb, in.n2, a);
+            const double k0 = dm(d.x, dt), k1 = dm(d.y, dt), k2 = dm(d.z, dt);
+            double *o = s2 + (r % 3) * rw + me;
+            o[0] = da(in.yb.x, half(k0));
+            o[1] = da(in.yb.y, half(k1));
+            o[2] = da(in.yb.z, half(k2));
+            ac[0] = da(ac[0], div3(k0));
+            ac[1] = da(ac[1], div3(k1));
+            ac[2] = da(ac[2], div3(k2));
+        };
+        auto st3 = [&](const SIn &in, int r, double *ac) {  // s3 = y + k, acc += k/3
+            const V3 d = llg_rhs_vals<J2, H, DAMP>(in.s, in.nb, in.n2, a);
+            const double k0 = dm(d.x, dt), k1 = dm(d.y, dt), k2 = dm(d.z, dt);
+            double *o = s3 + (r % 3) * rw + me;
+            o[0] = da(in.yb.x, k0);
+            o[1] = da(in.yb.y, k1);
+            o[2] = da(in.yb.z, k2);
+            ac[0] = da(ac[0], div3(k0));
+            ac[1] = da(ac[1], div3(k1));
+            ac[2] = da(ac[2], div3(k2));
+        };
+        auto st4 = [&](const SIn &in, int r, const double *ac) {  // acc + k/6, renormalised
+            const V3 d = llg_rhs_vals<J2, H, DAMP>(in.s, in.nb, in.n2, a);
+            const double k0 = dm(d.x, dt), k1 = dm(d.y, dt), k2 = dm(d.z, dt);
+            const double o0 = da(ac[0], div6(k0));
+            const double o1 = da(ac[1], div6(k1));
+            const double o2 = da(ac[2], div6(k2));
+            const double nrm = __dsqrt_rn(da(da(dm(o0, o0), dm(o1, o1)), dm(o2, o2)));
+            if (store) {
+                double *gp = yout + ((long)(R0 - 4 + r) * N + gcol) * K + 3L * (fbase + fl);
+                gp[0] = dq(dm(a.spin_len, o0), nrm);
+                gp[1] = dq(dm(a.spin_len, o1), nrm);
+                gp[2] = dq(dm(a.spin_len, o2), nrm);
+            }
+        };
+
+        double acc[5][3];  // row r's combination in acc[r % 5]
+        __syncthreads();   // the previous piece is done with every buffer
+        load_row(0);
+        cp_async_commit();
+        // Iteration j with R = j % 5 known at compile time, so acc[] is
+        // indexed statically.  Valid rows: stage s on relative rows s..rs+7-s.
+        auto iter = [&](auto rc, int j) {
+            constexpr int R = decltype(rc)::value;
+            if (j >= J) return;  // uniform over the CTA
+            cp_async_wait_all();
+            __syncthreads();  // phase A: stage 1 on row j-1, stage 3 on row j-4
+            if (comp) {
+                const bool d1 = j >= 2 && j <= rs + 7, d3 = j >= 7;
+                if (d1 && d3) {
+                    const SIn i1 = ld(ybuf, YR, j - 1, false), i3 = ld(s2, 3, j - 4, true);
+                    st1(i1, j - 1, acc[(R + 4) % 5]);
+                    st3(i3, j - 4, acc[(R + 1) % 5]);
+                } else if (d1) {
+                    st1(ld(ybuf, YR, j - 1, false), j - 1, acc[(R + 4) % 5]);
+                } else if (d3) {
+                    st3(ld(s2, 3, j - 4, true), j - 4, acc[(R + 1) % 5]);
                 }
             }
-        }
-        if (s < 4) {
-            __syncthreads();
-            double *t = in;
-            in = out;
-            out = t;
+            __syncthreads();  // phase B: prefetch, stage 2 on row j-2, stage 4 on row j-5
+            if (j + 1 <= rs + 7) load_row(j + 1);
+            cp_async_commit();
+            if (comp) {
+                const bool d2 = j >= 4 && j <= rs + 7, d4 = j >= 9;
+                if (d2 && d4) {
+                    const SIn i2 = ld(s1, 3, j - 2, true), i4 = ld(s3, 3, j - 5, false);
+                    st2(i2, j - 2, acc[(R + 3) % 5]);
+                    st4(i4, j - 5, acc[R]);
+                } else if (d2) {
+                    st2(ld(s1, 3, j - 2, true), j - 2, acc[(R + 3) % 5]);
+                } else if (d4) {
+                    st4(ld(s3, 3, j - 5, false), j - 5, acc[R]);
+                }
+            }
+        };
+        for (int j0 = 0; j0 < J; j0 += 5) {
+            iter(std::integral_constant<int, 0>{}, j0);
+            iter(std::integral_constant<int, 1>{}, j0 + 1);
+            iter(std::integral_constant<int, 2>{}, j0 + 2);
+            iter(std::integral_constant<int, 3>{}, j0 + 3);
+            iter(std::integral_constant<int, 4>{}, j0 + 4);
         }
     }
 }
 
-template <int F, int NT>
-cudaError_t launch_fused_t(const LLGArgs &a, const double *y, double *yout, cudaStream_t st) {
-    const int tiles_x = (a.N + FT - 1) / FT;
-    dim3 grid((unsigned)(tiles_x * tiles_x), (unsigned)((a.nfile + F - 1) / F));
-    if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
-    const size_t smem = 2ull * FP * FP * 3 * F * sizeof(double);
-    const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
-    cudaError_t e = cudaSuccess;
-#define ASD_FUSED_CASE(S, J, Hh, D)                                                         \
-    case S: {                                                                               \
-        auto k = llg_step_fused_kernel<F, NT, J, Hh, D>;                                    \
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        if (e == cudaSuccess) k<<<grid, NT, smem, st>>>(a, tiles_x, y, yout);               \
-        break;                                                                              \
-    }
-    switch (sel) {
-        ASD_FUSED_CASE(0, false, false, false)
-        ASD_FUSED_CASE(1, false, false, true)
-        ASD_FUSED_CASE(2, false, true, false)
-        ASD_FUSED_CASE(3, false, true, true)
-        ASD_FUSED_CASE(4, true, false, false)
-        ASD_FUSED_CASE(5, true, false, true)
-        ASD_FUSED_CASE(6, true, true, false)
-        ASD_FUSED_CASE(7, true, true, true)
-    }
-#undef ASD_FUSED_CASE
+size_t stream_smem_bytes(const StreamGeom &g) {
+    return (size_t)stream::ROWS * g.rw * sizeof(double);
+}
+
+template <bool J2, bool H, bool DAMP>
+cudaError_t launch_stream_t(const LLGArgs &a, const double *y, double *yout, cudaStream_t st) {
+    using namespace stream;
+    auto k = llg_step_stream_kernel<J2, H, DAMP>;
+    StreamGeom g;
+    g.nb = (a.N + WC_MAX - 1) / WC_MAX;
+    g.wc = ((a.N + g.nb - 1) / g.nb + 7) / 8 * 8;  // wt * SF is a whole number of warps
+    g.wt = g.wc + 8;
+    g.rw = g.wt * SF * 3;
+    g.ng = (a.nc + SF - 1) / SF;
+    const int threads = g.wt * SF;
+    const size_t smem = stream_smem_bytes(g);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem)) !=
+        cudaSuccess)
+        return e;
+    // One CTA per resident slot, each with an equal run of the rows of work
+    // (at least MIN_RUN, so the 9-iteration fill of a piece stays small).
+    const long total = (long)g.nb * g.ng * a.N;
+    const long slots = (long)sms * (per_sm > 0 ? per_sm : 1);
+    long run = (total + slots - 1) / slots;
+    if (run < MIN_RUN) run = MIN_RUN;
+    g.run = run;
+    const long blocks = (total + run - 1) / run;
+    if (blocks > 0x7fffffffL) return cudaErrorInvalidConfiguration;
+    k<<<(unsigned)blocks, threads, smem, st>>>(a, g, y, yout);
     return cudaGetLastError();
+}
+
+cudaError_t launch_stream(const LLGArgs &a, const double *y, double *yout, cudaStream_t st) {
+    if (a.f0 < 0 || a.nc < 1 || a.f0 + a.nc > a.nfile) return cudaErrorInvalidValue;
+    const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
+    switch (sel) {
+        case 0: return launch_stream_t<false, false, false>(a, y, yout, st);
+        case 1: return launch_stream_t<false, false, true>(a, y, yout, st);
+        case 2: return launch_stream_t<false, true, false>(a, y, yout, st);
+        case 3: return launch_stream_t<false, true, true>(a, y, yout, st);
+        case 4: return launch_stream_t<true, false, false>(a, y, yout, st);
+        case 5: return launch_stream_t<true, false, true>(a, y, yout, st);
+        case 6: return launch_stream_t<true, true, false>(a, y, yout, st);
+        default: return launch_stream_t<true, true, true>(a, y, yout, st);
+    }
 }
 
 // Tiled transpose between [nfile][M][3] and [M][nfile][3] through shared
@@ -421,8 +519,7 @@ cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const
 
 cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *yout,
                                   cudaStream_t st) {
-    // 2 replicas per CTA, 256 threads (55 KB of shared memory, 4 CTAs per SM)
-    return launch_fused_t<2, 256>(a, y, yout, st);
+    return launch_stream(a, y, yout, st);
 }
 
 cudaError_t launch_aos_to_sitemajor_range(const double *aos, double *sm, long M, int nfile,

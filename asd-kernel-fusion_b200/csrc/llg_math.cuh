@@ -14,21 +14,24 @@ __device__ __forceinline__ double half(double x) { return __dmul_rn(x, 0.5); }
 // x / d for the constants d = 3 and 6, correctly rounded, by Markstein's
 // correction step (P. Markstein, IBM J. Res. Dev. 34(1), 1990): with
 // yinv = RN(1/d), q = RN(x * yinv) is within one ulp of x/d, the remainder
-// r = x - q d is exact in one FMA, and RN(q + r * yinv) is RN(x/d).  Valid
-// away from overflow and the subnormal range, which the RK4 increments never
-// reach; zeros keep their sign.  Three FP64 operations instead of a
-// division routine; tests compare it with __ddiv_rn bit for bit.
+// x - q d is exact in one FMA, and RN(q + (x - q d) * yinv) is RN(x/d).  The
+// remainder is formed as -(q d - x): for x != 0 that is the same exact value
+// (a zero remainder is absorbed by q != 0), and for x = +-0 it makes the
+// result +-0, so zeros keep their sign without a compare.  Valid away from
+// overflow and the subnormal range, which the RK4 increments never reach.
+// Three FP64 operations instead of a division routine; tests compare it
+// with __ddiv_rn bit for bit.
 __device__ __forceinline__ double div3(double x) {
     constexpr double yinv = 1.0 / 3.0;  // RN(1/3), folded at compile time
     const double q = __dmul_rn(x, yinv);
-    const double r = __fma_rn(-q, 3.0, x);
-    return x == 0.0 ? x : __fma_rn(r, yinv, q);
+    const double t = __fma_rn(q, 3.0, -x);
+    return __fma_rn(-t, yinv, q);
 }
 __device__ __forceinline__ double div6(double x) {
     constexpr double yinv = 1.0 / 6.0;  // RN(1/6)
     const double q = __dmul_rn(x, yinv);
-    const double r = __fma_rn(-q, 6.0, x);
-    return x == 0.0 ? x : __fma_rn(r, yinv, q);
+    const double t = __fma_rn(q, 6.0, -x);
+    return __fma_rn(-t, yinv, q);
 }
 
 struct V3 {

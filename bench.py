@@ -39,7 +39,46 @@ CONFIG = dict(N=128, nfile=500, J1=-1.0, J2=0.0, alpha=0.05, h=(0.0, 0.0, 0.5), 
 WORKLOAD = "llg-rk4+sqt 128x128 lattice, 500 replicas, J=-1, h=(0,0,0.5), alpha=0.05, dt=0.005"
 METRIC = "LLG site-steps/s + S(q,t) GEMM TFLOP/s, mixed vs FP64 plain at stated error"
 LLG_BYTES_PER_SITE_STEP = 384  # 4 fused stage kernels: 3+5+5+3 FP64 3-vectors
-LLG_FUSED_BYTES_PER_SITE_STEP = 48  # one temporally blocked step: read y, write y
+LLG_FUSED_BYTES_PER_SITE_STEP = 48  # one streamed step: read y, write y
+
+
+def llg_fp64_ops(J2: bool, H: bool, damp: bool) -> int:
+    """FP64 operations of one site-step as the kernels write them (add, sub,
+    mul and fma 1 each; a division or square root 1 each, although the
+    hardware runs a short sequence for them): the right-hand side (exchange
+    12 mul + 12 add, J2 as much again, the field 3 add, H x S 9, damping 18)
+    and dt * f (3) in each of the 4 stages, then the stage combinations
+    (18 + 18 + 15) and stage 4's combination and renormalisation (24)."""
+    rhs = 24 + (24 if J2 else 0) + (3 if H else 0) + 9 + (18 if damp else 0)
+    return 4 * (rhs + 3) + 18 + 18 + 15 + 24
+
+
+def fp64_peak_tops(torch) -> float:
+    """Nominal FP64 issue rate: 64 FP64 lanes per SM per clock at the maximum
+    SM clock (1 operation per lane per clock; no measured FP64 figure exists)."""
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = 1965.0
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        mhz = json.loads(p.read_text()).get("sm_max_mhz", mhz)
+    return sms * 64 * mhz * 1e6 / 1e12
+
+
+def llg_report(ms_by_kernel, sites_replicas, ops, hbm, fp64_peak):
+    """Per LLG kernel: site-steps/s, DRAM bytes against the HBM peak (the
+    bound of the stage kernels) and FP64 operations against the FP64 issue
+    rate (the bound of the one-launch step)."""
+    out = {}
+    for k, ms in ms_by_kernel.items():
+        bps = LLG_BYTES_PER_SITE_STEP if k == "stages" else LLG_FUSED_BYTES_PER_SITE_STEP
+        rate = sites_replicas / (ms / 1e3)
+        out[k] = {"site_steps_per_s": rate, "ms": ms, "bytes_per_site_step": bps,
+                  "achieved_gbs": bps * rate / 1e9, "hbm_peak_gbs": hbm,
+                  "frac": bps * rate / 1e9 / hbm, "fp64_ops_per_site_step": ops,
+                  "achieved_fp64_tops": ops * rate / 1e12, "fp64_peak_tops_nominal": fp64_peak,
+                  "fp64_frac": ops * rate / 1e12 / fp64_peak,
+                  "bound": "hbm" if k == "stages" else "fp64"}
+    return out
 
 
 def aggregate(ms_per_step: float, units_per_rank: float, world: int, dist=None, device=None):
@@ -335,7 +374,7 @@ def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
     d = torch.zeros(2, dtype=torch.float64, device="cuda")
     reps = 30
     llg = {}
-    for kern, bps in (("stages", LLG_BYTES_PER_SITE_STEP), ("fused", LLG_FUSED_BYTES_PER_SITE_STEP)):
+    for kern in ("stages", "fused"):
         ctx.set_llg_kernel(kern)
         ctx.step(5)
         torch.cuda.synchronize()
@@ -343,9 +382,8 @@ def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
         ctx.step(reps)
         ev1.record(stream)
         torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1) / reps
-        llg[kern] = (ms, bps * M * nf / (ms / 1e3) / 1e9, bps)
-    ctx.set_llg_kernel("stages")
+        llg[kern] = ev0.elapsed_time(ev1) / reps
+    ctx.set_llg_kernel("fused")  # the default
     hbm, bf16, src = measured_peaks()
     sqt_ms, vals = {}, {}
     for mode in ("fp64", "tf32x3", "bf16x3"):
@@ -362,9 +400,9 @@ def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
     ref = vals["fp64"]
     flops = 2.0 * M * M * K
     report = {
-        "llg": {k: {"site_steps_per_s": M * nf / (v[0] / 1e3), "ms": v[0], "achieved_gbs": v[1],
-                    "hbm_peak_gbs": hbm, "frac": v[1] / hbm, "bytes_per_site_step": v[2]}
-                for k, v in llg.items()},
+        "llg": llg_report(llg, M * nf, llg_fp64_ops(CONFIG["J2"] != 0.0, any(CONFIG["h"]),
+                                                     CONFIG["alpha"] != 0.0),
+                          hbm, fp64_peak_tops(torch)),
         "sqt": {m: {"ms": sqt_ms[m], "tflops": flops / (sqt_ms[m] / 1e3) / 1e12,
                     "value": [vals[m].real, vals[m].imag],
                     "rel_err_vs_fp64": abs(vals[m] - ref) / abs(ref)} for m in sqt_ms},
@@ -432,7 +470,12 @@ def run_workload(args):
         ctx.step(3)
         step_ms = timed(torch, lambda: (ctx.step(1), ctx.sqt_async("bf16x3", d.data_ptr())),
                         args.steps)
-        llg_ms = timed(torch, lambda: ctx.step(1), 10)
+        llg_ms = {}
+        for kern in ("stages", "fused"):
+            ctx.set_llg_kernel(kern)
+            ctx.step(2)
+            llg_ms[kern] = timed(torch, lambda: ctx.step(1), 10)
+        ctx.set_llg_kernel("fused")
         vals, ms = {}, {}
         for mode, reps in (("bf16x3", 5), ("tf32x3", 3), ("fp64", 1)):
             ctx.sqt_async(mode, d.data_ptr())
@@ -444,8 +487,8 @@ def run_workload(args):
             "ms_per_step": step_ms, "dtype": "f64 RK4 + bf16x3 GEMM",
             "config": {"workload": "256x256 lattice, 1000 replicas, J=1, J2=-0.3, alpha=0.02, dt=0.005",
                        "gemm_m": M, "gemm_k": K},
-            "llg": {"ms": llg_ms, "achieved_gbs": LLG_BYTES_PER_SITE_STEP * M * nf / llg_ms / 1e6,
-                    "hbm_peak_gbs": hbm},
+            "llg": llg_report(llg_ms, M * nf, llg_fp64_ops(True, False, True), hbm,
+                              fp64_peak_tops(torch)),
             "sqt": {m: {"ms": ms[m], "tflops": flops / ms[m] / 1e9,
                         "rel_err_vs_fp64": abs(vals[m] - vals["fp64"]) / abs(vals["fp64"])}
                     for m in ms},

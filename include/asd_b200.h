@@ -182,15 +182,16 @@ int asd_ctx_shard_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_part, dou
 int asd_ctx_shard_sqt_finish(asd_ctx *ctx, const double *d_part, const double *d_sums,
                              double *d_out);
 
-/* How asd_ctx_step runs one RK4 step.  Both give bit-identical spins. */
-#define ASD_LLG_STAGES 0     /* default: four launches, one fused kernel per RK4
-                                stage, HBM-bound (384 B of DRAM traffic per
+/* How asd_ctx_step (and asd_ctx_step_host) runs one RK4 step.  Both give
+ * bit-identical spins. */
+#define ASD_LLG_STAGES 0     /* four launches, one fused kernel per RK4 stage,
+                                HBM-bound (384 B of DRAM traffic per
                                 site-step; about 75% of HBM bandwidth on B200) */
-#define ASD_LLG_FUSED_STEP 1 /* one launch per step, the four stages
-                                temporally blocked in shared memory (48 B of
-                                DRAM traffic per site-step, but FP64- and
-                                latency-bound: within 10% of the stages on
-                                B200, either way depending on the lattice)   */
+#define ASD_LLG_FUSED_STEP 1 /* default: one launch per step, the four stages
+                                streamed down the lattice through shared
+                                memory by column band (48 B of DRAM traffic per
+                                site-step; FP64-bound; 1.35x the stages at
+                                128x128x500, 1.6x at 256x256x1000 on B200)  */
 int asd_ctx_set_llg_kernel(asd_ctx *ctx, int kernel);
 
 /* K elements accumulated per TMEM chunk by the split S(q,t) modes (rounded

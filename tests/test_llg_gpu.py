@@ -24,10 +24,15 @@ CASES = [
     (3, 1, dict(J1=1.0, J2=0.5, h=(0.1, 0.2, 0.3), alpha=0.3, dt=0.02)),   # smallest lattice
     (37, 9, dict(J1=-0.8, J2=0.2, h=(0.0, 0.3, 0.1), alpha=0.07, dt=0.01)),  # ragged tiles
     (48, 4, dict(J1=1.0, dt=0.02)),                      # several whole tiles
-    # even replica counts take the two-replicas-per-thread stage kernels
+    # more combinations of the extensions, even and odd replica counts
     (14, 8, dict(J1=-1.0, J2=0.3, alpha=0.05, h=(0.1, 0.0, 0.4), dt=0.005)),
     (11, 6, dict(J1=0.9, J2=-0.2, h=(0.0, 0.2, 0.0), dt=0.01)),
     (7, 2, dict(J1=1.0, h=(0.0, 0.0, 0.5), alpha=0.2, dt=0.02, spin_len=1.5)),
+    # column bands of the one-launch step: 2 bands of 40, 3 of 48 (the last
+    # ragged), 4 of 64; replica groups of 4 with a partial last group
+    (70, 13, dict(J1=1.0, J2=-0.3, alpha=0.02, dt=0.005)),
+    (130, 5, dict(J1=-1.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005)),
+    (256, 3, dict(J1=1.0, J2=-0.3, h=(0.2, 0.0, 0.1), alpha=0.02, dt=0.005)),
 ]
 
 

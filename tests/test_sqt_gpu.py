@@ -178,11 +178,13 @@ def test_step_pipelined_behind_the_split_gemm(oracle, mode, kernel):
     assert np.array_equal(spins[0], want)
 
 
+@pytest.mark.parametrize("kernel", ["fused", "stages"])
 @pytest.mark.parametrize("nf,pinned", [(200, False), (200, True), (65, True), (128, True)])
-def test_step_host_in_replica_chunks(oracle, nf, pinned):
+def test_step_host_in_replica_chunks(oracle, nf, pinned, kernel):
     """Ensembles larger than one upload chunk (64 replicas and up) take the
-    pipelined asd_ctx_step_host: per replica chunk, upload, RK4, download and
-    a GEMM over that chunk's K columns.  200 replicas make chunks of 64, 64,
+    pipelined asd_ctx_step_host: per replica chunk, upload, RK4 (the one-launch
+    step into the other state buffer, or the four stage kernels in place),
+    download and a GEMM over that chunk's K columns.  200 replicas make chunks of 64, 64,
     64 and a ragged 8 (65: 64 + 1; 128: two whole chunks).  The spins must
     equal the device path and the oracle
     bit for bit; S(q,t) must equal the device path exactly in the FP64 modes
@@ -195,6 +197,7 @@ def test_step_host_in_replica_chunks(oracle, nf, pinned):
     kw = dict(J1=-1.0, J2=0.2, alpha=0.05, h=(0, 0, 0.5), dt=0.005)
     p = asd.Params.make(N, nf, vx=3, vy=2, **kw)
     with asd.Context(p) as a, asd.Context(p) as b:
+        a.set_llg_kernel(kernel)
         a.set_spins(s0, as_origin=True)
         b.set_spins(s0, as_origin=True)
         buf = torch.from_numpy(s0.reshape(-1).copy())
