@@ -276,6 +276,7 @@ def run_ours(args):
                              h=CONFIG["h"], dt=CONFIG["dt"])
     asd.load().asd_set_device(local)
     ctx = asd.Context(params, modes=["fp64", "tf32x3", "bf16x3"])
+    ctx.set_llg_kernel(args.llg_kernel)
     if args.chunk_k >= 0:
         ctx.set_chunk_k(args.chunk_k)
     stream = torch.cuda.current_stream()
@@ -339,7 +340,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": f"f64 RK4 + {mode} GEMM (fp32 accumulate, f64 reduction)",
         "data": "synthetic: seeded spins uniform on the sphere",
         "config": {"workload": WORKLOAD, "sites": M, "replicas": nf, "gemm_m": M, "gemm_n": M,
-                   "gemm_k": K, "sqt_mode": mode,
+                   "gemm_k": K, "sqt_mode": mode, "llg_kernel": args.llg_kernel,
                    "chunk_k": args.chunk_k if args.chunk_k >= 0 else (512 if mode == "tf32x3" else 1024),
                    "l2": "inputs larger than L2 (spin state 197 MB per array, operands 197 MB)"},
         "roofline": {"bound": "tensor", "kernel": f"umma_sqt_kernel ({mode})",
@@ -383,7 +384,7 @@ def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
         ev1.record(stream)
         torch.cuda.synchronize()
         llg[kern] = ev0.elapsed_time(ev1) / reps
-    ctx.set_llg_kernel("fused")  # the default
+    ctx.set_llg_kernel(args.llg_kernel)
     hbm, bf16, src = measured_peaks()
     sqt_ms, vals = {}, {}
     for mode in ("fp64", "tf32x3", "bf16x3"):
@@ -635,6 +636,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mode", choices=["tf32x3", "bf16x3", "fp64", "fp64_fused"], default="tf32x3")
+    ap.add_argument("--llg-kernel", choices=["fused", "stages"], default="fused",
+                    help="RK4 step of the headline: one streamed launch (default) or four "
+                         "stage kernels")
     ap.add_argument("--chunk-k", type=int, default=-1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
