@@ -46,7 +46,7 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
     "asd_ctx_sqt_grid_async", "asd_ctx_sqt_grid",
-    "asd_ctx_step_host", "asd_ctx_set_ensemble", "asd_ctx_shard_origin_sums",
+    "asd_ctx_step_host", "asd_ctx_step_host_async", "asd_ctx_synchronize", "asd_ctx_set_ensemble", "asd_ctx_shard_origin_sums",
     "asd_ctx_shard_set_origin_sums", "asd_ctx_shard_sqt_async", "asd_ctx_shard_sqt_finish",
     "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
     "asd_ctx_last_launches",
@@ -133,6 +133,8 @@ def load() -> C.CDLL:
         "asd_ctx_sqt_grid_async": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_sqt_grid": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_step_host": ([vp, vp, vp, C.c_int, dp], C.c_int),
+        "asd_ctx_step_host_async": ([vp, vp, vp, C.c_int, vp], C.c_int),
+        "asd_ctx_synchronize": ([vp], C.c_int),
         "asd_ctx_set_ensemble": ([vp, C.c_int], C.c_int),
         "asd_ctx_shard_origin_sums": ([vp, vp], C.c_int),
         "asd_ctx_shard_set_origin_sums": ([vp, vp], C.c_int),
@@ -314,6 +316,17 @@ class Context:
         _check(load().asd_ctx_step_host(self._h, C.c_void_p(spin_in_ptr),
                                         C.c_void_p(spin_out_ptr), mode, self._out))
         return complex(self._out[0], self._out[1])
+
+    def step_host_async(self, spin_in_ptr: int, spin_out_ptr: int, mode, sqt_out_ptr: int) -> None:
+        """Enqueues one host-buffer step (pinned host or device pointers) and
+        returns; the buffers are final after synchronize()."""
+        mode = MODES[mode] if isinstance(mode, str) else int(mode)
+        _check(load().asd_ctx_step_host_async(self._h, C.c_void_p(spin_in_ptr),
+                                              C.c_void_p(spin_out_ptr), mode,
+                                              C.c_void_p(sqt_out_ptr)))
+
+    def synchronize(self) -> None:
+        _check(load().asd_ctx_synchronize(self._h))
 
     # replica sharding of one ensemble (see asd_b200.shard) ------------------
     def set_ensemble(self, nfile_total: int) -> None:

@@ -116,6 +116,15 @@ struct asd_ctx {
     double *stage_in[2] = {}, *stage_out[2] = {};
     cudaStream_t h2d_stream = nullptr;
     cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
+    // asd_ctx_step_host_async: whole-state AoS staging in and out (so the
+    // copy engines never wait for a staging slot), and per replica chunk the
+    // events that order uploads, compute and downloads within a call and
+    // across consecutive calls.
+    static constexpr int kAsyncChunks = 16;
+    double *ast_in = nullptr, *ast_out = nullptr;
+    bool ast_events = false;
+    cudaEvent_t ast_in_ready[kAsyncChunks] = {}, ast_in_done[kAsyncChunks] = {},
+                ast_out_ready[kAsyncChunks] = {}, ast_out_done[kAsyncChunks] = {};
     // Replica sharding: this context holds nfile of the nfile_total replicas
     // of one ensemble (0: not sharded); zsums = the ensemble's origin site
     // sums once exchanged; zero3 = zero means for the FP64 partial GEMMs.
@@ -673,7 +682,8 @@ int host_chunk_replicas(int nfile) {
     return (target + 63) / 64 * 64;
 }
 
-int ensure_host_pipeline(asd_ctx *c, int cr) {
+// The upload and download streams (and the sync pipeline's events).
+int ensure_copy_streams(asd_ctx *c) {
     if (!c->copy_stream) {
         ASD_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
         ASD_CUDA_TRY(cudaEventCreateWithFlags(&c->spins_ready, cudaEventDisableTiming));
@@ -687,6 +697,12 @@ int ensure_host_pipeline(asd_ctx *c, int cr) {
                 ASD_CUDA_TRY(cudaEventCreateWithFlags(x, cudaEventDisableTiming));
         }
     }
+    return ASD_OK;
+}
+
+int ensure_host_pipeline(asd_ctx *c, int cr) {
+    int rc0 = ensure_copy_streams(c);
+    if (rc0 != ASD_OK) return rc0;
     if (c->hp_replicas == cr) return ASD_OK;
     for (int b = 0; b < 2; ++b) {
         if (c->stage_in[b]) cudaFree(c->stage_in[b]);
@@ -824,6 +840,102 @@ int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int m
     return sqt_async(c, mode, c->d_out);
 }
 
+// asd_ctx_step_host_async.  Per replica chunk r: upload (h2d_stream) into
+// the chunk's region of the whole-state staging buffer, site-major
+// transpose, RK4 on the chunk's replicas, AoS transpose, download
+// (copy_stream); then S(q,t) of the new state on the ctx stream.  Nothing
+// waits for the host, so consecutive calls overlap: the upload of chunk r
+// of the next call waits only for the download of chunk r of this one (the
+// caller may pass this call's output as the next call's input) and for the
+// transpose that emptied its staging region; the GEMM of one call runs
+// while the next call's chunks cross PCIe.
+int async_chunk_replicas(int nfile) {
+    const int target = (nfile + 7) / 8;
+    int cr = (target + 31) / 32 * 32;
+    while ((nfile + cr - 1) / cr > asd_ctx::kAsyncChunks) cr += 32;
+    return cr;
+}
+
+int ensure_async_pipeline(asd_ctx *c) {
+    int rc = ensure_copy_streams(c);
+    if (rc != ASD_OK) return rc;
+    if (!c->ast_events) {
+        for (int r = 0; r < asd_ctx::kAsyncChunks; ++r) {
+            cudaEvent_t *ev[] = {&c->ast_in_ready[r], &c->ast_in_done[r], &c->ast_out_ready[r],
+                                 &c->ast_out_done[r]};
+            for (cudaEvent_t *x : ev)
+                ASD_CUDA_TRY(cudaEventCreateWithFlags(x, cudaEventDisableTiming));
+        }
+        c->ast_events = true;
+    }
+    const size_t bytes = (size_t)c->M * c->K * sizeof(double);
+    if (!c->ast_in && (rc = dalloc(&c->ast_in, bytes)) != ASD_OK) return rc;
+    if (!c->ast_out && (rc = dalloc(&c->ast_out, bytes)) != ASD_OK) return rc;
+    return ASD_OK;
+}
+
+bool pinned_or_device(const void *p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost || at.type == cudaMemoryTypeDevice ||
+           at.type == cudaMemoryTypeManaged;
+}
+
+int step_host_async(asd_ctx *c, const double *spin_in, double *spin_out, int mode,
+                    double *sqt_out) {
+    const int nf = c->p.nfile;
+    const long M = c->M;
+    int rc = ensure_async_pipeline(c);
+    if (rc != ASD_OK) return rc;
+    const int cr = async_chunk_replicas(nf), nchunks = (nf + cr - 1) / cr;
+    const cudaStream_t comp = c->stream, up = c->h2d_stream, down = c->copy_stream;
+    const bool fused = c->llg_kernel == ASD_LLG_FUSED_STEP;
+    double *const ynew = fused ? c->ys_a : c->y;
+    LLGArgs a = c->a;
+    for (int r = 0; r < nchunks; ++r) {
+        const int f0 = r * cr, nc = (nf - f0 < cr) ? nf - f0 : cr;
+        const size_t off = (size_t)f0 * M * 3, bytes = (size_t)nc * M * 3 * sizeof(double);
+        ASD_CUDA_TRY(cudaStreamWaitEvent(up, c->ast_out_done[r], 0));
+        ASD_CUDA_TRY(cudaStreamWaitEvent(up, c->ast_in_done[r], 0));
+        ASD_CUDA_TRY(cudaMemcpyAsync(c->ast_in + off, spin_in + off, bytes,
+                                     cudaMemcpyHostToDevice, up));
+        ASD_CUDA_TRY(cudaEventRecord(c->ast_in_ready[r], up));
+        ASD_CUDA_TRY(cudaStreamWaitEvent(comp, c->ast_in_ready[r], 0));
+        ASD_CUDA_TRY(launch_aos_to_sitemajor_range(c->ast_in + off, c->y, M, nf, f0, nc, comp));
+        ASD_CUDA_TRY(cudaEventRecord(c->ast_in_done[r], comp));
+        a.f0 = f0;
+        a.nc = nc;
+        if (fused) {
+            ASD_CUDA_TRY(launch_llg_step_fused(a, c->y, ynew, comp));
+        } else {
+            ASD_CUDA_TRY(launch_llg_stage(1, a, c->y, c->y, c->acc, c->ys_a, comp));
+            ASD_CUDA_TRY(launch_llg_stage(2, a, c->y, c->ys_a, c->acc, c->ys_b, comp));
+            ASD_CUDA_TRY(launch_llg_stage(3, a, c->y, c->ys_b, c->acc, c->ys_a, comp));
+            ASD_CUDA_TRY(launch_llg_stage(4, a, nullptr, c->ys_a, c->acc, c->y, comp));
+        }
+        ASD_CUDA_TRY(cudaStreamWaitEvent(comp, c->ast_out_done[r], 0));
+        ASD_CUDA_TRY(launch_sitemajor_to_aos_range(ynew, c->ast_out + off, M, nf, f0, nc, comp));
+        ASD_CUDA_TRY(cudaEventRecord(c->ast_out_ready[r], comp));
+        ASD_CUDA_TRY(cudaStreamWaitEvent(down, c->ast_out_ready[r], 0));
+        ASD_CUDA_TRY(cudaMemcpyAsync(spin_out + off, c->ast_out + off, bytes,
+                                     cudaMemcpyDeviceToHost, down));
+        ASD_CUDA_TRY(cudaEventRecord(c->ast_out_done[r], down));
+        c->last_launches += fused ? 3 : 6;
+    }
+    if (fused) {  // ys_a holds the new state of every replica
+        c->ys_a = c->y;
+        c->y = ynew;
+    }
+    c->state_version += 2;  // as set_spins + step
+    c->has_state = true;
+    if ((rc = sqt_async(c, mode, c->d_out)) != ASD_OK) return rc;
+    ASD_CUDA_TRY(cudaMemcpyAsync(sqt_out, c->d_out, 2 * sizeof(double), cudaMemcpyDefault, comp));
+    return ASD_OK;
+}
+
 void destroy(asd_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
@@ -853,6 +965,14 @@ void destroy(asd_ctx *c) {
     if (c->h2d_stream) {
         cudaStreamSynchronize(c->h2d_stream);
         cudaStreamDestroy(c->h2d_stream);
+    }
+    if (c->ast_in) cudaFree(c->ast_in);
+    if (c->ast_out) cudaFree(c->ast_out);
+    for (int r = 0; c->ast_events && r < asd_ctx::kAsyncChunks; ++r) {
+        cudaEvent_t ev[] = {c->ast_in_ready[r], c->ast_in_done[r], c->ast_out_ready[r],
+                            c->ast_out_done[r]};
+        for (cudaEvent_t x : ev)
+            if (x) cudaEventDestroy(x);
     }
     if (c->llg_stream) {
         cudaStreamSynchronize(c->llg_stream);
@@ -1166,6 +1286,9 @@ int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_s
     if (!c->has_origin) return fail(ASD_ERR_STATE, "set the origin (t = 0 spins) first");
     ASD_CUDA_TRY(enter(c));
     c->last_launches = 0;
+    // Downloads of earlier asynchronous calls may still be writing the
+    // caller's buffers, which this call may read: let them finish first.
+    if (c->ast_events) ASD_CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
     int rc;
     const int cr = host_chunk_replicas(c->p.nfile);
     if (cr < c->p.nfile) {
@@ -1209,6 +1332,29 @@ int asd_ctx_step_host(asd_ctx *c, const double *spin_in, double *spin_out, asd_s
     sqt_out[0] = c->h_out[0];
     sqt_out[1] = c->h_out[1];
     return ASD_OK;
+}
+
+int asd_ctx_step_host_async(asd_ctx *c, const double *spin_in, double *spin_out,
+                            asd_sqt_mode mode, double *sqt_out) {
+    if (!c || !spin_in || !spin_out || !sqt_out) return fail(ASD_ERR_INVALID, "NULL argument");
+    if (!c->has_origin) return fail(ASD_ERR_STATE, "set the origin (t = 0 spins) first");
+    if ((int)mode < 0 || (int)mode > 3) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", (int)mode);
+    if (!(c->modes & (1u << (int)mode)))
+        return fail(ASD_ERR_STATE, "mode %d not enabled at create", (int)mode);
+    ASD_CUDA_TRY(enter(c));
+    if (!pinned_or_device(spin_in) || !pinned_or_device(spin_out) || !pinned_or_device(sqt_out))
+        return fail(ASD_ERR_INVALID, "asd_ctx_step_host_async needs pinned host (cudaMallocHost, "
+                                     "cudaHostRegister) or device buffers");
+    c->last_launches = 0;
+    return step_host_async(c, spin_in, spin_out, (int)mode, sqt_out);
+}
+
+int asd_ctx_synchronize(asd_ctx *c) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    ASD_CUDA_TRY(enter(c));
+    if (c->h2d_stream) ASD_CUDA_TRY(cudaStreamSynchronize(c->h2d_stream));
+    if (c->copy_stream) ASD_CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
+    return read_status(c);
 }
 
 int asd_ctx_set_ensemble(asd_ctx *c, int nfile_total) {

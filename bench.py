@@ -413,23 +413,38 @@ def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
 
 
 def e2e_measurement(ctx, asd, torch, spins0, mode, M, nf, args, world):
-    """asd_ctx_step_host: per step, pinned host spins in, RK4 + S(q,t), spins and
-    S(q,t) back to pinned host memory."""
+    """End to end through the host-buffer API, per step: pinned host spins in,
+    RK4 + S(q,t), spins and S(q,t) back to pinned host memory (each step's
+    input is the previous step's output).  The headline form enqueues the
+    steps with asd_ctx_step_host_async, so consecutive steps overlap chunk by
+    chunk, and synchronises once at the end; the synchronous
+    asd_ctx_step_host (one call = one complete step) is reported beside it."""
+    import torch.distributed as dist
+
     n = M * nf * 3
     h_in = torch.from_numpy(spins0.reshape(-1).copy()).pin_memory()
     h_out = torch.empty(n, dtype=torch.float64).pin_memory()
     steps = max(2, min(args.steps, 10))
+    h_sqt = torch.zeros(2 * steps, dtype=torch.float64).pin_memory()
     ctx.step_host(h_in.data_ptr(), h_out.data_ptr(), mode)  # warm
     t0 = time.perf_counter()
     for _ in range(steps):
         ctx.step_host(h_out.data_ptr(), h_out.data_ptr(), mode)
+    ms_sync = (time.perf_counter() - t0) / steps * 1e3
+    ctx.step_host_async(h_out.data_ptr(), h_out.data_ptr(), mode, h_sqt.data_ptr())  # warm
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    for i in range(steps):
+        ctx.step_host_async(h_out.data_ptr(), h_out.data_ptr(), mode, h_sqt.data_ptr() + 16 * i)
+    ctx.synchronize()
     ms = (time.perf_counter() - t0) / steps * 1e3
-    import torch.distributed as dist
-
     ms, value = aggregate(ms, M * nf, world, dist if world > 1 else None, "cuda")
+    ms_sync, value_sync = aggregate(ms_sync, M * nf, world, dist if world > 1 else None, "cuda")
     return {"value": value, "unit": "site-steps/s", "h2d_bytes_per_step": n * 8,
-            "d2h_bytes_per_step": n * 8 + 16, "ms_per_step": ms,
-            "api": "asd_ctx_step_host (pinned host buffers)"}
+            "d2h_bytes_per_step": n * 8 + 16, "ms_per_step": ms, "steps": steps,
+            "api": "asd_ctx_step_host_async x steps + asd_ctx_synchronize (pinned host buffers)",
+            "sync": {"value": value_sync, "ms_per_step": ms_sync,
+                     "api": "asd_ctx_step_host (pinned host buffers)"}}
 
 
 # ------------------------------------------------------ other configurations

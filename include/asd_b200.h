@@ -152,6 +152,22 @@ int asd_ctx_loss_grad(asd_ctx *ctx, int nsteps, int stride, int checkpoint, cons
 int asd_ctx_step_host(asd_ctx *ctx, const double *spin_in, double *spin_out,
                       asd_sqt_mode mode, double sqt_out[2]);
 
+/* asd_ctx_step_host without waiting: enqueues the upload of spin_in, one RK4
+ * step, the download into spin_out and S(q,t) into sqt_out (2 doubles), and
+ * returns.  The buffers must be pinned host memory (cudaMallocHost,
+ * cudaHostRegister) or device memory; they are final after
+ * asd_ctx_synchronize.  spin_in may equal spin_out, and one call's spin_out
+ * may be the next call's spin_in: the upload of each replica chunk waits for
+ * the previous call's download of the same chunk, so consecutive calls
+ * overlap (the next step's uploads cross PCIe while this step's S(q,t) GEMM
+ * runs).  Same results as asd_ctx_step_host; the S(q,t) GEMM runs once over
+ * the whole new state, as in asd_ctx_sqt. */
+int asd_ctx_step_host_async(asd_ctx *ctx, const double *spin_in, double *spin_out,
+                            asd_sqt_mode mode, double *sqt_out);
+/* Waits for everything the context enqueued (its stream and its copy
+ * streams) and reports a device-side failure, if any. */
+int asd_ctx_synchronize(asd_ctx *ctx);
+
 /* Replica sharding of one ensemble over several GPUs, one context per GPU.
  * Replicas never interact, so each context steps its own nfile replicas; the
  * correlation GEMM's K axis is the replica axis, so S(q,t) is the sum over

@@ -179,6 +179,63 @@ def test_step_pipelined_behind_the_split_gemm(oracle, mode, kernel):
 
 
 @pytest.mark.parametrize("kernel", ["fused", "stages"])
+@pytest.mark.parametrize("nf", [200, 40, 7])
+def test_step_host_async_consecutive_steps(oracle, nf, kernel):
+    """asd_ctx_step_host_async: five steps enqueued back to back on one pinned
+    buffer (each call's output is the next call's input, so every chunk's
+    upload must wait for the previous call's download of that chunk), then
+    one asd_ctx_synchronize.  200 replicas make chunks of 32 (six) and 8; 40
+    make 32 + 8; 7 one chunk.  The spins equal the device path and the oracle
+    bit for bit; each step's S(q,t) equals the device path's asd_ctx_sqt on
+    the same state exactly (the same kernels in the same order)."""
+    import torch
+
+    N = 16
+    s0 = asd.random_spins(N, nf, seed=21)
+    kw = dict(J1=-1.0, J2=0.2, alpha=0.05, h=(0, 0, 0.5), dt=0.005)
+    p = asd.Params.make(N, nf, vx=3, vy=2, **kw)
+    modes = ["tf32x3", "fp64", "bf16x3", "fp64_fused", "tf32x3"]
+    with asd.Context(p) as a, asd.Context(p) as b:
+        a.set_llg_kernel(kernel)
+        a.set_spins(s0, as_origin=True)
+        b.set_spins(s0, as_origin=True)
+        buf = torch.from_numpy(s0.reshape(-1).copy()).pin_memory()
+        sq = torch.zeros(2 * len(modes), dtype=torch.float64).pin_memory()
+        for i, mode in enumerate(modes):
+            a.step_host_async(buf.data_ptr(), buf.data_ptr(), mode, sq.data_ptr() + 16 * i)
+        a.synchronize()
+        want = s0
+        for i, mode in enumerate(modes):
+            b.step(1)
+            assert complex(*sq[2 * i:2 * i + 2].tolist()) == b.sqt(mode), (i, mode)
+            want = oracle.steps(orc.make_params(N, nf, **kw), want, 1)
+        assert np.array_equal(buf.numpy().reshape(s0.shape), b.get_spins())
+        assert np.array_equal(b.get_spins(), want)
+        # the context keeps working synchronously afterwards
+        got = a.step_host(buf.data_ptr(), buf.data_ptr(), "fp64")
+        b.step(1)
+        assert got == b.sqt("fp64")
+        assert np.array_equal(buf.numpy().reshape(s0.shape), b.get_spins())
+
+
+def test_step_host_async_needs_pinned_or_device_buffers():
+    """Pageable host memory cannot be copied asynchronously: the call fails
+    with ASD_ERR_INVALID before enqueueing anything."""
+    import torch
+
+    N, nf = 12, 4
+    s0 = asd.random_spins(N, nf, seed=3)
+    with asd.Context(asd.Params.make(N, nf, J1=1.0, dt=0.01), modes=["fp64"]) as a:
+        a.set_spins(s0, as_origin=True)
+        pageable = s0.reshape(-1).copy()
+        sq = torch.zeros(2, dtype=torch.float64).pin_memory()
+        with pytest.raises(asd.AsdError) as e:
+            a.step_host_async(pageable.ctypes.data, pageable.ctypes.data, "fp64", sq.data_ptr())
+        assert e.value.code == asd.ASD_ERR_INVALID
+        assert np.array_equal(a.get_spins(), s0)
+
+
+@pytest.mark.parametrize("kernel", ["fused", "stages"])
 @pytest.mark.parametrize("nf,pinned", [(200, False), (200, True), (65, True), (128, True)])
 def test_step_host_in_replica_chunks(oracle, nf, pinned, kernel):
     """Ensembles larger than one upload chunk (64 replicas and up) take the
