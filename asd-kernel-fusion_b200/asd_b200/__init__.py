@@ -54,7 +54,7 @@ EXPORTED_SYMBOLS = (
     "asd_check_bounded_wait", "asd_check_const_division", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
     "asd_spins_save", "asd_spins_load", "asd_batch_create", "asd_batch_destroy",
     "asd_batch_set_stream", "asd_batch_set_spins", "asd_batch_get_spins", "asd_batch_run",
-    "asd_batch_configure", "asd_batch_autotune", "asd_set_params", "euler", "runge_kutta",
+    "asd_batch_configure", "asd_batch_configure_cluster", "asd_batch_autotune", "asd_set_params", "euler", "runge_kutta",
     "fused_dgemm",
 )
 
@@ -158,6 +158,7 @@ def load() -> C.CDLL:
         "asd_batch_get_spins": ([vp, C.c_int, vp], C.c_int),
         "asd_batch_run": ([vp, C.c_int], C.c_int),
         "asd_batch_configure": ([vp, C.c_int, C.c_int], C.c_int),
+        "asd_batch_configure_cluster": ([vp, C.c_int, C.c_int], C.c_int),
         "asd_batch_autotune": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                 C.POINTER(C.c_double)], C.c_int),
         "asd_spins_save": ([C.c_char_p, C.c_int, C.c_int, C.c_long, C.c_double, vp], C.c_int),
@@ -499,7 +500,12 @@ class Batch:
         _check(load().asd_batch_run(self._h, int(nsteps)))
 
     def configure(self, tile: int, ctas_per_sm: int) -> None:
+        """Global-memory kernel with this work decomposition."""
         _check(load().asd_batch_configure(self._h, int(tile), int(ctas_per_sm)))
+
+    def configure_cluster(self, cluster_size: int, threads: int = 0) -> None:
+        """Cluster-resident kernel (raises AsdError if the batch does not fit)."""
+        _check(load().asd_batch_configure_cluster(self._h, int(cluster_size), int(threads)))
 
     def autotune(self, trial_steps: int = 20):
         t, c, ms = C.c_int(), C.c_int(), C.c_double()

@@ -18,6 +18,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <chrono>
 #include <vector>
 
@@ -51,32 +52,25 @@ __device__ __forceinline__ F3 ld3(const float *p, long M, long i) {
     return F3{__ldcg(p + i), __ldcg(p + M + i), __ldcg(p + 2 * M + i)};
 }
 
-__device__ __forceinline__ F3 rhs32(const float *ys, const BatchLattice &L, long i) {
-    const int N = L.N;
-    const long M = (long)N * N;
-    const int row = (int)(i / N), col = (int)(i - (long)row * N);
-    const int rp = (row + 1 == N) ? 0 : row + 1, rm = (row == 0) ? N - 1 : row - 1;
-    const int cp = (col + 1 == N) ? 0 : col + 1, cm = (col == 0) ? N - 1 : col - 1;
-    const F3 s = ld3(ys, M, i);
-    const long nb[4] = {(long)rp * N + col, (long)rm * N + col, (long)row * N + cm,
-                        (long)row * N + cp};
+// dS/dt from the centre s and the neighbours nb (nearest, in the reference's
+// order (row+1), (row-1), (col-1), (col+1)) and n2 (diagonals (+1,+1),
+// (+1,-1), (-1,+1), (-1,-1); read only with J2), FP32, explicitly rounded.
+// Both batch kernels go through this function: one operation order.
+__device__ __forceinline__ F3 rhs32_vals(const F3 &s, const F3 (&nb)[4], const F3 (&n2)[4],
+                                         const BatchLattice &L) {
     float ex = 0.f, ey = 0.f, ez = 0.f;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const F3 t = ld3(ys, M, nb[j]);
-        ex = fa(ex, fm(t.x, L.J1));
-        ey = fa(ey, fm(t.y, L.J1));
-        ez = fa(ez, fm(t.z, L.J1));
+        ex = fa(ex, fm(nb[j].x, L.J1));
+        ey = fa(ey, fm(nb[j].y, L.J1));
+        ez = fa(ez, fm(nb[j].z, L.J1));
     }
     if (L.use_j2) {
-        const long n2[4] = {(long)rp * N + cp, (long)rp * N + cm, (long)rm * N + cp,
-                            (long)rm * N + cm};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const F3 t = ld3(ys, M, n2[j]);
-            ex = fa(ex, fm(t.x, L.J2));
-            ey = fa(ey, fm(t.y, L.J2));
-            ez = fa(ez, fm(t.z, L.J2));
+            ex = fa(ex, fm(n2[j].x, L.J2));
+            ey = fa(ey, fm(n2[j].y, L.J2));
+            ez = fa(ez, fm(n2[j].z, L.J2));
         }
     }
     if (L.use_h) {
@@ -91,6 +85,27 @@ __device__ __forceinline__ F3 rhs32(const float *ys, const BatchLattice &L, long
     const float uz = fs(fm(s.x, tau.y), fm(s.y, tau.x));
     return F3{fm(L.g, fa(tau.x, fm(L.alpha, ux))), fm(L.g, fa(tau.y, fm(L.alpha, uy))),
               fm(L.g, fa(tau.z, fm(L.alpha, uz)))};
+}
+
+__device__ __forceinline__ F3 rhs32(const float *ys, const BatchLattice &L, long i) {
+    const int N = L.N;
+    const long M = (long)N * N;
+    const int row = (int)(i / N), col = (int)(i - (long)row * N);
+    const int rp = (row + 1 == N) ? 0 : row + 1, rm = (row == 0) ? N - 1 : row - 1;
+    const int cp = (col + 1 == N) ? 0 : col + 1, cm = (col == 0) ? N - 1 : col - 1;
+    const F3 s = ld3(ys, M, i);
+    F3 nb[4], n2[4];
+    nb[0] = ld3(ys, M, (long)rp * N + col);
+    nb[1] = ld3(ys, M, (long)rm * N + col);
+    nb[2] = ld3(ys, M, (long)row * N + cm);
+    nb[3] = ld3(ys, M, (long)row * N + cp);
+    if (L.use_j2) {
+        n2[0] = ld3(ys, M, (long)rp * N + cp);
+        n2[1] = ld3(ys, M, (long)rp * N + cm);
+        n2[2] = ld3(ys, M, (long)rm * N + cp);
+        n2[3] = ld3(ys, M, (long)rm * N + cm);
+    }
+    return rhs32_vals(s, nb, n2, L);
 }
 
 struct BarrierState {
@@ -194,6 +209,176 @@ __global__ void __launch_bounds__(256) batch_kernel(const BatchLattice *__restri
     }
 }
 
+// ------------------------------------------- cluster-resident batch kernel
+// The lattices live in shared memory for the whole run.  Each lattice
+// belongs to one thread-block cluster; its rows are split over the
+// cluster's CTAs (a CTA may hold rows of several lattices, one segment per
+// lattice).  A CTA keeps, as float planes (x, y, z), two stage buffers over
+// its segments' rows plus one halo row above and below each segment (the
+// stencil's inputs, ping-ponged by the four stages: y -> ys1 -> ys2 -> ys3
+// -> y_new), and per site the RK4 base value and the running combination.
+// After every stage the cluster synchronises (a hardware cluster barrier,
+// the same control flow in every CTA) and each CTA copies its segments' two
+// halo rows from the owning CTAs' shared memory (distributed shared memory),
+// then synchronises its own threads.  Threads walk each segment row by row
+// (thread t takes column t % N of rows t / N, t / N + T / N, ...), so a
+// lattice's parameters and a site's column and wrap offsets are uniform or
+// fixed per segment.  No grid-wide barrier and no global-memory traffic
+// between the first load and the final store.
+struct CSeg {
+    int lat;       // lattice
+    int N;         // its side
+    int r0, rows;  // lattice rows [r0, r0 + rows)
+    int base;      // slot of the top halo row; core row k at base + (k + 1) * N
+    int core0;     // first site of the segment in the CTA's site numbering
+    int top_rank, top_off, top_buf;  // top halo row (r0 - 1 mod N): owning CTA's
+    int bot_rank, bot_off, bot_buf;  //   rank, slot in its planes, its plane length
+};
+struct CCta {
+    int seg0, nseg;  // segments [seg0, seg0 + nseg)
+    int nsites;      // core sites
+    int buf;         // slots per plane
+};
+constexpr int CL_THREADS = 640;
+
+__host__ __device__ constexpr size_t cluster_smem_floats(int buf, int sites) {
+    return (size_t)6 * buf + (size_t)6 * sites;  // 2 x 3 planes, y base and combination
+}
+
+__global__ void __launch_bounds__(CL_THREADS, 1)
+    batch_cluster_kernel(const BatchLattice *__restrict__ lats, const CCta *__restrict__ ctas,
+                         const CSeg *__restrict__ segs, float *y, int nsteps) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ float cfs[];
+    const CCta me = ctas[blockIdx.x];
+    const int T = blockDim.x, tid = threadIdx.x, ns = me.nsites;
+    // plane c of stage buffer b: cfs + (3 b + c) * buf; y base [3][ns]; combination [3][ns]
+    auto plane = [&](int b, int c) { return cfs + (3 * b + c) * me.buf; };
+    float *const yb = cfs + 6 * (size_t)me.buf;
+    float *const ac = yb + 3 * (size_t)ns;
+
+    for (int k = me.seg0; k < me.seg0 + me.nseg; ++k) {
+        const CSeg sg = segs[k];
+        const long M = (long)sg.N * sg.N;
+        const float *Y = y + lats[sg.lat].off;
+        for (int e = tid; e < sg.rows * sg.N; e += T) {
+            const int row = e / sg.N, col = e - row * sg.N;
+            const long i = (long)(sg.r0 + row) * sg.N + col;
+            const int slot = sg.base + (row + 1) * sg.N + col, q = sg.core0 + e;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float v = Y[c * M + i];
+                yb[c * ns + q] = v;
+                plane(0, c)[slot] = v;
+            }
+        }
+    }
+    // halo rows of stage buffer b from the owning CTAs
+    auto halo = [&](int b) {
+        cluster.sync();
+        for (int k = me.seg0; k < me.seg0 + me.nseg; ++k) {
+            const CSeg sg = segs[k];
+            const float *rt = cluster.map_shared_rank(cfs, sg.top_rank) + sg.top_off;
+            const float *rb = cluster.map_shared_rank(cfs, sg.bot_rank) + sg.bot_off;
+            for (int col = tid; col < sg.N; col += T) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    plane(b, c)[sg.base + col] = rt[(3 * b + c) * sg.top_buf + col];
+                    plane(b, c)[sg.base + (sg.rows + 1) * sg.N + col] =
+                        rb[(3 * b + c) * sg.bot_buf + col];
+                }
+            }
+        }
+        __syncthreads();
+    };
+    halo(0);
+
+    auto stage = [&](auto sc) {
+        constexpr int S = decltype(sc)::value;
+        const float *ix = plane((S - 1) & 1, 0), *iy = plane((S - 1) & 1, 1),
+                    *iz = plane((S - 1) & 1, 2);
+        float *ox = plane(S & 1, 0), *oy = plane(S & 1, 1), *oz = plane(S & 1, 2);
+        for (int k = me.seg0; k < me.seg0 + me.nseg; ++k) {
+            const CSeg sg = segs[k];
+            const BatchLattice L = lats[sg.lat];
+            const int N = sg.N, rpp = T / N, r1 = tid / N, col = tid - r1 * N;
+            if (r1 >= rpp) continue;  // the last T % N threads
+            const int dl = (col == 0) ? N - 1 : -1, dr = (col == N - 1) ? 1 - N : 1;
+            for (int row = r1; row < sg.rows; row += rpp) {
+                const int c = sg.base + (row + 1) * N + col, q = sg.core0 + row * N + col;
+                auto at = [&](int o) { return F3{ix[o], iy[o], iz[o]}; };
+                F3 nb[4], n2[4];
+                nb[0] = at(c + N);
+                nb[1] = at(c - N);
+                nb[2] = at(c + dl);
+                nb[3] = at(c + dr);
+                if (L.use_j2) {
+                    n2[0] = at(c + N + dr);
+                    n2[1] = at(c + N + dl);
+                    n2[2] = at(c - N + dr);
+                    n2[3] = at(c - N + dl);
+                }
+                const F3 d = rhs32_vals(at(c), nb, n2, L);
+                const float k0 = fm(d.x, L.dt), k1 = fm(d.y, L.dt), k2 = fm(d.z, L.dt);
+                if (S == 4) {
+                    const double o0 = (double)fa(ac[q], fd(k0, 6.f));
+                    const double o1 = (double)fa(ac[ns + q], fd(k1, 6.f));
+                    const double o2 = (double)fa(ac[2 * ns + q], fd(k2, 6.f));
+                    const double nrm = __dsqrt_rn(__dadd_rn(
+                        __dadd_rn(__dmul_rn(o0, o0), __dmul_rn(o1, o1)), __dmul_rn(o2, o2)));
+                    const float n0 = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o0), nrm));
+                    const float n1 = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o1), nrm));
+                    const float n2v = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o2), nrm));
+                    yb[q] = ox[c] = n0;
+                    yb[ns + q] = oy[c] = n1;
+                    yb[2 * ns + q] = oz[c] = n2v;
+                } else {
+                    const float bx = yb[q], by = yb[ns + q], bz = yb[2 * ns + q];
+                    if (S == 3) {
+                        ox[c] = fa(bx, k0);
+                        oy[c] = fa(by, k1);
+                        oz[c] = fa(bz, k2);
+                    } else {
+                        ox[c] = fa(bx, fm(k0, 0.5f));
+                        oy[c] = fa(by, fm(k1, 0.5f));
+                        oz[c] = fa(bz, fm(k2, 0.5f));
+                    }
+                    if (S == 1) {
+                        ac[q] = fa(bx, fd(k0, 6.f));
+                        ac[ns + q] = fa(by, fd(k1, 6.f));
+                        ac[2 * ns + q] = fa(bz, fd(k2, 6.f));
+                    } else {
+                        ac[q] = fa(ac[q], fd(k0, 3.f));
+                        ac[ns + q] = fa(ac[ns + q], fd(k1, 3.f));
+                        ac[2 * ns + q] = fa(ac[2 * ns + q], fd(k2, 3.f));
+                    }
+                }
+            }
+        }
+        halo(S & 1);
+    };
+    for (int step = 0; step < nsteps; ++step) {
+        stage(std::integral_constant<int, 1>{});
+        stage(std::integral_constant<int, 2>{});
+        stage(std::integral_constant<int, 3>{});
+        stage(std::integral_constant<int, 4>{});
+    }
+    for (int k = me.seg0; k < me.seg0 + me.nseg; ++k) {
+        const CSeg sg = segs[k];
+        const long M = (long)sg.N * sg.N;
+        float *Y = y + lats[sg.lat].off;
+        for (int e = tid; e < sg.rows * sg.N; e += T) {
+            const int row = e / sg.N, col = e - row * sg.N;
+            const long i = (long)(sg.r0 + row) * sg.N + col;
+            const int q = sg.core0 + e;
+            Y[i] = yb[q];
+            Y[M + i] = yb[ns + q];
+            Y[2 * M + i] = yb[2 * ns + q];
+        }
+    }
+}
+
 // One CTA waits at a grid barrier sized for two: nothing arrives for the
 // second, so the bounded barrier must give up and record a timeout.
 __global__ void grid_barrier_probe_kernel(BarrierState *bs, unsigned *status) {
@@ -227,6 +412,13 @@ struct asd_batch {
     int nitems = 0, tile = 0, ctas_per_sm = 0, grid = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = -1;
+    // kernel 0: the global-memory kernel (tile, ctas_per_sm); 1: the
+    // cluster-resident kernel (cl_size CTAs per cluster, cl_count clusters)
+    int kind = 0;
+    int cl_size = 0, cl_count = 0, cl_threads = 0;
+    size_t cl_smem = 0;
+    CCta *d_ctas = nullptr;
+    CSeg *d_segs = nullptr;
 };
 
 namespace {
@@ -258,6 +450,166 @@ int configure(asd_batch *b, int tile, int ctas_per_sm) {
     if (rc != ASD_OK) return rc;
     b->ctas_per_sm = ctas_per_sm;
     b->grid = std::min(sms * ctas_per_sm, b->nitems);
+    b->kind = 0;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_steps = -1;
+    return ASD_OK;
+}
+
+// Cluster plan: lattices onto C clusters of S CTAs, longest first onto the
+// least-loaded cluster; each cluster's rows (lattice after lattice) split
+// over its CTAs by site count (a row goes to the CTA whose share holds the
+// row's middle site); per CTA its segments laid out one after another, each
+// with a halo row above and below.  False if a CTA would need more than
+// smem_limit bytes or a lattice row is wider than a CTA's threads.
+struct ClusterPlan {
+    std::vector<CCta> ctas;
+    std::vector<CSeg> segs;
+    int max_sites = 0, max_buf = 0;
+};
+
+bool plan_clusters(const std::vector<BatchLattice> &lat, int S, int C, int max_sites,
+                   size_t smem_limit, ClusterPlan &pl) {
+    const int nl = (int)lat.size();
+    std::vector<int> order(nl);
+    for (int l = 0; l < nl; ++l) order[l] = l;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b2) { return lat[a].N > lat[b2].N; });
+    std::vector<long> load(C, 0);
+    std::vector<std::vector<int>> members(C);
+    for (int l : order) {
+        const int c = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        members[c].push_back(l);
+        load[c] += (long)lat[l].N * lat[l].N;
+    }
+    for (const BatchLattice &L : lat)
+        if (L.N > CL_THREADS) return false;  // a row per thread pass
+    pl.ctas.assign((size_t)C * S, CCta{0, 0, 0, 1});
+    pl.segs.clear();
+    pl.max_sites = pl.max_buf = 0;
+    for (int c = 0; c < C; ++c) {
+        std::vector<std::vector<CSeg>> cs(S);
+        long acc = 0;
+        int r = 0;
+        for (int l : members[c]) {
+            const int N = lat[l].N;
+            for (int row = 0; row < N; ++row) {
+                while (r < S - 1 && 2 * (acc + N / 2) >= 2 * (long)(r + 1) * load[c] / S) ++r;
+                std::vector<CSeg> &v = cs[r];
+                if (!v.empty() && v.back().lat == l && v.back().r0 + v.back().rows == row) {
+                    ++v.back().rows;
+                } else {
+                    CSeg sg{};
+                    sg.lat = l;
+                    sg.N = N;
+                    sg.r0 = row;
+                    sg.rows = 1;
+                    v.push_back(sg);
+                }
+                acc += N;
+            }
+        }
+        for (int k = 0; k < S; ++k) {  // layout
+            int base = 0, core = 0;
+            for (CSeg &sg : cs[k]) {
+                sg.base = base;
+                sg.core0 = core;
+                base += (sg.rows + 2) * sg.N;
+                core += sg.rows * sg.N;
+            }
+            CCta &ct = pl.ctas[(size_t)c * S + k];
+            ct.nsites = core;
+            ct.buf = base > 0 ? base : 1;
+            pl.max_sites = std::max(pl.max_sites, core);
+            pl.max_buf = std::max(pl.max_buf, ct.buf);
+        }
+        // halo sources: the CTA and slot holding row `want` of lattice l
+        auto find = [&](int l, int want, int &rank, int &off, int &bufsz) {
+            for (int k = 0; k < S; ++k)
+                for (const CSeg &sg : cs[k])
+                    if (sg.lat == l && want >= sg.r0 && want < sg.r0 + sg.rows) {
+                        rank = k;
+                        off = sg.base + (want - sg.r0 + 1) * sg.N;
+                        bufsz = pl.ctas[(size_t)c * S + k].buf;
+                        return;
+                    }
+        };
+        for (int k = 0; k < S; ++k) {
+            CCta &ct = pl.ctas[(size_t)c * S + k];
+            ct.seg0 = (int)pl.segs.size();
+            ct.nseg = (int)cs[k].size();
+            for (CSeg sg : cs[k]) {
+                find(sg.lat, (sg.r0 - 1 + sg.N) % sg.N, sg.top_rank, sg.top_off, sg.top_buf);
+                find(sg.lat, (sg.r0 + sg.rows) % sg.N, sg.bot_rank, sg.bot_off, sg.bot_buf);
+                pl.segs.push_back(sg);
+            }
+        }
+    }
+    (void)max_sites;
+    return cluster_smem_floats(pl.max_buf, pl.max_sites) * sizeof(float) <= smem_limit;
+}
+
+cudaError_t launch_cluster(const asd_batch *b, int nsteps, bool query_only = false,
+                           int *active = nullptr) {
+    auto k = batch_cluster_kernel;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)b->cl_smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(b->cl_count * b->cl_size));
+    cfg.blockDim = dim3((unsigned)b->cl_threads);
+    cfg.dynamicSmemBytes = b->cl_smem;
+    cfg.stream = b->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)b->cl_size;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (query_only) return cudaOccupancyMaxActiveClusters(active, k, &cfg);
+    return cudaLaunchKernelEx(&cfg, k, (const BatchLattice *)b->d_lat, (const CCta *)b->d_ctas,
+                              (const CSeg *)b->d_segs, b->y, nsteps);
+}
+
+int configure_cluster(asd_batch *b, int S, int threads) {
+    if (S < 1 || S > 8) return fail(ASD_ERR_INVALID, "cluster size %d (1..8)", S);
+    if (threads == 0) threads = CL_THREADS;
+    if (threads < 128 || threads > CL_THREADS || threads % 32)
+        return fail(ASD_ERR_INVALID, "threads %d (128..%d, a multiple of 32)", threads, CL_THREADS);
+    int sms = 0, smem_optin = 0;
+    ASD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    ASD_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                        b->device));
+    int C = sms / S;
+    ClusterPlan pl;
+    for (;;) {
+        if (C < 1 || !plan_clusters(b->lat, S, C, 0, (size_t)smem_optin, pl) ||
+            [&] { for (const BatchLattice &L : b->lat) if (L.N > threads) return true; return false; }())
+            return fail(ASD_ERR_UNSUPPORTED,
+                        "the batch does not fit in shared memory with clusters of %d CTAs", S);
+        b->cl_size = S;
+        b->cl_count = C;
+        b->cl_threads = threads;
+        b->cl_smem = cluster_smem_floats(pl.max_buf, pl.max_sites) * sizeof(float);
+        int active = 0;
+        ASD_CUDA_TRY(launch_cluster(b, 0, true, &active));
+        if (active >= C) break;
+        C = active;  // every cluster resident at once: fewer, larger clusters
+    }
+    if (b->d_ctas) cudaFree(b->d_ctas);
+    if (b->d_segs) cudaFree(b->d_segs);
+    b->d_ctas = nullptr;
+    b->d_segs = nullptr;
+    ASD_CUDA_TRY(cudaMalloc(&b->d_ctas, pl.ctas.size() * sizeof(CCta)));
+    ASD_CUDA_TRY(cudaMalloc(&b->d_segs, std::max<size_t>(1, pl.segs.size()) * sizeof(CSeg)));
+    ASD_CUDA_TRY(cudaMemcpy(b->d_ctas, pl.ctas.data(), pl.ctas.size() * sizeof(CCta),
+                            cudaMemcpyHostToDevice));
+    if (!pl.segs.empty())
+        ASD_CUDA_TRY(cudaMemcpy(b->d_segs, pl.segs.data(), pl.segs.size() * sizeof(CSeg),
+                                cudaMemcpyHostToDevice));
+    b->kind = 1;
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
     b->graph_steps = -1;
@@ -265,6 +617,10 @@ int configure(asd_batch *b, int tile, int ctas_per_sm) {
 }
 
 int launch(asd_batch *b, int nsteps) {
+    if (b->kind == 1) {
+        ASD_CUDA_TRY(launch_cluster(b, nsteps));
+        return ASD_OK;
+    }
     // cooperative: every CTA resident, which the grid barrier relies on
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(b->grid);
@@ -325,7 +681,8 @@ void destroy(asd_batch *b) {
     if (!b) return;
     cudaSetDevice(b->device);
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    void *p[] = {b->d_lat, b->y, b->ysa, b->ysb, b->acc, b->bs, b->status, b->d_items};
+    void *p[] = {b->d_lat, b->y, b->ysa, b->ysb, b->acc, b->bs, b->status, b->d_items,
+                 b->d_ctas, b->d_segs};
     for (void *q : p)
         if (q) cudaFree(q);
     delete b;
@@ -443,6 +800,12 @@ int asd_batch_configure(asd_batch *b, int tile, int ctas_per_sm) {
     return configure(b, tile, ctas_per_sm);
 }
 
+int asd_batch_configure_cluster(asd_batch *b, int cluster_size, int threads) {
+    if (!b) return fail(ASD_ERR_INVALID, "batch is NULL");
+    ASD_CUDA_TRY(cudaSetDevice(b->device));
+    return configure_cluster(b, cluster_size, threads);
+}
+
 int asd_batch_autotune(asd_batch *b, int trial_steps, int *tile, int *ctas_per_sm,
                        double *ms_per_step) {
     if (!b || trial_steps < 1) return fail(ASD_ERR_INVALID, "bad argument");
@@ -455,13 +818,29 @@ int asd_batch_autotune(asd_batch *b, int trial_steps, int *tile, int *ctas_per_s
     ASD_CUDA_TRY(cudaMalloc(&save, bytes));
     cudaMemcpyAsync(save, b->y, bytes, cudaMemcpyDeviceToDevice, b->stream);
     double best = 1e300;
-    int bt = 128, bc = 1;
+    int bt = 128, bc = 1, bthreads = 0;  // bt = 0: cluster kernel, bc = cluster size
     const int tiles[] = {32, 64, 128, 256};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int rc = ASD_OK;
+    // the cluster-resident kernel, where the batch fits in shared memory
+    for (int S = 1; S <= 8; ++S) {
+        for (int threads : {256, 384, 512, CL_THREADS}) {
+            if (configure_cluster(b, S, threads) != ASD_OK) continue;  // does not fit
+            if ((rc = asd_batch_run(b, trial_steps)) != ASD_OK) break;  // captures and warms
+            cudaEventRecord(e0, b->stream);
+            if ((rc = run(b, trial_steps)) != ASD_OK) break;
+            cudaEventRecord(e1, b->stream);
+            if ((rc = check_status(b)) != ASD_OK) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) best = ms, bt = 0, bc = S, bthreads = threads;
+        }
+        if (rc != ASD_OK) break;
+    }
     for (int t : tiles) {
+        if (rc != ASD_OK) break;
         for (int c = 1; c <= std::min(occ, 8); c *= 2) {
             if ((rc = configure(b, t, c)) != ASD_OK) break;
             if ((rc = asd_batch_run(b, trial_steps)) != ASD_OK) break;  // captures and warms
@@ -481,7 +860,8 @@ int asd_batch_autotune(asd_batch *b, int trial_steps, int *tile, int *ctas_per_s
     cudaStreamSynchronize(b->stream);
     cudaFree(save);
     if (rc != ASD_OK) return rc;
-    if ((rc = configure(b, bt, bc)) != ASD_OK) return rc;
+    if ((rc = bt == 0 ? configure_cluster(b, bc, bthreads) : configure(b, bt, bc)) != ASD_OK)
+        return rc;
     if (tile) *tile = bt;
     if (ctas_per_sm) *ctas_per_sm = bc;
     if (ms_per_step) *ms_per_step = best / trial_steps;

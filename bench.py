@@ -547,17 +547,36 @@ def run_workload(args):
         for l, N in enumerate(sizes):
             b.set_spins(l, asd.noisy_ordered_spins(N, float(rng.uniform(0, 0.5)), l).astype(np.float32))
         tile, ctas, _ = b.autotune(20)
-        b.run(10)
-        t0 = time.perf_counter()
-        b.run(2000)
-        t = time.perf_counter() - t0
+
+        def time_run(n=2000):
+            b.run(10)
+            t0 = time.perf_counter()
+            b.run(n)
+            return time.perf_counter() - t0
+
+        t = time_run()
         sites = sum(N * N for N in sizes)
+        chosen = ({"kernel": "cluster-resident", "cluster_size": ctas} if tile == 0 else
+                  {"kernel": "global-memory", "tile": tile, "ctas_per_sm": ctas})
+        # the other kernel family, for comparison (its autotuned best is not kept)
+        if tile == 0:
+            b.configure(256, 4)
+            other = {"kernel": "global-memory", "tile": 256, "ctas_per_sm": 4}
+        else:
+            try:
+                b.configure_cluster(8, 512)
+                other = {"kernel": "cluster-resident", "cluster_size": 8}
+            except asd.AsdError:
+                other = None
+        if other is not None:
+            other["ms_per_step"] = time_run() / 2000 * 1e3
         out.update({
             "metric": "batched site-steps/s (one persistent launch, 2000 steps)",
             "value": sites * 2000 / t, "unit": "site-steps/s", "ms_per_step": t / 2000 * 1e3,
             "dtype": "f32 RK4 + f64 renorm",
             "config": {"workload": "48 lattices, sizes in {48,64,96,128,160}^2", "sites": sites,
-                       "tile": tile, "ctas_per_sm": ctas},
+                       **chosen},
+            "other_kernel": other,
         })
         b.close()
     print(json.dumps(out))

@@ -288,7 +288,7 @@ int asd_sqt_split_noalloc(int kind, long rows, int Kp, const void *a_hi, const v
 /* ------------------------------------------------------ batched lattices */
 /* Many independent lattices (one replica each) of different sizes and
  * parameters, stepped together by one persistent, graph-captured launch with
- * all spins resident on the GPU.  RK4 stages in FP32 (explicitly rounded, the
+ * all spins resident on the GPU (in shared memory, or in L2 and HBM).  RK4 stages in FP32 (explicitly rounded, the
  * reference's operation order), renormalisation in FP64.  No counterpart in
  * the reference, which runs one lattice per program. */
 typedef struct {
@@ -307,12 +307,28 @@ int asd_batch_get_spins(asd_batch *batch, int lattice, float *spin_aos);
  * per step count); synchronous; ASD_ERR_TIMEOUT if the kernel's bounded grid
  * barrier gave up. */
 int asd_batch_run(asd_batch *batch, int nsteps);
-/* Work decomposition: `tile` consecutive sites per work item (32..256, a
- * multiple of 32) and `ctas_per_sm` resident CTAs per SM. */
+/* Global-memory kernel: spins in L2/HBM, one cooperative launch whose CTAs
+ * take work items of `tile` consecutive sites (32..256, a multiple of 32),
+ * `ctas_per_sm` resident CTAs per SM, a bounded grid barrier per RK4 stage.
+ * Works for any batch. */
 int asd_batch_configure(asd_batch *batch, int tile, int ctas_per_sm);
-/* Times trial_steps steps for every tile in {32, 64, 128, 256} and CTAs per SM
- * in {1, 2, 4, 8} (as far as they fit), keeps the fastest and reports it; the
- * spins are restored afterwards. */
+/* Cluster-resident kernel: every lattice lives in the shared memory of one
+ * thread-block cluster of `cluster_size` CTAs (1..8; `threads` per CTA 128..640,
+ * a multiple of 32, 0 = 640) for the whole run; lattices are packed onto the
+ * clusters longest first and each cluster's rows split over its CTAs; halo
+ * rows cross between CTAs through distributed shared memory after a cluster
+ * barrier per RK4 stage.  As many clusters as the GPU holds at once.  Same
+ * arithmetic as the global-memory kernel, bit for bit.  ASD_ERR_UNSUPPORTED
+ * if the batch does not fit (48 bytes of shared memory per site plus halo
+ * rows; lattice rows no wider than `threads`). */
+int asd_batch_configure_cluster(asd_batch *batch, int cluster_size, int threads);
+/* Times trial_steps steps for every cluster-resident configuration that fits
+ * (cluster sizes 1..8 x 256, 384, 512 or 640 threads) and every global-memory
+ * configuration (tile in {32, 64, 128, 256} x CTAs per SM in {1, 2, 4, 8},
+ * as far as they fit), keeps the fastest and reports it: *tile and
+ * *ctas_per_sm for the global-memory kernel, or *tile = 0 and *ctas_per_sm =
+ * the cluster size for the cluster-resident one.  The spins are restored
+ * afterwards. */
 int asd_batch_autotune(asd_batch *batch, int trial_steps, int *tile, int *ctas_per_sm,
                        double *ms_per_step);
 

@@ -47,6 +47,43 @@ def test_batch_bit_exact(oracle, tile, ctas):
         check_bit_exact(oracle, lats, spins, b, 20)
 
 
+@pytest.mark.parametrize("cluster,threads,sizes", [
+    (8, 512, [48, 64, 37, 96, 5, 128, 160, 20]),   # 160^2 over 8 CTAs; 10 empty clusters
+    (4, 256, [48, 64, 37, 5, 20, 3, 33]),
+    (2, 512, [64, 37, 5, 20, 3]),
+    (1, 512, [37, 5, 20, 3, 48]),                   # one CTA per lattice, whole lattices
+    (6, 640, [160, 128, 96, 64, 48, 48]),           # a cluster size that is not a power of 2
+    (3, 384, [96, 5, 37, 64, 3]),
+])
+def test_batch_cluster_bit_exact(oracle, cluster, threads, sizes):
+    """The cluster-resident kernel (lattices in shared memory, rows split over
+    a cluster's CTAs, halo rows through distributed shared memory) equals the
+    FP32 oracle bit for bit, like the global-memory kernel."""
+    lats, spins = ensemble(sizes, seed=4)
+    with asd.Batch([asd.Lattice.make(N, **kw) for N, kw in lats]) as b:
+        b.configure_cluster(cluster, threads)
+        for l, s in enumerate(spins):
+            b.set_spins(l, s)
+        b.run(7)
+        b.run(13)
+        check_bit_exact(oracle, lats, spins, b, 20)
+        b.configure(128, 2)  # switching kernels keeps the state
+        b.run(3)
+        check_bit_exact(oracle, lats, spins, b, 23)
+
+
+def test_batch_cluster_rejects_a_batch_that_does_not_fit():
+    """A 160^2 lattice needs 25600 sites (1.2 MB of shared memory) in one
+    cluster: more than one CTA holds, and its rows are wider than 128
+    threads."""
+    with asd.Batch([asd.Lattice.make(160, J1=1.0, dt=0.01)]) as b:
+        for size, threads in ((1, 640), (8, 128)):
+            with pytest.raises(asd.AsdError) as e:
+                b.configure_cluster(size, threads)
+            assert e.value.code == asd.ASD_ERR_UNSUPPORTED
+        b.configure_cluster(8, 512)
+
+
 def test_batch_ensemble_configuration(oracle):
     """48 lattices with sizes drawn from {48, 64, 96, 128, 160}^2, noise
     amplitudes in [0, 0.5], alpha in [0.01, 0.2]; autotuned; 2000 steps.  The
@@ -58,7 +95,9 @@ def test_batch_ensemble_configuration(oracle):
         for l, s in enumerate(spins):
             b.set_spins(l, s)
         tile, ctas, ms = b.autotune(10)
-        assert tile in (32, 64, 128, 256) and ctas >= 1 and ms > 0
+        # tile 0: the cluster-resident kernel with clusters of `ctas` CTAs
+        assert (tile in (32, 64, 128, 256) or (tile == 0 and 1 <= ctas <= 8)) and ctas >= 1
+        assert ms > 0
         b.run(100)
         check_bit_exact(oracle, lats[:12], spins[:12], b, 100)
         b.run(1900)
