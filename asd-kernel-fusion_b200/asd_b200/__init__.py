@@ -51,7 +51,7 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
     "asd_ctx_last_launches",
     "asd_ctx_check_device_status",
-    "asd_check_bounded_wait", "asd_check_const_division", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
+    "asd_check_bounded_wait", "asd_check_const_division", "asd_check_const_division_f32", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
     "asd_spins_save", "asd_spins_load", "asd_batch_create", "asd_batch_destroy",
     "asd_batch_set_stream", "asd_batch_set_spins", "asd_batch_get_spins", "asd_batch_run",
     "asd_batch_configure", "asd_batch_configure_cluster", "asd_batch_autotune", "asd_set_params", "euler", "runge_kutta",
@@ -146,6 +146,7 @@ def load() -> C.CDLL:
         "asd_ctx_check_device_status": ([vp], C.c_int),
         "asd_check_bounded_wait": ([C.c_int, C.c_uint, vp], C.c_int),
         "asd_check_const_division": ([vp, C.c_long, vp, vp], C.c_int),
+        "asd_check_const_division_f32": ([vp, vp], C.c_int),
         "asd_umma_gemm_f32": ([C.c_int, C.c_long, C.c_int, vp, vp, vp, vp, vp, C.c_long, C.c_int,
                                vp],
                               C.c_int),
@@ -421,6 +422,11 @@ def check_const_division(x_ptr: int, n: int, bad_ptr: int, stream: int = 0) -> N
     """asd_check_const_division on device pointers (diagnostic)."""
     _check(load().asd_check_const_division(C.c_void_p(x_ptr), int(n), C.c_void_p(bad_ptr),
                                            C.c_void_p(stream)))
+
+
+def check_const_division_f32(bad_ptr: int, stream: int = 0) -> None:
+    """asd_check_const_division_f32: all 2^32 float patterns (diagnostic)."""
+    _check(load().asd_check_const_division_f32(C.c_void_p(bad_ptr), C.c_void_p(stream)))
 
 
 def save_spins(path, spins: np.ndarray, step: int = 0, spin_len: float = 1.0) -> None:

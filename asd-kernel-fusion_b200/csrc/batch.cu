@@ -41,7 +41,22 @@ constexpr uint32_t BARRIER_LIMIT = 1u << 22;
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+// x / d for the constants d = 3 and 6 in FP32, correctly rounded, by
+// Markstein's correction step (P. Markstein, IBM J. Res. Dev. 34(1), 1990),
+// as the FP64 forms of the LLG kernels: c = RN(1/d), q = RN(x c), the
+// remainder q d - x is exact in one FMA, and RN(q - (q d - x) c) = RN(x/d).
+// Outside 2^-100 <= |x| <= 2^100 (zeros, tiny and huge values, inf, NaN) the
+// division itself.  asd_check_const_division_f32 compares it with __fdiv_rn
+// over all 2^32 bit patterns.
+__device__ __forceinline__ float fdiv_const(float x, float d, float c) {
+    const float ax = fabsf(x);
+    if (!(ax >= 0x1p-100f && ax <= 0x1p100f)) return __fdiv_rn(x, d);
+    const float q = __fmul_rn(x, c);
+    const float t = __fmaf_rn(q, d, -x);
+    return __fmaf_rn(-t, c, q);
+}
+__device__ __forceinline__ float fd3(float x) { return fdiv_const(x, 3.f, 1.f / 3.f); }
+__device__ __forceinline__ float fd6(float x) { return fdiv_const(x, 6.f, 1.f / 6.f); }
 
 struct F3 {
     float x, y, z;
@@ -151,7 +166,7 @@ struct Item {
 };
 
 // One persistent launch for nsteps steps of every lattice.
-__global__ void __launch_bounds__(256) batch_kernel(const BatchLattice *__restrict__ lats,
+__global__ void __launch_bounds__(256, 4) batch_kernel(const BatchLattice *__restrict__ lats,
                                                     const Item *__restrict__ items, int nitems,
                                                     float *y, float *ysa, float *ysb, float *acc,
                                                     int nsteps, BarrierState *bs,
@@ -174,9 +189,9 @@ __global__ void __launch_bounds__(256) batch_kernel(const BatchLattice *__restri
                 const F3 d = rhs32(I, L, i);
                 const float k0 = fm(d.x, L.dt), k1 = fm(d.y, L.dt), k2 = fm(d.z, L.dt);
                 if (stage == 4) {
-                    const double o0 = (double)fa(__ldcg(A + i), fd(k0, 6.f));
-                    const double o1 = (double)fa(__ldcg(A + M + i), fd(k1, 6.f));
-                    const double o2 = (double)fa(__ldcg(A + 2 * M + i), fd(k2, 6.f));
+                    const double o0 = (double)fa(__ldcg(A + i), fd6(k0));
+                    const double o1 = (double)fa(__ldcg(A + M + i), fd6(k1));
+                    const double o2 = (double)fa(__ldcg(A + 2 * M + i), fd6(k2));
                     const double nrm = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(o0, o0),
                                                                       __dmul_rn(o1, o1)),
                                                             __dmul_rn(o2, o2)));
@@ -194,13 +209,13 @@ __global__ void __launch_bounds__(256) batch_kernel(const BatchLattice *__restri
                     O[M + i] = o.y;
                     O[2 * M + i] = o.z;
                     if (stage == 1) {
-                        A[i] = fa(yb.x, fd(kk.x, 6.f));
-                        A[M + i] = fa(yb.y, fd(kk.y, 6.f));
-                        A[2 * M + i] = fa(yb.z, fd(kk.z, 6.f));
+                        A[i] = fa(yb.x, fd6(kk.x));
+                        A[M + i] = fa(yb.y, fd6(kk.y));
+                        A[2 * M + i] = fa(yb.z, fd6(kk.z));
                     } else {
-                        A[i] = fa(__ldcg(A + i), fd(kk.x, 3.f));
-                        A[M + i] = fa(__ldcg(A + M + i), fd(kk.y, 3.f));
-                        A[2 * M + i] = fa(__ldcg(A + 2 * M + i), fd(kk.z, 3.f));
+                        A[i] = fa(__ldcg(A + i), fd3(kk.x));
+                        A[M + i] = fa(__ldcg(A + M + i), fd3(kk.y));
+                        A[2 * M + i] = fa(__ldcg(A + 2 * M + i), fd3(kk.z));
                     }
                 }
             }
@@ -322,9 +337,9 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
                 const F3 d = rhs32_vals(at(c), nb, n2, L);
                 const float k0 = fm(d.x, L.dt), k1 = fm(d.y, L.dt), k2 = fm(d.z, L.dt);
                 if (S == 4) {
-                    const double o0 = (double)fa(ac[q], fd(k0, 6.f));
-                    const double o1 = (double)fa(ac[ns + q], fd(k1, 6.f));
-                    const double o2 = (double)fa(ac[2 * ns + q], fd(k2, 6.f));
+                    const double o0 = (double)fa(ac[q], fd6(k0));
+                    const double o1 = (double)fa(ac[ns + q], fd6(k1));
+                    const double o2 = (double)fa(ac[2 * ns + q], fd6(k2));
                     const double nrm = __dsqrt_rn(__dadd_rn(
                         __dadd_rn(__dmul_rn(o0, o0), __dmul_rn(o1, o1)), __dmul_rn(o2, o2)));
                     const float n0 = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o0), nrm));
@@ -345,13 +360,13 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
                         oz[c] = fa(bz, fm(k2, 0.5f));
                     }
                     if (S == 1) {
-                        ac[q] = fa(bx, fd(k0, 6.f));
-                        ac[ns + q] = fa(by, fd(k1, 6.f));
-                        ac[2 * ns + q] = fa(bz, fd(k2, 6.f));
+                        ac[q] = fa(bx, fd6(k0));
+                        ac[ns + q] = fa(by, fd6(k1));
+                        ac[2 * ns + q] = fa(bz, fd6(k2));
                     } else {
-                        ac[q] = fa(ac[q], fd(k0, 3.f));
-                        ac[ns + q] = fa(ac[ns + q], fd(k1, 3.f));
-                        ac[2 * ns + q] = fa(ac[2 * ns + q], fd(k2, 3.f));
+                        ac[q] = fa(ac[q], fd3(k0));
+                        ac[ns + q] = fa(ac[ns + q], fd3(k1));
+                        ac[2 * ns + q] = fa(ac[2 * ns + q], fd3(k2));
                     }
                 }
             }
@@ -388,7 +403,27 @@ __global__ void grid_barrier_probe_kernel(BarrierState *bs, unsigned *status) {
     grid_barrier(bs, 2u, status, &s_fail);
 }
 
+// Every 32-bit pattern x: counts those for which fd3 / fd6 differ from
+// __fdiv_rn in any bit (NaN results count as equal).
+__global__ void fdiv_const_check_kernel(unsigned long long *bad) {
+    unsigned long long n = 0;
+    for (unsigned long long u = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         u < (1ull << 32); u += (unsigned long long)gridDim.x * blockDim.x) {
+        const float x = __uint_as_float((unsigned)u);
+        const float a3 = fd3(x), b3 = __fdiv_rn(x, 3.f), a6 = fd6(x), b6 = __fdiv_rn(x, 6.f);
+        const bool ok3 = __float_as_uint(a3) == __float_as_uint(b3) || (a3 != a3 && b3 != b3);
+        const bool ok6 = __float_as_uint(a6) == __float_as_uint(b6) || (a6 != a6 && b6 != b6);
+        n += !ok3 + !ok6;
+    }
+    if (n) atomicAdd(bad, n);
+}
+
 }  // namespace
+
+cudaError_t launch_fdiv_const_check(unsigned long long *bad, cudaStream_t st) {
+    fdiv_const_check_kernel<<<148 * 8, 256, 0, st>>>(bad);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_grid_barrier_probe(void *bs, unsigned *status, cudaStream_t st) {
     grid_barrier_probe_kernel<<<1, 32, 0, st>>>(static_cast<BarrierState *>(bs), status);
@@ -869,6 +904,13 @@ int asd_batch_autotune(asd_batch *b, int trial_steps, int *tile, int *ctas_per_s
 }
 
 }  // extern "C"
+
+extern "C" int asd_check_const_division_f32(unsigned long long *bad, void *stream) {
+    using namespace asd;
+    if (!bad) return fail(ASD_ERR_INVALID, "bad is NULL");
+    ASD_CUDA_TRY(launch_fdiv_const_check(bad, (cudaStream_t)stream));
+    return ASD_OK;
+}
 
 extern "C" int asd_check_bounded_wait(int which, unsigned limit, void *stream) {
     using namespace asd;

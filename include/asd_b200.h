@@ -240,6 +240,11 @@ int asd_check_bounded_wait(int which, unsigned limit, void *stream);
  * correction step) differ in any bit from the correctly rounded division.
  * No counterpart in the reference; tests use it.  Asynchronous on stream. */
 int asd_check_const_division(const double *x, long n, unsigned long long *bad, void *stream);
+/* Diagnostic: adds to *bad (device counter) the number of float bit patterns,
+ * out of all 2^32, for which the batched kernels' FP32 divisions by 3 and 6
+ * differ in any bit from the correctly rounded division (NaN = NaN).  No
+ * counterpart in the reference; tests use it.  Asynchronous on stream. */
+int asd_check_const_division_f32(unsigned long long *bad, void *stream);
 
 /* Diagnostic: the bare tensor-core product of the split S(q,t) GEMM,
  * C[i*ldc + j] = sum_k Ah[i][k]Bh[j][k] + Ah[i][k]Bl[j][k] + Al[i][k]Bh[j][k]

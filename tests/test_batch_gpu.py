@@ -105,3 +105,16 @@ def test_batch_ensemble_configuration(oracle):
             s = b.get_spins(l)
             assert np.all(np.isfinite(s))
             assert np.allclose(np.linalg.norm(s.astype(np.float64), axis=-1), 1.0, atol=1e-6)
+
+
+def test_fp32_constant_division_is_correctly_rounded():
+    """The batched kernels divide by 3 and 6 with Markstein's correction step;
+    over all 2^32 float bit patterns it must equal the correctly rounded
+    division bit for bit (NaN = NaN), so the kernels still match the FP32
+    oracle, which divides."""
+    import torch
+
+    bad = torch.zeros(1, dtype=torch.int64, device="cuda")
+    asd.check_const_division_f32(bad.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert int(bad.item()) == 0
