@@ -379,6 +379,9 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
         stage(std::integral_constant<int, 3>{});
         stage(std::integral_constant<int, 4>{});
     }
+    // No CTA may exit while another CTA of its cluster can still read its
+    // shared memory (the last halo copy).
+    cluster.sync();
     for (int k = me.seg0; k < me.seg0 + me.nseg; ++k) {
         const CSeg sg = segs[k];
         const long M = (long)sg.N * sg.N;
