@@ -71,8 +71,9 @@ __device__ __forceinline__ F3 ld3(const float *p, long M, long i) {
 // order (row+1), (row-1), (col-1), (col+1)) and n2 (diagonals (+1,+1),
 // (+1,-1), (-1,+1), (-1,-1); read only with J2), FP32, explicitly rounded.
 // Both batch kernels go through this function: one operation order.
-__device__ __forceinline__ F3 rhs32_vals(const F3 &s, const F3 (&nb)[4], const F3 (&n2)[4],
-                                         const BatchLattice &L) {
+template <bool J2, bool H, bool DAMP>
+__device__ __forceinline__ F3 rhs32_vals_t(const F3 &s, const F3 (&nb)[4], const F3 (&n2)[4],
+                                           const BatchLattice &L) {
     float ex = 0.f, ey = 0.f, ez = 0.f;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -80,7 +81,7 @@ __device__ __forceinline__ F3 rhs32_vals(const F3 &s, const F3 (&nb)[4], const F
         ey = fa(ey, fm(nb[j].y, L.J1));
         ez = fa(ez, fm(nb[j].z, L.J1));
     }
-    if (L.use_j2) {
+    if (J2) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             ex = fa(ex, fm(n2[j].x, L.J2));
@@ -88,18 +89,32 @@ __device__ __forceinline__ F3 rhs32_vals(const F3 &s, const F3 (&nb)[4], const F
             ez = fa(ez, fm(n2[j].z, L.J2));
         }
     }
-    if (L.use_h) {
+    if (H) {
         ex = fa(ex, L.hx);
         ey = fa(ey, L.hy);
         ez = fa(ez, L.hz);
     }
     F3 tau{fs(fm(ey, s.z), fm(ez, s.y)), fs(fm(ez, s.x), fm(ex, s.z)), fs(fm(ex, s.y), fm(ey, s.x))};
-    if (!L.use_damp) return tau;
+    if (!DAMP) return tau;
     const float ux = fs(fm(s.y, tau.z), fm(s.z, tau.y));
     const float uy = fs(fm(s.z, tau.x), fm(s.x, tau.z));
     const float uz = fs(fm(s.x, tau.y), fm(s.y, tau.x));
     return F3{fm(L.g, fa(tau.x, fm(L.alpha, ux))), fm(L.g, fa(tau.y, fm(L.alpha, uy))),
               fm(L.g, fa(tau.z, fm(L.alpha, uz)))};
+}
+
+__device__ __forceinline__ F3 rhs32_vals(const F3 &s, const F3 (&nb)[4], const F3 (&n2)[4],
+                                         const BatchLattice &L) {
+    switch ((L.use_j2 ? 4 : 0) | (L.use_h ? 2 : 0) | (L.use_damp ? 1 : 0)) {
+        case 0: return rhs32_vals_t<false, false, false>(s, nb, n2, L);
+        case 1: return rhs32_vals_t<false, false, true>(s, nb, n2, L);
+        case 2: return rhs32_vals_t<false, true, false>(s, nb, n2, L);
+        case 3: return rhs32_vals_t<false, true, true>(s, nb, n2, L);
+        case 4: return rhs32_vals_t<true, false, false>(s, nb, n2, L);
+        case 5: return rhs32_vals_t<true, false, true>(s, nb, n2, L);
+        case 6: return rhs32_vals_t<true, true, false>(s, nb, n2, L);
+        default: return rhs32_vals_t<true, true, true>(s, nb, n2, L);
+    }
 }
 
 __device__ __forceinline__ F3 rhs32(const float *ys, const BatchLattice &L, long i) {
@@ -254,7 +269,7 @@ struct CCta {
     int nsites;      // core sites
     int buf;         // slots per plane
 };
-constexpr int CL_THREADS = 640;
+constexpr int CL_THREADS = 896;
 
 __host__ __device__ constexpr size_t cluster_smem_floats(int buf, int sites) {
     return (size_t)6 * buf + (size_t)6 * sites;  // 2 x 3 planes, y base and combination
@@ -320,55 +335,73 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
             const int N = sg.N, rpp = T / N, r1 = tid / N, col = tid - r1 * N;
             if (r1 >= rpp) continue;  // the last T % N threads
             const int dl = (col == 0) ? N - 1 : -1, dr = (col == N - 1) ? 1 - N : 1;
-            for (int row = r1; row < sg.rows; row += rpp) {
-                const int c = sg.base + (row + 1) * N + col, q = sg.core0 + row * N + col;
-                auto at = [&](int o) { return F3{ix[o], iy[o], iz[o]}; };
-                F3 nb[4], n2[4];
-                nb[0] = at(c + N);
-                nb[1] = at(c - N);
-                nb[2] = at(c + dl);
-                nb[3] = at(c + dr);
-                if (L.use_j2) {
-                    n2[0] = at(c + N + dr);
-                    n2[1] = at(c + N + dl);
-                    n2[2] = at(c - N + dr);
-                    n2[3] = at(c - N + dl);
-                }
-                const F3 d = rhs32_vals(at(c), nb, n2, L);
-                const float k0 = fm(d.x, L.dt), k1 = fm(d.y, L.dt), k2 = fm(d.z, L.dt);
-                if (S == 4) {
-                    const double o0 = (double)fa(ac[q], fd6(k0));
-                    const double o1 = (double)fa(ac[ns + q], fd6(k1));
-                    const double o2 = (double)fa(ac[2 * ns + q], fd6(k2));
-                    const double nrm = __dsqrt_rn(__dadd_rn(
-                        __dadd_rn(__dmul_rn(o0, o0), __dmul_rn(o1, o1)), __dmul_rn(o2, o2)));
-                    const float n0 = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o0), nrm));
-                    const float n1 = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o1), nrm));
-                    const float n2v = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o2), nrm));
-                    yb[q] = ox[c] = n0;
-                    yb[ns + q] = oy[c] = n1;
-                    yb[2 * ns + q] = oz[c] = n2v;
-                } else {
-                    const float bx = yb[q], by = yb[ns + q], bz = yb[2 * ns + q];
-                    if (S == 3) {
-                        ox[c] = fa(bx, k0);
-                        oy[c] = fa(by, k1);
-                        oz[c] = fa(bz, k2);
-                    } else {
-                        ox[c] = fa(bx, fm(k0, 0.5f));
-                        oy[c] = fa(by, fm(k1, 0.5f));
-                        oz[c] = fa(bz, fm(k2, 0.5f));
+            // the segment's rows with the lattice's model terms fixed at compile time
+            auto rows_t = [&](auto j2c, auto hc, auto dc) {
+                constexpr bool J2 = decltype(j2c)::value, H = decltype(hc)::value,
+                               DAMP = decltype(dc)::value;
+                for (int row = r1; row < sg.rows; row += rpp) {
+                    const int c = sg.base + (row + 1) * N + col, q = sg.core0 + row * N + col;
+                    auto at = [&](int o) { return F3{ix[o], iy[o], iz[o]}; };
+                    F3 nb[4], n2[4];
+                    nb[0] = at(c + N);
+                    nb[1] = at(c - N);
+                    nb[2] = at(c + dl);
+                    nb[3] = at(c + dr);
+                    if (J2) {
+                        n2[0] = at(c + N + dr);
+                        n2[1] = at(c + N + dl);
+                        n2[2] = at(c - N + dr);
+                        n2[3] = at(c - N + dl);
                     }
-                    if (S == 1) {
-                        ac[q] = fa(bx, fd6(k0));
-                        ac[ns + q] = fa(by, fd6(k1));
-                        ac[2 * ns + q] = fa(bz, fd6(k2));
+                    const F3 d = rhs32_vals_t<J2, H, DAMP>(at(c), nb, n2, L);
+                    const float k0 = fm(d.x, L.dt), k1 = fm(d.y, L.dt), k2 = fm(d.z, L.dt);
+                    if (S == 4) {
+                        const double o0 = (double)fa(ac[q], fd6(k0));
+                        const double o1 = (double)fa(ac[ns + q], fd6(k1));
+                        const double o2 = (double)fa(ac[2 * ns + q], fd6(k2));
+                        const double nrm = __dsqrt_rn(__dadd_rn(
+                            __dadd_rn(__dmul_rn(o0, o0), __dmul_rn(o1, o1)), __dmul_rn(o2, o2)));
+                        const float n0 = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o0), nrm));
+                        const float n1 = __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o1), nrm));
+                        const float n2v =
+                            __double2float_rn(__ddiv_rn(__dmul_rn(L.spin_len, o2), nrm));
+                        yb[q] = ox[c] = n0;
+                        yb[ns + q] = oy[c] = n1;
+                        yb[2 * ns + q] = oz[c] = n2v;
                     } else {
-                        ac[q] = fa(ac[q], fd3(k0));
-                        ac[ns + q] = fa(ac[ns + q], fd3(k1));
-                        ac[2 * ns + q] = fa(ac[2 * ns + q], fd3(k2));
+                        const float bx = yb[q], by = yb[ns + q], bz = yb[2 * ns + q];
+                        if (S == 3) {
+                            ox[c] = fa(bx, k0);
+                            oy[c] = fa(by, k1);
+                            oz[c] = fa(bz, k2);
+                        } else {
+                            ox[c] = fa(bx, fm(k0, 0.5f));
+                            oy[c] = fa(by, fm(k1, 0.5f));
+                            oz[c] = fa(bz, fm(k2, 0.5f));
+                        }
+                        if (S == 1) {
+                            ac[q] = fa(bx, fd6(k0));
+                            ac[ns + q] = fa(by, fd6(k1));
+                            ac[2 * ns + q] = fa(bz, fd6(k2));
+                        } else {
+                            ac[q] = fa(ac[q], fd3(k0));
+                            ac[ns + q] = fa(ac[ns + q], fd3(k1));
+                            ac[2 * ns + q] = fa(ac[2 * ns + q], fd3(k2));
+                        }
                     }
                 }
+            };
+            using TT = std::true_type;
+            using FF = std::false_type;
+            switch ((L.use_j2 ? 4 : 0) | (L.use_h ? 2 : 0) | (L.use_damp ? 1 : 0)) {
+                case 0: rows_t(FF{}, FF{}, FF{}); break;
+                case 1: rows_t(FF{}, FF{}, TT{}); break;
+                case 2: rows_t(FF{}, TT{}, FF{}); break;
+                case 3: rows_t(FF{}, TT{}, TT{}); break;
+                case 4: rows_t(TT{}, FF{}, FF{}); break;
+                case 5: rows_t(TT{}, FF{}, TT{}); break;
+                case 6: rows_t(TT{}, TT{}, FF{}); break;
+                default: rows_t(TT{}, TT{}, TT{}); break;
             }
         }
         halo(S & 1);
@@ -864,7 +897,7 @@ int asd_batch_autotune(asd_batch *b, int trial_steps, int *tile, int *ctas_per_s
     int rc = ASD_OK;
     // the cluster-resident kernel, where the batch fits in shared memory
     for (int S = 1; S <= 8; ++S) {
-        for (int threads : {256, 384, 512, CL_THREADS}) {
+        for (int threads : {256, 384, 512, 640, 768, CL_THREADS}) {
             if (configure_cluster(b, S, threads) != ASD_OK) continue;  // does not fit
             if ((rc = asd_batch_run(b, trial_steps)) != ASD_OK) break;  // captures and warms
             cudaEventRecord(e0, b->stream);

@@ -546,7 +546,11 @@ def run_workload(args):
         b = asd.Batch(lats)
         for l, N in enumerate(sizes):
             b.set_spins(l, asd.noisy_ordered_spins(N, float(rng.uniform(0, 0.5)), l).astype(np.float32))
-        tile, ctas, _ = b.autotune(20)
+        if args.batch_cluster:
+            b.configure_cluster(args.batch_cluster, 0)
+            tile, ctas = 0, args.batch_cluster
+        else:
+            tile, ctas, _ = b.autotune(20)
 
         def time_run(n=2000):
             b.run(10)
@@ -670,6 +674,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mode", choices=["tf32x3", "bf16x3", "fp64", "fp64_fused"], default="tf32x3")
+    ap.add_argument("--batch-cluster", type=int, default=0,
+                    help="batch48: clusters of this many CTAs instead of the autotuner's choice")
     ap.add_argument("--llg-kernel", choices=["fused", "stages"], default="fused",
                     help="RK4 step of the headline: one streamed launch (default) or four "
                          "stage kernels")

@@ -318,8 +318,8 @@ int asd_batch_run(asd_batch *batch, int nsteps);
  * Works for any batch. */
 int asd_batch_configure(asd_batch *batch, int tile, int ctas_per_sm);
 /* Cluster-resident kernel: every lattice lives in the shared memory of one
- * thread-block cluster of `cluster_size` CTAs (1..8; `threads` per CTA 128..640,
- * a multiple of 32, 0 = 640) for the whole run; lattices are packed onto the
+ * thread-block cluster of `cluster_size` CTAs (1..8; `threads` per CTA 128..896,
+ * a multiple of 32, 0 = 896) for the whole run; lattices are packed onto the
  * clusters longest first and each cluster's rows split over its CTAs; halo
  * rows cross between CTAs through distributed shared memory after a cluster
  * barrier per RK4 stage.  As many clusters as the GPU holds at once.  Same
@@ -328,7 +328,7 @@ int asd_batch_configure(asd_batch *batch, int tile, int ctas_per_sm);
  * rows; lattice rows no wider than `threads`). */
 int asd_batch_configure_cluster(asd_batch *batch, int cluster_size, int threads);
 /* Times trial_steps steps for every cluster-resident configuration that fits
- * (cluster sizes 1..8 x 256, 384, 512 or 640 threads) and every global-memory
+ * (cluster sizes 1..8 x 256..896 threads) and every global-memory
  * configuration (tile in {32, 64, 128, 256} x CTAs per SM in {1, 2, 4, 8},
  * as far as they fit), keeps the fastest and reports it: *tile and
  * *ctas_per_sm for the global-memory kernel, or *tile = 0 and *ctas_per_sm =
