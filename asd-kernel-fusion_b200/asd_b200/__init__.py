@@ -30,6 +30,7 @@ ASD_ERR_UNSUPPORTED = -6
 
 LLG_STAGES = 0
 LLG_FUSED_STEP = 1
+LLG_AUTO = 2
 
 SQT_FP64 = 0
 SQT_TF32X3 = 1
@@ -352,7 +353,7 @@ class Context:
 
     def set_llg_kernel(self, kernel) -> None:
         """"stages" (four launches, the default) or "fused" (one launch per step)."""
-        k = {"fused": LLG_FUSED_STEP, "stages": LLG_STAGES}.get(kernel, kernel)
+        k = {"fused": LLG_FUSED_STEP, "stages": LLG_STAGES, "auto": LLG_AUTO}.get(kernel, kernel)
         _check(load().asd_ctx_set_llg_kernel(self._h, int(k)))
 
     def set_chunk_k(self, chunk_k: int) -> None:

@@ -91,7 +91,7 @@ struct asd_ctx {
     // asd_ctx_step_host: copy stream and event for the overlapped read-back
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t spins_ready = nullptr;
-    int llg_kernel = ASD_LLG_FUSED_STEP;
+    int llg_kernel = ASD_LLG_AUTO;
     // Pipelining of asd_ctx_step behind asd_ctx_sqt_async: once a split-mode
     // S(q,t) has turned y into its GEMM operands, the GEMM reads none of the
     // LLG buffers, so the next RK4 step may run beside it on llg_stream.
@@ -259,8 +259,15 @@ int set_spins_common(asd_ctx *c, const double *aos, bool host, int as_origin) {
     return ASD_OK;
 }
 
+// The LLG kernel for replicas [a.f0, a.f0 + a.nc): the one-launch step or
+// the four stage kernels (ASD_LLG_AUTO: the former where it fills the GPU).
+bool use_fused(const asd_ctx *c, const LLGArgs &a) {
+    return c->llg_kernel == ASD_LLG_FUSED_STEP ||
+           (c->llg_kernel == ASD_LLG_AUTO && llg_fused_fills(a));
+}
+
 int run_steps(asd_ctx *c, int nsteps) {
-    if (c->llg_kernel == ASD_LLG_FUSED_STEP) {
+    if (use_fused(c, c->a)) {
         for (int s = 0; s < nsteps; ++s) {
             ASD_CUDA_TRY(launch_llg_step_fused(c->a, c->y, c->ys_a, c->stream));
             double *t = c->y;  // ping-pong: the new state becomes y
@@ -503,8 +510,12 @@ int loss_grad(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target
     ASD_CUDA_TRY(cudaMemcpyAsync(ck[0], c->origin, sb, cudaMemcpyDeviceToDevice, st));
     double *cur = seg[0], *nxt = seg[1];
     ASD_CUDA_TRY(cudaMemcpyAsync(cur, c->origin, sb, cudaMemcpyDeviceToDevice, st));
+    // Only states are kept on the way forward: one launch per step where
+    // that fills the GPU.
+    const bool fwd_fused = use_fused(c, c->a);
     for (int n = 1; n <= nsteps; ++n) {
-        if ((rc = step_into(c, cur, s2, s3, s4, acc, nxt)) != ASD_OK) return rc;
+        if (fwd_fused) ASD_CUDA_TRY(launch_llg_step_fused(c->a, cur, nxt, st));
+        else if ((rc = step_into(c, cur, s2, s3, s4, acc, nxt)) != ASD_OK) return rc;
         double *t = cur;
         cur = nxt;
         nxt = t;
@@ -543,8 +554,10 @@ int loss_grad(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target
         const int base = cidx * ckpt;
         const int len = (nsteps - base < ckpt) ? nsteps - base : ckpt;
         ASD_CUDA_TRY(cudaMemcpyAsync(seg[0], ck[cidx], sb, cudaMemcpyDeviceToDevice, st));
-        for (int j = 1; j <= len; ++j)
-            if ((rc = step_into(c, seg[j - 1], s2, s3, s4, acc, seg[j])) != ASD_OK) return rc;
+        for (int j = 1; j <= len; ++j) {
+            if (fwd_fused) ASD_CUDA_TRY(launch_llg_step_fused(c->a, seg[j - 1], seg[j], st));
+            else if ((rc = step_into(c, seg[j - 1], s2, s3, s4, acc, seg[j])) != ASD_OK) return rc;
+        }
         for (int n = base + len; n > base; --n) {
             const int j = n - base;
             if (n % stride == 0 && n / stride <= E) {
@@ -759,7 +772,9 @@ int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int m
     long nparts = 0;
     // The one-launch step is out of place: each chunk's new state goes to
     // ys_a (its replicas only), and y and ys_a swap after the last chunk.
-    const bool fused = c->llg_kernel == ASD_LLG_FUSED_STEP;
+    LLGArgs ac = c->a;  // a whole chunk decides the kernel for every chunk
+    ac.nc = cr < nf ? cr : nf;
+    const bool fused = use_fused(c, ac);
     double *const ynew = fused ? c->ys_a : c->y;
     for (int r = 0; r < nchunks; ++r) {
         const int f0 = r * cr, nc = (nf - f0 < cr) ? nf - f0 : cr, b = r & 1;
@@ -892,7 +907,9 @@ int step_host_async(asd_ctx *c, const double *spin_in, double *spin_out, int mod
     if (rc != ASD_OK) return rc;
     const int cr = async_chunk_replicas(nf), nchunks = (nf + cr - 1) / cr;
     const cudaStream_t comp = c->stream, up = c->h2d_stream, down = c->copy_stream;
-    const bool fused = c->llg_kernel == ASD_LLG_FUSED_STEP;
+    LLGArgs ac = c->a;  // a whole chunk decides the kernel for every chunk
+    ac.nc = cr < nf ? cr : nf;
+    const bool fused = use_fused(c, ac);
     double *const ynew = fused ? c->ys_a : c->y;
     LLGArgs a = c->a;
     for (int r = 0; r < nchunks; ++r) {
@@ -1416,7 +1433,7 @@ int asd_ctx_shard_sqt_finish(asd_ctx *c, const double *d_part, const double *d_s
 
 int asd_ctx_set_llg_kernel(asd_ctx *c, int kernel) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
-    if (kernel != ASD_LLG_FUSED_STEP && kernel != ASD_LLG_STAGES)
+    if (kernel != ASD_LLG_FUSED_STEP && kernel != ASD_LLG_STAGES && kernel != ASD_LLG_AUTO)
         return fail(ASD_ERR_INVALID, "unknown LLG kernel %d", kernel);
     c->llg_kernel = kernel;
     return ASD_OK;

@@ -517,6 +517,19 @@ cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const
     return cudaErrorInvalidValue;
 }
 
+bool llg_fused_fills(const LLGArgs &a) {
+    using namespace stream;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    const long nb = (a.N + WC_MAX - 1) / WC_MAX, ng = (a.nc + SF - 1) / SF;
+    const long slots = 2L * sms;  // two CTAs of the streamed step per SM
+    return nb * ng * a.N >= 16 * slots;
+}
+
 cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *yout,
                                   cudaStream_t st) {
     return launch_stream(a, y, yout, st);

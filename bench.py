@@ -491,7 +491,7 @@ def run_workload(args):
             ctx.set_llg_kernel(kern)
             ctx.step(2)
             llg_ms[kern] = timed(torch, lambda: ctx.step(1), 10)
-        ctx.set_llg_kernel("fused")
+        ctx.set_llg_kernel("auto")
         vals, ms = {}, {}
         for mode, reps in (("bf16x3", 5), ("tf32x3", 3), ("fp64", 1)):
             ctx.sqt_async(mode, d.data_ptr())
@@ -676,9 +676,9 @@ def main():
     ap.add_argument("--mode", choices=["tf32x3", "bf16x3", "fp64", "fp64_fused"], default="tf32x3")
     ap.add_argument("--batch-cluster", type=int, default=0,
                     help="batch48: clusters of this many CTAs instead of the autotuner's choice")
-    ap.add_argument("--llg-kernel", choices=["fused", "stages"], default="fused",
-                    help="RK4 step of the headline: one streamed launch (default) or four "
-                         "stage kernels")
+    ap.add_argument("--llg-kernel", choices=["auto", "fused", "stages"], default="auto",
+                    help="RK4 step of the headline: one streamed launch where it fills the GPU "
+                         "(auto, default), always (fused) or four stage kernels (stages)")
     ap.add_argument("--chunk-k", type=int, default=-1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",

@@ -203,11 +203,15 @@ int asd_ctx_shard_sqt_finish(asd_ctx *ctx, const double *d_part, const double *d
 #define ASD_LLG_STAGES 0     /* four launches, one fused kernel per RK4 stage,
                                 HBM-bound (384 B of DRAM traffic per
                                 site-step; about 75% of HBM bandwidth on B200) */
-#define ASD_LLG_FUSED_STEP 1 /* default: one launch per step, the four stages
+#define ASD_LLG_FUSED_STEP 1 /* one launch per step, the four stages
                                 streamed down the lattice through shared
                                 memory by column band (48 B of DRAM traffic per
                                 site-step; FP64-bound; 1.35x the stages at
                                 128x128x500, 1.6x at 256x256x1000 on B200)  */
+#define ASD_LLG_AUTO 2       /* default: the one-launch step when the lattice
+                                and replicas give it at least 16 rows of work
+                                per resident CTA (e.g. 128x128x500), else the
+                                stage kernels (e.g. 64x64x100)               */
 int asd_ctx_set_llg_kernel(asd_ctx *ctx, int kernel);
 
 /* K elements accumulated per TMEM chunk by the split S(q,t) modes (rounded

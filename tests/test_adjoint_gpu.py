@@ -100,6 +100,26 @@ def test_checkpoint_interval_does_not_change_the_gradient():
             assert np.array_equal(got[1], ref[1])
 
 
+def test_llg_kernel_does_not_change_the_gradient():
+    """The forward pass and the segment recomputation step with the one-launch
+    kernel or the stage kernels (asd_ctx_set_llg_kernel; the default picks by
+    size): the same states bit for bit, so the same loss, gradient and S(q,t)."""
+    N, nf, nsteps, stride = 20, 12, 24, 4
+    s0 = asd.random_spins(N, nf, seed=6)
+    p = asd.Params.make(N, nf, J1=1.0, J2=-0.2, alpha=0.1, h=(0.0, 0.1, 0.2), dt=0.02)
+    target = np.linspace(0.2, 0.6, nsteps // stride) - 0.1j
+    with asd.Context(p, modes=["fp64"]) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        got = {}
+        for kern in ("fused", "stages", "auto"):
+            ctx.set_llg_kernel(kern)
+            got[kern] = ctx.loss_grad(nsteps, stride, 5, target)
+        for kern in ("stages", "auto"):
+            assert got[kern][0] == got["fused"][0]
+            assert np.array_equal(got[kern][1], got["fused"][1])
+            assert np.array_equal(got[kern][2], got["fused"][2])
+
+
 def test_differentiation_configuration_finite_differences():
     N, nf, nsteps, stride, ck, dt = 64, 100, 1000, 10, 50, 0.01
     s0 = asd.random_spins(N, nf, seed=0)

@@ -36,7 +36,7 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("kernel", ["fused", "stages"])
+@pytest.mark.parametrize("kernel", ["fused", "stages", "auto"])
 @pytest.mark.parametrize("N,nfile,kw", CASES)
 def test_ctx_steps_bit_exact(oracle, N, nfile, kw, kernel):
     s0 = asd.random_spins(N, nfile, seed=N + nfile, spin_len=kw.get("spin_len", 1.0))
