@@ -61,7 +61,7 @@ cudaError_t launch_llg_stage(int stage, const LLGArgs &a, const double *y, const
 cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *yout,
                                   cudaStream_t st);
 // True if the streamed one-launch step has enough work for this lattice and
-// replica range to fill the GPU (at least 16 rows per resident CTA).
+// replica range to fill the GPU (at least 8 rows per resident CTA).
 bool llg_fused_fills(const LLGArgs &a);
 
 // Counts the x[i] for which the constant divisions by 3 and 6 of the LLG

@@ -527,7 +527,7 @@ bool llg_fused_fills(const LLGArgs &a) {
     }
     const long nb = (a.N + WC_MAX - 1) / WC_MAX, ng = (a.nc + SF - 1) / SF;
     const long slots = 2L * sms;  // two CTAs of the streamed step per SM
-    return nb * ng * a.N >= 16 * slots;
+    return nb * ng * a.N >= 8 * slots;
 }
 
 cudaError_t launch_llg_step_fused(const LLGArgs &a, const double *y, double *yout,

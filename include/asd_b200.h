@@ -209,9 +209,10 @@ int asd_ctx_shard_sqt_finish(asd_ctx *ctx, const double *d_part, const double *d
                                 site-step; FP64-bound; 1.35x the stages at
                                 128x128x500, 1.6x at 256x256x1000 on B200)  */
 #define ASD_LLG_AUTO 2       /* default: the one-launch step when the lattice
-                                and replicas give it at least 16 rows of work
-                                per resident CTA (e.g. 128x128x500), else the
-                                stage kernels (e.g. 64x64x100)               */
+                                and replicas give it at least 8 rows of work
+                                per resident CTA (e.g. 128x128x500, or its
+                                64-replica chunks), else the stage kernels
+                                (e.g. 64x64x100)                             */
 int asd_ctx_set_llg_kernel(asd_ctx *ctx, int kernel);
 
 /* K elements accumulated per TMEM chunk by the split S(q,t) modes (rounded
