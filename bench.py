@@ -218,7 +218,41 @@ def cpu_reference_sample(N, nfile, J1, dt, spins, target_s=2.0, llg=True):
     return dict(t_llg=t_llg, t_sqt=t_sqt, threads=threads, sample=sample, rows=rows)
 
 
+def cpu_reference_openblas(N, nfile, J1, dt, spins):
+    """Times the reference's gemm program (gemm/llg_sqt_mkl.c, compiled from its
+    sources into oracle/_ref/libref_gemm.so against the image's OpenBLAS) on the
+    host cores: runge_kutta + renormalisation on the whole lattice and its
+    S(q,t) -- cblas_dgemm of the whole (N^2 x N^2) correlation matrix, then the
+    outer-product subtraction and the phase reduction (gemm/llg_sqt_mkl.c:
+    369-423) -- on the full workload.  Returns a cpu_baseline-style dict."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+
+    if not orc.RefLib.available("gemm"):
+        return None
+    r = orc.RefLib("gemm")
+    threads = r.setup(N, nfile, J1=J1, dt=dt, threads=0)
+    M = N * N
+    s = r.steps(spins, 1, 1.0)  # warm
+    t0 = time.perf_counter()
+    s = r.steps(s, 1, 1.0)
+    t_llg = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    r.gemm_sqt(s, spins)
+    t_sqt = time.perf_counter() - t0
+    return {"value": M * nfile / (t_llg + t_sqt), "unit": "site-steps/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"reference gemm program (OpenBLAS cblas_dgemm): runge_kutta+renorm and "
+                      f"S(q,t) on all {M}x{nfile} site-replicas, one step, {threads} OpenMP threads",
+            "llg_site_steps_per_s": M * nfile / t_llg,
+            "sqt_tflops": 2.0 * M * M * 3 * nfile / t_sqt / 1e12}
+
+
 def run_reference(args):
+    """The reference's CPU implementations of the path on the host cores: its
+    fused-AVX2 program (fused_dgemm, sampled on a band of rows each step) and
+    its OpenBLAS program (full workload, up to 3 samples).  `value` is the
+    faster of the two, so the comparison is against the reference's best."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
@@ -238,20 +272,28 @@ def run_reference(args):
         if it >= args.warmup:
             vals.append(info["t_llg"] + info["t_sqt"])
     t = statistics.median(vals)
-    value = N * N * nf / t
+    fused = {"value": N * N * nf / t, "unit": "site-steps/s", "cores": info["threads"],
+             "kind": "reference", "sample": info["sample"],
+             "llg_site_steps_per_s": N * N * nf / info["t_llg"],
+             "sqt_tflops": 2.0 * (N * N) ** 2 * 3 * nf / info["t_sqt"] / 1e12}
+    ob = [cpu_reference_openblas(N, nf, CONFIG["J1"], CONFIG["dt"], spins)
+          for _ in range(min(max(args.steps, 1), 3))]
+    openblas = None
+    if ob[0] is not None:
+        openblas = sorted(ob, key=lambda d: d["value"])[len(ob) // 2]
+    best = fused if openblas is None or fused["value"] >= openblas["value"] else openblas
+    value = best["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "site-steps/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": N * N * nf / value * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded spins uniform on the sphere",
         "config": {"workload": WORKLOAD, "sites": N * N, "replicas": nf, "gemm_m": N * N,
                    "gemm_k": 3 * nf},
-        "cpu_baseline": {"value": value, "unit": "site-steps/s", "cores": info["threads"],
-                         "kind": "reference", "sample": info["sample"]},
+        "cpu_baseline": {k: best[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": value, "unit": "site-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "llg_site_steps_per_s": N * N * nf / info["t_llg"],
-        "sqt_tflops": 2.0 * (N * N) ** 2 * 3 * nf / info["t_sqt"] / 1e12,
+        "paths": {"fused_avx2": fused, "openblas": openblas},
     }
     print(json.dumps(line))
     return 0
@@ -356,11 +398,20 @@ def run_ours(args):
     }
     line.update(extra["report"])
     if world == 1 and not args.no_cpu_baseline and not args.no_extras:
+        # the reference's two CPU programs; cpu_baseline is the faster one
         info = cpu_reference_sample(N, nf, CONFIG["J1"], CONFIG["dt"], spins0, target_s=1.5)
+        paths = {}
         if info is not None:
             v = M * nf / (info["t_llg"] + info["t_sqt"])
-            line["cpu_baseline"] = {"value": v, "unit": "site-steps/s", "cores": info["threads"],
-                                    "kind": "reference", "sample": info["sample"]}
+            paths["fused_avx2"] = {"value": v, "unit": "site-steps/s", "cores": info["threads"],
+                                   "kind": "reference", "sample": info["sample"]}
+        ob = cpu_reference_openblas(N, nf, CONFIG["J1"], CONFIG["dt"], spins0)
+        if ob is not None:
+            paths["openblas"] = ob
+        if paths:
+            best = max(paths.values(), key=lambda d: d["value"])
+            line["cpu_baseline"] = {k: best[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            line["cpu_baseline_paths"] = paths
     print(json.dumps(line))
     ctx.close()
     if world > 1:
