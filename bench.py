@@ -513,6 +513,8 @@ def timed(torch, fn, reps):
 
 def run_workload(args):
     """Secondary workloads, one JSON line each (not the headline):
+    grid32   32x32 lattice, 200 replicas, 2000 steps, FP64, S(q,t) on the whole q
+             grid after every step
     sqt256   256x256 lattice, 1000 replicas, J=1, J2=-0.3, alpha=0.02, dt=0.005:
              one RK4 step + S(q,t) in BF16x3, with the FP64 path's time and error
     adjoint64  64x64 lattice, 100 replicas, 1000 steps, S(q,t) every 10 steps,
@@ -564,6 +566,37 @@ def run_workload(args):
                          "achieved": flops / ms["bf16x3"] / 1e9, "peak": bf16, "unit": "TFLOP/s",
                          "frac": flops / ms["bf16x3"] / 1e9 / bf16, "traffic": None,
                          **split_ceiling("bf16x3", flops / ms["bf16x3"] / 1e9 / bf16)},
+        })
+        ctx.close()
+    elif args.workload == "grid32":
+        # 32x32 lattice, 200 replicas, J=1, alpha=0.1, dt=0.01, 2000 RK4 steps, S(q,t) on the
+        # whole 32x32 q grid after every step (FP64 GEMM + displacement bins + 2-D DFT)
+        N, nf, nsteps = 32, 200, 2000
+        M = N * N
+        ctx = asd.Context(asd.Params.make(N, nf, J1=1.0, alpha=0.1, dt=0.01), modes=["fp64"])
+        stream = torch.cuda.current_stream()
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_spins(asd.random_spins(N, nf, seed=0), as_origin=True)
+        grid = torch.zeros(2 * M * nsteps, dtype=torch.float64, device="cuda")
+
+        def run(n):
+            for i in range(n):
+                ctx.step(1)
+                ctx.sqt_grid_async("fp64", grid.data_ptr() + 16 * M * i)
+
+        run(5)
+        ms = timed(torch, lambda: run(nsteps), 1) / nsteps
+        step_ms = timed(torch, lambda: ctx.step(1), 200)
+        out.update({
+            "metric": "RK4 steps with the full-q-grid S(q,t) per second (FP64)",
+            "value": 1e3 / ms, "unit": "steps/s", "higher_is_better": True,
+            "ms_per_step": ms, "dtype": "f64", "site_steps_per_s": M * nf / (ms / 1e3),
+            "config": {"workload": "32x32 lattice, 200 replicas, J=1, alpha=0.1, dt=0.01, "
+                                   "2000 steps, S(q,t) on the 32x32 q grid every step",
+                       "sites": M, "replicas": nf},
+            "llg_ms_per_step": step_ms,
+            "sqt_grid_ms": ms - step_ms,
+            "l2": "the whole state (4.9 MB) is L2-resident: not an HBM measurement",
         })
         ctx.close()
     elif args.workload == "adjoint64":
@@ -736,7 +769,7 @@ def main():
                     help="only the timed steps (for profiling): no per-component timings, e2e "
                          "or CPU baseline after the timed region")
     ap.add_argument("--ref-target-s", type=float, default=2.0)
-    ap.add_argument("--workload", choices=["headline", "sqt256", "adjoint64", "batch48"],
+    ap.add_argument("--workload", choices=["headline", "grid32", "sqt256", "adjoint64", "batch48"],
                     default="headline", help="secondary workloads print their own line")
     ap.add_argument("--shard", action="store_true",
                     help="strong scaling: split the one headline ensemble by replicas over the "
