@@ -17,12 +17,14 @@
  *     these functions itself.
  *
  *  2. A context API (asd_ctx_*) that keeps the replicas' spins resident in
- *     HBM and runs a whole step on one CUDA stream: four fused RK4 stage
- *     kernels (the last one renormalises), then S(q,t) through a tcgen05
- *     tensor-core GEMM in split precision (TF32x3 or BF16x3) whose epilogue
- *     applies the phase, the connected-part subtraction and the reduction,
- *     or through the FP64 path.  It replaces the per-step body of main()
- *     (llg_sqt_baseline.c:289-426, llg_sqt_fusion.c:340-449).
+ *     HBM and runs a whole step on one CUDA stream: the RK4 step with its
+ *     renormalisation (one launch, or one kernel per stage), then S(q,t)
+ *     through a tcgen05 tensor-core GEMM in split precision (TF32x3 or
+ *     BF16x3) whose epilogue applies the phase, the connected-part
+ *     subtraction and the reduction, or through the FP64 path.  It replaces
+ *     the per-step body of main() (llg_sqt_baseline.c:289-426,
+ *     llg_sqt_fusion.c:340-449); host-buffer forms keep the reference's data
+ *     flow (spins in host memory between steps).
  *
  * Spin arrays crossing the ABI use the reference's layout, "AoS":
  * double[nfile][N*N][3] (llg_sqt_baseline.c:185, :202), site index
@@ -46,7 +48,8 @@ extern "C" {
 #define ASD_ERR_NOMEM (-3)       /* device or host allocation failed         */
 #define ASD_ERR_TIMEOUT (-4)     /* a bounded device-side wait gave up       */
 #define ASD_ERR_STATE (-5)       /* call order (e.g. no spins set yet)       */
-#define ASD_ERR_UNSUPPORTED (-6) /* the device is not sm_100                 */
+#define ASD_ERR_UNSUPPORTED (-6) /* the device is not sm_100, or a size is
+                                    beyond a kernel's stated limits          */
 
 /* Arithmetic of the S(q,t) correlation GEMM. */
 typedef enum {
@@ -298,9 +301,10 @@ int asd_sqt_split_noalloc(int kind, long rows, int Kp, const void *a_hi, const v
 /* ------------------------------------------------------ batched lattices */
 /* Many independent lattices (one replica each) of different sizes and
  * parameters, stepped together by one persistent, graph-captured launch with
- * all spins resident on the GPU (in shared memory, or in L2 and HBM).  RK4 stages in FP32 (explicitly rounded, the
- * reference's operation order), renormalisation in FP64.  No counterpart in
- * the reference, which runs one lattice per program. */
+ * all spins resident on the GPU (in shared memory, or in L2 and HBM).  RK4
+ * stages in FP32 (explicitly rounded, the reference's operation order),
+ * renormalisation in FP64.  No counterpart in the reference, which runs one
+ * lattice per program. */
 typedef struct {
     int N;
     double J1, J2, alpha, hx, hy, hz, dt, spin_len;
