@@ -917,8 +917,8 @@ int step_host_async(asd_ctx *c, const double *spin_in, double *spin_out, int mod
         const size_t off = (size_t)f0 * M * 3, bytes = (size_t)nc * M * 3 * sizeof(double);
         ASD_CUDA_TRY(cudaStreamWaitEvent(up, c->ast_out_done[r], 0));
         ASD_CUDA_TRY(cudaStreamWaitEvent(up, c->ast_in_done[r], 0));
-        ASD_CUDA_TRY(cudaMemcpyAsync(c->ast_in + off, spin_in + off, bytes,
-                                     cudaMemcpyHostToDevice, up));
+        ASD_CUDA_TRY(cudaMemcpyAsync(c->ast_in + off, spin_in + off, bytes, cudaMemcpyDefault,
+                                     up));  // pinned host or device memory
         ASD_CUDA_TRY(cudaEventRecord(c->ast_in_ready[r], up));
         ASD_CUDA_TRY(cudaStreamWaitEvent(comp, c->ast_in_ready[r], 0));
         ASD_CUDA_TRY(launch_aos_to_sitemajor_range(c->ast_in + off, c->y, M, nf, f0, nc, comp));
@@ -937,8 +937,8 @@ int step_host_async(asd_ctx *c, const double *spin_in, double *spin_out, int mod
         ASD_CUDA_TRY(launch_sitemajor_to_aos_range(ynew, c->ast_out + off, M, nf, f0, nc, comp));
         ASD_CUDA_TRY(cudaEventRecord(c->ast_out_ready[r], comp));
         ASD_CUDA_TRY(cudaStreamWaitEvent(down, c->ast_out_ready[r], 0));
-        ASD_CUDA_TRY(cudaMemcpyAsync(spin_out + off, c->ast_out + off, bytes,
-                                     cudaMemcpyDeviceToHost, down));
+        ASD_CUDA_TRY(cudaMemcpyAsync(spin_out + off, c->ast_out + off, bytes, cudaMemcpyDefault,
+                                     down));
         ASD_CUDA_TRY(cudaEventRecord(c->ast_out_done[r], down));
         c->last_launches += fused ? 3 : 6;
     }

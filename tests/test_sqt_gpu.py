@@ -178,16 +178,18 @@ def test_step_pipelined_behind_the_split_gemm(oracle, mode, kernel):
     assert np.array_equal(spins[0], want)
 
 
-@pytest.mark.parametrize("kernel", ["fused", "stages"])
+@pytest.mark.parametrize("kernel,where", [("fused", "pinned"), ("stages", "pinned"),
+                                          ("fused", "device")])
 @pytest.mark.parametrize("nf", [200, 40, 7])
-def test_step_host_async_consecutive_steps(oracle, nf, kernel):
+def test_step_host_async_consecutive_steps(oracle, nf, kernel, where):
     """asd_ctx_step_host_async: five steps enqueued back to back on one pinned
     buffer (each call's output is the next call's input, so every chunk's
     upload must wait for the previous call's download of that chunk), then
     one asd_ctx_synchronize.  200 replicas make chunks of 32 (six) and 8; 40
     make 32 + 8; 7 one chunk.  The spins equal the device path and the oracle
     bit for bit; each step's S(q,t) equals the device path's asd_ctx_sqt on
-    the same state exactly (the same kernels in the same order)."""
+    the same state exactly (the same kernels in the same order).  The
+    buffers may also be device memory."""
     import torch
 
     N = 16
@@ -199,11 +201,17 @@ def test_step_host_async_consecutive_steps(oracle, nf, kernel):
         a.set_llg_kernel(kernel)
         a.set_spins(s0, as_origin=True)
         b.set_spins(s0, as_origin=True)
-        buf = torch.from_numpy(s0.reshape(-1).copy()).pin_memory()
-        sq = torch.zeros(2 * len(modes), dtype=torch.float64).pin_memory()
+        buf = torch.from_numpy(s0.reshape(-1).copy())
+        sq = torch.zeros(2 * len(modes), dtype=torch.float64)
+        if where == "pinned":
+            buf, sq = buf.pin_memory(), sq.pin_memory()
+        else:
+            buf, sq = buf.cuda(), sq.cuda()
         for i, mode in enumerate(modes):
             a.step_host_async(buf.data_ptr(), buf.data_ptr(), mode, sq.data_ptr() + 16 * i)
         a.synchronize()
+        if where == "device":
+            buf, sq = buf.cpu(), sq.cpu()
         want = s0
         for i, mode in enumerate(modes):
             b.step(1)
@@ -212,6 +220,7 @@ def test_step_host_async_consecutive_steps(oracle, nf, kernel):
         assert np.array_equal(buf.numpy().reshape(s0.shape), b.get_spins())
         assert np.array_equal(b.get_spins(), want)
         # the context keeps working synchronously afterwards
+        buf = buf.pin_memory()
         got = a.step_host(buf.data_ptr(), buf.data_ptr(), "fp64")
         b.step(1)
         assert got == b.sqt("fp64")
