@@ -489,11 +489,27 @@ def e2e_measurement(ctx, asd, torch, spins0, mode, M, nf, args, world):
         ctx.step_host_async(h_out.data_ptr(), h_out.data_ptr(), mode, h_sqt.data_ptr() + 16 * i)
     ctx.synchronize()
     ms = (time.perf_counter() - t0) / steps * 1e3
+    # the floor: the same bytes up and down at once on two streams, no compute
+    d_a = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_b = torch.empty(n, dtype=torch.float64, device="cuda")
+    s_up, s_down = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        with torch.cuda.stream(s_up):
+            d_a.copy_(h_in, non_blocking=True)
+        with torch.cuda.stream(s_down):
+            h_out.copy_(d_b, non_blocking=True)
+    torch.cuda.synchronize()
+    copy_ms = (time.perf_counter() - t0) / 3 * 1e3
+    del d_a, d_b
     ms, value = aggregate(ms, M * nf, world, dist if world > 1 else None, "cuda")
     ms_sync, value_sync = aggregate(ms_sync, M * nf, world, dist if world > 1 else None, "cuda")
     return {"value": value, "unit": "site-steps/s", "h2d_bytes_per_step": n * 8,
             "d2h_bytes_per_step": n * 8 + 16, "ms_per_step": ms, "steps": steps,
             "api": "asd_ctx_step_host_async x steps + asd_ctx_synchronize (pinned host buffers)",
+            "copy_bound_ms_per_step": copy_ms, "frac_of_copy_bound": copy_ms / ms,
+            "copy_bound": "the step's bytes up and down at once on two streams, no compute",
             "sync": {"value": value_sync, "ms_per_step": ms_sync,
                      "api": "asd_ctx_step_host (pinned host buffers)"}}
 
