@@ -1,0 +1,94 @@
+"""The configurations at their full sizes: the 128 x 128 lattice with 500
+replicas (J = -1, h = (0, 0, 0.5), alpha = 0.05, dt = 0.005; S(q,t) in TF32x3
+and FP64) and the 256 x 256 lattice with 1000 replicas (J = 1, J2 = -0.3,
+alpha = 0.02, dt = 0.005; S(q,t) in BF16x3 and FP64).
+
+* One RK4 step against the oracle, bit for bit, through every way of
+  stepping: the one-launch kernel, the stage kernels, the default choice, and
+  the host-buffer steps (synchronous and pipelined).
+* Properties that hold at any size: the step commutes with a translation of
+  the periodic lattice and with a permutation of the replicas, bit for bit,
+  and the renormalised spins have the set length.
+* S(q,t): the FP64 GEMM path against the oracle's factorised form (1e-12),
+  the split modes within 1e-5 of the FP64 path.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import asd_b200 as asd
+import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = {
+    "128x128x500": (128, 500, dict(J1=-1.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005),
+                    ["fp64", "tf32x3", "bf16x3"]),
+    "256x256x1000": (256, 1000, dict(J1=1.0, J2=-0.3, alpha=0.02, dt=0.005),
+                     ["fp64", "bf16x3", "tf32x3"]),
+}
+
+
+def roll(s, N, dr, dc):
+    """Periodic translation of every replica's lattice by (dr, dc)."""
+    nf = s.shape[0]
+    return np.ascontiguousarray(np.roll(s.reshape(nf, N, N, 3), (dr, dc), axis=(1, 2))
+                                .reshape(nf, N * N, 3))
+
+
+@pytest.fixture(scope="module", params=list(CONFIGS))
+def case(request, oracle):
+    N, nf, kw, modes = CONFIGS[request.param]
+    s0 = asd.random_spins(N, nf, seed=3)
+    want = oracle.steps(orc.make_params(N, nf, **kw), s0, 1)
+    return N, nf, kw, modes, s0, want
+
+
+def test_one_step_bit_exact_every_way(case):
+    import torch
+
+    N, nf, kw, modes, s0, want = case
+    p = asd.Params.make(N, nf, **kw)
+    with asd.Context(p, modes=["fp64"]) as ctx:
+        for kern in ("fused", "stages", "auto"):
+            ctx.set_llg_kernel(kern)
+            ctx.set_spins(s0, as_origin=True)
+            ctx.step(1)
+            assert np.array_equal(ctx.get_spins(), want), kern
+        ctx.set_llg_kernel("auto")
+        buf = torch.from_numpy(s0.reshape(-1).copy()).pin_memory()
+        ctx.step_host(buf.data_ptr(), buf.data_ptr(), "fp64")
+        assert np.array_equal(buf.numpy().reshape(s0.shape), want), "step_host"
+        buf.copy_(torch.from_numpy(s0.reshape(-1)))
+        sq = torch.zeros(2, dtype=torch.float64).pin_memory()
+        ctx.step_host_async(buf.data_ptr(), buf.data_ptr(), "fp64", sq.data_ptr())
+        ctx.synchronize()
+        assert np.array_equal(buf.numpy().reshape(s0.shape), want), "step_host_async"
+    lens = np.linalg.norm(want, axis=-1)
+    assert np.abs(lens - 1.0).max() < 1e-15
+
+
+def test_step_commutes_with_translation_and_replica_permutation(case):
+    N, nf, kw, modes, s0, want = case
+    perm = np.random.default_rng(1).permutation(nf)
+    with asd.Context(asd.Params.make(N, nf, **kw), modes=["fp64"]) as ctx:
+        ctx.set_spins(roll(s0, N, 5, -17), as_origin=True)
+        ctx.step(1)
+        assert np.array_equal(ctx.get_spins(), roll(want, N, 5, -17))
+        ctx.set_spins(np.ascontiguousarray(s0[perm]), as_origin=True)
+        ctx.step(1)
+        assert np.array_equal(ctx.get_spins(), want[perm])
+
+
+def test_sqt_fp64_against_oracle_and_split_modes_within_tolerance(case, oracle):
+    N, nf, kw, modes, s0, want = case
+    ref = oracle.sqt_factorized(N, nf, N // 10, N // 10, want, s0)
+    with asd.Context(asd.Params.make(N, nf, **kw), modes=modes) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        ctx.step(1)
+        got = {m: ctx.sqt(m) for m in modes}
+    assert abs(got["fp64"] - ref) <= 1e-12 * abs(ref)
+    for m in modes:
+        if m != "fp64":
+            assert abs(got[m] - got["fp64"]) <= 1e-5 * abs(got["fp64"]), m
