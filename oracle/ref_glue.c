@@ -1,7 +1,7 @@
 /*
  * ref_glue.c -- a harness around the reference's OWN compiled functions.
  *
- * TEST INFRASTRUCTURE ONLY.  oracle/build_ref.sh compiles this file together
+ * TEST INFRASTRUCTURE ONLY.  `make -C oracle ref` compiles this file together
  * with one of the reference's programs, taken unmodified from where it lies
  * (main renamed by -Dmain=asd_ref_main), into oracle/_ref/libref_<variant>.so.
  * The reference keeps its state in globals defined by that program
