@@ -14,7 +14,9 @@
  *        runge_kutta      <- baseline/llg_sqt_baseline.c:95
  *        fused_dgemm      <- kernel_fusion/gemm_kernel.h:355
  *     A C program of the reference links libasd_b200.so instead of defining
- *     these functions itself.
+ *     these functions itself (deleting their bodies and including this
+ *     header; the program's globals N, Nfile, J1, dt are read through weak
+ *     references).
  *
  *  2. A context API (asd_ctx_*) that keeps the replicas' spins resident in
  *     HBM and runs a whole step on one CUDA stream: the RK4 step with its
