@@ -55,7 +55,8 @@ EXPORTED_SYMBOLS = (
     "asd_check_bounded_wait", "asd_check_const_division", "asd_check_const_division_f32", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
     "asd_spins_save", "asd_spins_load", "asd_batch_create", "asd_batch_destroy",
     "asd_batch_set_stream", "asd_batch_set_spins", "asd_batch_get_spins", "asd_batch_run",
-    "asd_batch_configure", "asd_batch_configure_cluster", "asd_batch_autotune", "asd_set_params", "euler", "runge_kutta",
+    "asd_batch_configure", "asd_batch_configure_cluster", "asd_batch_autotune",
+    "asd_batch_plan_clusters", "asd_set_params", "euler", "runge_kutta",
     "fused_dgemm",
 )
 
@@ -161,6 +162,8 @@ def load() -> C.CDLL:
         "asd_batch_run": ([vp, C.c_int], C.c_int),
         "asd_batch_configure": ([vp, C.c_int, C.c_int], C.c_int),
         "asd_batch_configure_cluster": ([vp, C.c_int, C.c_int], C.c_int),
+        "asd_batch_plan_clusters": ([vp, C.c_int, C.c_int, C.c_int, C.c_long, vp, vp, C.c_int, vp,
+                                     vp], C.c_int),
         "asd_batch_autotune": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                 C.POINTER(C.c_double)], C.c_int),
         "asd_spins_save": ([C.c_char_p, C.c_int, C.c_int, C.c_long, C.c_double, vp], C.c_int),
@@ -519,6 +522,22 @@ class Batch:
         _check(load().asd_batch_autotune(self._h, int(trial_steps), C.byref(t), C.byref(c),
                                          C.byref(ms)))
         return t.value, c.value, ms.value
+
+
+def batch_plan_clusters(sizes, cluster_size: int, clusters: int, smem_limit: int = 232448):
+    """asd_batch_plan_clusters (host only): (ctas [n][4], segs [m][12], smem
+    bytes, fits) -- see the header for the columns."""
+    sz = np.ascontiguousarray(sizes, dtype=np.int32)
+    ctas = np.zeros((clusters * cluster_size, 4), dtype=np.int32)
+    cap = int(sum(int(n) for n in sizes) + clusters * cluster_size)
+    segs = np.zeros((cap, 12), dtype=np.int32)
+    nsegs, smem = C.c_int(), C.c_long()
+    rc = load().asd_batch_plan_clusters(_ptr(sz), len(sz), int(cluster_size), int(clusters),
+                                        int(smem_limit), _ptr(ctas), _ptr(segs), cap,
+                                        C.byref(nsegs), C.byref(smem))
+    if rc not in (ASD_OK, ASD_ERR_UNSUPPORTED):
+        _check(rc)
+    return ctas, segs[: nsegs.value], smem.value, rc == ASD_OK
 
 
 def noisy_ordered_spins(N: int, eta: float, seed: int) -> np.ndarray:

@@ -941,6 +941,41 @@ int asd_batch_autotune(asd_batch *b, int trial_steps, int *tile, int *ctas_per_s
 
 }  // extern "C"
 
+extern "C" int asd_batch_plan_clusters(const int *sizes, int count, int cluster_size,
+                                       int clusters, long smem_limit, int *ctas_out,
+                                       int *segs_out, int seg_capacity, int *nsegs,
+                                       long *smem_bytes) {
+    using namespace asd;
+    if (!sizes || count < 1 || cluster_size < 1 || cluster_size > 8 || clusters < 1 ||
+        smem_limit < 0 || !ctas_out || !nsegs || !smem_bytes || seg_capacity < 0)
+        return fail(ASD_ERR_INVALID, "bad argument");
+    std::vector<BatchLattice> lat((size_t)count);
+    for (int l = 0; l < count; ++l) {
+        if (sizes[l] < 1) return fail(ASD_ERR_INVALID, "lattice %d: N=%d", l, sizes[l]);
+        lat[l] = BatchLattice{};
+        lat[l].N = sizes[l];
+    }
+    ClusterPlan pl;
+    const bool fits = plan_clusters(lat, cluster_size, clusters, 0, (size_t)smem_limit, pl);
+    *nsegs = (int)pl.segs.size();
+    *smem_bytes = (long)(cluster_smem_floats(pl.max_buf, pl.max_sites) * sizeof(float));
+    for (size_t i = 0; i < pl.ctas.size(); ++i) {
+        const CCta &c = pl.ctas[i];
+        const int v[4] = {c.seg0, c.nseg, c.nsites, c.buf};
+        for (int k = 0; k < 4; ++k) ctas_out[4 * i + k] = v[k];
+    }
+    if (segs_out && (int)pl.segs.size() <= seg_capacity) {
+        for (size_t i = 0; i < pl.segs.size(); ++i) {
+            const CSeg &g = pl.segs[i];
+            const int v[12] = {g.lat, g.N, g.r0, g.rows, g.base, g.core0,
+                               g.top_rank, g.top_off, g.top_buf, g.bot_rank, g.bot_off, g.bot_buf};
+            for (int k = 0; k < 12; ++k) segs_out[12 * i + k] = v[k];
+        }
+    }
+    if (!fits) return fail(ASD_ERR_UNSUPPORTED, "the plan does not fit the limits");
+    return ASD_OK;
+}
+
 extern "C" int asd_check_const_division_f32(unsigned long long *bad, void *stream) {
     using namespace asd;
     if (!bad) return fail(ASD_ERR_INVALID, "bad is NULL");

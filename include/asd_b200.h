@@ -347,6 +347,19 @@ int asd_batch_configure_cluster(asd_batch *batch, int cluster_size, int threads)
  * afterwards. */
 int asd_batch_autotune(asd_batch *batch, int trial_steps, int *tile, int *ctas_per_sm,
                        double *ms_per_step);
+/* Diagnostic (host only, no GPU): the cluster-resident kernel's plan for
+ * lattices of the given sides on `clusters` clusters of `cluster_size` CTAs.
+ * ctas_out receives 4 ints per CTA (clusters * cluster_size CTAs, cluster by
+ * cluster): first segment, segments, sites, slots per plane; segs_out (if it
+ * holds seg_capacity segments) 12 ints per segment: lattice, N, first row,
+ * rows, slot of its top halo row, first site, and the top and the bottom halo
+ * rows' owning CTA (rank in the cluster), slot there and that CTA's slots per
+ * plane; *smem_bytes the dynamic shared memory a CTA needs.  ASD_ERR_UNSUPPORTED
+ * (with the outputs filled) if it exceeds smem_limit.  No counterpart in the
+ * reference; tests use it. */
+int asd_batch_plan_clusters(const int *sizes, int count, int cluster_size, int clusters,
+                            long smem_limit, int *ctas_out, int *segs_out, int seg_capacity,
+                            int *nsegs, long *smem_bytes);
 
 /* --------------------------------------------------------- spin-state I/O */
 /* The reference keeps spins only in memory; these define a file format for
