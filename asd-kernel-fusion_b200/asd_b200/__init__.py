@@ -51,7 +51,7 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_shard_set_origin_sums", "asd_ctx_shard_sqt_async", "asd_ctx_shard_sqt_finish",
     "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
     "asd_ctx_last_launches",
-    "asd_ctx_check_device_status",
+    "asd_ctx_check_device_status", "asd_debug_fail_alloc", "asd_ctx_debug_poison",
     "asd_check_bounded_wait", "asd_check_const_division", "asd_check_const_division_f32", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
     "asd_spins_save", "asd_spins_load", "asd_batch_create", "asd_batch_destroy",
     "asd_batch_set_stream", "asd_batch_set_spins", "asd_batch_get_spins", "asd_batch_run",
@@ -146,6 +146,8 @@ def load() -> C.CDLL:
         "asd_ctx_set_chunk_k": ([vp, C.c_int], C.c_int),
         "asd_ctx_last_launches": ([vp], C.c_int),
         "asd_ctx_check_device_status": ([vp], C.c_int),
+        "asd_debug_fail_alloc": ([C.c_long], C.c_int),
+        "asd_ctx_debug_poison": ([vp], C.c_int),
         "asd_check_bounded_wait": ([C.c_int, C.c_uint, vp], C.c_int),
         "asd_check_const_division": ([vp, C.c_long, vp, vp], C.c_int),
         "asd_check_const_division_f32": ([vp, vp], C.c_int),
@@ -355,7 +357,9 @@ class Context:
                                                C.c_void_p(_addr(d_out))))
 
     def set_llg_kernel(self, kernel) -> None:
-        """"stages" (four launches, the default) or "fused" (one launch per step)."""
+        """"auto" (the default: the one-launch step where the lattice fills the
+        GPU, else the stage kernels), "fused" (one launch per step) or
+        "stages" (four launches, one per RK4 stage)."""
         k = {"fused": LLG_FUSED_STEP, "stages": LLG_STAGES, "auto": LLG_AUTO}.get(kernel, kernel)
         _check(load().asd_ctx_set_llg_kernel(self._h, int(k)))
 
@@ -367,6 +371,17 @@ class Context:
 
     def check_device_status(self) -> None:
         _check(load().asd_ctx_check_device_status(self._h))
+
+    def debug_poison(self) -> None:
+        """asd_ctx_debug_poison: NaN into every buffer that does not carry
+        state between calls (tests of uninitialised reads)."""
+        _check(load().asd_ctx_debug_poison(self._h))
+
+
+def debug_fail_alloc(n: int) -> None:
+    """asd_debug_fail_alloc: the n-th device allocation of the context API
+    from now on fails with ASD_ERR_NOMEM (0 switches it off)."""
+    _check(load().asd_debug_fail_alloc(int(n)))
 
 
 # ------------------------------------------------------------ drop-in layer

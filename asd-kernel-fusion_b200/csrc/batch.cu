@@ -804,10 +804,15 @@ int asd_batch_create(const asd_lattice *lats, int count, asd_batch **out) {
         destroy(b);
         return fail(ASD_ERR_NOMEM, "cudaMalloc for the batch failed");
     }
-    cudaMemcpy(b->d_lat, b->lat.data(), count * sizeof(BatchLattice), cudaMemcpyHostToDevice);
-    cudaMemset(b->bs, 0, sizeof(BarrierState));
-    cudaMemset(b->status, 0, sizeof(unsigned));
-    cudaMemset(b->y, 0, bytes);
+    e = cudaMemcpy(b->d_lat, b->lat.data(), count * sizeof(BatchLattice),
+                   cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(b->bs, 0, sizeof(BarrierState));
+    if (e == cudaSuccess) e = cudaMemset(b->status, 0, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(b->y, 0, bytes);
+    if (e != cudaSuccess) {
+        destroy(b);
+        return cuda_fail(e, "batch set-up copies");
+    }
     if ((rc = configure(b, 128, 2)) != ASD_OK) {
         destroy(b);
         return rc;

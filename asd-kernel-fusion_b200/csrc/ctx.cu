@@ -11,6 +11,7 @@
 // The AoS <-> site-major transposes stage through ys_b.
 #include <cublas_v2.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -135,8 +136,25 @@ struct asd_ctx {
 
 namespace {
 
+// Host-side allocation-failure injection (asd_debug_fail_alloc): while
+// g_fail_in > 0, every device allocation of the context API counts it down,
+// and the one that takes it from 1 to 0 fails as cudaMalloc does on a full
+// device.  No GPU fault is involved.
+std::atomic<long> g_fail_in{0};
+
+bool injected_failure() {
+    long n = g_fail_in.load(std::memory_order_relaxed);
+    while (n > 0 && !g_fail_in.compare_exchange_weak(n, n - 1, std::memory_order_relaxed)) {
+    }
+    return n == 1;
+}
+
 template <class T>
 int dalloc(T **p, size_t bytes) {
+    if (injected_failure()) {
+        *p = nullptr;
+        return fail(ASD_ERR_NOMEM, "cudaMalloc(%zu bytes): injected failure", bytes);
+    }
     cudaError_t e = cudaMalloc((void **)p, bytes < 16 ? 16 : bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -598,10 +616,10 @@ int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
         return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t): mode %d not supported", mode);
     if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
     int rc;
-    if (!c->grid_g) {
-        if ((rc = dalloc(&c->grid_g, (size_t)M * sizeof(double))) != ASD_OK) return rc;
-        if ((rc = dalloc(&c->grid_t, (size_t)M * sizeof(double2))) != ASD_OK) return rc;
-    }
+    // each checked on its own: after a failed allocation of grid_t, grid_g
+    // is already there and the next call must still allocate grid_t
+    if (!c->grid_g && (rc = dalloc(&c->grid_g, (size_t)M * sizeof(double))) != ASD_OK) return rc;
+    if (!c->grid_t && (rc = dalloc(&c->grid_t, (size_t)M * sizeof(double2))) != ASD_OK) return rc;
     ASD_CUDA_TRY(launch_site_mean(c->y, c->M, c->p.nfile, c->uphase, c->mean_t, c->row4, c->row1,
                                   c->stream));
     c->rows_ready = true;
@@ -1451,6 +1469,59 @@ int asd_ctx_check_device_status(asd_ctx *c) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
     ASD_CUDA_TRY(enter(c));
     return read_status(c);
+}
+
+int asd_debug_fail_alloc(long n) {
+    if (n < 0) return fail(ASD_ERR_INVALID, "n=%ld is negative", n);
+    g_fail_in.store(n);
+    return ASD_OK;
+}
+
+// Every device buffer of the context whose contents do not carry over from
+// one call to the next: RK4 stage states and the running combination, the
+// replica means at t, the FP64 path's C band, the GEMM partials and result,
+// the q-grid bins and result, the host-step staging and the adjoint's
+// state-sized work buffers (checkpoints, recomputed states, adjoint
+// variables).  Kept as they are: the spins, the origin and its means, the
+// phases, the epilogue vectors and the split operands (their padding rows
+// and columns are zeroed once at creation and stay zero).
+int asd_ctx_debug_poison(asd_ctx *c) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    ASD_CUDA_TRY(enter(c));
+    const cudaStream_t streams[] = {c->stream, c->llg_stream, c->gemm_stream, c->copy_stream,
+                                    c->h2d_stream};
+    for (cudaStream_t s : streams)
+        if (s) ASD_CUDA_TRY(cudaStreamSynchronize(s));
+    const size_t sb = (size_t)c->M * c->K * sizeof(double);
+    const size_t chunk = (size_t)c->hp_replicas * c->M * 3 * sizeof(double);
+    struct Buf {
+        void *p;
+        size_t n;
+    };
+    std::vector<Buf> bufs = {
+        {c->ys_a, sb},
+        {c->ys_b, sb},
+        {c->acc, sb},
+        {c->mean_t, (size_t)c->M * 3 * sizeof(double)},
+        {c->band, (size_t)c->band_rows * c->M * sizeof(double)},
+        {c->part, (size_t)c->part_cap * sizeof(double2)},
+        {c->d_out, 2 * sizeof(double)},
+        {c->grid_g, (size_t)c->M * sizeof(double)},
+        {c->grid_t, (size_t)c->M * sizeof(double2)},
+        {c->grid_out, (size_t)c->M * 2 * sizeof(double)},
+        {c->ast_in, sb},
+        {c->ast_out, sb},
+    };
+    for (int b = 0; b < 2; ++b) {
+        bufs.push_back({c->stage_in[b], chunk});
+        bufs.push_back({c->stage_out[b], chunk});
+    }
+    for (long i = 0; i < c->adj_states && i < (long)c->adj_bufs.size(); ++i)
+        bufs.push_back({c->adj_bufs[i], sb});
+    for (const Buf &b : bufs)
+        if (b.p && b.n) ASD_CUDA_TRY(cudaMemsetAsync(b.p, 0xFF, b.n, c->stream));
+    ASD_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return ASD_OK;
 }
 
 }  // extern "C"

@@ -237,6 +237,25 @@ int asd_ctx_last_launches(const asd_ctx *ctx);
  * returns ASD_OK or ASD_ERR_TIMEOUT and clears it. */
 int asd_ctx_check_device_status(asd_ctx *ctx);
 
+/* Diagnostic, host-side fault injection: the n-th device allocation of the
+ * context API from now on (asd_ctx_create and the calls that allocate work
+ * space on first use: host-buffer steps, the q grid, the adjoint, the FP64
+ * partials) fails as cudaMalloc does on a full device, so the call returns
+ * ASD_ERR_NOMEM and frees what it had taken; n = 0 switches it off.  Process
+ * wide.  No counterpart in the reference (which never checks an allocation);
+ * the failure-path tests use it. */
+int asd_debug_fail_alloc(long n);
+
+/* Diagnostic: waits until the context is idle, then fills with NaN bytes
+ * (0xFF) every device buffer of the context whose contents do not carry over
+ * between calls (stage states, the running RK4 combination, replica means at
+ * t, the FP64 band, GEMM partials and result, q-grid bins, host-step staging,
+ * the adjoint's state-sized work buffers).  A kernel that read any of them
+ * before writing it would show NaN or changed results.  The spins, the
+ * origin, the phases, the epilogue vectors and the split operands are kept.
+ * No counterpart in the reference; the tests use it. */
+int asd_ctx_debug_poison(asd_ctx *ctx);
+
 /* Diagnostic: runs one of the library's bounded waits against a condition
  * that nothing satisfies -- which = 0: the mbarrier wait of the tensor-core
  * GEMM (`limit` polls); which = 1: the grid barrier of the batched kernel --

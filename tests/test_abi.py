@@ -59,6 +59,9 @@ def test_null_arguments_are_errors():
     assert lib.asd_ctx_step(None, 1) == asd.ASD_ERR_INVALID
     assert lib.asd_ctx_sqt(None, 0, None) == asd.ASD_ERR_INVALID
     assert lib.asd_set_params(0, 1, 1.0, 0.1) == asd.ASD_ERR_INVALID
+    assert lib.asd_ctx_debug_poison(None) == asd.ASD_ERR_INVALID
+    assert lib.asd_debug_fail_alloc(-1) == asd.ASD_ERR_INVALID
+    assert lib.asd_debug_fail_alloc(0) == asd.ASD_OK
 
 
 def test_no_cpu_fallback_without_gpu():
