@@ -128,8 +128,10 @@ int asd_ctx_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
  * bins every connected C_ij by the displacement r_i - r_j (mod N), followed by
  * a 2-D DFT of the N*N bins; d_out[2*(vx*N+vy)] equals asd_ctx_sqt's value.
  * Modes ASD_SQT_FP64, ASD_SQT_TF32X3 and ASD_SQT_BF16X3; lattices with
- * N*N <= 4096 (the bins live in shared memory).  The split modes sum in FP32
- * shared-memory atomics, so their last bits vary from run to run.
+ * N*N <= 4096 (the bins live in shared memory).  The bins are summed with
+ * shared-memory atomics (FP64 in the FP64 mode, FP32 in the split modes), so
+ * the last bits vary from run to run: about 1e-17 absolute in FP64, 1e-8
+ * relative in the split modes.
  * No counterpart in the reference (its programs evaluate one q). */
 int asd_ctx_sqt_grid_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
 /* Same into host memory (2*N*N doubles); synchronous. */

@@ -10,7 +10,8 @@
   carries nothing from one call to the next, before every call of a sequence
   that runs every kernel of the context API.  A kernel that read such a
   buffer before writing it would give NaN or other numbers; the results must
-  equal an unpoisoned context's bit for bit.
+  equal an unpoisoned context's bit for bit (S(q,t) on the q grid within the
+  run-to-run variation of its atomic bin sums).
 """
 from __future__ import annotations
 
@@ -74,11 +75,26 @@ def _calls(s0, target):
         return tuple(sq.tolist()), buf.numpy().copy()
 
     return {
-        "sqt_grid": lambda c: c.sqt_grid("fp64"),
+        "sqt_grid": lambda c: Grid(c.sqt_grid("fp64"), GRID_RTOL["fp64"]),
         "step_host": step_host,
         "step_host_async": step_host_async,
         "loss_grad": lambda c: c.loss_grad(8, 2, 3, target),
     }
+
+
+class Grid:
+    """S(q,t) on the q grid: its bins are summed with shared-memory atomics,
+    so repeated runs agree to rtol of the largest value, not bit for bit."""
+
+    def __init__(self, v, rtol):
+        self.v, self.rtol = v, rtol
+
+    def __eq__(self, other):
+        return bool(np.isfinite(self.v).all() and np.isfinite(other.v).all() and
+                    np.abs(self.v - other.v).max() <= self.rtol * np.abs(other.v).max())
+
+
+GRID_RTOL = {"fp64": 1e-12, "tf32x3": 1e-6, "bf16x3": 1e-6}
 
 
 def _same(x, y):
@@ -96,7 +112,8 @@ def test_failed_work_space_allocation_leaves_the_context_usable(call):
     With the 1st, 2nd, ... of those allocations failing, the call returns
     ASD_ERR_NOMEM each time, until it makes fewer allocations than the
     injection counts and succeeds; then, with the spins set again, it gives
-    what a context that never failed gives, bit for bit."""
+    what a context that never failed gives, bit for bit (the q grid within
+    the run-to-run variation of its atomic bin sums)."""
     import torch
 
     N, nf = 16, 72
@@ -157,7 +174,7 @@ def test_scratch_poisoning_changes_nothing(kernel):
             out.append(ctx.sqt(mode))
         for mode in ("fp64", "tf32x3", "bf16x3"):
             P()
-            out.append(ctx.sqt_grid(mode))
+            out.append(Grid(ctx.sqt_grid(mode), GRID_RTOL[mode]))
         P()
         cur = ctx.get_spins()
         buf = torch.from_numpy(cur.reshape(-1).copy()).pin_memory()
