@@ -36,7 +36,7 @@ constexpr int BN = 256;
 constexpr int NUM_THREADS = 192;
 constexpr int TMEM_COLS = 512;
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
-constexpr int GROUP_M = 16;
+constexpr int GROUP_M = 16;  // default tile rows per raster group (umma_group_m)
 constexpr int kGridMaxBins = 4096;  // q-grid histogram: N*N FP32 bins in shared memory
 
 // Pipeline geometry.  ROWB = bytes of K per operand row in one pipeline
@@ -77,11 +77,15 @@ constexpr int smem_bytes() {
            (int)((sizeof(SmemTail) + 15) & ~size_t(15));
 }
 
-__device__ __forceinline__ void tile_coords(int tile, int num_m, int num_n, int &mb, int &nb) {
-    const int per_group = GROUP_M * num_n;
+// Tile raster: groups of group_m row tiles, each walked over all column tiles
+// with the row index fastest, so the concurrent tiles share a few B bands and
+// the group's A bands stay in L2 while B streams past once per group.
+__device__ __forceinline__ void tile_coords(int tile, int num_m, int num_n, int group_m, int &mb,
+                                            int &nb) {
+    const int per_group = group_m * num_n;
     const int group = tile / per_group;
-    const int first_m = group * GROUP_M;
-    const int gsz = min(GROUP_M, num_m - first_m);
+    const int first_m = group * group_m;
+    const int gsz = min(group_m, num_m - first_m);
     const int r = tile - group * per_group;
     mb = first_m + r % gsz;
     nb = r / gsz;
@@ -125,7 +129,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     const float *__restrict__ row1, const float4 *__restrict__ col4,
                     const float *__restrict__ col1, float alpha, double2 *__restrict__ part,
                     unsigned *__restrict__ status, float *__restrict__ dbg_c, long dbg_ldc,
-                    int lat_n, long n_sites, double *__restrict__ gpart) {
+                    int lat_n, long n_sites, double *__restrict__ gpart, int group_m) {
     using G = Geo<ROWB, PAIR>;
     constexpr bool STORE = (EPI == EPI_STORE);
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -197,7 +201,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const uint32_t full0 = PAIR ? ptx::mapa(ptx::smem_u32(&tail->full[0]), 0u) : 0u;
             for (int tile = first_tile; tile < num_tiles && ok; tile += tile_step) {
                 int mb, nb;
-                tile_coords(tile, num_m, num_n, mb, nb);
+                tile_coords(tile, num_m, num_n, group_m, mb, nb);
                 const int arow = mb * G::TILE_M + (int)rank * BM;
                 const int brow = nb * BN + (int)rank * G::BN_LOC;
                 for (int kb = kb_begin; kb < kb_end; ++kb) {
@@ -366,7 +370,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         const uint32_t tempty0 = PAIR ? ptx::mapa(ptx::smem_u32(&tail->tempty[0]), 0u) : 0u;
         for (int tile = first_tile; tile < num_tiles; tile += tile_step, ++tcount) {
             int mb, nb;
-            tile_coords(tile, num_m, num_n, mb, nb);
+            tile_coords(tile, num_m, num_n, group_m, mb, nb);
             const long i = (long)mb * G::TILE_M + (long)rank * BM + rloc;
             const long j0 = (long)nb * BN;
             const int tb = tcount & 1;
@@ -595,6 +599,16 @@ bool umma_pairs() {
     return on;
 }
 
+int umma_group_m() {
+    // Row tiles per raster group: 16 by default, ASD_UMMA_GROUP_M overrides.
+    static int g = [] {
+        const char *e = getenv("ASD_UMMA_GROUP_M");
+        const int v = e ? atoi(e) : 0;
+        return (v >= 1 && v <= 4096) ? v : GROUP_M;
+    }();
+    return g;
+}
+
 int umma_row_bytes() {
     // Pipeline stage width: 128 (2 x 96 KB stages, the default) or 64
     // (4 x 48 KB stages, ASD_UMMA_ROWB=64).  Measured on B200, the two-stage
@@ -668,7 +682,7 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
         cfg.gridDim = dim3((unsigned)grid, 1, 1);
         return cudaLaunchKernelEx(&cfg, kern, tah, tal, tbh, tbl, num_m, num_n, kb_begin, kb_end,
                                   kpc, a.outer, a.row4, a.row1, a.col4, a.col1, a.alpha, a.part, a.status,
-                                  a.dbg_c, a.dbg_ldc, a.lat_n, a.M, a.gpart);
+                                  a.dbg_c, a.dbg_ldc, a.lat_n, a.M, a.gpart, umma_group_m());
     };
     const int epi = a.dbg_c ? EPI_STORE : (a.gpart ? EPI_GRID : EPI_PHASE);
     if (epi == EPI_GRID && (a.lat_n < 1 || (long)a.lat_n * a.lat_n != a.M ||
