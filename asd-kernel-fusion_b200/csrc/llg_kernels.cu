@@ -212,17 +212,35 @@ __global__ void __launch_bounds__(stream::NT_MAX, 2)
         const bool store = cl >= 4 && cl < 4 + g.wc && gcol < N && fl < nvalid;
         const int J = rs + 9;  // iterations: stage 4 reaches relative row rs + 3 at j = rs + 8
 
+        // A row buffer holds rw = 3 * blockDim.x doubles, so each thread
+        // copies three of them per row: column c = x / 12 of the band
+        // (periodic), value w = x % 12 of its 4 replicas x 3 components.
+        // Their offsets within a lattice row are the same for every row of
+        // the piece, so they are formed once here, not once per row.
+        long goff[3];
+        bool gval[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int x = tid + k * (int)blockDim.x;
+            const int c = x / (SF * 3), w = x - c * (SF * 3);
+            int gc = (C0 - 4 + c) % N;
+            if (gc < 0) gc += N;
+            gval[k] = w < 3 * nvalid;
+            goff[k] = (long)gc * K + 3L * fbase + w;
+        }
+        const long row_stride = (long)N * K;
         // y row R0 - 4 + j (periodic) of this band and replica group -> y ring
         auto load_row = [&](int j) {
-            int gr = (R0 - 4 + j) % N;
-            if (gr < 0) gr += N;
+            int gr = R0 - 4 + j;  // in [-4, N + 4): at most two wraps for N >= 3
+            while (gr < 0) gr += N;
+            while (gr >= N) gr -= N;
+            const double *src = y + (long)gr * row_stride;
             double *dst = ybuf + (j % YR) * rw;
-            for (int x = tid; x < rw; x += blockDim.x) {
-                const int c = x / (SF * 3), w = x - c * (SF * 3);
-                int gc = (C0 - 4 + c) % N;
-                if (gc < 0) gc += N;
-                if (w < 3 * nvalid)
-                    cp_async8(dst + x, y + ((long)gr * N + gc) * K + 3L * fbase + w);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int x = tid + k * (int)blockDim.x;
+                if (gval[k])
+                    cp_async8(dst + x, src + goff[k]);
                 else
                     dst[x] = 0.0;
             }
