@@ -370,8 +370,9 @@ def run_ours(args):
 
     hbm, bf16, src = measured_peaks()
     gemm_flops = 2.0 * M * M * K
-    gemm_ms = extra["sqt_ms"].get(mode, float("nan"))
-    achieved = gemm_flops / (gemm_ms / 1e3) / 1e12
+    gemm_ms = extra["sqt_ms"].get(mode)  # absent with --no-extras: the GEMM is not timed alone
+    achieved = gemm_flops / (gemm_ms / 1e3) / 1e12 if gemm_ms else None
+    frac = achieved / bf16 if achieved is not None else None
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
@@ -387,10 +388,10 @@ def run_ours(args):
                    "l2": "inputs larger than L2 (spin state 197 MB per array, operands 197 MB)"},
         "roofline": {"bound": "tensor", "kernel": f"umma_sqt_kernel ({mode})",
                      "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                     "frac": achieved / bf16, "traffic": traffic,
+                     "frac": frac, "traffic": traffic,
                      "peak_source": f"{src} dense bf16 burst (MEASURED_PEAKS.json)",
                      "achieved_counts": "useful 2*M*M*K per evaluation; the 3-term split issues 3x that on the tensor pipe",
-                     **split_ceiling(mode, achieved / bf16)},
+                     **(split_ceiling(mode, frac) if frac is not None else {})},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "e2e": e2e,
