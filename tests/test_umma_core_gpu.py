@@ -93,3 +93,35 @@ def test_cta_pair_kernel_matches():
     r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
+
+
+@pytest.mark.parametrize("group", [7, 64])
+def test_raster_group_size_changes_only_the_tile_order(group):
+    """ASD_UMMA_GROUP_M (row tiles per raster group, read once per process)
+    only reorders the tiles, so in a child process every product element
+    still meets the bound above.  2048 rows give 16 row tiles, i.e. groups of
+    7, 7 and 2, or one group smaller than 64.  S(q,t) through a context
+    (1792 padded rows, 14 row tiles) stays within 1e-5 of the FP64 path."""
+    import os
+    import subprocess
+    import sys
+
+    code = (
+        "import sys; sys.path[:0] = {paths!r}\n"
+        "import test_umma_core_gpu as t\n"
+        "for case in ((1, 2048, 64, 0), (2, 2048, 128, 0)):\n"
+        "    t.test_umma_core_matches_fp64_product(*case)\n"
+        "import asd_b200 as asd\n"
+        "p = asd.Params.make(40, 12, J1=-1.0, alpha=0.05, h=(0, 0, 0.5), dt=0.005, vx=2, vy=1)\n"
+        "with asd.Context(p) as c:\n"
+        "    c.set_spins(asd.random_spins(40, 12, seed=3), as_origin=True)\n"
+        "    c.step(4)\n"
+        "    ref = c.sqt('fp64')\n"
+        "    for m in ('tf32x3', 'bf16x3'):\n"
+        "        assert abs(c.sqt(m) - ref) <= 1e-5 * abs(ref), m\n"
+        "print('ok')\n"
+    ).format(paths=[os.path.dirname(__file__)] + sys.path)
+    env = dict(os.environ, ASD_UMMA_GROUP_M=str(group))
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
