@@ -83,3 +83,44 @@ def test_sqt_forms_agree(oracle):
     assert rel_err(grid[vx, vx], ref) < 1e-13
     # q and -q are complex conjugates for real spins
     assert abs(grid[vx, vx] - np.conj(grid[(-vx) % N, (-vx) % N])) < 1e-12
+
+
+def _energy(s, N, J1, J2, h):
+    """E = -J1 sum_bonds S_i.S_j - J2 sum_diagonal_bonds S_i.S_j - h.sum S_i per
+    replica, each bond once, so that -dE/dS_i is the effective field the
+    derivative uses (J1 over the 4 nearest, J2 over the 4 diagonal
+    neighbours, plus h)."""
+    S = s.reshape(s.shape[0], N, N, 3)
+    nn = (S * np.roll(S, -1, 1)).sum((1, 2, 3)) + (S * np.roll(S, -1, 2)).sum((1, 2, 3))
+    nnn = ((S * np.roll(S, (-1, -1), (1, 2))).sum((1, 2, 3)) +
+           (S * np.roll(S, (-1, 1), (1, 2))).sum((1, 2, 3)))
+    return -J1 * nn - J2 * nnn - (S * np.asarray(h)).sum((1, 2, 3))
+
+
+def test_energy_is_conserved_to_fourth_order_without_damping(oracle):
+    """Precession conserves E exactly, so its drift over a fixed time is RK4's
+    global error: it must shrink about 2^4 = 16-fold per halving of dt."""
+    N, nf = 12, 3
+    kw = dict(J1=1.0, J2=-0.3, h=(0.1, 0.0, 0.5))
+    s0 = orc.random_spins(N, nf, seed=5)
+    E0 = _energy(s0, N, **kw)
+    drift = []
+    for dt, n in ((0.02, 50), (0.01, 100), (0.005, 200)):  # to t = 1 each
+        s = oracle.steps(orc.make_params(N, nf, alpha=0.0, dt=dt, **kw), s0, n)
+        drift.append(np.abs(_energy(s, N, **kw) - E0).max() / np.abs(E0).max())
+    assert drift[1] < 1e-7
+    assert drift[0] / drift[1] > 12 and drift[1] / drift[2] > 12, drift
+
+
+def test_damping_dissipates_energy_every_step(oracle):
+    """With Gilbert damping dE/dt = -g alpha sum |H x S|^2 <= 0: E falls at
+    every step (J2 and the field included)."""
+    N, nf = 12, 3
+    kw = dict(J1=1.0, J2=-0.3, h=(0.1, 0.0, 0.5))
+    p = orc.make_params(N, nf, alpha=0.1, dt=0.01, **kw)
+    s = orc.random_spins(N, nf, seed=6)
+    E = [_energy(s, N, **kw)]
+    for _ in range(100):
+        s = oracle.steps(p, s, 1)
+        E.append(_energy(s, N, **kw))
+    assert np.all(np.diff(np.array(E), axis=0) < 0)
