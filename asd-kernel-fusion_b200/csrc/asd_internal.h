@@ -178,11 +178,13 @@ struct UmmaSqtArgs {
     // ranges, one of them with outer set, add up to S(q,t).
     int k_begin = 0, k_end = 0;
     int outer = 1;
+    int max_grid = 0;         // > 0: launch at most this many CTAs (partials)
 };
 // Returns the number of CTAs launched (partials written) or a negative error.
 int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st);
-bool umma_pairs();         // CTA-pair (cta_group::2) GEMM selected
 long umma_row_pad(long M);   // rows/cols padded to the tile multiple
+// CTAs launch_umma_sqt launches for M rows on num_sms SMs (max_grid unset).
+long umma_max_grid_for(long M, int num_sms);
 cudaError_t launch_mbar_timeout_probe(uint32_t limit, unsigned *status, cudaStream_t st);
 cudaError_t launch_grid_barrier_probe(void *bs, unsigned *status, cudaStream_t st);
 

@@ -144,79 +144,6 @@ __device__ __forceinline__ void tmem_ld_wait() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// ------------------------------------------------- CTA pairs (cta_group::2)
-// A cluster of two CTAs on two SMs shares one tcgen05.mma of M = 256: CTA
-// rank r holds rows [128 r, 128 r + 128) of A, half of B's N columns, and
-// its 128 rows of the accumulator in its own TMEM.  Rank 0 issues the MMAs.
-__device__ __forceinline__ uint32_t cluster_ctarank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-// All threads of both CTAs; memory operations before it are visible to the
-// other CTA after it.  The .aligned form needs a converged warp.
-__device__ __forceinline__ void cluster_sync() {
-    __syncwarp();
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
-                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-// Address in CTA `rank`'s shared memory of the variable at local address a.
-__device__ __forceinline__ uint32_t mapa(uint32_t a, uint32_t rank) {
-    uint32_t d;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(rank));
-    return d;
-}
-__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
-                 : "memory");
-}
-// Tile load into this CTA's shared memory whose completed bytes are counted
-// on the mbarrier at bar_cluster (in either CTA of the pair).
-__device__ __forceinline__ void tma_load_2d_pair(void *smem_dst, const void *desc,
-                                                 uint32_t bar_cluster, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(smem_dst)),
-        "l"(reinterpret_cast<uint64_t>(desc)), "r"(bar_cluster), "r"(x), "r"(y)
-        : "memory");
-}
-// TMEM allocation for the pair: one warp of EACH CTA executes it.
-__device__ __forceinline__ void tmem_alloc_pair(uint32_t *dst_smem, uint32_t ncols) {
-    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(dst_smem)),
-                 "r"(ncols));
-}
-__device__ __forceinline__ void tmem_relinquish_pair() {
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
-}
-__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
-    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
-}
-__device__ __forceinline__ void umma_f16_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                              uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-__device__ __forceinline__ void umma_tf32_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                               uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-// Arrives once on the mbarrier at bar_cluster (this CTA's or the peer's) when
-// every pair MMA issued so far by this thread has completed.
-__device__ __forceinline__ void umma_commit_pair(uint32_t bar_cluster) {
-    asm volatile(
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            bar_cluster)
-        : "memory");
-}
-
 // Shared-memory matrix descriptor for a K-major operand tile stored with a
 // ROWB-byte swizzle (ROWB = 128 or 64): rows of ROWB bytes, 8-row swizzle
 // atoms laid out contiguously, so the stride between 8-row groups (SBO) is

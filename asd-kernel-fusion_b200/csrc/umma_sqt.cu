@@ -22,7 +22,6 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
-#include <cstdlib>
 #include <mutex>
 
 #include "asd_internal.h"
@@ -36,22 +35,21 @@ constexpr int BN = 256;
 constexpr int NUM_THREADS = 192;
 constexpr int TMEM_COLS = 512;
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
-constexpr int GROUP_M = 16;  // default tile rows per raster group (umma_group_m)
+// Row tiles per raster group.  Measured on B200 at 128x128x500 and
+// 256x256x1000: groups of 16 keep the DRAM traffic lowest (the group's A
+// bands, 24-48 MB, stay in L2 while B streams past once per group).
+constexpr int GROUP_M = 16;
 constexpr int kGridMaxBins = 4096;  // q-grid histogram: N*N FP32 bins in shared memory
 
-// Pipeline geometry.  ROWB = bytes of K per operand row in one pipeline
-// stage (= the swizzle width).  Single CTA (PAIR = false): a 128 x 256 tile
-// per CTA, ROWB 64 -> 4 stages of 48 KB, 128 -> 2 stages of 96 KB.  CTA pair
-// (PAIR = true): a 256 x 256 tile per pair of SMs, each CTA loading 128 rows
-// of A and 128 of the 256 B rows, so a stage is 64 KB per SM for the same
-// MMA work per SM as the single-CTA 96 KB stage, and 3 stages fit.
-template <int ROWB, bool PAIR = false>
+// Pipeline geometry: 128 bytes of K per operand row per stage (the 128-byte
+// swizzle width), two stages of 96 KB (Ah, Al 128 x 128 B; Bh, Bl 256 x 128 B).
+// Measured on B200, two 96 KB stages are as fast as or faster than four of
+// 48 KB with a 64-byte swizzle (fewer barrier round trips per flop).
 struct Geo {
-    static constexpr int STAGES = PAIR ? 3 : ((ROWB == 64) ? 4 : 2);
-    static constexpr int BN_LOC = PAIR ? BN / 2 : BN;  // B rows loaded by one CTA
-    static constexpr int TILE_M = PAIR ? 2 * BM : BM;  // accumulator rows per tile
+    static constexpr int ROWB = 128;
+    static constexpr int STAGES = 2;
     static constexpr int A_TILE = BM * ROWB;
-    static constexpr int B_TILE = BN_LOC * ROWB;
+    static constexpr int B_TILE = BN * ROWB;
     static constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
     static constexpr int KSTEPS = ROWB / 32;  // 32-byte MMA k steps per stage
     static constexpr int PIPE_BYTES = STAGES * STAGE_BYTES;
@@ -60,8 +58,8 @@ struct Geo {
 };
 
 struct SmemTail {
-    uint64_t full[4];
-    uint64_t empty[4];
+    uint64_t full[Geo::STAGES];
+    uint64_t empty[Geo::STAGES];
     uint64_t tfull[2];
     uint64_t tempty[2];
     uint64_t drain;
@@ -71,9 +69,8 @@ struct SmemTail {
     double red[2][4];
 };
 
-template <int ROWB, bool PAIR = false>
 constexpr int smem_bytes() {
-    return 1024 /*alignment slack*/ + Geo<ROWB, PAIR>::PIPE_BYTES + Geo<ROWB, PAIR>::TABLE_BYTES +
+    return 1024 /*alignment slack*/ + Geo::PIPE_BYTES + Geo::TABLE_BYTES +
            (int)((sizeof(SmemTail) + 15) & ~size_t(15));
 }
 
@@ -115,11 +112,8 @@ __device__ __forceinline__ bool epilogue_sync(uint64_t *bar, uint32_t &phase,
 //              alpha C_ij - m_i.z_j goes to bin (r_i - r_j) mod N of a
 //              per-tile FP32 shared histogram, flushed after each tile into
 //              this CTA's FP64 histogram gpart[blockIdx.x][N*N]
-// PAIR: launched in clusters of two CTAs that share every tcgen05.mma
-// (cta_group::2, M = 256); tiles are 256 x 256, num_m counts 256-row blocks,
-// and each CTA's epilogue handles its own 128 rows of the tile.
 constexpr int EPI_PHASE = 0, EPI_STORE = 1, EPI_GRID = 2;
-template <int KIND, int EPI, int ROWB, bool PAIR>
+template <int KIND, int EPI>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     umma_sqt_kernel(const __grid_constant__ CUtensorMap tm_ah,
                     const __grid_constant__ CUtensorMap tm_al,
@@ -130,7 +124,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     const float *__restrict__ col1, float alpha, double2 *__restrict__ part,
                     unsigned *__restrict__ status, float *__restrict__ dbg_c, long dbg_ldc,
                     int lat_n, long n_sites, double *__restrict__ gpart, int group_m) {
-    using G = Geo<ROWB, PAIR>;
+    using G = Geo;
     constexpr bool STORE = (EPI == EPI_STORE);
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -144,11 +138,6 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
     const int num_tiles = num_m * num_n;
-    // Tile schedule: single CTAs stride over tiles by CTA, pairs by cluster.
-    const uint32_t rank = PAIR ? ptx::cluster_ctarank() : 0u;
-    const bool leader = (rank == 0);
-    const int first_tile = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
-    const int tile_step = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < G::STAGES; ++s) {
@@ -157,7 +146,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             ptx::mbar_init(&tail->tfull[b], 1);
-            ptx::mbar_init(&tail->tempty[b], PAIR ? 8 : 4);  // epilogue warps (of both CTAs)
+            ptx::mbar_init(&tail->tempty[b], 4);  // one arrival per epilogue warp
         }
         ptx::mbar_init(&tail->drain, 1);
         ptx::mbar_init(&tail->ebar, 4);
@@ -165,22 +154,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         ptx::fence_mbar_init();
     }
     if (warp == 0) {
-        if (PAIR) {
-            ptx::tmem_alloc_pair(&tail->tmem_base, TMEM_COLS);
-            ptx::tmem_relinquish_pair();
-        } else {
-            ptx::tmem_alloc(&tail->tmem_base, TMEM_COLS);
-            ptx::tmem_relinquish();
-        }
+        ptx::tmem_alloc(&tail->tmem_base, TMEM_COLS);
+        ptx::tmem_relinquish();
     }
     ptx::tc_fence_before();
-    // Pairs: the peer's barriers must be initialised before this CTA's
-    // loads and commits reach them.  Every CTA of a cluster is resident
-    // together, so this barrier cannot wait on a CTA that never starts.
-    if (PAIR)
-        ptx::cluster_sync();
-    else
-        __syncthreads();
+    __syncthreads();
     ptx::tc_fence_after();
     const uint32_t tmem_base = tail->tmem_base;
     volatile int *abort_flag = &tail->abort_flag;
@@ -191,19 +169,17 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             ptx::tma_prefetch_desc(&tm_al);
             ptx::tma_prefetch_desc(&tm_bh);
             ptx::tma_prefetch_desc(&tm_bl);
-            constexpr int KE = ROWB / ((KIND == 2) ? 2 : 4);  // elements per stage row
+            constexpr int KE = G::ROWB / ((KIND == 2) ? 2 : 4);  // elements per stage row
             int stage = 0;
             uint32_t phase = 0;
             bool issued[G::STAGES] = {};
             uint32_t issued_parity[G::STAGES] = {};
             bool ok = true;
-            // Pairs: both CTAs' bytes complete on the leader's full barrier.
-            const uint32_t full0 = PAIR ? ptx::mapa(ptx::smem_u32(&tail->full[0]), 0u) : 0u;
-            for (int tile = first_tile; tile < num_tiles && ok; tile += tile_step) {
+            for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
                 int mb, nb;
                 tile_coords(tile, num_m, num_n, group_m, mb, nb);
-                const int arow = mb * G::TILE_M + (int)rank * BM;
-                const int brow = nb * BN + (int)rank * G::BN_LOC;
+                const int arow = mb * BM;
+                const int brow = nb * BN;
                 for (int kb = kb_begin; kb < kb_end; ++kb) {
                     if (!ptx::mbar_wait_bounded(&tail->empty[stage], phase ^ 1u, abort_flag,
                                                 WAIT_LIMIT)) {
@@ -213,22 +189,12 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     }
                     uint8_t *st = smem + stage * G::STAGE_BYTES;
                     const int x = kb * KE;
-                    if (PAIR) {
-                        if (leader)
-                            ptx::mbar_arrive_expect_tx(&tail->full[stage], 2 * G::STAGE_BYTES);
-                        const uint32_t fb = full0 + (uint32_t)(stage * sizeof(uint64_t));
-                        ptx::tma_load_2d_pair(st, &tm_ah, fb, x, arow);
-                        ptx::tma_load_2d_pair(st + G::A_TILE, &tm_al, fb, x, arow);
-                        ptx::tma_load_2d_pair(st + 2 * G::A_TILE, &tm_bh, fb, x, brow);
-                        ptx::tma_load_2d_pair(st + 2 * G::A_TILE + G::B_TILE, &tm_bl, fb, x, brow);
-                    } else {
-                        ptx::mbar_arrive_expect_tx(&tail->full[stage], G::STAGE_BYTES);
-                        ptx::tma_load_2d(st, &tm_ah, &tail->full[stage], x, arow);
-                        ptx::tma_load_2d(st + G::A_TILE, &tm_al, &tail->full[stage], x, arow);
-                        ptx::tma_load_2d(st + 2 * G::A_TILE, &tm_bh, &tail->full[stage], x, brow);
-                        ptx::tma_load_2d(st + 2 * G::A_TILE + G::B_TILE, &tm_bl,
-                                         &tail->full[stage], x, brow);
-                    }
+                    ptx::mbar_arrive_expect_tx(&tail->full[stage], G::STAGE_BYTES);
+                    ptx::tma_load_2d(st, &tm_ah, &tail->full[stage], x, arow);
+                    ptx::tma_load_2d(st + G::A_TILE, &tm_al, &tail->full[stage], x, arow);
+                    ptx::tma_load_2d(st + 2 * G::A_TILE, &tm_bh, &tail->full[stage], x, brow);
+                    ptx::tma_load_2d(st + 2 * G::A_TILE + G::B_TILE, &tm_bl, &tail->full[stage],
+                                     x, brow);
                     issued[stage] = true;
                     issued_parity[stage] = phase;
                     if (++stage == G::STAGES) {
@@ -239,11 +205,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             }
             // Never leave the CTA with bulk copies still landing in shared
             // memory: wait (bounded, ignoring the abort flag) for the last
-            // fill of every stage.  In a pair the leader's full barriers
-            // count both CTAs' bytes, so the leader waits for both, and the
-            // closing cluster barrier keeps the peer until then.
+            // fill of every stage.
             for (int s = 0; s < G::STAGES; ++s) {
-                if (!issued[s] || !leader) continue;
+                if (!issued[s]) continue;
                 uint32_t i = 0;
                 while (!ptx::mbar_try_wait(&tail->full[s], issued_parity[s]) && i < WAIT_LIMIT) {
                     ++i;
@@ -253,26 +217,15 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             }
         }
     } else if (warp == 1) {
-        // Pairs: only the leader issues; its commits arrive on the barriers
-        // of both CTAs (own address, and the peer's through mapa).
-        if (lane == 0 && leader) {
-            constexpr uint32_t IDESC = ptx::umma_idesc(KIND == 2 ? 1u : 2u, G::TILE_M, BN);
-            auto commit_both = [&](uint64_t *bar) {
-                if (PAIR) {
-                    const uint32_t a = ptx::smem_u32(bar);
-                    ptx::umma_commit_pair(a);
-                    ptx::umma_commit_pair(ptx::mapa(a, 1u));
-                } else {
-                    ptx::umma_commit(bar);
-                }
-            };
+        if (lane == 0) {
+            constexpr uint32_t IDESC = ptx::umma_idesc(KIND == 2 ? 1u : 2u, BM, BN);
             int stage = 0;
             uint32_t phase = 0;
             int abuf = 0;
             uint32_t aphase = 0;
             bool ok = true;
             const uint32_t smem_base = ptx::smem_u32(smem);
-            for (int tile = first_tile; tile < num_tiles && ok; tile += tile_step) {
+            for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
                 // K is accumulated in chunks of kb_per_chunk k blocks, each
                 // into a fresh TMEM buffer: the tensor core's FP32
                 // accumulation loses precision with the number of
@@ -296,24 +249,16 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         }
                         ptx::tc_fence_after();
                         const uint32_t s0 = smem_base + stage * G::STAGE_BYTES;
-                        const uint64_t dah = ptx::umma_desc_kmajor<ROWB>(s0);
-                        const uint64_t dal = ptx::umma_desc_kmajor<ROWB>(s0 + G::A_TILE);
-                        const uint64_t dbh = ptx::umma_desc_kmajor<ROWB>(s0 + 2 * G::A_TILE);
+                        const uint64_t dah = ptx::umma_desc_kmajor<G::ROWB>(s0);
+                        const uint64_t dal = ptx::umma_desc_kmajor<G::ROWB>(s0 + G::A_TILE);
+                        const uint64_t dbh = ptx::umma_desc_kmajor<G::ROWB>(s0 + 2 * G::A_TILE);
                         const uint64_t dbl =
-                            ptx::umma_desc_kmajor<ROWB>(s0 + 2 * G::A_TILE + G::B_TILE);
+                            ptx::umma_desc_kmajor<G::ROWB>(s0 + 2 * G::A_TILE + G::B_TILE);
 #pragma unroll
                         for (int kk = 0; kk < G::KSTEPS; ++kk) {
                             const uint64_t adv = (uint64_t)(2 * kk);  // 32 bytes per k step
                             const uint32_t accum = (kb > kb0 || kk > 0) ? 1u : 0u;
-                            if (PAIR && KIND == 2) {
-                                ptx::umma_f16_pair(d_tmem, dah + adv, dbh + adv, IDESC, accum);
-                                ptx::umma_f16_pair(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
-                                ptx::umma_f16_pair(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
-                            } else if (PAIR) {
-                                ptx::umma_tf32_pair(d_tmem, dah + adv, dbh + adv, IDESC, accum);
-                                ptx::umma_tf32_pair(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
-                                ptx::umma_tf32_pair(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
-                            } else if (KIND == 2) {
+                            if (KIND == 2) {
                                 ptx::umma_f16(d_tmem, dah + adv, dbh + adv, IDESC, accum);
                                 ptx::umma_f16(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
                                 ptx::umma_f16(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
@@ -323,14 +268,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                                 ptx::umma_tf32(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
                             }
                         }
-                        commit_both(&tail->empty[stage]);
+                        ptx::umma_commit(&tail->empty[stage]);
                         if (++stage == G::STAGES) {
                             stage = 0;
                             phase ^= 1u;
                         }
                     }
                     if (!ok) break;
-                    commit_both(&tail->tfull[abuf]);
+                    ptx::umma_commit(&tail->tfull[abuf]);
                     if (++abuf == 2) {
                         abuf = 0;
                         aphase ^= 1u;
@@ -338,10 +283,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 }
             }
             // Wait for every issued MMA before TMEM can be released.
-            if (PAIR)
-                ptx::umma_commit_pair(ptx::smem_u32(&tail->drain));
-            else
-                ptx::umma_commit(&tail->drain);
+            ptx::umma_commit(&tail->drain);
             uint32_t i = 0;
             while (!ptx::mbar_try_wait(&tail->drain, 0u) && i < WAIT_LIMIT) {
                 ++i;
@@ -366,12 +308,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 gp[b] = 0.0;
             }
         }
-        // Pairs: the accumulator buffers are released on the leader's tempty.
-        const uint32_t tempty0 = PAIR ? ptx::mapa(ptx::smem_u32(&tail->tempty[0]), 0u) : 0u;
-        for (int tile = first_tile; tile < num_tiles; tile += tile_step, ++tcount) {
+        for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++tcount) {
             int mb, nb;
             tile_coords(tile, num_m, num_n, group_m, mb, nb);
-            const long i = (long)mb * G::TILE_M + (long)rank * BM + rloc;
+            const long i = (long)mb * BM + rloc;
             const long j0 = (long)nb * BN;
             const int tb = tcount & 1;
             float2 *w_tab = tab_w + tb * BN;
@@ -485,12 +425,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 }
                 ptx::tc_fence_before();
                 __syncwarp();
-                if (lane == 0) {
-                    if (PAIR)
-                        ptx::mbar_arrive_remote(tempty0 + (uint32_t)(abuf * sizeof(uint64_t)));
-                    else
-                        ptx::mbar_arrive(&tail->tempty[abuf]);
-                }
+                if (lane == 0) ptx::mbar_arrive(&tail->tempty[abuf]);
                 if (++abuf == 2) {
                     abuf = 0;
                     aphase ^= 1u;
@@ -528,25 +463,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     }
 
     ptx::tc_fence_before();
-    // Pairs: neither CTA leaves (or frees TMEM) while the leader's MMAs may
-    // still read the peer's shared memory or write its TMEM: the leader's
-    // MMA thread has drained them before it arrives here.
-    if (PAIR)
-        ptx::cluster_sync();
-    else
-        __syncthreads();
+    __syncthreads();
     ptx::tc_fence_after();
     if (threadIdx.x == 0 && EPI == EPI_PHASE) {
         const double re = (tail->red[0][0] + tail->red[0][1]) + (tail->red[0][2] + tail->red[0][3]);
         const double im = (tail->red[1][0] + tail->red[1][1]) + (tail->red[1][2] + tail->red[1][3]);
         part[blockIdx.x] = make_double2(re, im);
     }
-    if (warp == 0) {
-        if (PAIR)
-            ptx::tmem_dealloc_pair(tmem_base, TMEM_COLS);
-        else
-            ptx::tmem_dealloc(tmem_base, TMEM_COLS);
-    }
+    if (warp == 0) ptx::tmem_dealloc(tmem_base, TMEM_COLS);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
@@ -563,7 +487,8 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
     return fn;
 }
 
-// Row-major [rows][Kp] operand, box = 128 bytes of K x box_rows rows, 128B swizzle.
+// Row-major [rows][Kp] operand, box = rowb (128) bytes of K x box_rows rows,
+// 128-byte swizzle.
 int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int box_rows,
               int rowb) {
     auto enc = get_encode_fn();
@@ -577,7 +502,7 @@ int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int
     cuuint32_t estride[2] = {1, 1};
     CUresult r = enc(m, dt, 2, const_cast<void *>(base), gdim, gstride, box, estride,
                      CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     rowb == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_SWIZZLE_128B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(ASD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return ASD_OK;
@@ -587,58 +512,27 @@ int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int
 
 long umma_row_pad(long M) { return (M + BN - 1) / BN * BN; }
 
-bool umma_pairs() {
-    // ASD_UMMA_PAIR=1 selects the CTA-pair (cta_group::2) kernel.  Measured on
-    // B200 it is within a few per cent of the single-CTA kernel (faster for
-    // TF32x3 at 16384 sites, slower for BF16x3): both already keep the tensor
-    // pipe near its ceiling, so the single-CTA form stays the default.
-    static bool on = [] {
-        const char *e = getenv("ASD_UMMA_PAIR");
-        return e && e[0] == '1';
-    }();
-    return on;
-}
-
-int umma_group_m() {
-    // Row tiles per raster group: 16 by default, ASD_UMMA_GROUP_M overrides.
-    static int g = [] {
-        const char *e = getenv("ASD_UMMA_GROUP_M");
-        const int v = e ? atoi(e) : 0;
-        return (v >= 1 && v <= 4096) ? v : GROUP_M;
-    }();
-    return g;
-}
-
-int umma_row_bytes() {
-    // Pipeline stage width: 128 (2 x 96 KB stages, the default) or 64
-    // (4 x 48 KB stages, ASD_UMMA_ROWB=64).  Measured on B200, the two-stage
-    // form is as fast or faster (fewer barrier round trips per flop).
-    static int rowb = [] {
-        const char *e = getenv("ASD_UMMA_ROWB");
-        return (e && atoi(e) == 64) ? 64 : 128;
-    }();
-    return rowb;
+long umma_max_grid_for(long M, int num_sms) {
+    const long Mp = umma_row_pad(M);
+    const long tiles = (Mp / BM) * (Mp / BN);
+    return tiles < num_sms ? tiles : num_sms;
 }
 
 int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     const long Mp = umma_row_pad(a.M);
     const int esize = (a.kind == 2) ? 2 : 4;
-    if (a.Kp <= 0 || (a.Kp * esize) % 128 != 0)
+    if (a.Kp <= 0 || (a.Kp * esize) % Geo::ROWB != 0)
         return fail(ASD_ERR_INVALID, "Kp=%d: rows must be a multiple of 128 bytes", a.Kp);
     if (((uintptr_t)a.a_hi | (uintptr_t)a.a_lo | (uintptr_t)a.b_hi | (uintptr_t)a.b_lo) & 15)
         return fail(ASD_ERR_INVALID, "operand base not 16-byte aligned");
-    const int rowb = umma_row_bytes();
-    const bool pair = umma_pairs() && rowb == 128;
-    const int ke = rowb / esize;  // K elements per pipeline stage
-    const int tile_m = pair ? 2 * BM : BM;
-    const int b_rows = pair ? BN / 2 : BN;  // B rows one CTA loads per tile
+    const int ke = Geo::ROWB / esize;  // K elements per pipeline stage
     CUtensorMap tah, tal, tbh, tbl;
     int rc;
-    if ((rc = make_tmap(&tah, a.a_hi, a.kind, Mp, a.Kp, BM, rowb)) != ASD_OK) return rc;
-    if ((rc = make_tmap(&tal, a.a_lo, a.kind, Mp, a.Kp, BM, rowb)) != ASD_OK) return rc;
-    if ((rc = make_tmap(&tbh, a.b_hi, a.kind, Mp, a.Kp, b_rows, rowb)) != ASD_OK) return rc;
-    if ((rc = make_tmap(&tbl, a.b_lo, a.kind, Mp, a.Kp, b_rows, rowb)) != ASD_OK) return rc;
-    const int num_m = (int)(Mp / tile_m), num_n = (int)(Mp / BN), num_kb = a.Kp / ke;
+    if ((rc = make_tmap(&tah, a.a_hi, a.kind, Mp, a.Kp, BM, Geo::ROWB)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tal, a.a_lo, a.kind, Mp, a.Kp, BM, Geo::ROWB)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tbh, a.b_hi, a.kind, Mp, a.Kp, BN, Geo::ROWB)) != ASD_OK) return rc;
+    if ((rc = make_tmap(&tbl, a.b_lo, a.kind, Mp, a.Kp, BN, Geo::ROWB)) != ASD_OK) return rc;
+    const int num_m = (int)(Mp / BM), num_n = (int)(Mp / BN), num_kb = a.Kp / ke;
     const int k_end = a.k_end > 0 ? a.k_end : a.Kp;
     if (a.k_begin < 0 || a.k_begin % ke != 0 || k_end % ke != 0 || k_end > a.Kp ||
         a.k_begin >= k_end)
@@ -650,59 +544,36 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     int kpc = a.chunk_k > 0 ? (a.chunk_k + ke - 1) / ke : num_kb;
     if (kpc < 1) kpc = 1;
     if (kpc > num_kb) kpc = num_kb;
-    int grid = 0;
-    cudaError_t e;
-    auto go = [&](auto kern, int smem) {
-        cudaError_t r =
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (r != cudaSuccess) return r;
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute attr[1];
-        cfg.blockDim = dim3(NUM_THREADS, 1, 1);
-        cfg.dynamicSmemBytes = (size_t)smem;
-        cfg.stream = st;
-        if (pair) {
-            // One cluster of two CTAs per SM pair, as many as fit at once.
-            attr[0].id = cudaLaunchAttributeClusterDimension;
-            attr[0].val.clusterDim.x = 2;
-            attr[0].val.clusterDim.y = 1;
-            attr[0].val.clusterDim.z = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            cfg.gridDim = dim3(2, 1, 1);
-            int clusters = 0;
-            r = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
-            if (r != cudaSuccess) return r;
-            if (clusters < 1) return cudaErrorInvalidConfiguration;
-            if (clusters > tiles) clusters = tiles;
-            grid = 2 * clusters;
-        } else {
-            grid = tiles < a.num_sms ? tiles : a.num_sms;
-        }
-        cfg.gridDim = dim3((unsigned)grid, 1, 1);
-        return cudaLaunchKernelEx(&cfg, kern, tah, tal, tbh, tbl, num_m, num_n, kb_begin, kb_end,
-                                  kpc, a.outer, a.row4, a.row1, a.col4, a.col1, a.alpha, a.part, a.status,
-                                  a.dbg_c, a.dbg_ldc, a.lat_n, a.M, a.gpart, umma_group_m());
-    };
+    // One persistent CTA per SM (or per tile, if fewer); every CTA strides
+    // over the tiles, so any grid size is correct and a caller's cap (the
+    // partials it has room for) only lengthens each CTA's tile list.
+    int grid = tiles < a.num_sms ? tiles : a.num_sms;
+    if (a.max_grid > 0 && grid > a.max_grid) grid = a.max_grid;
+    if (grid < 1) return fail(ASD_ERR_INVALID, "no tiles to launch");
     const int epi = a.dbg_c ? EPI_STORE : (a.gpart ? EPI_GRID : EPI_PHASE);
     if (epi == EPI_GRID && (a.lat_n < 1 || (long)a.lat_n * a.lat_n != a.M ||
                             a.lat_n * a.lat_n > kGridMaxBins))
         return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t) supports N*N <= %d sites", kGridMaxBins);
-    const int hist_bytes = (epi == EPI_GRID) ? 4 * a.lat_n * a.lat_n + 16 : 0;
-#define ASD_UMMA_GO(K, E, R, P) go(umma_sqt_kernel<K, E, R, P>, smem_bytes<R, P>() + hist_bytes)
-#define ASD_UMMA_EPI(K, R, P)                                                                 \
-    (epi == EPI_STORE ? ASD_UMMA_GO(K, EPI_STORE, R, P)                                         \
-     : epi == EPI_GRID ? ASD_UMMA_GO(K, EPI_GRID, R, P) : ASD_UMMA_GO(K, EPI_PHASE, R, P))
-    if (pair)
-        e = (a.kind == 2) ? ASD_UMMA_EPI(2, 128, true) : ASD_UMMA_EPI(1, 128, true);
-    else if (rowb == 64)
-        e = (a.kind == 2) ? ASD_UMMA_EPI(2, 64, false) : ASD_UMMA_EPI(1, 64, false);
+    const int smem = smem_bytes() + ((epi == EPI_GRID) ? 4 * a.lat_n * a.lat_n + 16 : 0);
+    auto go = [&](auto kern) {
+        cudaError_t r =
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (r != cudaSuccess) return r;
+        kern<<<grid, NUM_THREADS, smem, st>>>(tah, tal, tbh, tbl, num_m, num_n, kb_begin, kb_end,
+                                              kpc, a.outer, a.row4, a.row1, a.col4, a.col1,
+                                              a.alpha, a.part, a.status, a.dbg_c, a.dbg_ldc,
+                                              a.lat_n, a.M, a.gpart, GROUP_M);
+        return cudaGetLastError();
+    };
+    cudaError_t e;
+    if (a.kind == 2)
+        e = epi == EPI_STORE  ? go(umma_sqt_kernel<2, EPI_STORE>)
+            : epi == EPI_GRID ? go(umma_sqt_kernel<2, EPI_GRID>)
+                              : go(umma_sqt_kernel<2, EPI_PHASE>);
     else
-        e = (a.kind == 2) ? ASD_UMMA_EPI(2, 128, false) : ASD_UMMA_EPI(1, 128, false);
-#undef ASD_UMMA_EPI
-#undef ASD_UMMA_GO
-    if (e != cudaSuccess) return cuda_fail(e, "umma_sqt setup");
-    e = cudaGetLastError();
+        e = epi == EPI_STORE  ? go(umma_sqt_kernel<1, EPI_STORE>)
+            : epi == EPI_GRID ? go(umma_sqt_kernel<1, EPI_GRID>)
+                              : go(umma_sqt_kernel<1, EPI_PHASE>);
     if (e != cudaSuccess) return cuda_fail(e, "umma_sqt launch");
     return grid;
 }
@@ -777,28 +648,18 @@ namespace {
 constexpr int kNoAllocMaxCtas = 1024;  // partials: at most one per CTA
 constexpr size_t kNoAllocPartBytes = kNoAllocMaxCtas * sizeof(double2);
 constexpr size_t kNoAllocScratchBytes = kNoAllocPartBytes + 256;  // + status word
-constexpr int kMaxDevices = 64;
-
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mu;
-void *g_noalloc_addr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device.  The symbol's
-// name in host code is only a host-side stand-in; the device address is
-// looked up once per device, with that device current.
+// Device address of g_noalloc_scratch in the current device's context.  The
+// symbol's name in host code is only a host-side stand-in for it.  The
+// address is looked up on every call (a host-side query that allocates
+// nothing), so it stays right after cudaDeviceReset, under another context,
+// and when the caller switches devices between calls.
 int noalloc_scratch(unsigned char **out) {
-    int dev = 0;
-    ASD_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(ASD_ERR_UNSUPPORTED, "device index %d", dev);
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        g_noalloc_addr[dev] = p;
-    }
-    *out = static_cast<unsigned char *>(g_noalloc_addr[dev]);
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    *out = static_cast<unsigned char *>(p);
     return ASD_OK;
 }
 
@@ -847,11 +708,17 @@ extern "C" int asd_sqt_split_noalloc(int kind, long rows, int Kp, const void *a_
     if (((uintptr_t)row4 | (uintptr_t)col4) & 15)
         return fail(ASD_ERR_INVALID, "row4/col4 must be 16-byte aligned");
     if (chunk_k < 0) return fail(ASD_ERR_INVALID, "chunk_k < 0");
-    int dev = 0, sms = 0;
+    int dev = 0, sms = 0, sdev = 0;
     ASD_CUDA_TRY(cudaGetDevice(&dev));
+    cudaStream_t st = (cudaStream_t)stream;
+    // The scratch address is the current device's; a stream of another
+    // device would run the kernels there with this device's address.
+    ASD_CUDA_TRY(cudaStreamGetDevice(st, &sdev));
+    if (sdev != dev)
+        return fail(ASD_ERR_INVALID, "stream belongs to device %d, the current device is %d", sdev,
+                    dev);
     ASD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const long tiles = (rows / 128) * (rows / 256);
-    const long ctas = tiles < sms ? tiles : sms;
+    const long ctas = umma_max_grid_for(rows, sms);
     if (ctas > kNoAllocMaxCtas)
         return fail(ASD_ERR_UNSUPPORTED,
                     "the fixed scratch holds %d CTA partials; this launch needs %ld", kNoAllocMaxCtas,
@@ -861,7 +728,6 @@ extern "C" int asd_sqt_split_noalloc(int kind, long rows, int Kp, const void *a_
     if (rc != ASD_OK) return rc;
     double2 *part = reinterpret_cast<double2 *>(scratch);
     unsigned *status = reinterpret_cast<unsigned *>(scratch + kNoAllocPartBytes);
-    cudaStream_t st = (cudaStream_t)stream;
     // the status word keeps the last call's value: clear it
     ASD_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned), st));
     UmmaSqtArgs u{};
@@ -880,6 +746,7 @@ extern "C" int asd_sqt_split_noalloc(int kind, long rows, int Kp, const void *a_
     u.part = part;
     u.status = status;
     u.num_sms = sms;
+    u.max_grid = kNoAllocMaxCtas;  // never more partials than the array holds
     u.chunk_k = chunk_k;
     const int grid = launch_umma_sqt(u, st);
     if (grid < 0) return grid;

@@ -209,7 +209,8 @@ int asd_ctx_shard_sqt_finish(asd_ctx *ctx, const double *d_part, const double *d
  * bit-identical spins. */
 #define ASD_LLG_STAGES 0     /* four launches, one fused kernel per RK4 stage,
                                 HBM-bound (384 B of DRAM traffic per
-                                site-step; about 75% of HBM bandwidth on B200) */
+                                site-step; 75-85% of the measured HBM copy
+                                bandwidth on B200)                           */
 #define ASD_LLG_FUSED_STEP 1 /* one launch per step, the four stages
                                 streamed down the lattice through shared
                                 memory by column band (48 B of DRAM traffic per
@@ -310,9 +311,12 @@ int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, const void 
  * status word) is a fixed array in the library's device memory that every GPU
  * which loads the library keeps until the process exits.  Limit: at most 1024
  * CTAs, i.e. devices with up to 1024 SMs; larger launches are rejected with
- * ASD_ERR_UNSUPPORTED.  The first call on a device looks up that array's
- * device address (once per device); make that first call before any stream
- * capture.  All calls share the one array, so calls whose work overlaps on
+ * ASD_ERR_UNSUPPORTED.  Every call looks up that array's device address in
+ * the current device's context (a host-side query that allocates nothing; the
+ * first call on a device also loads the library's device code there, so make
+ * it before any stream capture); after cudaDeviceReset the next call finds the
+ * array again.  `stream` must belong to the current device (else
+ * ASD_ERR_INVALID).  All calls share the one array, so calls whose work overlaps on
  * the GPU (different streams, or different host threads) race and must be
  * ordered by the caller.  If a bounded wait in the kernel gives up, d_out
  * receives NaN. */

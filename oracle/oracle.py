@@ -49,8 +49,8 @@ def build(quiet: bool = True) -> None:
     if quiet:
         kw.update(stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     subprocess.run(["make", "liboracle.so"], **kw)
-    ref = Path(os.environ.get("ASD_REFERENCE", "/root/reference"))
-    if (ref / "baseline" / "llg_sqt_baseline.c").exists():
+    ref = Path(os.environ.get("ASD_REFERENCE", "")).expanduser()
+    if os.environ.get("ASD_REFERENCE") and (ref / "baseline" / "llg_sqt_baseline.c").exists():
         subprocess.run(["make", "ref", f"REF={ref}"], **kw)
 
 

@@ -64,64 +64,22 @@ def test_umma_core_matches_fp64_product(kind, rows, Kp, chunk):
     assert (C.double() - exact).abs().max().item() <= bound
 
 
-def test_cta_pair_kernel_matches():
-    """The CTA-pair form of the GEMM (cta_group::2, M = 256 over two SMs,
-    selected by ASD_UMMA_PAIR=1, read once per process), checked in a child
-    process: the raw product on several shapes against the same bound as
-    above, and S(q,t) through a context against the FP64 path."""
-    import os
-    import subprocess
-    import sys
-
-    code = (
-        "import sys; sys.path[:0] = {paths!r}\n"
-        "import test_umma_core_gpu as t\n"
-        "for case in ((1, 256, 32, 0), (2, 768, 192, 0), (1, 1024, 1504, 256),\n"
-        "             (2, 512, 1536, 512)):\n"
-        "    t.test_umma_core_matches_fp64_product(*case)\n"
-        "import asd_b200 as asd\n"
-        "p = asd.Params.make(40, 12, J1=-1.0, alpha=0.05, h=(0, 0, 0.5), dt=0.005, vx=2, vy=1)\n"
-        "with asd.Context(p) as c:\n"
-        "    c.set_spins(asd.random_spins(40, 12, seed=3), as_origin=True)\n"
-        "    c.step(4)\n"
-        "    ref = c.sqt('fp64')\n"
-        "    for m in ('tf32x3', 'bf16x3'):\n"
-        "        assert abs(c.sqt(m) - ref) <= 1e-5 * abs(ref), m\n"
-        "print('ok')\n"
-    ).format(paths=[os.path.dirname(__file__)] + sys.path)
-    env = dict(os.environ, ASD_UMMA_PAIR="1")
-    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
-                       timeout=300)
-    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
+@pytest.mark.parametrize("kind,rows,Kp", [(1, 2560, 64), (2, 2560, 128), (2, 4096, 64)])
+def test_partial_raster_group(kind, rows, Kp):
+    """Tiles are walked in raster groups of 16 row tiles.  2560 rows give 20
+    row tiles (one group of 16, then a partial group of 4) and 4096 rows give
+    32 (two whole groups): every product element still meets the bound of the
+    test above, so the raster only reorders the tiles."""
+    test_umma_core_matches_fp64_product(kind, rows, Kp, 0)
 
 
-@pytest.mark.parametrize("group", [7, 64])
-def test_raster_group_size_changes_only_the_tile_order(group):
-    """ASD_UMMA_GROUP_M (row tiles per raster group, read once per process)
-    only reorders the tiles, so in a child process every product element
-    still meets the bound above.  2048 rows give 16 row tiles, i.e. groups of
-    7, 7 and 2, or one group smaller than 64.  S(q,t) through a context
-    (1792 padded rows, 14 row tiles) stays within 1e-5 of the FP64 path."""
-    import os
-    import subprocess
-    import sys
-
-    code = (
-        "import sys; sys.path[:0] = {paths!r}\n"
-        "import test_umma_core_gpu as t\n"
-        "for case in ((1, 2048, 64, 0), (2, 2048, 128, 0)):\n"
-        "    t.test_umma_core_matches_fp64_product(*case)\n"
-        "import asd_b200 as asd\n"
-        "p = asd.Params.make(40, 12, J1=-1.0, alpha=0.05, h=(0, 0, 0.5), dt=0.005, vx=2, vy=1)\n"
-        "with asd.Context(p) as c:\n"
-        "    c.set_spins(asd.random_spins(40, 12, seed=3), as_origin=True)\n"
-        "    c.step(4)\n"
-        "    ref = c.sqt('fp64')\n"
-        "    for m in ('tf32x3', 'bf16x3'):\n"
-        "        assert abs(c.sqt(m) - ref) <= 1e-5 * abs(ref), m\n"
-        "print('ok')\n"
-    ).format(paths=[os.path.dirname(__file__)] + sys.path)
-    env = dict(os.environ, ASD_UMMA_GROUP_M=str(group))
-    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
-                       timeout=300)
-    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
+def test_partial_raster_group_sqt():
+    """S(q,t) through a context whose padded rows (1792 = 14 row tiles) form
+    one partial raster group stays within 1e-5 of the FP64 path."""
+    p = asd.Params.make(40, 12, J1=-1.0, alpha=0.05, h=(0, 0, 0.5), dt=0.005, vx=2, vy=1)
+    with asd.Context(p) as c:
+        c.set_spins(asd.random_spins(40, 12, seed=3), as_origin=True)
+        c.step(4)
+        ref = c.sqt("fp64")
+        for m in ("tf32x3", "bf16x3"):
+            assert abs(c.sqt(m) - ref) <= 1e-5 * abs(ref), m

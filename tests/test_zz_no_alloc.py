@@ -5,8 +5,11 @@ an allocation call would synchronise the device inside their step loop).
 
 The test builds the entry point's inputs itself (split operands and epilogue
 vectors, with torch), calls it twice in a row through the C ABI and compares
-both results with the context API's S(q,t) for the same spins, within the
-split modes' tolerance.  It sits in its own file, collected last."""
+both results with the context API's S(q,t) for the same spins and with the
+oracle's FP64 value, within the split modes' tolerance.  After a first call
+(which may load the library's device code), further calls must leave both
+torch's allocator and the device's free memory unchanged.  It sits in its own
+file, collected last."""
 from __future__ import annotations
 
 import math
@@ -73,7 +76,7 @@ def inputs(torch, spins_t, spins_0, N, nfile, kind, vx):
 
 
 @pytest.mark.parametrize("mode,kind", [("bf16x3", 2), ("tf32x3", 1)])
-def test_noalloc_matches_context_api(mode, kind):
+def test_noalloc_matches_context_api(mode, kind, oracle):
     import torch
 
     N, nfile = 32, 40
@@ -86,16 +89,25 @@ def test_noalloc_matches_context_api(mode, kind):
     rows, Kp, ops, vecs = inputs(torch, st, s0, N, nfile, kind, N // 10)
     out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    got = []
-    for _ in range(2):  # two calls in a row share the fixed scratch
+
+    def call():
         out.fill_(float("nan"))
         asd.sqt_split_noalloc(kind, rows, Kp, *(t.data_ptr() for t in ops),
                               *(v.data_ptr() for v in vecs), 1.0 / nfile, 1.0 / (N * N), 512,
                               out.data_ptr(), stream)
         torch.cuda.synchronize()
-        got.append(complex(*out.tolist()))
+        return complex(*out.tolist())
+
+    call()  # the first call on this device may load the library's device code
+    torch_bytes = torch.cuda.memory_allocated()
+    free_bytes = torch.cuda.mem_get_info()[0]
+    got = [call(), call()]  # two calls in a row share the fixed scratch
+    assert torch.cuda.memory_allocated() == torch_bytes
+    assert torch.cuda.mem_get_info()[0] == free_bytes
+    want = oracle.sqt_factorized(N, nfile, N // 10, N // 10, st, s0)
     for g in got:
         assert rel_err(g, ref) < TOL, (g, ref)
+        assert rel_err(g, want) < TOL, (g, want)
     assert got[0] == got[1]
 
 
