@@ -35,8 +35,7 @@ LLG_AUTO = 2
 SQT_FP64 = 0
 SQT_TF32X3 = 1
 SQT_BF16X3 = 2
-SQT_FP64_FUSED = 3
-MODE_NAMES = {SQT_FP64: "fp64", SQT_TF32X3: "tf32x3", SQT_BF16X3: "bf16x3", SQT_FP64_FUSED: "fp64_fused"}
+MODE_NAMES = {SQT_FP64: "fp64", SQT_TF32X3: "tf32x3", SQT_BF16X3: "bf16x3"}
 MODES = {v: k for k, v in MODE_NAMES.items()}
 
 # every symbol include/asd_b200.h declares
@@ -46,13 +45,15 @@ EXPORTED_SYMBOLS = (
     "asd_ctx_set_params", "asd_ctx_loss_grad",
     "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
+    "asd_ctx_sqt_magnitude",
     "asd_ctx_sqt_grid_async", "asd_ctx_sqt_grid",
     "asd_ctx_step_host", "asd_ctx_step_host_async", "asd_ctx_synchronize", "asd_ctx_set_ensemble", "asd_ctx_shard_origin_sums",
     "asd_ctx_shard_set_origin_sums", "asd_ctx_shard_sqt_async", "asd_ctx_shard_sqt_finish",
     "asd_ctx_set_llg_kernel", "asd_ctx_set_chunk_k",
-    "asd_ctx_last_launches",
+    "asd_ctx_last_launches", "asd_ctx_time_kernels", "asd_ctx_kernel_time",
     "asd_ctx_check_device_status", "asd_debug_fail_alloc", "asd_ctx_debug_poison",
     "asd_check_bounded_wait", "asd_check_const_division", "asd_check_const_division_f32", "asd_umma_gemm_f32", "asd_sqt_split_noalloc",
+    "asd_measure_fp64_peak", "asd_check_dmma_layout",
     "asd_spins_save", "asd_spins_load", "asd_batch_create", "asd_batch_destroy",
     "asd_batch_set_stream", "asd_batch_set_spins", "asd_batch_get_spins", "asd_batch_run",
     "asd_batch_configure", "asd_batch_configure_cluster", "asd_batch_autotune",
@@ -132,6 +133,7 @@ def load() -> C.CDLL:
         "asd_ctx_step": ([vp, C.c_int], C.c_int),
         "asd_ctx_sqt": ([vp, C.c_int, dp], C.c_int),
         "asd_ctx_sqt_async": ([vp, C.c_int, vp], C.c_int),
+        "asd_ctx_sqt_magnitude": ([vp, dp], C.c_int),
         "asd_ctx_sqt_grid_async": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_sqt_grid": ([vp, C.c_int, vp], C.c_int),
         "asd_ctx_step_host": ([vp, vp, vp, C.c_int, dp], C.c_int),
@@ -145,6 +147,10 @@ def load() -> C.CDLL:
         "asd_ctx_set_llg_kernel": ([vp, C.c_int], C.c_int),
         "asd_ctx_set_chunk_k": ([vp, C.c_int], C.c_int),
         "asd_ctx_last_launches": ([vp], C.c_int),
+        "asd_ctx_time_kernels": ([vp, C.c_int], C.c_int),
+        "asd_ctx_kernel_time": ([vp, C.c_int, dp, C.POINTER(C.c_int)], C.c_int),
+        "asd_measure_fp64_peak": ([C.c_int, dp, dp, vp], C.c_int),
+        "asd_check_dmma_layout": ([vp, vp, vp, vp], C.c_int),
         "asd_ctx_check_device_status": ([vp], C.c_int),
         "asd_debug_fail_alloc": ([C.c_long], C.c_int),
         "asd_ctx_debug_poison": ([vp], C.c_int),
@@ -304,6 +310,12 @@ class Context:
         _check(load().asd_ctx_sqt(self._h, mode, self._out))
         return complex(self._out[0], self._out[1])
 
+    def sqt_magnitude(self) -> float:
+        """asd_ctx_sqt_magnitude: (1/M) sum_ij |C_ij - m_i . z_j| in FP64."""
+        v = C.c_double(0.0)
+        _check(load().asd_ctx_sqt_magnitude(self._h, C.byref(v)))
+        return v.value
+
     def sqt_async(self, mode, d_out_ptr: int) -> None:
         mode = MODES[mode] if isinstance(mode, str) else int(mode)
         _check(load().asd_ctx_sqt_async(self._h, mode, C.c_void_p(d_out_ptr)))
@@ -369,6 +381,20 @@ class Context:
     def last_launches(self) -> int:
         return int(load().asd_ctx_last_launches(self._h))
 
+    def time_kernels(self, on: bool = True) -> None:
+        """asd_ctx_time_kernels: record CUDA events around the RK4 step kernels
+        and the S(q,t) GEMM on the stream each is launched on."""
+        _check(load().asd_ctx_time_kernels(self._h, int(bool(on))))
+
+    def kernel_time(self, which: str):
+        """asd_ctx_kernel_time: (total ms, launches) of the timed RK4 step
+        kernels ("llg") or S(q,t) GEMMs ("gemm") since the last read."""
+        ms = C.c_double(0.0)
+        n = C.c_int(0)
+        _check(load().asd_ctx_kernel_time(self._h, {"llg": 0, "gemm": 1}[which], C.byref(ms),
+                                          C.byref(n)))
+        return ms.value, n.value
+
     def check_device_status(self) -> None:
         _check(load().asd_ctx_check_device_status(self._h))
 
@@ -424,6 +450,22 @@ def umma_gemm_f32(kind: int, rows: int, Kp: int, a_hi: int, a_lo: int, b_hi: int
     _check(load().asd_umma_gemm_f32(int(kind), int(rows), int(Kp), C.c_void_p(a_hi),
                                     C.c_void_p(a_lo), C.c_void_p(b_hi), C.c_void_p(b_lo),
                                     C.c_void_p(c), int(ldc), int(chunk_k), C.c_void_p(stream)))
+
+
+def measure_fp64_peak(which: str, stream: int = 0):
+    """asd_measure_fp64_peak: (TFLOP/s, ms) of the FP64 FMA ("fma") or FP64
+    tensor-core MMA ("dmma") throughput kernel on the current device."""
+    tf = C.c_double(0.0)
+    ms = C.c_double(0.0)
+    _check(load().asd_measure_fp64_peak({"fma": 0, "dmma": 1}[which], C.byref(tf), C.byref(ms),
+                                        C.c_void_p(stream)))
+    return tf.value, ms.value
+
+
+def check_dmma_layout(A: int, B: int, D: int, stream: int = 0) -> None:
+    """asd_check_dmma_layout on device pointers (diagnostic)."""
+    _check(load().asd_check_dmma_layout(C.c_void_p(A), C.c_void_p(B), C.c_void_p(D),
+                                        C.c_void_p(stream)))
 
 
 def sqt_split_noalloc(kind: int, rows: int, Kp: int, a_hi: int, a_lo: int, b_hi: int, b_lo: int,

@@ -109,19 +109,34 @@ cudaError_t launch_split_range(int kind, const double *state, long M, int K, int
 cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, void *hi,
                          void *lo, cudaStream_t st);
 
-// Plain FP64 epilogue over a band of C (rows [i0, i0+mb), all n columns,
-// column-major, ldc = mb), C already scaled by 1/nfile: partial sums of
-// u_i w_j (C_ij - m_i . z_j) per block into part[2*block].
-cudaError_t launch_plain_epilogue(const double *C, long i0, long mb, long n, const double *mrow,
-                                  const double *zcol, const double2 *uphase,
-                                  const double2 *wphase, double2 *part, int nblocks_x,
-                                  int nblocks_y, cudaStream_t st);
+// ------------------------------------------ FP64 tensor-core GEMM S(q,t)
+// (dmma_sqt.cu) C = alpha A B^T over site-major [M][K] FP64 operands, never
+// stored: per 128 x 128 tile either the S(q,t) partial (part != nullptr and
+// tdiag == nullptr) or the q-grid diagonal partials (tdiag != nullptr).
+struct DmmaSqtArgs {
+    const double *A, *B;  // [M][K], the state at t and the origin
+    long M;
+    int K;
+    double alpha;
+    int outer;            // subtract m_i . z_j (0: a shard's partial GEMM value)
+    const double *mrow, *zcol;       // [M][3] replica means at t and 0
+    const double2 *uphase, *wphase;  // [M]
+    double2 *part;        // one partial per tile, dmma_sqt_tiles(M) of them
+    int lat_n = 0;        // q grid: lattice side
+    double *tdiag = nullptr;  // q grid: [tiles][dmma_sqt_tile() * 2 - 1][2]
+    int abs_sum = 0;      // sum |alpha C_ij - m_i . z_j| instead (no phase)
+};
+constexpr int kDmmaTile = 128;  // tile rows = tile columns
+long dmma_sqt_tiles(long M);
+int launch_dmma_sqt(const DmmaSqtArgs &p, cudaStream_t st);
 
-// q grid, FP64 path: bins alpha-scaled C band elements minus m_i . z_j by
-// displacement into per-block FP64 histograms gpart[block][N*N].
-cudaError_t launch_bin_band(const double *C, long i0, long mb, long n, int lat_n,
-                            const double *mrow, const double *zcol, double *gpart, int nblocks_x,
-                            int nblocks_y, cudaStream_t st);
+// q grid (qgrid.cu): from per-tile diagonal partials tdiag[mb][nb][bm+bn-1][2]
+// of num_m x num_n tiles of bm x bn sites (bn a multiple of bm) to the N*N
+// displacement bins G, in a fixed order; ds holds qgrid_keys() * (bm+bn-1) * 2
+// doubles of work space.
+long qgrid_keys(int num_m, int num_n, int bm, int bn);
+cudaError_t launch_qgrid_bins(const double *tdiag, int num_m, int num_n, int bm, int bn, int lat_n,
+                              double *ds, double *G, cudaStream_t st);
 // G[b] = sum over p < nparts of gpart[p][b], fixed order.
 cudaError_t launch_hist_reduce(const double *gpart, int nparts, int nbins, double *G,
                                cudaStream_t st);

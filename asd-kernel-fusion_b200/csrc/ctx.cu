@@ -7,9 +7,8 @@
 //   y, ys_a, ys_b, acc   RK4 state, stage inputs, running combination  4*M*K
 //   origin               the t = 0 snapshot (B of the GEMM)               M*K
 //   a/b hi/lo            split operands, [Mp][Kp] per enabled split kind
-//   band                 C band of the plain FP64 path (<= 2 GiB)
+//   q-grid work          per-tile diagonal partials (on the first q grid)
 // The AoS <-> site-major transposes stage through ys_b.
-#include <cublas_v2.h>
 
 #include <atomic>
 #include <cstdarg>
@@ -19,7 +18,6 @@
 #include <vector>
 
 #include "asd_internal.h"
-#include "fp64_gemm.h"
 
 namespace asd {
 
@@ -71,14 +69,11 @@ struct asd_ctx {
     int Kp[3] = {};
     long a_version[3] = {-1, -1, -1};
     long b_version[3] = {-1, -1, -1};
-    double *band = nullptr;
-    long band_rows = 0;
     double2 *part = nullptr;
     long part_cap = 0;
     double *d_out = nullptr;
     double *h_out = nullptr;  // pinned
     unsigned *status = nullptr;
-    cublasHandle_t blas = nullptr;
     long state_version = 0, origin_version = -1;
     bool has_state = false, has_origin = false;
     int last_launches = 0;
@@ -86,6 +81,10 @@ struct asd_ctx {
     double *grid_g = nullptr;     // q grid: N*N displacement bins (FP64)
     double2 *grid_t = nullptr;    // q grid: DFT intermediate
     double *grid_out = nullptr;   // q grid: device result for the host-buffer form
+    double *grid_tdiag = nullptr; // q grid: per-tile diagonal partials
+    size_t grid_tdiag_n = 0;
+    double *grid_ds = nullptr;    // q grid: diagonal partials summed by tile key
+    size_t grid_ds_n = 0;
     // adjoint work space (allocated on the first asd_ctx_loss_grad)
     std::vector<double *> adj_bufs;
     long adj_states = 0;
@@ -128,10 +127,20 @@ struct asd_ctx {
                 ast_out_ready[kAsyncChunks] = {}, ast_out_done[kAsyncChunks] = {};
     // Replica sharding: this context holds nfile of the nfile_total replicas
     // of one ensemble (0: not sharded); zsums = the ensemble's origin site
-    // sums once exchanged; zero3 = zero means for the FP64 partial GEMMs.
+    // sums once exchanged.
     int nfile_total = 0;
-    double *zsums = nullptr, *zero3 = nullptr;
+    double *zsums = nullptr;
     bool has_zsums = false;
+    // asd_ctx_time_kernels: CUDA events recorded on the launching stream
+    // around the RK4 step kernels (which = 0) and the S(q,t) GEMM (which = 1),
+    // read and recycled by asd_ctx_kernel_time.
+    struct Timed {
+        int which, launches;
+        cudaEvent_t b, e;
+    };
+    bool timing = false;
+    std::vector<Timed> timed;
+    std::vector<cudaEvent_t> ev_pool;
 };
 
 namespace {
@@ -247,6 +256,47 @@ int join_gemm(asd_ctx *c, cudaStream_t gemm) {
     return ASD_OK;
 }
 
+// Kernel timing: an event recorded on stream s before a timed launch (null
+// when timing is off or s is being captured into a graph).
+cudaEvent_t time_begin(asd_ctx *c, cudaStream_t s) {
+    if (!c->timing || stream_capturing(s)) return nullptr;
+    cudaEvent_t ev = nullptr;
+    if (!c->ev_pool.empty()) {
+        ev = c->ev_pool.back();
+        c->ev_pool.pop_back();
+    } else if (cudaEventCreate(&ev) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (cudaEventRecord(ev, s) != cudaSuccess) {
+        cudaGetLastError();
+        c->ev_pool.push_back(ev);
+        return nullptr;
+    }
+    return ev;
+}
+
+// ... and after it: the pair is kept for asd_ctx_kernel_time.
+void time_end(asd_ctx *c, int which, int launches, cudaStream_t s, cudaEvent_t b) {
+    if (!b) return;
+    cudaEvent_t ev = nullptr;
+    if (!c->ev_pool.empty()) {
+        ev = c->ev_pool.back();
+        c->ev_pool.pop_back();
+    } else if (cudaEventCreate(&ev) != cudaSuccess) {
+        cudaGetLastError();
+        c->ev_pool.push_back(b);
+        return;
+    }
+    if (cudaEventRecord(ev, s) != cudaSuccess) {
+        cudaGetLastError();
+        c->ev_pool.push_back(b);
+        c->ev_pool.push_back(ev);
+        return;
+    }
+    c->timed.push_back({which, launches, b, ev});
+}
+
 int refresh_origin(asd_ctx *c) {
     // origin mean and the column epilogue vectors
     ASD_CUDA_TRY(launch_site_mean(c->origin, c->M, c->p.nfile, c->wphase, c->mean_0, c->col4,
@@ -287,7 +337,9 @@ bool use_fused(const asd_ctx *c, const LLGArgs &a) {
 int run_steps(asd_ctx *c, int nsteps) {
     if (use_fused(c, c->a)) {
         for (int s = 0; s < nsteps; ++s) {
+            cudaEvent_t t0 = time_begin(c, c->stream);
             ASD_CUDA_TRY(launch_llg_step_fused(c->a, c->y, c->ys_a, c->stream));
+            time_end(c, 0, 1, c->stream, t0);
             double *t = c->y;  // ping-pong: the new state becomes y
             c->y = c->ys_a;
             c->ys_a = t;
@@ -297,22 +349,15 @@ int run_steps(asd_ctx *c, int nsteps) {
         return ASD_OK;
     }
     for (int s = 0; s < nsteps; ++s) {
+        cudaEvent_t t0 = time_begin(c, c->stream);
         ASD_CUDA_TRY(launch_llg_stage(1, c->a, c->y, c->y, c->acc, c->ys_a, c->stream));
         ASD_CUDA_TRY(launch_llg_stage(2, c->a, c->y, c->ys_a, c->acc, c->ys_b, c->stream));
         ASD_CUDA_TRY(launch_llg_stage(3, c->a, c->y, c->ys_b, c->acc, c->ys_a, c->stream));
         ASD_CUDA_TRY(launch_llg_stage(4, c->a, nullptr, c->ys_a, c->acc, c->y, c->stream));
+        time_end(c, 0, 4, c->stream, t0);
         c->last_launches += 4;
         c->state_version++;
     }
-    return ASD_OK;
-}
-
-// Zero site means: the FP64 GEMM paths without their connected-part term.
-int ensure_zero3(asd_ctx *c) {
-    if (c->zero3) return ASD_OK;
-    int rc = dalloc(&c->zero3, (size_t)c->M * 3 * sizeof(double));
-    if (rc != ASD_OK) return rc;
-    ASD_CUDA_TRY(cudaMemset(c->zero3, 0, (size_t)c->M * 3 * sizeof(double)));
     return ASD_OK;
 }
 
@@ -323,72 +368,35 @@ double gemm_alpha(const asd_ctx *c, bool shard) {
     return 1.0 / (double)((shard && c->nfile_total > 0) ? c->nfile_total : c->p.nfile);
 }
 
-int sqt_plain(asd_ctx *c, double *d_out, bool shard) {
-    const long M = c->M;
-    const int K = c->K;
-    const double alpha = gemm_alpha(c, shard);
-    if (shard) {
-        int rc = ensure_zero3(c);
-        if (rc != ASD_OK) return rc;
-    }
-    const double *mrow = shard ? c->zero3 : c->mean_t, *zcol = shard ? c->zero3 : c->mean_0;
-    const double beta = 0.0;
-    const long mb = c->band_rows;
-    const int nby = 64;
-    long nparts = 0;
-    for (long i0 = 0; i0 < M; i0 += mb) {
-        const long rows = (M - i0 < mb) ? M - i0 : mb;
-        nparts += ((rows + 127) / 128) * nby;
-    }
-    int rc = ensure_part(c, nparts);
-    if (rc != ASD_OK) return rc;
-    long off = 0;
-    for (long i0 = 0; i0 < M; i0 += mb) {
-        const long rows = (M - i0 < mb) ? M - i0 : mb;
-        cublasStatus_t bs =
-            cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)rows, (int)M, K, &alpha,
-                        c->y + i0 * K, K, c->origin, K, &beta, c->band, (int)rows);
-        if (bs != CUBLAS_STATUS_SUCCESS) return fail(ASD_ERR_CUDA, "cublasDgemm failed (%d)", (int)bs);
-        const int nbx = (int)((rows + 127) / 128);
-        ASD_CUDA_TRY(launch_plain_epilogue(c->band, i0, rows, M, mrow, zcol, c->uphase,
-                                           c->wphase, c->part + off, nbx, nby, c->stream));
-        off += (long)nbx * nby;
-        c->last_launches += 1;  // the epilogue; the DGEMM is cuBLAS's
-    }
-    ASD_CUDA_TRY(launch_finalize(c->part, (int)off, 1.0 / (double)M, d_out, c->stream));
-    c->last_launches += 1;
-    return ASD_OK;
-}
-
-int sqt_fp64_fused(asd_ctx *c, double *d_out, bool shard) {
-    if (shard) {
-        int rc = ensure_zero3(c);
-        if (rc != ASD_OK) return rc;
-    }
-    Fp64GemmArgs g{};
-    g.dropin = 0;
-    g.m = c->M;
-    g.n = c->M;
-    g.k = c->K;
-    g.a = c->y;
-    g.sai = c->K;
-    g.sak = 1;
-    g.a_k_fast = 1;
-    g.b = c->origin;
-    g.sbk = 1;
-    g.sbj = c->K;
-    g.b_k_fast = 1;
+// The plain FP64 path: the FP64 tensor-core GEMM with the fused epilogue,
+// one partial per tile, then the fixed-order final sum.
+DmmaSqtArgs dmma_args(const asd_ctx *c, bool shard) {
+    DmmaSqtArgs g{};
+    g.A = c->y;
+    g.B = c->origin;
+    g.M = c->M;
+    g.K = c->K;
     g.alpha = gemm_alpha(c, shard);
-    g.mrow = shard ? c->zero3 : c->mean_t;
-    g.zcol = shard ? c->zero3 : c->mean_0;
+    g.outer = shard ? 0 : 1;
+    g.mrow = c->mean_t;
+    g.zcol = c->mean_0;
     g.uphase = c->uphase;
     g.wphase = c->wphase;
-    const long np = fp64_gemm_num_parts(g);
-    int rc = ensure_part(c, np);
+    return g;
+}
+
+int sqt_plain(asd_ctx *c, double *d_out, bool shard) {
+    const long tiles = dmma_sqt_tiles(c->M);
+    if (tiles > 0x7fffffffL) return fail(ASD_ERR_UNSUPPORTED, "lattice too large for the FP64 GEMM");
+    int rc = ensure_part(c, tiles);
     if (rc != ASD_OK) return rc;
+    DmmaSqtArgs g = dmma_args(c, shard);
     g.part = c->part;
-    ASD_CUDA_TRY(launch_fp64_gemm(g, c->stream));
-    ASD_CUDA_TRY(launch_finalize(c->part, (int)np, 1.0 / (double)c->M, d_out, c->stream));
+    cudaEvent_t t0 = time_begin(c, c->stream);
+    rc = launch_dmma_sqt(g, c->stream);
+    time_end(c, 1, 1, c->stream, t0);
+    if (rc != ASD_OK) return rc;
+    ASD_CUDA_TRY(launch_finalize(c->part, (int)tiles, 1.0 / (double)c->M, d_out, c->stream));
     c->last_launches += 2;
     return ASD_OK;
 }
@@ -432,7 +440,9 @@ int sqt_split(asd_ctx *c, int kind, double *d_out, bool shard) {
     // Same number of tensor-core accumulation steps per chunk for both kinds
     // (TF32 MMAs take 8 K elements per step, BF16 ones 16).
     u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
+    cudaEvent_t t0 = time_begin(c, gemm);
     const int grid = launch_umma_sqt(u, gemm);
+    time_end(c, 1, 1, gemm, t0);
     if (grid >= 0) {
         const cudaError_t e = launch_finalize(c->part, grid, 1.0 / (double)c->M, d_out, gemm);
         if (e != cudaSuccess) rc = cuda_fail(e, "launch_finalize");
@@ -447,7 +457,7 @@ int sqt_split(asd_ctx *c, int kind, double *d_out, bool shard) {
 int sqt_async(asd_ctx *c, int mode, double *d_out, bool shard = false) {
     if (!c->has_state || !c->has_origin)
         return fail(ASD_ERR_STATE, "set the spins and the origin before S(q,t)");
-    if (mode < 0 || mode > 3) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
+    if (mode < 0 || mode > 2) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
     if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
     ASD_CUDA_TRY(launch_site_mean(c->y, c->M, c->p.nfile, c->uphase, c->mean_t, c->row4, c->row1,
                                   c->stream));
@@ -455,7 +465,6 @@ int sqt_async(asd_ctx *c, int mode, double *d_out, bool shard = false) {
     c->last_launches += 1;
     switch (mode) {
         case ASD_SQT_FP64: return sqt_plain(c, d_out, shard);
-        case ASD_SQT_FP64_FUSED: return sqt_fp64_fused(c, d_out, shard);
         case ASD_SQT_TF32X3: return sqt_split(c, 1, d_out, shard);
         case ASD_SQT_BF16X3: return sqt_split(c, 2, d_out, shard);
     }
@@ -602,18 +611,38 @@ int loss_grad(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target
     return ASD_OK;
 }
 
-constexpr int kGridMaxSites = 4096;
+constexpr int kGridMaxSitesSplit = 4096;  // split modes: bins in shared memory
+
+// Work space of the q grid's diagonal partials, grown on demand.
+int ensure_grid_work(asd_ctx *c, size_t tdiag_n, size_t ds_n) {
+    int rc;
+    if (tdiag_n > c->grid_tdiag_n) {
+        if (c->grid_tdiag) cudaFree(c->grid_tdiag);
+        c->grid_tdiag = nullptr;
+        c->grid_tdiag_n = 0;
+        if ((rc = dalloc(&c->grid_tdiag, tdiag_n * sizeof(double))) != ASD_OK) return rc;
+        c->grid_tdiag_n = tdiag_n;
+    }
+    if (ds_n > c->grid_ds_n) {
+        if (c->grid_ds) cudaFree(c->grid_ds);
+        c->grid_ds = nullptr;
+        c->grid_ds_n = 0;
+        if ((rc = dalloc(&c->grid_ds, ds_n * sizeof(double))) != ASD_OK) return rc;
+        c->grid_ds_n = ds_n;
+    }
+    return ASD_OK;
+}
 
 int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
     if (!c->has_state || !c->has_origin)
         return fail(ASD_ERR_STATE, "set the spins and the origin before S(q,t)");
     const int N = c->p.N;
     const long M = c->M;
-    if (M > kGridMaxSites)
-        return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t) supports N*N <= %d sites (N=%d)",
-                    kGridMaxSites, N);
     if (mode != ASD_SQT_FP64 && mode != ASD_SQT_TF32X3 && mode != ASD_SQT_BF16X3)
         return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t): mode %d not supported", mode);
+    if (mode != ASD_SQT_FP64 && M > kGridMaxSitesSplit)
+        return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t) in split precision supports N*N <= %d sites (N=%d)",
+                    kGridMaxSitesSplit, N);
     if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
     int rc;
     // each checked on its own: after a failed allocation of grid_t, grid_g
@@ -624,30 +653,25 @@ int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
                                   c->stream));
     c->rows_ready = true;
     c->last_launches += 1;
-    int nparts = 0;
     if (mode == ASD_SQT_FP64) {
-        const double alpha = 1.0 / (double)c->p.nfile, beta = 0.0;
-        const long mb = c->band_rows;
-        const int nby = 8;
-        long total = 0;
-        for (long i0 = 0; i0 < M; i0 += mb) total += ((((M - i0 < mb) ? M - i0 : mb) + 127) / 128) * nby;
-        if ((rc = ensure_part(c, (total * M + 1) / 2)) != ASD_OK) return rc;
-        double *gpart = reinterpret_cast<double *>(c->part);
-        long off = 0;
-        for (long i0 = 0; i0 < M; i0 += mb) {
-            const long rows = (M - i0 < mb) ? M - i0 : mb;
-            cublasStatus_t bs =
-                cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)rows, (int)M, c->K, &alpha,
-                            c->y + i0 * c->K, c->K, c->origin, c->K, &beta, c->band, (int)rows);
-            if (bs != CUBLAS_STATUS_SUCCESS) return fail(ASD_ERR_CUDA, "cublasDgemm failed (%d)", (int)bs);
-            const int nbx = (int)((rows + 127) / 128);
-            ASD_CUDA_TRY(launch_bin_band(c->band, i0, rows, M, N, c->mean_t, c->mean_0,
-                                         gpart + off * M, nbx, nby, c->stream));
-            off += (long)nbx * nby;
-            c->last_launches += 1;
-        }
-        nparts = (int)off;
-    } else {
+        const long nm = (M + kDmmaTile - 1) / kDmmaTile;
+        if (nm * nm > 0x7fffffffL) return fail(ASD_ERR_UNSUPPORTED, "lattice too large for the FP64 GEMM");
+        const size_t nd2 = 2 * (2 * kDmmaTile - 1);
+        rc = ensure_grid_work(c, (size_t)(nm * nm) * nd2,
+                              (size_t)qgrid_keys((int)nm, (int)nm, kDmmaTile, kDmmaTile) * nd2);
+        if (rc != ASD_OK) return rc;
+        DmmaSqtArgs g = dmma_args(c, false);
+        g.lat_n = N;
+        g.tdiag = c->grid_tdiag;
+        if ((rc = launch_dmma_sqt(g, c->stream)) != ASD_OK) return rc;
+        ASD_CUDA_TRY(launch_qgrid_bins(c->grid_tdiag, (int)nm, (int)nm, kDmmaTile, kDmmaTile, N,
+                                       c->grid_ds, c->grid_g, c->stream));
+        ASD_CUDA_TRY(launch_grid_dft(c->grid_g, N, 1.0 / (double)M, c->grid_t, d_out, c->stream));
+        c->last_launches += 5;
+        return ASD_OK;
+    }
+    int nparts = 0;
+    {
         const int kind = (mode == ASD_SQT_TF32X3) ? 1 : 2;
         if (!c->a_hi[kind]) return fail(ASD_ERR_STATE, "split mode %d not enabled at create", kind);
         if (c->a_version[kind] != c->state_version) {
@@ -765,7 +789,7 @@ int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int m
     const int nf = c->p.nfile;
     const long M = c->M;
     const int kind = (mode == ASD_SQT_TF32X3) ? 1 : (mode == ASD_SQT_BF16X3) ? 2 : 0;
-    if (mode < 0 || mode > 3) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
+    if (mode < 0 || mode > 2) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
     if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
     int rc = ensure_host_pipeline(c, cr);
     if (rc != ASD_OK) return rc;
@@ -976,7 +1000,7 @@ void destroy(asd_ctx *c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     void *ptrs[] = {c->y, c->ys_a, c->ys_b, c->acc, c->origin, c->mean_t, c->mean_0, c->uphase,
-                    c->wphase, c->row4, c->col4, c->row1, c->col1, c->band, c->part, c->d_out,
+                    c->wphase, c->row4, c->col4, c->row1, c->col1, c->grid_tdiag, c->grid_ds, c->part, c->d_out,
                     c->status, c->grid_g, c->grid_t, c->grid_out};
     for (void *q : ptrs)
         if (q) cudaFree(q);
@@ -1019,10 +1043,13 @@ void destroy(asd_ctx *c) {
     }
     if (c->gemm_done) cudaEventDestroy(c->gemm_done);
     if (c->zsums) cudaFree(c->zsums);
-    if (c->zero3) cudaFree(c->zero3);
     if (c->y_free) cudaEventDestroy(c->y_free);
     if (c->llg_done) cudaEventDestroy(c->llg_done);
-    if (c->blas) cublasDestroy(c->blas);
+    for (auto &t : c->timed) {
+        cudaEventDestroy(t.b);
+        cudaEventDestroy(t.e);
+    }
+    for (cudaEvent_t ev : c->ev_pool) cudaEventDestroy(ev);
     delete c;
 }
 
@@ -1080,7 +1107,11 @@ int asd_ctx_create(const asd_params *p, unsigned mode_mask, asd_ctx **out) {
     c->M = (long)p->N * p->N;
     c->Mp = umma_row_pad(c->M);
     c->K = 3 * p->nfile;
-    c->modes = mode_mask ? mode_mask : 0xFu;
+    if (mode_mask & ~0x7u) {
+        delete c;
+        return fail(ASD_ERR_INVALID, "mode_mask 0x%x has bits beyond the three S(q,t) modes", mode_mask);
+    }
+    c->modes = mode_mask ? mode_mask : 0x7u;
     const size_t sbytes = (size_t)c->M * c->K * sizeof(double);
 #define ASD_ALLOC(ptr, bytes)                 \
     do {                                      \
@@ -1116,18 +1147,6 @@ int asd_ctx_create(const asd_params *p, unsigned mode_mask, asd_ctx **out) {
         ASD_CUDA_TRY(cudaMemset(c->a_lo[kind], 0, ob));
         ASD_CUDA_TRY(cudaMemset(c->b_hi[kind], 0, ob));
         ASD_CUDA_TRY(cudaMemset(c->b_lo[kind], 0, ob));
-    }
-    if (c->modes & (1u << ASD_SQT_FP64)) {
-        long mb = (long)((2048.0 * 1024 * 1024) / (8.0 * c->M));
-        mb = mb / 128 * 128;
-        if (mb < 128) mb = 128;
-        if (mb > c->M) mb = c->M;
-        c->band_rows = mb;
-        ASD_ALLOC(c->band, (size_t)mb * c->M * sizeof(double));
-        if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) {
-            destroy(c);
-            return fail(ASD_ERR_CUDA, "cublasCreate failed");
-        }
     }
 #undef ASD_ALLOC
     ASD_CUDA_TRY(cudaMemset(c->row4, 0, (size_t)c->Mp * sizeof(float4)));
@@ -1175,7 +1194,6 @@ int asd_ctx_set_stream(asd_ctx *c, void *stream) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
     c->y_free_armed = false;
     c->stream = (cudaStream_t)stream;
-    if (c->blas) cublasSetStream(c->blas, c->stream);
     return ASD_OK;
 }
 
@@ -1298,6 +1316,33 @@ int asd_ctx_sqt_grid(asd_ctx *c, asd_sqt_mode mode, double *out) {
     if ((rc = sqt_grid_async(c, (int)mode, c->grid_out)) != ASD_OK) return rc;
     ASD_CUDA_TRY(cudaMemcpyAsync(out, c->grid_out, bytes, cudaMemcpyDeviceToHost, c->stream));
     return read_status(c);  // synchronises
+}
+
+int asd_ctx_sqt_magnitude(asd_ctx *c, double *out) {
+    if (!c || !out) return fail(ASD_ERR_INVALID, "NULL argument");
+    if (!c->has_state || !c->has_origin)
+        return fail(ASD_ERR_STATE, "set the spins and the origin before S(q,t)");
+    if (!(c->modes & (1u << ASD_SQT_FP64))) return fail(ASD_ERR_STATE, "the FP64 mode is not enabled");
+    ASD_CUDA_TRY(enter(c));
+    c->last_launches = 0;
+    ASD_CUDA_TRY(launch_site_mean(c->y, c->M, c->p.nfile, c->uphase, c->mean_t, c->row4, c->row1,
+                                  c->stream));
+    c->rows_ready = true;
+    const long tiles = dmma_sqt_tiles(c->M);
+    int rc = ensure_part(c, tiles);
+    if (rc != ASD_OK) return rc;
+    DmmaSqtArgs g = dmma_args(c, false);
+    g.part = c->part;
+    g.abs_sum = 1;
+    if ((rc = launch_dmma_sqt(g, c->stream)) != ASD_OK) return rc;
+    ASD_CUDA_TRY(launch_finalize(c->part, (int)tiles, 1.0 / (double)c->M, c->d_out, c->stream));
+    c->last_launches = 3;
+    ASD_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    rc = read_status(c);  // synchronises
+    if (rc != ASD_OK) return rc;
+    *out = c->h_out[0];
+    return ASD_OK;
 }
 
 int asd_ctx_sqt(asd_ctx *c, asd_sqt_mode mode, double out[2]) {
@@ -1465,6 +1510,40 @@ int asd_ctx_set_chunk_k(asd_ctx *c, int chunk_k) {
 
 int asd_ctx_last_launches(const asd_ctx *c) { return c ? c->last_launches : 0; }
 
+int asd_ctx_time_kernels(asd_ctx *c, int on) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    c->timing = (on != 0);
+    return ASD_OK;
+}
+
+int asd_ctx_kernel_time(asd_ctx *c, int which, double *ms, int *launches) {
+    if (!c || !ms || !launches) return fail(ASD_ERR_INVALID, "NULL argument");
+    if (which != 0 && which != 1) return fail(ASD_ERR_INVALID, "which must be 0 or 1");
+    ASD_CUDA_TRY(cudaSetDevice(c->device));
+    double total = 0.0;
+    int n = 0;
+    std::vector<asd_ctx::Timed> keep;
+    int rc = ASD_OK;
+    for (auto &t : c->timed) {
+        if (t.which != which) {
+            keep.push_back(t);
+            continue;
+        }
+        float dt = 0.f;
+        cudaError_t e = cudaEventSynchronize(t.e);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&dt, t.b, t.e);
+        if (e != cudaSuccess && rc == ASD_OK) rc = cuda_fail(e, "cudaEventElapsedTime");
+        total += dt;
+        n += t.launches;
+        c->ev_pool.push_back(t.b);
+        c->ev_pool.push_back(t.e);
+    }
+    c->timed.swap(keep);
+    *ms = total;
+    *launches = n;
+    return rc;
+}
+
 int asd_ctx_check_device_status(asd_ctx *c) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
     ASD_CUDA_TRY(enter(c));
@@ -1479,8 +1558,8 @@ int asd_debug_fail_alloc(long n) {
 
 // Every device buffer of the context whose contents do not carry over from
 // one call to the next: RK4 stage states and the running combination, the
-// replica means at t, the FP64 path's C band, the GEMM partials and result,
-// the q-grid bins and result, the host-step staging and the adjoint's
+// replica means at t, the GEMM partials and result, the q-grid diagonal
+// partials, bins and result, the host-step staging and the adjoint's
 // state-sized work buffers (checkpoints, recomputed states, adjoint
 // variables).  Kept as they are: the spins, the origin and its means, the
 // phases, the epilogue vectors and the split operands (their padding rows
@@ -1503,7 +1582,8 @@ int asd_ctx_debug_poison(asd_ctx *c) {
         {c->ys_b, sb},
         {c->acc, sb},
         {c->mean_t, (size_t)c->M * 3 * sizeof(double)},
-        {c->band, (size_t)c->band_rows * c->M * sizeof(double)},
+        {c->grid_tdiag, c->grid_tdiag_n * sizeof(double)},
+        {c->grid_ds, c->grid_ds_n * sizeof(double)},
         {c->part, (size_t)c->part_cap * sizeof(double2)},
         {c->d_out, 2 * sizeof(double)},
         {c->grid_g, (size_t)c->M * sizeof(double)},

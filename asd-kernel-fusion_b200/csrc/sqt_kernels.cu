@@ -171,77 +171,6 @@ __global__ void __launch_bounds__(256) split_bf16_kernel(const double *__restric
     lo[o] = __halves2bfloat162(l0, l1);
 }
 
-// Plain FP64 epilogue.  Block (bx, by): rows [i0 + 128*bx, +128) of the band,
-// columns j = by, by + gridDim.y, ...  Thread = one row; a warp reads 32
-// consecutive rows of one column (coalesced, column-major C).
-__global__ void __launch_bounds__(128) plain_epilogue_kernel(
-    const double *__restrict__ C, long i0, long mb, long n, const double *__restrict__ mrow,
-    const double *__restrict__ zcol, const double2 *__restrict__ uphase,
-    const double2 *__restrict__ wphase, double2 *__restrict__ part) {
-    const long li = (long)blockIdx.x * 128 + threadIdx.x;
-    double tre = 0.0, tim = 0.0;
-    if (li < mb) {
-        const long i = i0 + li;
-        const double mx = mrow[i * 3], my = mrow[i * 3 + 1], mz = mrow[i * 3 + 2];
-        double sre = 0.0, sim = 0.0;
-        for (long j = blockIdx.y; j < n; j += gridDim.y) {
-            const double outer = mx * zcol[j * 3] + my * zcol[j * 3 + 1] + mz * zcol[j * 3 + 2];
-            const double v = C[li + j * mb] - outer;
-            const double2 w = wphase[j];
-            sre += w.x * v;
-            sim += w.y * v;
-        }
-        const double2 u = uphase[i];
-        tre = u.x * sre - u.y * sim;
-        tim = u.x * sim + u.y * sre;
-    }
-    __shared__ double red[2][4];
-    tre = warp_sum(tre);
-    tim = warp_sum(tim);
-    if ((threadIdx.x & 31) == 0) {
-        red[0][threadIdx.x / 32] = tre;
-        red[1][threadIdx.x / 32] = tim;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const double a = (red[0][0] + red[0][1]) + (red[0][2] + red[0][3]);
-        const double b = (red[1][0] + red[1][1]) + (red[1][2] + red[1][3]);
-        part[(long)blockIdx.y * gridDim.x + blockIdx.x] = make_double2(a, b);
-    }
-}
-
-// q grid, FP64 path.  Block (bx, by): rows [i0 + 128 bx, +128) of the band,
-// columns by, by + gridDim.y, ...; each element C_ij - m_i . z_j goes to bin
-// (r_i - r_j, c_i - c_j) mod N of a shared FP64 histogram, which the block
-// then writes to its own slice of gpart.
-__global__ void __launch_bounds__(128) bin_band_kernel(const double *__restrict__ C, long i0,
-                                                       long mb, long n, int N,
-                                                       const double *__restrict__ mrow,
-                                                       const double *__restrict__ zcol,
-                                                       double *__restrict__ gpart) {
-    extern __shared__ double hist[];
-    const int nbins = N * N;
-    for (int b = threadIdx.x; b < nbins; b += 128) hist[b] = 0.0;
-    __syncthreads();
-    const long li = (long)blockIdx.x * 128 + threadIdx.x;
-    if (li < mb) {
-        const long i = i0 + li;
-        const int ri = (int)(i / N), ci = (int)(i % N);
-        const double mx = mrow[i * 3], my = mrow[i * 3 + 1], mz = mrow[i * 3 + 2];
-        for (long j = blockIdx.y; j < n; j += gridDim.y) {
-            const double outer = mx * zcol[j * 3] + my * zcol[j * 3 + 1] + mz * zcol[j * 3 + 2];
-            const double v = C[li + j * mb] - outer;
-            int dr = ri - (int)(j / N), dc = ci - (int)(j % N);
-            dr += (dr < 0) ? N : 0;
-            dc += (dc < 0) ? N : 0;
-            atomicAdd(&hist[dr * N + dc], v);
-        }
-    }
-    __syncthreads();
-    double *g = gpart + ((long)blockIdx.y * gridDim.x + blockIdx.x) * nbins;
-    for (int b = threadIdx.x; b < nbins; b += 128) g[b] = hist[b];
-}
-
 __global__ void hist_reduce_kernel(const double *__restrict__ gpart, int nparts, int nbins,
                                    double *__restrict__ G) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -357,23 +286,7 @@ cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, v
     return launch_split_range(kind, state, M, K, Kp, 0, Kp, hi, lo, st);
 }
 
-cudaError_t launch_plain_epilogue(const double *C, long i0, long mb, long n, const double *mrow,
-                                  const double *zcol, const double2 *uphase,
-                                  const double2 *wphase, double2 *part, int nblocks_x,
-                                  int nblocks_y, cudaStream_t st) {
-    dim3 grid((unsigned)nblocks_x, (unsigned)nblocks_y);
-    plain_epilogue_kernel<<<grid, 128, 0, st>>>(C, i0, mb, n, mrow, zcol, uphase, wphase, part);
-    return cudaGetLastError();
-}
 
-cudaError_t launch_bin_band(const double *C, long i0, long mb, long n, int lat_n,
-                            const double *mrow, const double *zcol, double *gpart, int nblocks_x,
-                            int nblocks_y, cudaStream_t st) {
-    dim3 grid((unsigned)nblocks_x, (unsigned)nblocks_y);
-    const size_t smem = (size_t)lat_n * lat_n * sizeof(double);
-    bin_band_kernel<<<grid, 128, smem, st>>>(C, i0, mb, n, lat_n, mrow, zcol, gpart);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_hist_reduce(const double *gpart, int nparts, int nbins, double *G,
                                cudaStream_t st) {

@@ -1,23 +1,32 @@
 #!/usr/bin/env python
-"""Benchmark of the hot path: one RK4 step of the LLG equation for every
-replica plus one S(q,t) evaluation, on the 128 x 128 lattice with 500
-replicas (antiferromagnetic J = -1, h = (0, 0, 0.5), alpha = 0.05,
-dt = 0.005), the correlation GEMM in TF32x3.
+"""Benchmark of the hot path: per step, one RK4 step of the LLG equation for
+every replica and one S(q,t) evaluation (the correlation GEMM with its fused
+phase epilogue).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sqt256|sqt128|grid32|adjoint64|batch48]
+
+Default workload: the 256 x 256 lattice with 1000 replicas (J = 1,
+J2 = -0.3, alpha = 0.02, h = 0, dt = 0.005), S(q,t) in BF16x3 split precision
+-- a GEMM of M = 65536 sites by K = 3000 per step.  ``sqt128`` is the
+128 x 128 lattice with 500 replicas (J = -1, h = (0, 0, 0.5), alpha = 0.05,
+dt = 0.005), S(q,t) in TF32x3.
 
 Prints one JSON line on rank 0.  ``value`` is the whole job's throughput in
 site-steps/s (a site-step = one spin of one replica advanced one RK4 step,
-with the step's S(q,t) evaluation included), with the spins resident in HBM.
-``e2e`` is the same metric through asd_ctx_step_host: the spins come from
+with the step's S(q,t) evaluation included), spins resident in HBM.  ``e2e``
+is the same metric through asd_ctx_step_host_async: the spins come from
 pinned host memory and go back every step, as the reference's runge_kutta
-contract has them.  Under torchrun every rank runs its own lattice (weak
+contract has them.  The roofline is that of the S(q,t) GEMM, the dominant
+kernel, whose duration is measured by CUDA events on its own stream inside
+the timed region.  Under torchrun every rank runs its own lattice (weak
 scaling, no collective in the data path); the time is the max over ranks.
 
-``--impl reference`` times the reference's own C code (oracle/_ref, compiled
-from its sources) on the host cores: runge_kutta + renormalisation on the full
-lattice and fused_dgemm's S(q,t) on a band of rows, scaled to the full
-lattice.
+``--impl reference`` times the reference's own C programs (oracle/_ref,
+compiled from its sources) on the host cores for the same workload, each step
+a bounded sample: runge_kutta + renormalisation on a subset of the replicas
+and the S(q,t) of its fused-AVX2 and OpenBLAS programs on a band of GEMM rows,
+each scaled to the whole workload.
 """
 from __future__ import annotations
 
@@ -35,11 +44,20 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "asd-kernel-fusion_b200"))
 
-CONFIG = dict(N=128, nfile=500, J1=-1.0, J2=0.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005)
-WORKLOAD = "llg-rk4+sqt 128x128 lattice, 500 replicas, J=-1, h=(0,0,0.5), alpha=0.05, dt=0.005"
 METRIC = "LLG site-steps/s + S(q,t) GEMM TFLOP/s, mixed vs FP64 plain at stated error"
+WORKLOADS = {
+    "sqt256": dict(N=256, nfile=1000, J1=1.0, J2=-0.3, alpha=0.02, h=(0.0, 0.0, 0.0), dt=0.005,
+                   mode="bf16x3",
+                   desc="llg-rk4+sqt 256x256 lattice, 1000 replicas, J=1, J2=-0.3, alpha=0.02, "
+                        "dt=0.005, S(q,t) in BF16x3"),
+    "sqt128": dict(N=128, nfile=500, J1=-1.0, J2=0.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005,
+                   mode="tf32x3",
+                   desc="llg-rk4+sqt 128x128 lattice, 500 replicas, J=-1, h=(0,0,0.5), "
+                        "alpha=0.05, dt=0.005, S(q,t) in TF32x3"),
+}
 LLG_BYTES_PER_SITE_STEP = 384  # 4 fused stage kernels: 3+5+5+3 FP64 3-vectors
 LLG_FUSED_BYTES_PER_SITE_STEP = 48  # one streamed step: read y, write y
+DEFAULT_CHUNK_K = {"tf32x3": 512, "bf16x3": 1024}
 
 
 def llg_fp64_ops(J2: bool, H: bool, damp: bool) -> int:
@@ -53,21 +71,34 @@ def llg_fp64_ops(J2: bool, H: bool, damp: bool) -> int:
     return 4 * (rhs + 3) + 18 + 18 + 15 + 24
 
 
-def fp64_peak_tops(torch) -> float:
-    """Nominal FP64 issue rate: 64 FP64 lanes per SM per clock at the maximum
-    SM clock (1 operation per lane per clock; no measured FP64 figure exists)."""
-    sms = torch.cuda.get_device_properties(0).multi_processor_count
-    mhz = 1965.0
+def measured_peaks():
+    """HBM GB/s and dense BF16 TFLOP/s of this pool's B200s (MEASURED_PEAKS.json,
+    written per machine), else the earlier measurement on this pool."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
-        mhz = json.loads(p.read_text()).get("sm_max_mhz", mhz)
-    return sms * 64 * mhz * 1e6 / 1e12
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "bf16_burst": d.get("bf16_tflops", 1590.0),
+                "bf16_sustained": d.get("bf16_tflops_sustained", d.get("bf16_tflops", 1400.0)),
+                "source": "measured (MEASURED_PEAKS.json)"}
+    return {"hbm_gbs": 6650.0, "bf16_burst": 1590.0, "bf16_sustained": 1400.0,
+            "source": "fallback (earlier measurement on this pool)"}
 
 
-def llg_report(ms_by_kernel, sites_replicas, ops, hbm, fp64_peak):
+def split_ceiling(mode, frac):
+    """The highest useful-flop fraction of the dense BF16 peak a 3-term split
+    GEMM can reach: three tensor-core products per useful one, and TF32
+    products run at half the BF16 rate on B200.  frac_of_ceiling is how close
+    the kernel is to that bound."""
+    ceil = {"tf32x3": 1.0 / 6.0, "bf16x3": 1.0 / 3.0}.get(mode)
+    if ceil is None or frac is None:
+        return {}
+    return {"split_ceiling_frac": ceil, "frac_of_split_ceiling": frac / ceil}
+
+
+def llg_report(ms_by_kernel, sites_replicas, ops, hbm, fma_tops):
     """Per LLG kernel: site-steps/s, DRAM bytes against the HBM peak (the
-    bound of the stage kernels) and FP64 operations against the FP64 issue
-    rate (the bound of the one-launch step)."""
+    bound of the stage kernels) and FP64 operations against the measured FP64
+    FMA issue rate (the bound of the one-launch step)."""
     out = {}
     for k, ms in ms_by_kernel.items():
         bps = LLG_BYTES_PER_SITE_STEP if k == "stages" else LLG_FUSED_BYTES_PER_SITE_STEP
@@ -75,8 +106,9 @@ def llg_report(ms_by_kernel, sites_replicas, ops, hbm, fp64_peak):
         out[k] = {"site_steps_per_s": rate, "ms": ms, "bytes_per_site_step": bps,
                   "achieved_gbs": bps * rate / 1e9, "hbm_peak_gbs": hbm,
                   "frac": bps * rate / 1e9 / hbm, "fp64_ops_per_site_step": ops,
-                  "achieved_fp64_tops": ops * rate / 1e12, "fp64_peak_tops_nominal": fp64_peak,
-                  "fp64_frac": ops * rate / 1e12 / fp64_peak,
+                  "achieved_fp64_tops": ops * rate / 1e12,
+                  "fp64_fma_peak_tops": fma_tops,
+                  "fp64_frac": ops * rate / 1e12 / fma_tops if fma_tops else None,
                   "bound": "hbm" if k == "stages" else "fp64"}
     return out
 
@@ -104,23 +136,17 @@ def env_rank():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def measured_peaks():
-    p = ROOT / "MEASURED_PEAKS.json"
-    if p.exists():
-        d = json.loads(p.read_text())
-        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
-    return 6650.0, 1590.0, "fallback"
-
-
-def split_ceiling(mode, frac):
-    """The highest useful-flop fraction of the dense BF16 peak a 3-term split
-    GEMM can reach: three tensor-core products per useful one, and TF32
-    products run at half the BF16 rate on B200.  frac_of_ceiling is how close
-    the kernel is to that bound."""
-    ceil = {"tf32x3": 1.0 / 6.0, "bf16x3": 1.0 / 3.0}.get(mode)
-    if ceil is None:
-        return {}
-    return {"split_ceiling_frac": ceil, "frac_of_split_ceiling": frac / ceil}
+def bench_config(name: str, args) -> dict:
+    """The workload description both arms print, key for key."""
+    w = WORKLOADS[name]
+    N, nf = w["N"], w["nfile"]
+    M, K = N * N, 3 * nf
+    mode = args.mode or w["mode"]
+    state_mb = M * K * 8 / 1e6
+    return {"workload": w["desc"], "sites": M, "replicas": nf, "gemm_m": M, "gemm_n": M,
+            "gemm_k": K, "sqt_mode": mode, "llg_kernel": args.llg_kernel,
+            "chunk_k": args.chunk_k if args.chunk_k >= 0 else DEFAULT_CHUNK_K.get(mode, 0),
+            "l2": f"inputs larger than L2 (spin state {state_mb:.0f} MB per array)"}
 
 
 class ClockSampler:
@@ -176,130 +202,186 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- CPU arms
-def cpu_reference_sample(N, nfile, J1, dt, spins, target_s=2.0, llg=True):
-    """Times the reference's own compiled code (oracle/_ref/libref_fusion.so) on
-    the host cores: runge_kutta + renormalisation on the whole lattice, and the
-    fused S(q,t) (llg_sqt_fusion.c:370-441 around fused_dgemm) on a band of
-    rows, scaled to all rows.  Returns seconds per full step and a description.
-    The reference model has no damping or field: its RK4 costs the same
-    regardless of those parameters."""
+def _orc():
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
 
-    if not orc.RefLib.available("fusion"):
-        return None
-    r = orc.RefLib("fusion")
-    threads = r.setup(N, nfile, J1=J1, dt=dt, threads=0)
-    M = N * N
-    t_llg = 0.0
-    if llg:
-        s = spins.copy()
-        r.steps(s, 1, 1.0)  # warm
-        t0 = time.perf_counter()
-        s = r.steps(s, 1, 1.0)
-        t_llg = time.perf_counter() - t0
-    # size the band of GEMM rows so one evaluation takes about target_s
-    rows = 256
-    r.fusion_init(spins, rows)
-    t0 = time.perf_counter()
-    r.fusion_sqt(spins)
-    t_small = time.perf_counter() - t0
-    rows = int(min(M, max(256, rows * target_s / max(t_small, 1e-6))))
-    rows -= rows % 256
-    rows = max(rows, 256)
-    r.fusion_init(spins, rows)
-    t0 = time.perf_counter()
-    r.fusion_sqt(spins)
-    t_band = time.perf_counter() - t0
-    r.lib.ref_fusion_free()
-    t_sqt = t_band * M / rows
-    sample = (f"reference runge_kutta+renorm on all {M}x{nfile} site-replicas, fused_dgemm S(q,t) "
-              f"on {rows} of {M} rows scaled by {M / rows:.2f}, {threads} OpenMP threads")
-    return dict(t_llg=t_llg, t_sqt=t_sqt, threads=threads, sample=sample, rows=rows)
+    return orc
 
 
-def cpu_reference_openblas(N, nfile, J1, dt, spins):
-    """Times the reference's gemm program (gemm/llg_sqt_mkl.c, compiled from its
-    sources into oracle/_ref/libref_gemm.so against the image's OpenBLAS) on the
-    host cores: runge_kutta + renormalisation on the whole lattice and its
-    S(q,t) -- cblas_dgemm of the whole (N^2 x N^2) correlation matrix, then the
-    outer-product subtraction and the phase reduction (gemm/llg_sqt_mkl.c:
-    369-423) -- on the full workload.  Returns a cpu_baseline-style dict."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as orc
+class CpuReference:
+    """The reference's own compiled programs (oracle/_ref, built from its
+    sources) on the host cores, for one workload, in bounded samples:
 
-    if not orc.RefLib.available("gemm"):
-        return None
-    r = orc.RefLib("gemm")
-    threads = r.setup(N, nfile, J1=J1, dt=dt, threads=0)
-    M = N * N
-    s = r.steps(spins, 1, 1.0)  # warm
-    t0 = time.perf_counter()
-    s = r.steps(s, 1, 1.0)
-    t_llg = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    r.gemm_sqt(s, spins)
-    t_sqt = time.perf_counter() - t0
-    return {"value": M * nfile / (t_llg + t_sqt), "unit": "site-steps/s", "cores": threads,
-            "kind": "reference",
-            "sample": f"reference gemm program (OpenBLAS cblas_dgemm): runge_kutta+renorm and "
-                      f"S(q,t) on all {M}x{nfile} site-replicas, one step, {threads} OpenMP threads",
-            "llg_site_steps_per_s": M * nfile / t_llg,
-            "sqt_tflops": 2.0 * M * M * 3 * nfile / t_sqt / 1e12}
+    * LLG: runge_kutta + renormalisation (llg_sqt_baseline.c:95-142, :298-309)
+      on the first `llg_replicas` replicas, scaled to all of them (replicas
+      are independent, the cost is linear in them);
+    * S(q,t), fused-AVX2 program (llg_sqt_fusion.c:370-441 around
+      fused_dgemm) and OpenBLAS program (gemm/llg_sqt_mkl.c:369-423 around
+      cblas_dgemm): the per-step A pack and replica means (O(M K), timed
+      whole) plus the GEMM and its epilogue on a band of C's rows (O(rows M
+      K), scaled to all M rows).  The whole C and qmat would take
+      4 M^2 x 8 bytes of host memory (137 GB at 256 x 256).
+
+    The fused program's value is wrong for K > 240 (the running C is summed
+    once per K block, gemm_kernel.h:378-407); its time is not."""
+
+    def __init__(self, name: str, spins: np.ndarray, target_s: float = 1.0):
+        orc = _orc()
+        w = WORKLOADS[name]
+        self.N, self.nf = w["N"], w["nfile"]
+        self.J1, self.dt = w["J1"], w["dt"]
+        self.M, self.K = self.N * self.N, 3 * self.nf
+        self.spins = spins
+        self.target_s = target_s
+        self.fusion = orc.RefLib("fusion") if orc.RefLib.available("fusion") else None
+        self.gemm = orc.RefLib("gemm") if orc.RefLib.available("gemm") else None
+        self.threads = 0
+        self.llg_replicas = None
+        self.rows = {}
+        if self.fusion is not None:
+            self._size()
+
+    def available(self) -> bool:
+        return self.fusion is not None
+
+    def _size(self):
+        """Sample sizes for about target_s of host time per part."""
+        f = self.fusion
+        nf0 = min(self.nf, max(1, int(2e5 / self.M)))
+        self.threads = f.setup(self.N, nf0, J1=self.J1, dt=self.dt, threads=0)
+        t = f.step_time(self.spins[:nf0])
+        self.llg_replicas = int(min(self.nf, max(1, nf0 * self.target_s / max(t, 1e-6))))
+        f.setup(self.N, self.nf, J1=self.J1, dt=self.dt, threads=0)
+        rows = min(self.M, 256)
+        f.fusion_init(self.spins, rows)
+        _, _, tb = f.fusion_sqt_timed(self.spins)
+        rows = int(min(self.M, max(256, rows * self.target_s / max(tb, 1e-6))))
+        self.rows["fused_avx2"] = max(256, rows - rows % 256)
+        f.fusion_init(self.spins, self.rows["fused_avx2"])
+        if self.gemm is not None:
+            self.gemm.setup(self.N, self.nf, J1=self.J1, dt=self.dt, threads=0)
+            r0 = min(self.M, 256)
+            _, _, tb = self.gemm.gemm_sqt_band(self.spins, self.spins, r0)
+            rows = int(min(self.M, max(256, r0 * self.target_s / max(tb, 1e-6))))
+            self.rows["openblas"] = max(256, rows - rows % 256)
+
+    def sample(self) -> dict:
+        """One bounded sample of one step of each program: seconds per full
+        step, extrapolated as described above."""
+        f = self.fusion
+        f.setup(self.N, self.llg_replicas, J1=self.J1, dt=self.dt, threads=0)
+        t_llg = f.step_time(self.spins[:self.llg_replicas]) * self.nf / self.llg_replicas
+        f.setup(self.N, self.nf, J1=self.J1, dt=self.dt, threads=0)
+        out = {}
+        _, tp, tb = f.fusion_sqt_timed(self.spins)
+        out["fused_avx2"] = (t_llg, tp + tb * self.M / self.rows["fused_avx2"])
+        if self.gemm is not None:
+            self.gemm.setup(self.N, self.nf, J1=self.J1, dt=self.dt, threads=0)
+            _, tp, tb = self.gemm.gemm_sqt_band(self.spins, self.spins, self.rows["openblas"])
+            out["openblas"] = (t_llg, tp + tb * self.M / self.rows["openblas"])
+        return out
+
+    def describe(self, path: str, t_llg: float, t_sqt: float) -> dict:
+        M, nf, K = self.M, self.nf, self.K
+        rows = self.rows[path]
+        prog = ("fused-AVX2 program (fused_dgemm)" if path == "fused_avx2"
+                else "OpenBLAS program (cblas_dgemm)")
+        sample = (f"reference {prog}: runge_kutta+renorm on {self.llg_replicas} of {nf} replicas "
+                  f"scaled x{nf / self.llg_replicas:.2f}; S(q,t) A pack whole + GEMM/epilogue on "
+                  f"{rows} of {M} rows scaled x{M / rows:.2f}; {self.threads} OpenMP threads")
+        d = {"value": M * nf / (t_llg + t_sqt), "unit": "site-steps/s", "cores": self.threads,
+             "kind": "reference", "sample": sample,
+             "llg_site_steps_per_s": M * nf / t_llg,
+             "sqt_tflops": 2.0 * M * M * K / t_sqt / 1e12, "ms_per_step": (t_llg + t_sqt) * 1e3}
+        if path == "fused_avx2" and K > 240:
+            d["value_valid"] = False
+            d["note"] = ("time only: the fused program's S(q,t) is wrong for K > 240 "
+                         "(sum taken once per K block)")
+        return d
+
+    def close(self):
+        if self.fusion is not None:
+            self.fusion.lib.ref_fusion_free()
+
+
+def cpu_baseline_line(name: str, spins: np.ndarray, samples: int = 1, target_s: float = 1.0):
+    """The reference's programs, `samples` samples each (median); returns
+    (cpu_baseline dict of the faster program, all paths) or (None, None)."""
+    ref = CpuReference(name, spins, target_s)
+    if not ref.available():
+        return None, None
+    runs = [ref.sample() for _ in range(samples)]
+    paths = {}
+    for path in runs[0]:
+        t_llg = statistics.median(r[path][0] for r in runs)
+        t_sqt = statistics.median(r[path][1] for r in runs)
+        paths[path] = ref.describe(path, t_llg, t_sqt)
+    ref.close()
+    best = max(paths.values(), key=lambda d: d["value"])
+    return {k: best[k] for k in ("value", "unit", "cores", "kind", "sample")}, paths
 
 
 def run_reference(args):
-    """The reference's CPU implementations of the path on the host cores: its
-    fused-AVX2 program (fused_dgemm, sampled on a band of rows each step) and
-    its OpenBLAS program (full workload, up to 3 samples).  `value` is the
-    faster of the two, so the comparison is against the reference's best."""
+    """--impl reference: the reference's CPU programs on the host cores, each
+    step a bounded sample of the workload; `value` is the faster program's.
+    Under torchrun rank 0 alone runs; the other ranks exit without work."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
-    N, nf = CONFIG["N"], CONFIG["nfile"]
+    name = args.workload
+    w = WORKLOADS[name]
+    N, nf = w["N"], w["nfile"]
     import asd_b200 as asd
 
     spins = asd.random_spins(N, nf, seed=0)
-    vals = []
-    info = None
+    ref = CpuReference(name, spins, target_s=args.ref_target_s)
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libref_fusion.so not built (make -C oracle ref REF=...)"}))
+        return 0
+    runs = []
     for it in range(args.warmup + args.steps):
-        info = cpu_reference_sample(N, nf, CONFIG["J1"], CONFIG["dt"], spins,
-                                    target_s=args.ref_target_s)
-        if info is None:
-            print(json.dumps({"impl": "reference", "unavailable":
-                              "oracle/_ref/libref_fusion.so not built (make -C oracle ref)"}))
-            return 0
+        r = ref.sample()
         if it >= args.warmup:
-            vals.append(info["t_llg"] + info["t_sqt"])
-    t = statistics.median(vals)
-    fused = {"value": N * N * nf / t, "unit": "site-steps/s", "cores": info["threads"],
-             "kind": "reference", "sample": info["sample"],
-             "llg_site_steps_per_s": N * N * nf / info["t_llg"],
-             "sqt_tflops": 2.0 * (N * N) ** 2 * 3 * nf / info["t_sqt"] / 1e12}
-    ob = [cpu_reference_openblas(N, nf, CONFIG["J1"], CONFIG["dt"], spins)
-          for _ in range(min(max(args.steps, 1), 3))]
-    openblas = None
-    if ob[0] is not None:
-        openblas = sorted(ob, key=lambda d: d["value"])[len(ob) // 2]
-    best = fused if openblas is None or fused["value"] >= openblas["value"] else openblas
+            runs.append(r)
+    paths = {}
+    for path in runs[0]:
+        t_llg = statistics.median(r[path][0] for r in runs)
+        t_sqt = statistics.median(r[path][1] for r in runs)
+        paths[path] = ref.describe(path, t_llg, t_sqt)
+    ref.close()
+    best = max(paths.values(), key=lambda d: d["value"])
     value = best["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "site-steps/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": N * N * nf / value * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": N * N * nf / value * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded spins uniform on the sphere",
-        "config": {"workload": WORKLOAD, "sites": N * N, "replicas": nf, "gemm_m": N * N,
-                   "gemm_k": 3 * nf},
+        "config": bench_config(name, args),
         "cpu_baseline": {k: best[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": value, "unit": "site-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "paths": {"fused_avx2": fused, "openblas": openblas},
+        "paths": paths,
     }
     print(json.dumps(line))
     return 0
 
 
 # --------------------------------------------------------------- GPU arm
+def traffic_for(kernel_key: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None, None
+    d = json.loads(p.read_text())
+    e = d.get(kernel_key)
+    if isinstance(e, dict):
+        return e.get("bytes"), e.get("source")
+    return e, None
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -311,13 +393,15 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", device_id=torch.device("cuda", local),
                                 timeout=__import__("datetime").timedelta(seconds=120))
-    N, nf = CONFIG["N"], CONFIG["nfile"]
+    name = args.workload
+    w = WORKLOADS[name]
+    N, nf = w["N"], w["nfile"]
     M, K = N * N, 3 * nf
-    mode = args.mode
-    params = asd.Params.make(N, nf, J1=CONFIG["J1"], J2=CONFIG["J2"], alpha=CONFIG["alpha"],
-                             h=CONFIG["h"], dt=CONFIG["dt"])
+    mode = args.mode or w["mode"]
+    params = asd.Params.make(N, nf, J1=w["J1"], J2=w["J2"], alpha=w["alpha"], h=w["h"], dt=w["dt"])
     asd.load().asd_set_device(local)
-    ctx = asd.Context(params, modes=["fp64", "tf32x3", "bf16x3"])
+    extras = not args.no_extras
+    ctx = asd.Context(params, modes=(["fp64", "tf32x3", "bf16x3"] if extras else [mode]))
     ctx.set_llg_kernel(args.llg_kernel)
     if args.chunk_k >= 0:
         ctx.set_chunk_k(args.chunk_k)
@@ -334,9 +418,12 @@ def run_ours(args):
         ctx.sqt_async(mode, d_out.data_ptr() + 16 * i)
         return n1 + ctx.last_launches()
 
+    ctx.time_kernels(True)
     for i in range(args.warmup):
         one_step(i)
     torch.cuda.synchronize()
+    ctx.kernel_time("gemm")  # forget the warm-up launches
+    ctx.kernel_time("llg")
     if world > 1:
         dist.barrier()
     launches = 0
@@ -349,17 +436,19 @@ def run_ours(args):
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
+    gemm_ms, gemm_n = ctx.kernel_time("gemm")
+    llg_ms, llg_n = ctx.kernel_time("llg")
+    ctx.time_kernels(False)
     ctx.check_device_status()
     ms, value = aggregate(ms, M * nf, world, dist if world > 1 else None, "cuda")
     if world > 1:
         dist.barrier()
     sqt_last = complex(*d_out[2 * (total - 1):2 * total].tolist())
 
-    extra = {"sqt_ms": {}, "report": {}}
-    if rank == 0 and not args.no_extras:
-        extra = component_measurements(ctx, asd, torch, stream, M, K, nf, args)
-    e2e = None if args.no_extras else e2e_measurement(ctx, asd, torch, spins0, mode, M, nf,
-                                                      args, world)
+    report = {}
+    if rank == 0 and extras:
+        report = component_measurements(ctx, asd, torch, stream, name, mode, args)
+    e2e = e2e_measurement(ctx, asd, torch, spins0, mode, M, nf, args, world) if extras else None
     if world > 1:
         dist.barrier()
     if rank != 0:
@@ -368,50 +457,50 @@ def run_ours(args):
             dist.destroy_process_group()
         return 0
 
-    hbm, bf16, src = measured_peaks()
+    peaks = measured_peaks()
     gemm_flops = 2.0 * M * M * K
-    gemm_ms = extra["sqt_ms"].get(mode)  # absent with --no-extras: the GEMM is not timed alone
-    achieved = gemm_flops / (gemm_ms / 1e3) / 1e12 if gemm_ms else None
-    frac = achieved / bf16 if achieved is not None else None
-    traffic = None
-    tfile = ROOT / "profiles" / "traffic.json"
-    if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(f"umma_sqt_{mode}")
+    gemm_avg_ms = gemm_ms / gemm_n if gemm_n else None
+    achieved = gemm_flops / (gemm_avg_ms / 1e3) / 1e12 if gemm_avg_ms else None
+    frac = achieved / peaks["bf16_sustained"] if achieved is not None else None
+    traffic, traffic_src = traffic_for(f"umma_sqt_{mode}_{N}x{N}x{nf}")
+    roofline = {
+        "bound": "tensor", "kernel": f"umma_sqt_kernel ({mode})", "achieved": achieved,
+        "peak": peaks["bf16_sustained"], "unit": "TFLOP/s", "frac": frac, "traffic": traffic,
+        "peak_source": f"{peaks['source']}, dense bf16 sustained (the GEMM runs back to back "
+                       f"for the whole timed region)",
+        "achieved_counts": "useful 2*M*M*K per launch / mean launch time by CUDA events on the "
+                           "GEMM's stream inside the timed region; the 3-term split issues 3x "
+                           "that on the tensor pipe",
+        "launches_timed": gemm_n, "ms_per_launch": gemm_avg_ms,
+        "algorithmic_operand_bytes": 4 * M * (K + (-K) % 64) * (2 if mode == "bf16x3" else 4),
+        "traffic_source": traffic_src,
+        **split_ceiling(mode, frac),
+    }
+    if mode == "fp64" and achieved is not None:
+        roofline.update({"bound": "fp64 tensor", "kernel": "dmma_sqt_kernel (fp64)"})
     line = {
         "metric": METRIC, "value": value, "unit": "site-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": f"f64 RK4 + {mode} GEMM (fp32 accumulate, f64 reduction)",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": f"f64 RK4 + {mode} GEMM (fp32 accumulate, f64 reduction)",
         "data": "synthetic: seeded spins uniform on the sphere",
-        "config": {"workload": WORKLOAD, "sites": M, "replicas": nf, "gemm_m": M, "gemm_n": M,
-                   "gemm_k": K, "sqt_mode": mode, "llg_kernel": args.llg_kernel,
-                   "chunk_k": args.chunk_k if args.chunk_k >= 0 else (512 if mode == "tf32x3" else 1024),
-                   "l2": "inputs larger than L2 (spin state 197 MB per array, operands 197 MB)"},
-        "roofline": {"bound": "tensor", "kernel": f"umma_sqt_kernel ({mode})",
-                     "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                     "frac": frac, "traffic": traffic,
-                     "peak_source": f"{src} dense bf16 burst (MEASURED_PEAKS.json)",
-                     "achieved_counts": "useful 2*M*M*K per evaluation; the 3-term split issues 3x that on the tensor pipe",
-                     **(split_ceiling(mode, frac) if frac is not None else {})},
+        "config": bench_config(name, args),
+        "roofline": roofline,
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "e2e": e2e,
+        "timed_region_s": ms * args.steps / 1e3,
+        "llg_in_timed_region": {"ms_per_step": llg_ms / max(1, args.steps),
+                                "launches": llg_n,
+                                "site_steps_per_s": M * nf / (llg_ms / max(1, args.steps) / 1e3)
+                                if llg_ms else None},
         "sqt_last": [sqt_last.real, sqt_last.imag],
     }
-    line.update(extra["report"])
-    if world == 1 and not args.no_cpu_baseline and not args.no_extras:
-        # the reference's two CPU programs; cpu_baseline is the faster one
-        info = cpu_reference_sample(N, nf, CONFIG["J1"], CONFIG["dt"], spins0, target_s=1.5)
-        paths = {}
-        if info is not None:
-            v = M * nf / (info["t_llg"] + info["t_sqt"])
-            paths["fused_avx2"] = {"value": v, "unit": "site-steps/s", "cores": info["threads"],
-                                   "kind": "reference", "sample": info["sample"]}
-        ob = cpu_reference_openblas(N, nf, CONFIG["J1"], CONFIG["dt"], spins0)
-        if ob is not None:
-            paths["openblas"] = ob
-        if paths:
-            best = max(paths.values(), key=lambda d: d["value"])
-            line["cpu_baseline"] = {k: best[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    line.update(report)
+    if world == 1 and extras and not args.no_cpu_baseline:
+        base, paths = cpu_baseline_line(name, spins0, samples=1, target_s=1.0)
+        if base is not None:
+            line["cpu_baseline"] = base
             line["cpu_baseline_paths"] = paths
     print(json.dumps(line))
     ctx.close()
@@ -420,16 +509,23 @@ def run_ours(args):
     return 0
 
 
-def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
-    """LLG alone, every S(q,t) mode alone, and the split modes' error against
-    the FP64 path, on the current state (rank 0)."""
+def component_measurements(ctx, asd, torch, stream, name, mode, args):
+    """Rank 0, after the timed region: the measured FP64 peaks, each LLG
+    kernel alone, every S(q,t) mode alone (its GEMM kernel by CUDA events on
+    its own stream), the split modes' error against the FP64 path relative to
+    |S| and to the magnitude of the summed terms."""
+    w = WORKLOADS[name]
+    N, nf = w["N"], w["nfile"]
+    M, K = N * N, 3 * nf
+    peaks = measured_peaks()
+    fma_tf, _ = asd.measure_fp64_peak("fma", stream.cuda_stream)
+    dmma_tf, _ = asd.measure_fp64_peak("dmma", stream.cuda_stream)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    d = torch.zeros(2, dtype=torch.float64, device="cuda")
-    reps = 30
+    reps = 10
     llg = {}
     for kern in ("stages", "fused"):
         ctx.set_llg_kernel(kern)
-        ctx.step(5)
+        ctx.step(2)
         torch.cuda.synchronize()
         ev0.record(stream)
         ctx.step(reps)
@@ -437,31 +533,48 @@ def component_measurements(ctx, asd, torch, stream, M, K, nf, args):
         torch.cuda.synchronize()
         llg[kern] = ev0.elapsed_time(ev1) / reps
     ctx.set_llg_kernel(args.llg_kernel)
-    hbm, bf16, src = measured_peaks()
-    sqt_ms, vals = {}, {}
-    for mode in ("fp64", "tf32x3", "bf16x3"):
-        n = 2 if mode == "fp64" else 5
-        ctx.sqt_async(mode, d.data_ptr())  # operands split, warm
+    d = torch.zeros(2, dtype=torch.float64, device="cuda")
+    sqt_ms, kern_ms, vals = {}, {}, {}
+    ctx.time_kernels(True)
+    for m in ("fp64", "tf32x3", "bf16x3"):
+        n = 1 if m == "fp64" else 3
+        ctx.sqt_async(m, d.data_ptr())  # operands split, warm
         torch.cuda.synchronize()
+        ctx.kernel_time("gemm")
         ev0.record(stream)
         for _ in range(n):
-            ctx.sqt_async(mode, d.data_ptr())
+            ctx.sqt_async(m, d.data_ptr())
         ev1.record(stream)
         torch.cuda.synchronize()
-        sqt_ms[mode] = ev0.elapsed_time(ev1) / n
-        vals[mode] = complex(*d.tolist())
+        sqt_ms[m] = ev0.elapsed_time(ev1) / n
+        km, kn = ctx.kernel_time("gemm")
+        kern_ms[m] = km / kn if kn else None
+        vals[m] = complex(*d.tolist())
+    ctx.time_kernels(False)
+    mag = ctx.sqt_magnitude()
     ref = vals["fp64"]
     flops = 2.0 * M * M * K
-    report = {
-        "llg": llg_report(llg, M * nf, llg_fp64_ops(CONFIG["J2"] != 0.0, any(CONFIG["h"]),
-                                                     CONFIG["alpha"] != 0.0),
-                          hbm, fp64_peak_tops(torch)),
-        "sqt": {m: {"ms": sqt_ms[m], "tflops": flops / (sqt_ms[m] / 1e3) / 1e12,
-                    "value": [vals[m].real, vals[m].imag],
-                    "rel_err_vs_fp64": abs(vals[m] - ref) / abs(ref)} for m in sqt_ms},
+    sqt = {}
+    for m in sqt_ms:
+        e = {"ms": sqt_ms[m], "gemm_kernel_ms": kern_ms[m],
+             "tflops": flops / (sqt_ms[m] / 1e3) / 1e12,
+             "value": [vals[m].real, vals[m].imag],
+             "rel_err_vs_fp64": abs(vals[m] - ref) / abs(ref),
+             "err_vs_fp64_rel_to_term_magnitude": abs(vals[m] - ref) / mag}
+        if m == "fp64":
+            e["fp64_dmma_peak_tflops"] = dmma_tf
+            e["frac_of_fp64_dmma_peak"] = (flops / (kern_ms[m] / 1e3) / 1e12 / dmma_tf
+                                           if kern_ms[m] else None)
+        sqt[m] = e
+    return {
+        "fp64_peaks": {"fma_tflops": fma_tf, "fma_tops": fma_tf / 2.0, "dmma_tflops": dmma_tf,
+                       "source": "asd_measure_fp64_peak, this GPU, this run (burst, ~1 ms)"},
+        "llg": llg_report(llg, M * nf, llg_fp64_ops(w["J2"] != 0.0, any(w["h"]), w["alpha"] != 0.0),
+                          peaks["hbm_gbs"], fma_tf / 2.0),
+        "sqt": sqt,
+        "sqt_term_magnitude": mag,
         "sqt_speedup_vs_fp64": {m: sqt_ms["fp64"] / sqt_ms[m] for m in ("tf32x3", "bf16x3")},
     }
-    return {"sqt_ms": sqt_ms, "report": report}
 
 
 def e2e_measurement(ctx, asd, torch, spins0, mode, M, nf, args, world):
@@ -528,12 +641,10 @@ def timed(torch, fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
-def run_workload(args):
+def run_secondary(args):
     """Secondary workloads, one JSON line each (not the headline):
     grid32   32x32 lattice, 200 replicas, 2000 steps, FP64, S(q,t) on the whole q
              grid after every step
-    sqt256   256x256 lattice, 1000 replicas, J=1, J2=-0.3, alpha=0.02, dt=0.005:
-             one RK4 step + S(q,t) in BF16x3, with the FP64 path's time and error
     adjoint64  64x64 lattice, 100 replicas, 1000 steps, S(q,t) every 10 steps,
              checkpoints every 50: loss + gradient wrt (J1, J2, alpha, h)
     batch48  48 lattices of sizes in {48,64,96,128,160}^2, noise amplitude in
@@ -543,49 +654,8 @@ def run_workload(args):
     import asd_b200 as asd
 
     torch.cuda.set_device(0)
-    hbm, bf16, src = measured_peaks()
     out = {"impl": "ours", "workload": args.workload, "n_gpus": 1, "data": "synthetic"}
-    if args.workload == "sqt256":
-        N, nf = 256, 1000
-        M, K = N * N, 3 * nf
-        ctx = asd.Context(asd.Params.make(N, nf, J1=1.0, J2=-0.3, alpha=0.02, dt=0.005),
-                          modes=["fp64", "bf16x3", "tf32x3"])
-        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
-        ctx.set_spins(asd.random_spins(N, nf, seed=0), as_origin=True)
-        d = torch.zeros(2, dtype=torch.float64, device="cuda")
-        ctx.step(3)
-        step_ms = timed(torch, lambda: (ctx.step(1), ctx.sqt_async("bf16x3", d.data_ptr())),
-                        args.steps)
-        llg_ms = {}
-        for kern in ("stages", "fused"):
-            ctx.set_llg_kernel(kern)
-            ctx.step(2)
-            llg_ms[kern] = timed(torch, lambda: ctx.step(1), 10)
-        ctx.set_llg_kernel("auto")
-        vals, ms = {}, {}
-        for mode, reps in (("bf16x3", 5), ("tf32x3", 3), ("fp64", 1)):
-            ctx.sqt_async(mode, d.data_ptr())
-            ms[mode] = timed(torch, lambda: ctx.sqt_async(mode, d.data_ptr()), reps)
-            vals[mode] = complex(*d.tolist())
-        flops = 2.0 * M * M * K
-        out.update({
-            "metric": METRIC, "value": M * nf / (step_ms / 1e3), "unit": "site-steps/s",
-            "ms_per_step": step_ms, "dtype": "f64 RK4 + bf16x3 GEMM",
-            "config": {"workload": "256x256 lattice, 1000 replicas, J=1, J2=-0.3, alpha=0.02, dt=0.005",
-                       "gemm_m": M, "gemm_k": K},
-            "llg": llg_report(llg_ms, M * nf, llg_fp64_ops(True, False, True), hbm,
-                              fp64_peak_tops(torch)),
-            "sqt": {m: {"ms": ms[m], "tflops": flops / ms[m] / 1e9,
-                        "rel_err_vs_fp64": abs(vals[m] - vals["fp64"]) / abs(vals["fp64"])}
-                    for m in ms},
-            "sqt_speedup_vs_fp64": {m: ms["fp64"] / ms[m] for m in ("bf16x3", "tf32x3")},
-            "roofline": {"bound": "tensor", "kernel": "umma_sqt_kernel (bf16x3)",
-                         "achieved": flops / ms["bf16x3"] / 1e9, "peak": bf16, "unit": "TFLOP/s",
-                         "frac": flops / ms["bf16x3"] / 1e9 / bf16, "traffic": None,
-                         **split_ceiling("bf16x3", flops / ms["bf16x3"] / 1e9 / bf16)},
-        })
-        ctx.close()
-    elif args.workload == "grid32":
+    if args.workload == "grid32":
         # 32x32 lattice, 200 replicas, J=1, alpha=0.1, dt=0.01, 2000 RK4 steps, S(q,t) on the
         # whole 32x32 q grid after every step (FP64 GEMM + displacement bins + 2-D DFT)
         N, nf, nsteps = 32, 200, 2000
@@ -689,8 +759,8 @@ def run_workload(args):
 
 
 def run_sharded(args):
-    """--shard: the headline ensemble (128x128, 500 replicas) split by replicas
-    over the ranks -- strong scaling of one system.  Each rank steps its
+    """--shard: the workload's one ensemble split by replicas over the ranks --
+    strong scaling of one system.  Each rank steps its
     replicas; every step's S(q,t) is exchanged through asd_b200.shard
     (all-reduces of 2 and 3*N*N doubles over NCCL) and is the same on every
     rank.  Device-resident: no e2e leg."""
@@ -705,12 +775,13 @@ def run_sharded(args):
     if world > 1:
         dist.init_process_group("nccl", device_id=torch.device("cuda", local),
                                 timeout=__import__("datetime").timedelta(seconds=120))
-    N, nf = CONFIG["N"], CONFIG["nfile"]
+    w = WORKLOADS[args.workload]
+    N, nf = w["N"], w["nfile"]
     M = N * N
     b, e = shard_range(nf, rank, world)
-    mode = args.mode
-    params = asd.Params.make(N, e - b, J1=CONFIG["J1"], J2=CONFIG["J2"], alpha=CONFIG["alpha"],
-                             h=CONFIG["h"], dt=CONFIG["dt"])
+    mode = args.mode or w["mode"]
+    params = asd.Params.make(N, e - b, J1=w["J1"], J2=w["J2"], alpha=w["alpha"], h=w["h"],
+                             dt=w["dt"])
     asd.load().asd_set_device(local)
     ctx = asd.Context(params, modes=[mode])
     stream = torch.cuda.current_stream()
@@ -758,10 +829,9 @@ def run_sharded(args):
         "scaling": "strong", "vs_baseline": None,
         "dtype": f"f64 RK4 + {mode} GEMM (fp32 accumulate, f64 reduction)",
         "data": "synthetic: seeded spins uniform on the sphere",
-        "config": {"workload": WORKLOAD + ", one ensemble split by replicas", "sites": M,
-                   "replicas": nf, "parallelism": f"replicas/{world}", "sqt_mode": mode,
-                   "exchange_doubles_per_step": 2 + 3 * M,
-                   "l2": "inputs larger than L2 at 1 and 2 GPUs"},
+        "config": {**bench_config(args.workload, args),
+                   "workload": w["desc"] + ", one ensemble split by replicas",
+                   "parallelism": f"replicas/{world}", "exchange_doubles_per_step": 2 + 3 * M},
         "gpu_launches": launches, "clocks": clk.summary(), "e2e": None,
         "sqt_last": [sqt_last.real, sqt_last.imag],
     }))
@@ -774,30 +844,34 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["tf32x3", "bf16x3", "fp64", "fp64_fused"], default="tf32x3")
+    ap.add_argument("--workload", choices=["sqt256", "sqt128", "grid32", "adjoint64", "batch48"],
+                    default="sqt256",
+                    help="sqt256 (default) and sqt128 print the full line; the others a line of "
+                         "their own")
+    ap.add_argument("--mode", choices=["tf32x3", "bf16x3", "fp64"], default=None,
+                    help="S(q,t) arithmetic (default: the workload's)")
     ap.add_argument("--batch-cluster", type=int, default=0,
                     help="batch48: clusters of this many CTAs instead of the autotuner's choice")
     ap.add_argument("--llg-kernel", choices=["auto", "fused", "stages"], default="auto",
-                    help="RK4 step of the headline: one streamed launch where it fills the GPU "
-                         "(auto, default), always (fused) or four stage kernels (stages)")
+                    help="RK4 step: one streamed launch where it fills the GPU (auto, default), "
+                         "always (fused) or four stage kernels (stages)")
     ap.add_argument("--chunk-k", type=int, default=-1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="only the timed steps (for profiling): no per-component timings, e2e "
-                         "or CPU baseline after the timed region")
-    ap.add_argument("--ref-target-s", type=float, default=2.0)
-    ap.add_argument("--workload", choices=["headline", "grid32", "sqt256", "adjoint64", "batch48"],
-                    default="headline", help="secondary workloads print their own line")
+                    help="only the timed steps (for profiling): one S(q,t) mode allocated, no "
+                         "per-component timings, e2e or CPU baseline")
+    ap.add_argument("--ref-target-s", type=float, default=0.5,
+                    help="--impl reference: host seconds per sampled part of a step")
     ap.add_argument("--shard", action="store_true",
-                    help="strong scaling: split the one headline ensemble by replicas over the "
+                    help="strong scaling: split the workload's one ensemble by replicas over the "
                          "ranks (S(q,t) exchanged every step) instead of one ensemble per rank")
     args = ap.parse_args()
-    if args.workload != "headline":
-        return run_workload(args)
-    if args.shard and args.impl == "ours":
-        return run_sharded(args)
+    if args.workload not in WORKLOADS:
+        return run_secondary(args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.shard:
+        return run_sharded(args)
     return run_ours(args)
 
 

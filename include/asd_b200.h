@@ -46,7 +46,7 @@ extern "C" {
 
 #define ASD_OK 0
 #define ASD_ERR_INVALID (-1)     /* a parameter is out of range            */
-#define ASD_ERR_CUDA (-2)        /* a CUDA runtime or cuBLAS call failed     */
+#define ASD_ERR_CUDA (-2)        /* a CUDA runtime or driver call failed     */
 #define ASD_ERR_NOMEM (-3)       /* device or host allocation failed         */
 #define ASD_ERR_TIMEOUT (-4)     /* a bounded device-side wait gave up       */
 #define ASD_ERR_STATE (-5)       /* call order (e.g. no spins set yet)       */
@@ -55,10 +55,10 @@ extern "C" {
 
 /* Arithmetic of the S(q,t) correlation GEMM. */
 typedef enum {
-    ASD_SQT_FP64 = 0,   /* FP64 GEMM (cuBLAS DGEMM) + FP64 phase epilogue: the plain path */
+    ASD_SQT_FP64 = 0,   /* the plain path: FP64 tensor-core GEMM (mma.sync .f64) with
+                           the phase, connected-part and reduction epilogue fused */
     ASD_SQT_TF32X3 = 1, /* tcgen05 kind::tf32, hi*hi + hi*lo + lo*hi, FP32 accumulate   */
-    ASD_SQT_BF16X3 = 2, /* tcgen05 kind::f16 (bf16), hi*hi + hi*lo + lo*hi, FP32 accum. */
-    ASD_SQT_FP64_FUSED = 3 /* FP64 CUDA-core GEMM with the phase epilogue fused          */
+    ASD_SQT_BF16X3 = 2  /* tcgen05 kind::f16 (bf16), hi*hi + hi*lo + lo*hi, FP32 accum. */
 } asd_sqt_mode;
 
 /* Model parameters.  The reference hard-wires alpha = J2 = h = 0,
@@ -121,6 +121,13 @@ int asd_ctx_step(asd_ctx *ctx, int nsteps);
 int asd_ctx_sqt(asd_ctx *ctx, asd_sqt_mode mode, double out[2]);
 /* Asynchronous form: writes out[0..1] (a device pointer) on the stream. */
 int asd_ctx_sqt_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
+/* The magnitude of the terms S(q,t) sums, *out = (1/M) sum_ij |C_ij - m_i . z_j|
+ * (C the correlation GEMM, m and z the replica means at t and 0), through the
+ * FP64 GEMM; synchronous.  S(q,t) is a phase-weighted sum of these terms and
+ * can be much smaller than their magnitude, so an error of S relative to this
+ * scale measures the arithmetic apart from cancellation.  Needs the FP64 mode.
+ * No counterpart in the reference. */
+int asd_ctx_sqt_magnitude(asd_ctx *ctx, double *out);
 
 /* S(q,t) for every q = 2*pi*(a, b)/N of the N x N grid, into d_out[2*(a*N+b)]
  * (real) and d_out[2*(a*N+b)+1] (imaginary), a device buffer of 2*N*N
@@ -236,6 +243,17 @@ int asd_ctx_set_chunk_k(asd_ctx *ctx, int chunk_k);
 /* Number of kernels the last asd_ctx_step / asd_ctx_sqt* call launched. */
 int asd_ctx_last_launches(const asd_ctx *ctx);
 
+/* Diagnostic: with on != 0, later calls record CUDA events on the stream each
+ * kernel is launched on, around every RK4 step (the one-launch step kernel, or
+ * the four stage kernels of one step) and every S(q,t) GEMM kernel (the
+ * tcgen05 split GEMM or the FP64 GEMM); nothing is recorded while a stream is
+ * being captured.  No counterpart in the reference; the benchmark uses it. */
+int asd_ctx_time_kernels(asd_ctx *ctx, int on);
+/* Waits for the events recorded since the last read and returns the summed
+ * duration in ms and the number of kernel launches of `which` (0 = RK4 step
+ * kernels, 1 = S(q,t) GEMM), then forgets them. */
+int asd_ctx_kernel_time(asd_ctx *ctx, int which, double *ms, int *launches);
+
 /* Status word set by device code (bounded waits that gave up, etc.);
  * returns ASD_OK or ASD_ERR_TIMEOUT and clears it. */
 int asd_ctx_check_device_status(asd_ctx *ctx);
@@ -288,6 +306,19 @@ int asd_check_const_division_f32(unsigned long long *bad, void *stream);
 int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, const void *a_lo,
                       const void *b_hi, const void *b_lo, float *c, long ldc, int chunk_k,
                       void *stream);
+
+/* Diagnostic: measured FP64 throughput of the current device, the
+ * denominators of the FP64 roofline fractions.  which = 0: independent
+ * __fma_rn chains on the CUDA cores (an FMA counts 2 flops); which = 1:
+ * independent mma.sync m16n8k8 .f64 tensor-core products (2*16*8*8 flops
+ * each).  32 warps per SM, about a millisecond; *tflops and *ms of the second
+ * of two launches.  Synchronous.  No counterpart in the reference. */
+int asd_measure_fp64_peak(int which, double *tflops, double *ms, void *stream);
+/* Diagnostic: one warp computes D[16][8] = A[16][8] B[8][8] (row-major device
+ * arrays) with mma.sync m16n8k8 .f64, loading and storing the fragments in the
+ * layout the FP64 GEMM assumes; a test compares D with a host product.
+ * Asynchronous on stream.  No counterpart in the reference. */
+int asd_check_dmma_layout(const double *A, const double *B, double *D, void *stream);
 
 /* S(q,t) through the split tensor-core GEMM without allocating anything.
  * No counterpart in the reference.  For callers that may not call cudaMalloc

@@ -158,16 +158,24 @@ class RefLib:
         lib.ref_runge_kutta.argtypes = [_dp] * 6
         lib.ref_steps.argtypes = [_dp, C.c_int, C.c_double]
         lib.ref_steps.restype = C.c_int
+        lib.ref_steps_timed.argtypes = [_dp, C.c_int, C.c_double, C.POINTER(C.c_double)]
+        lib.ref_steps_timed.restype = C.c_int
         if variant == "fusion":
             lib.ref_fusion_init.argtypes = [_dp, C.c_long]
             lib.ref_fusion_init.restype = C.c_int
             lib.ref_fusion_sqt.argtypes = [_dp, _dp]
             lib.ref_fusion_sqt.restype = C.c_int
+            lib.ref_fusion_sqt_timed.argtypes = [_dp, _dp, C.POINTER(C.c_double),
+                                                 C.POINTER(C.c_double)]
+            lib.ref_fusion_sqt_timed.restype = C.c_int
             lib.ref_fused_dgemm.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, _dp, C.c_int,
                                             _dp, C.c_int, _dp, C.c_int, _dp, _dp]
         if variant == "gemm":
             lib.ref_gemm_sqt.argtypes = [_dp, _dp, _dp]
             lib.ref_gemm_sqt.restype = C.c_int
+            lib.ref_gemm_sqt_band.argtypes = [_dp, _dp, C.c_long, _dp, C.POINTER(C.c_double),
+                                              C.POINTER(C.c_double)]
+            lib.ref_gemm_sqt_band.restype = C.c_int
         self.lib = lib
         self.variant = variant
         self.threads = 1
@@ -196,6 +204,35 @@ class RefLib:
         if self.lib.ref_steps(s, int(nsteps), float(spin_len)) != 0:
             raise MemoryError("ref_steps")
         return s
+
+    def step_time(self, spin, spin_len=1.0) -> float:
+        """Seconds of one runge_kutta + renormalisation step of the reference
+        on `spin` (a second step, timed after a first that touches the work
+        buffers, as main's loop reuses them)."""
+        s = np.array(spin, dtype=np.float64, copy=True, order="C")
+        t = C.c_double(0.0)
+        if self.lib.ref_steps_timed(s, 2, float(spin_len), C.byref(t)) != 0:
+            raise MemoryError("ref_steps_timed")
+        return t.value
+
+    def fusion_sqt_timed(self, spin_t):
+        """(S(q,t) over the band, seconds of the O(M K) pack, seconds of the band)."""
+        out = np.zeros(2)
+        tp, tb = C.c_double(0.0), C.c_double(0.0)
+        if self.lib.ref_fusion_sqt_timed(np.ascontiguousarray(spin_t), out, C.byref(tp),
+                                         C.byref(tb)) != 0:
+            raise RuntimeError("ref_fusion_sqt_timed")
+        return complex(out[0], out[1]), tp.value, tb.value
+
+    def gemm_sqt_band(self, spin_t, spin_0, rows):
+        """The gemm program's S(q,t) over the first `rows` rows of C:
+        (value over the band, seconds of the O(M K) packs, seconds of the band)."""
+        out = np.zeros(2)
+        tp, tb = C.c_double(0.0), C.c_double(0.0)
+        if self.lib.ref_gemm_sqt_band(np.ascontiguousarray(spin_t), np.ascontiguousarray(spin_0),
+                                      int(rows), out, C.byref(tp), C.byref(tb)) != 0:
+            raise MemoryError("ref_gemm_sqt_band")
+        return complex(out[0], out[1]), tp.value, tb.value
 
     def fusion_init(self, spin_0, rows=0):
         rc = self.lib.ref_fusion_init(np.ascontiguousarray(spin_0), int(rows))

@@ -73,14 +73,17 @@ void ref_runge_kutta(double *spin, double *cur, double *k1, double *k2, double *
 }
 
 /* nsteps of runge_kutta + main's renormalisation (llg_sqt_baseline.c:296-309;
- * spin_len 1.5 reproduces llg_sqt_fusion.c:350-361). */
-int ref_steps(double *spin, int nsteps, double spin_len)
+ * spin_len 1.5 reproduces llg_sqt_fusion.c:350-361).  With t_last != NULL it
+ * receives the wall time of the last step alone (the work buffers, like
+ * main's, are allocated and touched before it). */
+int ref_steps_timed(double *spin, int nsteps, double spin_len, double *t_last)
 {
     const size_t n = (size_t)Nfile * N * N * 3;
     double *buf = (double *)malloc(5 * n * sizeof(double));
     if (!buf) return -1;
     double *cur = buf, *k1 = buf + n, *k2 = buf + 2 * n, *k3 = buf + 3 * n, *k4 = buf + 4 * n;
     for (int s = 0; s < nsteps; s++) {
+        const double t0 = omp_get_wtime();
         runge_kutta(spin, cur, k1, k2, k3, k4);
 #pragma omp parallel for
         for (long j = 0; j < (long)Nfile * N * N; j++) {
@@ -97,9 +100,15 @@ int ref_steps(double *spin, int nsteps, double spin_len)
             }
             spin[j * 3] = tx, spin[j * 3 + 1] = ty, spin[j * 3 + 2] = tz;
         }
+        if (t_last) *t_last = omp_get_wtime() - t0;
     }
     free(buf);
     return 0;
+}
+
+int ref_steps(double *spin, int nsteps, double spin_len)
+{
+    return ref_steps_timed(spin, nsteps, spin_len, NULL);
 }
 
 static void mean_over_replicas(const double *spin, double *avg)
@@ -175,11 +184,15 @@ int ref_fusion_init(const double *spin_0, long rows)
     return 0;
 }
 
-/* One S(q,t) evaluation, llg_sqt_fusion.c:370-441, over the first g_rows rows. */
-int ref_fusion_sqt(const double *spin_all, double out[2])
+/* One S(q,t) evaluation, llg_sqt_fusion.c:370-441, over the first g_rows
+ * rows.  t_pack (if not NULL) receives the time of the A pack and the replica
+ * means (O(M K), the same for any band), t_band the time of the C set-up and
+ * fused_dgemm over the band (proportional to its rows). */
+int ref_fusion_sqt_timed(const double *spin_all, double out[2], double *t_pack, double *t_band)
 {
     const long M = (long)N * N, mm = g_rows;
     if (!g_cmat) return -1;
+    const double t0 = omp_get_wtime();
 #pragma omp parallel for
     for (long j = 0; j < M; j++)
         for (int i = 0; i < Nfile; i++) {
@@ -188,6 +201,7 @@ int ref_fusion_sqt(const double *spin_all, double out[2])
             g_spint[j + (i * 3 + 2) * M] = spin_all[i * M * 3 + j * 3 + 2];
         }
     mean_over_replicas(spin_all, g_fint);
+    const double t1 = omp_get_wtime();
 #pragma omp parallel for
     for (long j = 0; j < M; j++) {
         double zx = g_zerot[j * 3], zy = g_zerot[j * 3 + 1], zz = g_zerot[j * 3 + 2];
@@ -209,7 +223,15 @@ int ref_fusion_sqt(const double *spin_all, double out[2])
     res /= (double)(N * N);
     out[0] = creal(res);
     out[1] = cimag(res);
+    const double t2 = omp_get_wtime();
+    if (t_pack) *t_pack = t1 - t0;
+    if (t_band) *t_band = t2 - t1;
     return 0;
+}
+
+int ref_fusion_sqt(const double *spin_all, double out[2])
+{
+    return ref_fusion_sqt_timed(spin_all, out, NULL, NULL);
 }
 
 /* Direct access to the reference's fused_dgemm, for element-level pins. */
@@ -221,37 +243,56 @@ void ref_fused_dgemm(int m, int n, int k, double alpha, double *a, int lda, doub
 #endif
 
 #if defined(REF_VARIANT_GEMM)
-/* gemm/llg_sqt_mkl.c:349-423 with the reference's cblas_dgemm call (:378). */
-int ref_gemm_sqt(const double *spin_all, const double *spin_0, double out[2])
+/* gemm/llg_sqt_mkl.c:349-423 with the reference's cblas_dgemm call (:378),
+ * over the first `rows` rows of C (all M when rows <= 0 or rows > M), so that
+ * a bounded CPU sample of the same program can be timed where the whole
+ * (M x M) C does not fit in host memory.  t_pack (if not NULL) receives the
+ * time of the per-step A pack and replica means (O(M K), the same for any
+ * band; the program's one-time B pack is not timed), t_band the time of
+ * cblas_dgemm and the subtraction / phase sweep over the band (proportional
+ * to its rows). */
+int ref_gemm_sqt_band(const double *spin_all, const double *spin_0, long rows, double out[2],
+                      double *t_pack, double *t_band)
 {
     const long M = (long)N * N;
     const int K = Nfile * 3;
+    const long mm = (rows <= 0 || rows > M) ? M : rows;
     double *spin_zero = (double *)malloc((size_t)M * K * sizeof(double));
     double *spint = (double *)malloc((size_t)M * K * sizeof(double));
     double *zerot = (double *)malloc((size_t)M * 3 * sizeof(double));
     double *fint = (double *)malloc((size_t)M * 3 * sizeof(double));
-    double *cmat = (double *)malloc((size_t)M * M * sizeof(double));
-    if (!spin_zero || !spint || !zerot || !fint || !cmat) return -2;
+    double *cmat = (double *)malloc((size_t)mm * M * sizeof(double));
+    if (!spin_zero || !spint || !zerot || !fint || !cmat) {
+        free(spin_zero), free(spint), free(zerot), free(fint), free(cmat);
+        return -2;
+    }
+    memset(cmat, 0, (size_t)mm * M * sizeof(double)); /* first touch outside the timing */
+    /* the program's one-time set-up (spin_zero and zerot before the time loop) */
+#pragma omp parallel for
     for (long i = 0; i < M; i++)
         for (int j = 0; j < Nfile; j++)
             for (int c = 0; c < 3; c++) spin_zero[i * Nfile * 3 + j * 3 + c] = spin_0[j * M * 3 + i * 3 + c];
     mean_over_replicas(spin_0, zerot);
+    /* per step: the replica means and the A pack, then the GEMM and the sweep */
+    const double t0 = omp_get_wtime();
     mean_over_replicas(spin_all, fint);
+#pragma omp parallel for
     for (long j = 0; j < M; j++)
         for (int i = 0; i < Nfile; i++)
             for (int c = 0; c < 3; c++) spint[j + (i * 3 + c) * M] = spin_all[i * M * 3 + j * 3 + c];
+    const double t1 = omp_get_wtime();
     const double alpha = 1.0 / (double)Nfile;
-    cblas_dgemm(102 /*ColMajor*/, 111 /*NoTrans*/, 111, (int)M, (int)M, K, alpha, spint, (int)M,
-                spin_zero, K, 0.0, cmat, (int)M);
+    cblas_dgemm(102 /*ColMajor*/, 111 /*NoTrans*/, 111, (int)mm, (int)M, K, alpha, spint, (int)M,
+                spin_zero, K, 0.0, cmat, (int)mm);
     const double qx = 2.0 * M_PI * vx / (double)N;
     const double qy = 2.0 * M_PI * vy / (double)N;
     double re = 0.0, im = 0.0;
 #pragma omp parallel for reduction(+ : re, im)
     for (long j = 0; j < M; j++) {
         double zx = zerot[j * 3], zy = zerot[j * 3 + 1], zz = zerot[j * 3 + 2];
-        for (long i = 0; i < M; i++) {
+        for (long i = 0; i < mm; i++) {
             double outer = fint[i * 3] * zx + fint[i * 3 + 1] * zy + fint[i * 3 + 2] * zz;
-            double cij = cmat[i + j * M] - outer;
+            double cij = cmat[i + j * mm] - outer;
             int ri = (int)(i / N), ci = (int)(i % N), rj = (int)(j / N), cj = (int)(j % N);
             double dffr = ri - rj, dffc = ci - cj;
             double complex q = cexp(CMPLX(0.0, -1.0) * (qx * dffr + qy * dffc));
@@ -259,9 +300,17 @@ int ref_gemm_sqt(const double *spin_all, const double *spin_0, double out[2])
             im += cij * cimag(q);
         }
     }
+    const double t2 = omp_get_wtime();
     out[0] = re / (double)(N * N);
     out[1] = im / (double)(N * N);
+    if (t_pack) *t_pack = t1 - t0;
+    if (t_band) *t_band = t2 - t1;
     free(spin_zero), free(spint), free(zerot), free(fint), free(cmat);
     return 0;
+}
+
+int ref_gemm_sqt(const double *spin_all, const double *spin_0, double out[2])
+{
+    return ref_gemm_sqt_band(spin_all, spin_0, 0, out, NULL, NULL);
 }
 #endif

@@ -167,7 +167,7 @@ def test_scratch_poisoning_changes_nothing(kernel):
         ctx.set_llg_kernel(kernel)
         P()
         ctx.set_spins(s0, as_origin=True)
-        for mode in ("fp64", "fp64_fused", "tf32x3", "bf16x3"):
+        for mode in ("fp64", "tf32x3", "bf16x3"):
             P()
             ctx.step(1)
             P()

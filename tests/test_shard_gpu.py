@@ -50,7 +50,7 @@ def test_shards_add_up_to_the_whole_ensemble(oracle, N, nf, parts):
             c.step(1)
             assert np.array_equal(c.get_spins(), want_spins[b:e]), (step, b)
         ref = whole.sqt("fp64")
-        for mode in ("fp64", "fp64_fused", "tf32x3", "bf16x3"):
+        for mode in ("fp64", "tf32x3", "bf16x3"):
             parts_t = [torch.zeros(2, **f64) for _ in shards]
             sums_t = [torch.zeros(3 * M, **f64) for _ in shards]
             for (_, _, c), p, s in zip(shards, parts_t, sums_t):

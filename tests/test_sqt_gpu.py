@@ -14,7 +14,7 @@ from conftest import rel_err
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp64": 1e-12, "fp64_fused": 1e-12, "tf32x3": 1e-5, "bf16x3": 1e-5}
+TOL = {"fp64": 1e-12, "tf32x3": 1e-5, "bf16x3": 1e-5}
 
 
 @pytest.mark.parametrize("name", ["llg_n12_f4", "llg_n20_f6"])
@@ -196,7 +196,7 @@ def test_step_host_async_consecutive_steps(oracle, nf, kernel, where):
     s0 = asd.random_spins(N, nf, seed=21)
     kw = dict(J1=-1.0, J2=0.2, alpha=0.05, h=(0, 0, 0.5), dt=0.005)
     p = asd.Params.make(N, nf, vx=3, vy=2, **kw)
-    modes = ["tf32x3", "fp64", "bf16x3", "fp64_fused", "tf32x3"]
+    modes = ["tf32x3", "fp64", "bf16x3", "fp64", "tf32x3"]
     with asd.Context(p) as a, asd.Context(p) as b:
         a.set_llg_kernel(kernel)
         a.set_spins(s0, as_origin=True)
@@ -270,7 +270,7 @@ def test_step_host_in_replica_chunks(oracle, nf, pinned, kernel):
         if pinned:
             buf = buf.pin_memory()
         want_spins = s0
-        for step, mode in enumerate(["tf32x3", "fp64", "bf16x3", "fp64_fused", "tf32x3"]):
+        for step, mode in enumerate(["tf32x3", "fp64", "bf16x3", "fp64", "tf32x3"]):
             got = a.step_host(buf.data_ptr(), buf.data_ptr(), mode)
             b.step(1)
             ref = b.sqt("fp64")

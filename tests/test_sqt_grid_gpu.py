@@ -54,9 +54,11 @@ def test_grid_largest_and_too_large():
         assert rel_err(g[0, 0], ctx.sqt("fp64")) < 1e-11
     with asd.Context(asd.Params.make(65, 1)) as ctx:
         ctx.set_spins(asd.random_spins(65, 1, seed=1), as_origin=True)
-        with pytest.raises(asd.AsdError) as e:
-            ctx.sqt_grid("fp64")
-        assert e.value.code == asd.ASD_ERR_UNSUPPORTED
+        assert np.all(np.isfinite(ctx.sqt_grid("fp64")))  # no size limit in FP64
+        for mode in ("tf32x3", "bf16x3"):
+            with pytest.raises(asd.AsdError) as e:
+                ctx.sqt_grid(mode)
+            assert e.value.code == asd.ASD_ERR_UNSUPPORTED
 
 
 def test_fp64_configuration_32x32_full_run(oracle):
