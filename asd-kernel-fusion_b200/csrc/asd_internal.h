@@ -137,9 +137,6 @@ int launch_dmma_sqt(const DmmaSqtArgs &p, cudaStream_t st);
 long qgrid_keys(int num_m, int num_n, int bm, int bn);
 cudaError_t launch_qgrid_bins(const double *tdiag, int num_m, int num_n, int bm, int bn, int lat_n,
                               double *ds, double *G, cudaStream_t st);
-// G[b] = sum over p < nparts of gpart[p][b], fixed order.
-cudaError_t launch_hist_reduce(const double *gpart, int nparts, int nbins, double *G,
-                               cudaStream_t st);
 // out[2*(a*N+b)+{0,1}] = scale * sum_d G[d] e^{-2 pi i (a dr + b dc)/N}; tmp holds N*N double2.
 cudaError_t launch_grid_dft(const double *G, int lat_n, double scale, double2 *tmp, double *out,
                             cudaStream_t st);
@@ -185,7 +182,8 @@ struct UmmaSqtArgs {
     int chunk_k = 0;          // K elements per TMEM accumulation chunk (0: all)
     float *dbg_c = nullptr;   // diagnostic: store the accumulator instead
     long dbg_ldc = 0;
-    double *gpart = nullptr;  // q grid: per-CTA FP64 histograms [grid][N*N]
+    double *tdiag = nullptr;  // q grid: per-tile diagonal partials
+                              // [Mp/BM][Mp/BN][BM+BN-1][2] (qgrid.cu)
     int lat_n = 0;            // lattice side (q grid)
     // K sub-range [k_begin, k_end) in elements (multiples of the k block;
     // k_end = 0: to Kp).  The epilogue applies the connected-part term only
@@ -198,6 +196,8 @@ struct UmmaSqtArgs {
 // Returns the number of CTAs launched (partials written) or a negative error.
 int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st);
 long umma_row_pad(long M);   // rows/cols padded to the tile multiple
+int umma_tile_rows();        // BM = 128 (the q grid's tile geometry)
+int umma_tile_cols();        // BN = 256
 // CTAs launch_umma_sqt launches for M rows on num_sms SMs (max_grid unset).
 long umma_max_grid_for(long M, int num_sms);
 cudaError_t launch_mbar_timeout_probe(uint32_t limit, unsigned *status, cudaStream_t st);

@@ -611,8 +611,6 @@ int loss_grad(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target
     return ASD_OK;
 }
 
-constexpr int kGridMaxSitesSplit = 4096;  // split modes: bins in shared memory
-
 // Work space of the q grid's diagonal partials, grown on demand.
 int ensure_grid_work(asd_ctx *c, size_t tdiag_n, size_t ds_n) {
     int rc;
@@ -640,9 +638,6 @@ int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
     const long M = c->M;
     if (mode != ASD_SQT_FP64 && mode != ASD_SQT_TF32X3 && mode != ASD_SQT_BF16X3)
         return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t): mode %d not supported", mode);
-    if (mode != ASD_SQT_FP64 && M > kGridMaxSitesSplit)
-        return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t) in split precision supports N*N <= %d sites (N=%d)",
-                    kGridMaxSitesSplit, N);
     if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
     int rc;
     // each checked on its own: after a failed allocation of grid_t, grid_g
@@ -670,51 +665,51 @@ int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
         c->last_launches += 5;
         return ASD_OK;
     }
-    int nparts = 0;
-    {
-        const int kind = (mode == ASD_SQT_TF32X3) ? 1 : 2;
-        if (!c->a_hi[kind]) return fail(ASD_ERR_STATE, "split mode %d not enabled at create", kind);
-        if (c->a_version[kind] != c->state_version) {
-            ASD_CUDA_TRY(launch_split(kind, c->y, c->M, c->K, c->Kp[kind], c->a_hi[kind],
-                                      c->a_lo[kind], c->stream));
-            c->a_version[kind] = c->state_version;
-            c->last_launches += 1;
-        }
-        if (c->b_version[kind] != c->origin_version) {
-            ASD_CUDA_TRY(launch_split(kind, c->origin, c->M, c->K, c->Kp[kind], c->b_hi[kind],
-                                      c->b_lo[kind], c->stream));
-            c->b_version[kind] = c->origin_version;
-            c->last_launches += 1;
-        }
-        if ((rc = ensure_part(c, ((long)c->num_sms * M + 1) / 2)) != ASD_OK) return rc;
-        UmmaSqtArgs u{};
-        u.kind = kind;
-        u.M = c->M;
-        u.Kp = c->Kp[kind];
-        u.a_hi = c->a_hi[kind];
-        u.a_lo = c->a_lo[kind];
-        u.b_hi = c->b_hi[kind];
-        u.b_lo = c->b_lo[kind];
-        u.row4 = c->row4;
-        u.row1 = c->row1;
-        u.col4 = c->col4;
-        u.col1 = c->col1;
-        u.alpha = (float)(1.0 / (double)c->p.nfile);
-        u.part = c->part;
-        u.status = c->status;
-        u.num_sms = c->num_sms;
-        u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
-        u.gpart = reinterpret_cast<double *>(c->part);
-        u.lat_n = N;
-        const int grid = launch_umma_sqt(u, c->stream);
-        if (grid < 0) return grid;
+    const int kind = (mode == ASD_SQT_TF32X3) ? 1 : 2;
+    if (!c->a_hi[kind]) return fail(ASD_ERR_STATE, "split mode %d not enabled at create", kind);
+    if (c->a_version[kind] != c->state_version) {
+        ASD_CUDA_TRY(launch_split(kind, c->y, c->M, c->K, c->Kp[kind], c->a_hi[kind],
+                                  c->a_lo[kind], c->stream));
+        c->a_version[kind] = c->state_version;
         c->last_launches += 1;
-        nparts = grid;
     }
-    ASD_CUDA_TRY(launch_hist_reduce(reinterpret_cast<double *>(c->part), nparts, (int)M, c->grid_g,
-                                    c->stream));
-    ASD_CUDA_TRY(launch_grid_dft(c->grid_g, N, 1.0 / (double)M, c->grid_t, d_out, c->stream));
+    if (c->b_version[kind] != c->origin_version) {
+        ASD_CUDA_TRY(launch_split(kind, c->origin, c->M, c->K, c->Kp[kind], c->b_hi[kind],
+                                  c->b_lo[kind], c->stream));
+        c->b_version[kind] = c->origin_version;
+        c->last_launches += 1;
+    }
+    const int bm = umma_tile_rows(), bn = umma_tile_cols();
+    const int num_m = (int)(c->Mp / bm), num_n = (int)(c->Mp / bn);
+    const size_t nd2 = 2 * (size_t)(bm + bn - 1);
+    rc = ensure_grid_work(c, (size_t)num_m * num_n * nd2, (size_t)qgrid_keys(num_m, num_n, bm, bn) * nd2);
+    if (rc != ASD_OK) return rc;
+    UmmaSqtArgs u{};
+    u.kind = kind;
+    u.M = c->M;
+    u.Kp = c->Kp[kind];
+    u.a_hi = c->a_hi[kind];
+    u.a_lo = c->a_lo[kind];
+    u.b_hi = c->b_hi[kind];
+    u.b_lo = c->b_lo[kind];
+    u.row4 = c->row4;
+    u.row1 = c->row1;
+    u.col4 = c->col4;
+    u.col1 = c->col1;
+    u.alpha = (float)(1.0 / (double)c->p.nfile);
+    u.part = c->part;
+    u.status = c->status;
+    u.num_sms = c->num_sms;
+    u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
+    u.tdiag = c->grid_tdiag;
+    u.lat_n = N;
+    const int grid = launch_umma_sqt(u, c->stream);
+    if (grid < 0) return grid;
+    ASD_CUDA_TRY(launch_qgrid_bins(c->grid_tdiag, num_m, num_n, bm, bn, N, c->grid_ds, c->grid_g,
+                                   c->stream));
     c->last_launches += 3;
+    ASD_CUDA_TRY(launch_grid_dft(c->grid_g, N, 1.0 / (double)M, c->grid_t, d_out, c->stream));
+    c->last_launches += 1;
     return ASD_OK;
 }
 

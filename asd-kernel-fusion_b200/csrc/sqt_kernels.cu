@@ -171,14 +171,6 @@ __global__ void __launch_bounds__(256) split_bf16_kernel(const double *__restric
     lo[o] = __halves2bfloat162(l0, l1);
 }
 
-__global__ void hist_reduce_kernel(const double *__restrict__ gpart, int nparts, int nbins,
-                                   double *__restrict__ G) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nbins) return;
-    double s = 0.0;
-    for (int p = 0; p < nparts; ++p) s += gpart[(long)p * nbins + b];
-    G[b] = s;
-}
 
 // Separable 2-D DFT of the displacement histogram: T[dr][b] = sum_dc G[dr][dc]
 // e^{-2 pi i b dc / N}, then S[a][b] = scale * sum_dr T[dr][b] e^{-2 pi i a dr / N}.
@@ -288,11 +280,6 @@ cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, v
 
 
 
-cudaError_t launch_hist_reduce(const double *gpart, int nparts, int nbins, double *G,
-                               cudaStream_t st) {
-    hist_reduce_kernel<<<(nbins + 255) / 256, 256, 0, st>>>(gpart, nparts, nbins, G);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_grid_dft(const double *G, int lat_n, double scale, double2 *tmp, double *out,
                             cudaStream_t st) {

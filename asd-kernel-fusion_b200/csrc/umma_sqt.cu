@@ -39,7 +39,12 @@ constexpr uint32_t WAIT_LIMIT = 1u << 24;
 // 256x256x1000: groups of 16 keep the DRAM traffic lowest (the group's A
 // bands, 24-48 MB, stay in L2 while B streams past once per group).
 constexpr int GROUP_M = 16;
-constexpr int kGridMaxBins = 4096;  // q-grid histogram: N*N FP32 bins in shared memory
+// q grid: per warp, a 32 x 32 transposition buffer (FP32) while a tile is
+// binned, then the warp's tile-diagonal partials (9 x 32 x 2 FP64) when it is
+// combined; the two uses alternate, so they share one region.
+constexpr int GRID_DIAG_M = 9;  // diagonals per lane and warp: 32 m + lane, 9 values of m
+constexpr int GRID_SCRATCH_BYTES = 4 * GRID_DIAG_M * 32 * 2 * 8;  // >= 4 * 32 * 32 * 4
+constexpr int GRID_ND = BM + BN - 1;  // diagonals r - c of a 128 x 256 tile
 
 // Pipeline geometry: 128 bytes of K per operand row per stage (the 128-byte
 // swizzle width), two stages of 96 KB (Ah, Al 128 x 128 B; Bh, Bl 256 x 128 B).
@@ -105,13 +110,77 @@ __device__ __forceinline__ bool epilogue_sync(uint64_t *bar, uint32_t &phase,
     return ok;
 }
 
+// q grid: one 32 x 32 block (column group c) of a warp's accumulator rows.
+// Lane l holds v[jj] = acc(row 32 q + l, column 32 c + jj).  The block's
+// diagonals are lambda = l - jj in [-31, 31]; lane L owns lambda = L (tile
+// diagonal 32 (q - c) + L, register gd[8 - c]) and lambda = L - 32 (tile
+// diagonal 32 (q - c - 1) + L, gd[7 - c]).  Lane l writes v[jj] to row
+// (l - jj) mod 32, column l of the warp's buffer; lane L then reads its row,
+// from column L onwards (conflict-free both ways), and adds each value to
+// its diagonal and class.  a_first is (i - j) mod N on lambda = L of block 0;
+// the column displacement a of a diagonal decides the class of an element of
+// row x (its lattice column): class 0 iff x >= a.
+__device__ __forceinline__ void grid_block(const uint32_t (&v)[32], int c, int lane,
+                                           const float4 &r4, const float4 *z_tab, float alpha,
+                                           bool last, int x_row, int a_first, int N, float *xp,
+                                           double (&gd)[9][2]) {
+    const float4 *zq = z_tab + c * 32;
+#pragma unroll
+    for (int jj = 0; jj < 32; ++jj) {
+        float val = alpha * __uint_as_float(v[jj]);
+        if (last) {
+            const float4 z = zq[jj];
+            float o = r4.x * z.x;
+            o = fmaf(r4.y, z.y, o);
+            o = fmaf(r4.z, z.z, o);
+            val -= o;
+        }
+        xp[((lane - jj) & 31) * 32 + lane] = val;
+    }
+    __syncwarp();
+    // diagonal lambda = L of block c: i - j shifted by -32 c from block 0
+    int aa = (a_first - ((32 * c) % N)) % N;
+    if (aa < 0) aa += N;
+    int ab = (aa - (32 % N)) % N;  // lambda = L - 32
+    if (ab < 0) ab += N;
+    // column of source row l = lane + s (mod 32): x_row of lane l
+    const int x0 = __shfl_sync(0xffffffffu, x_row, 0);  // row 32 q + 0
+    float pa0 = 0.f, pa1 = 0.f, pb0 = 0.f, pb1 = 0.f;
+#pragma unroll 8
+    for (int s = 0; s < 32; ++s) {
+        const int l = (lane + s) & 31;
+        const float val = xp[lane * 32 + l];
+        int x = x0 + l;
+        if (x >= N) x = (N >= 32) ? x - N : x % N;
+        const bool b = s >= 32 - lane;  // l < lane: lambda = L - 32
+        const bool c1 = x < (b ? ab : aa);
+        pa0 += (!b && !c1) ? val : 0.f;
+        pa1 += (!b && c1) ? val : 0.f;
+        pb0 += (b && !c1) ? val : 0.f;
+        pb1 += (b && c1) ? val : 0.f;
+    }
+    __syncwarp();  // the buffer is free for the next block
+    gd[8 - c][0] += (double)pa0;
+    gd[8 - c][1] += (double)pa1;
+    gd[7 - c][0] += (double)pb0;  // zero in lane 0, which has no lambda = -32
+    gd[7 - c][1] += (double)pb1;
+}
+
 // KIND: 1 = TF32x3, 2 = BF16x3.  EPI selects the epilogue:
 //   EPI_PHASE  S(q,t) at one q: per-CTA partial sum of u_i w_j (alpha C - m.z)
 //   EPI_STORE  the raw FP32 accumulator to dbg_c[i * dbg_ldc + j] (diagnostic)
-//   EPI_GRID   displacement bins for the whole q grid: every element
-//              alpha C_ij - m_i.z_j goes to bin (r_i - r_j) mod N of a
-//              per-tile FP32 shared histogram, flushed after each tile into
-//              this CTA's FP64 histogram gpart[blockIdx.x][N*N]
+//   EPI_GRID   the whole q grid: per tile, the sums of alpha C_ij - m_i.z_j
+//              along each diagonal d = r - c of the tile, split by whether
+//              the lattice column of j wraps (class 0: col(j) <= col(i)),
+//              into tdiag[mb][nb][d + BN - 1][class] (qgrid.cu bins them).
+//              Each epilogue lane owns the diagonals d = 32 m + lane of its
+//              warp's 32 rows: a 32 x 32 block of the accumulator goes
+//              through shared memory transposed along its diagonals (lane l
+//              writes its value of column jj to row (l - jj) mod 32), each
+//              lane sums its two diagonals of the block in a fixed order
+//              (FP32, at most 32 terms) into FP64 registers, and the four
+//              warps' registers are combined per tile in warp order.  No
+//              atomics: the bins repeat bit for bit.
 constexpr int EPI_PHASE = 0, EPI_STORE = 1, EPI_GRID = 2;
 template <int KIND, int EPI>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
@@ -123,7 +192,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     const float *__restrict__ row1, const float4 *__restrict__ col4,
                     const float *__restrict__ col1, float alpha, double2 *__restrict__ part,
                     unsigned *__restrict__ status, float *__restrict__ dbg_c, long dbg_ldc,
-                    int lat_n, long n_sites, double *__restrict__ gpart, int group_m) {
+                    int lat_n, double *__restrict__ tdiag, int group_m) {
     using G = Geo;
     constexpr bool STORE = (EPI == EPI_STORE);
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -132,9 +201,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     float2 *tab_w = reinterpret_cast<float2 *>(smem + G::PIPE_BYTES);           // [2][BN]
     float4 *tab_z = reinterpret_cast<float4 *>(smem + G::PIPE_BYTES + 2 * BN * sizeof(float2));
     SmemTail *tail = reinterpret_cast<SmemTail *>(smem + G::PIPE_BYTES + G::TABLE_BYTES);
-    float *hist = reinterpret_cast<float *>(smem + G::PIPE_BYTES + G::TABLE_BYTES +
-                                            ((sizeof(SmemTail) + 15) & ~size_t(15)));
-    const int nbins = lat_n * lat_n;
+    uint8_t *gscr = smem + G::PIPE_BYTES + G::TABLE_BYTES + ((sizeof(SmemTail) + 15) & ~size_t(15));
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
     const int num_tiles = num_m * num_n;
@@ -301,13 +368,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         double tot_re = 0.0, tot_im = 0.0;
         int tcount = 0;
         uint32_t ephase = 0;
-        double *gp = (EPI == EPI_GRID) ? gpart + (long)blockIdx.x * nbins : nullptr;
-        if (EPI == EPI_GRID) {
-            for (int b = etid; b < nbins; b += 128) {
-                hist[b] = 0.f;
-                gp[b] = 0.0;
-            }
-        }
+        float *xpose = reinterpret_cast<float *>(gscr) + quarter * 32 * 32;  // [32][32]
+        double *wdiag = reinterpret_cast<double *>(gscr);                       // [4][9][32][2]
         for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++tcount) {
             int mb, nb;
             tile_coords(tile, num_m, num_n, group_m, mb, nb);
@@ -336,6 +398,20 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const float ui = STORE ? 0.f : row1[i];
             double s_re = 0.0, s_im = 0.0;
             bool ok = true;
+            // q grid: this lane's diagonals d = 32 (quarter - 8 + mm) + lane of
+            // the tile, both classes; the column of its own row's site;
+            // the columns a = (i - j) mod N of its first block's two diagonals.
+            double gd[GRID_DIAG_M][2];
+            int x_row = 0, a_first = 0;
+            if (EPI == EPI_GRID) {
+#pragma unroll
+                for (int mm = 0; mm < GRID_DIAG_M; ++mm) gd[mm][0] = gd[mm][1] = 0.0;
+                x_row = (int)((mb * (long)BM + quarter * 32 + lane) % lat_n);
+                // diagonal d = 32 quarter + lane of block c = 0: i - j = i0 - j0 + d
+                long dl = (long)mb * BM - (long)nb * BN + quarter * 32 + lane;
+                dl %= lat_n;
+                a_first = (int)(dl < 0 ? dl + lat_n : dl);
+            }
             for (int kb0 = kb_begin; kb0 < kb_end; kb0 += kb_per_chunk) {
                 const bool first = (kb0 == kb_begin);
                 // the connected-part term, once per row: in the last chunk
@@ -349,8 +425,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 ptx::tc_fence_after();
                 // Per 32-column group, in FP32: a = sum_j w_j acc_ij and, in the
                 // last chunk only, o = sum_j w_j (m_i . z_j); the row sum
-                // s_i = alpha * a - o is carried in FP64.
-#pragma unroll 1
+                // s_i = alpha * a - o is carried in FP64.  (The q grid unrolls
+                // the groups: its per-lane diagonal registers are indexed by c.)
+                constexpr int CU = (EPI == EPI_GRID) ? BN / 32 : 1;
+#pragma unroll CU
                 for (int c = 0; c < BN / 32; ++c) {
                     uint32_t v[32];
                     const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) +
@@ -365,32 +443,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         continue;
                     }
                     if (EPI == EPI_GRID) {
-                        if (i >= n_sites) continue;  // padding row
-                        const int r_i = (int)(i / lat_n), c_i = (int)(i - (long)r_i * lat_n);
-                        const long js = j0 + c * 32;
-                        int rj = (int)(js / lat_n), cj = (int)(js - (long)rj * lat_n);
-                        const float4 *zq = z_tab + c * 32;
-#pragma unroll 4
-                        for (int jj = 0; jj < 32; ++jj) {
-                            if (js + jj < n_sites) {
-                                float val = alpha * __uint_as_float(v[jj]);
-                                if (last) {
-                                    const float4 z = zq[jj];
-                                    float o = r4.x * z.x;
-                                    o = fmaf(r4.y, z.y, o);
-                                    o = fmaf(r4.z, z.z, o);
-                                    val -= o;
-                                }
-                                int dr = r_i - rj, dc = c_i - cj;
-                                dr += (dr < 0) ? lat_n : 0;
-                                dc += (dc < 0) ? lat_n : 0;
-                                atomicAdd(&hist[dr * lat_n + dc], val);
-                            }
-                            if (++cj == lat_n) {
-                                cj = 0;
-                                ++rj;
-                            }
-                        }
+                        grid_block(v, c, lane, r4, z_tab, alpha, last, x_row, a_first, lat_n,
+                                   xpose, gd);
                         continue;
                     }
                     const float4 *wq = reinterpret_cast<const float4 *>(w_tab + c * 32);
@@ -433,14 +487,34 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             }
             if (!ok) break;
             if (EPI == EPI_GRID) {
-                // tile histogram -> this CTA's FP64 histogram, then clear it
+                // the four warps' diagonals -> tdiag[tile], in warp order; the
+                // shared region served as transposition buffers until now
                 if (!epilogue_sync(&tail->ebar, ephase, abort_flag)) {
                     raise_abort(tail, status);
                     break;
                 }
-                for (int b = etid; b < nbins; b += 128) {
-                    gp[b] += (double)hist[b];
-                    hist[b] = 0.f;
+                double *wq = wdiag + quarter * (GRID_DIAG_M * 32 * 2);
+#pragma unroll
+                for (int mm = 0; mm < GRID_DIAG_M; ++mm) {
+                    wq[(mm * 32 + lane) * 2] = gd[mm][0];
+                    wq[(mm * 32 + lane) * 2 + 1] = gd[mm][1];
+                }
+                if (!epilogue_sync(&tail->ebar, ephase, abort_flag)) {
+                    raise_abort(tail, status);
+                    break;
+                }
+                double *td = tdiag + ((long)mb * num_n + nb) * GRID_ND * 2;
+                for (int idx = etid; idx < GRID_ND * 2; idx += 128) {
+                    const int d = idx / 2 - (BN - 1), cls = idx & 1;
+                    const int L = (d + 256) & 31, m = (d - L) / 32;
+                    double sum = 0.0;
+#pragma unroll
+                    for (int w = 0; w < 4; ++w) {
+                        const int mm = m - w + 8;
+                        if (mm >= 0 && mm < GRID_DIAG_M)
+                            sum += wdiag[((w * GRID_DIAG_M + mm) * 32 + L) * 2 + cls];
+                    }
+                    td[idx] = sum;
                 }
                 if (!epilogue_sync(&tail->ebar, ephase, abort_flag)) {
                     raise_abort(tail, status);
@@ -512,6 +586,9 @@ int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int
 
 long umma_row_pad(long M) { return (M + BN - 1) / BN * BN; }
 
+int umma_tile_rows() { return BM; }
+int umma_tile_cols() { return BN; }
+
 long umma_max_grid_for(long M, int num_sms) {
     const long Mp = umma_row_pad(M);
     const long tiles = (Mp / BM) * (Mp / BN);
@@ -550,11 +627,11 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     int grid = tiles < a.num_sms ? tiles : a.num_sms;
     if (a.max_grid > 0 && grid > a.max_grid) grid = a.max_grid;
     if (grid < 1) return fail(ASD_ERR_INVALID, "no tiles to launch");
-    const int epi = a.dbg_c ? EPI_STORE : (a.gpart ? EPI_GRID : EPI_PHASE);
-    if (epi == EPI_GRID && (a.lat_n < 1 || (long)a.lat_n * a.lat_n != a.M ||
-                            a.lat_n * a.lat_n > kGridMaxBins))
-        return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t) supports N*N <= %d sites", kGridMaxBins);
-    const int smem = smem_bytes() + ((epi == EPI_GRID) ? 4 * a.lat_n * a.lat_n + 16 : 0);
+    const int epi = a.dbg_c ? EPI_STORE : (a.tdiag ? EPI_GRID : EPI_PHASE);
+    if (epi == EPI_GRID && (a.lat_n < 1 || (long)a.lat_n * a.lat_n != a.M || a.k_begin != 0 ||
+                            (a.k_end != 0 && a.k_end != a.Kp)))
+        return fail(ASD_ERR_INVALID, "q grid: M must be N*N and K whole");
+    const int smem = smem_bytes() + ((epi == EPI_GRID) ? GRID_SCRATCH_BYTES : 0);
     auto go = [&](auto kern) {
         cudaError_t r =
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -562,7 +639,7 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
         kern<<<grid, NUM_THREADS, smem, st>>>(tah, tal, tbh, tbl, num_m, num_n, kb_begin, kb_end,
                                               kpc, a.outer, a.row4, a.row1, a.col4, a.col1,
                                               a.alpha, a.part, a.status, a.dbg_c, a.dbg_ldc,
-                                              a.lat_n, a.M, a.gpart, GROUP_M);
+                                              a.lat_n, a.tdiag, GROUP_M);
         return cudaGetLastError();
     };
     cudaError_t e;

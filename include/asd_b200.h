@@ -131,14 +131,14 @@ int asd_ctx_sqt_magnitude(asd_ctx *ctx, double *out);
 
 /* S(q,t) for every q = 2*pi*(a, b)/N of the N x N grid, into d_out[2*(a*N+b)]
  * (real) and d_out[2*(a*N+b)+1] (imaginary), a device buffer of 2*N*N
- * doubles; asynchronous.  The same correlation GEMM, with an epilogue that
- * bins every connected C_ij by the displacement r_i - r_j (mod N), followed by
- * a 2-D DFT of the N*N bins; d_out[2*(vx*N+vy)] equals asd_ctx_sqt's value.
- * Modes ASD_SQT_FP64, ASD_SQT_TF32X3 and ASD_SQT_BF16X3; lattices with
- * N*N <= 4096 (the bins live in shared memory).  The bins are summed with
- * shared-memory atomics (FP64 in the FP64 mode, FP32 in the split modes), so
- * the last bits vary from run to run: about 1e-17 absolute in FP64, 1e-8
- * relative in the split modes.
+ * doubles; asynchronous.  The same correlation GEMM (FP64, TF32x3 or BF16x3),
+ * with an epilogue that sums every connected C_ij - m_i . z_j along the
+ * diagonals i - j of each tile; the diagonal sums are binned by displacement
+ * r_i - r_j (mod N) and a 2-D DFT of the N*N bins gives S at every q.
+ * d_out[2*(vx*N+vy)] equals asd_ctx_sqt's value up to rounding.  Any N; work
+ * space on the first call: 8 * (128 + BN - 1) * 2 bytes per GEMM tile (BN =
+ * 128 in FP64, 256 in the split modes; 1.1 GB / 0.8 GB at N = 256).  Every
+ * sum runs in a fixed order, so results repeat bit for bit.
  * No counterpart in the reference (its programs evaluate one q). */
 int asd_ctx_sqt_grid_async(asd_ctx *ctx, asd_sqt_mode mode, double *d_out);
 /* Same into host memory (2*N*N doubles); synchronous. */

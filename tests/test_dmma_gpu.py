@@ -6,9 +6,9 @@
 * S(q,t) at one q within 1e-12 of the oracle's factorised FP64 value, for even
   K (16-byte copies) and odd K (8-byte copies), lattices whose site count is
   not a multiple of the 128-site tile, and repeated calls bit for bit.
-* The q grid through the diagonal partials at lattices beyond the shared-memory
-  bins' limit (N = 100, 128, 136), on a sample of q against the oracle's
-  factorised value at that q, and two runs bit for bit.
+* The q grid through the diagonal partials, every mode, at N = 100, 128 and
+  136, on a sample of q against the oracle's factorised value at that q, and
+  two runs bit for bit.
 * The measured FP64 peaks the benchmark quotes are plausible."""
 from __future__ import annotations
 
@@ -82,24 +82,28 @@ def test_fp64_kernel_is_timed():
 
 
 @pytest.mark.parametrize("N,nfile", [(100, 6), (128, 12), (136, 5)])
-def test_fp64_qgrid_large_lattices(oracle, N, nfile):
+def test_qgrid_large_lattices(oracle, N, nfile):
     """N*N = 10000 (tiles span several lattice rows), 16384 (tiles are whole
-    half rows) and 18496 sites: sampled q against the oracle's factorised
-    FP64 value at that q (1e-12 of max |S| over the sample), and the grid
-    twice, bit for bit."""
+    half rows) and 18496 sites, in every mode: sampled q against the oracle's
+    factorised FP64 value at that q (FP64 1e-12, split modes 1e-5, of max |S|
+    over the sample), and the grid twice, bit for bit."""
     s0 = asd.random_spins(N, nfile, seed=N + nfile)
     kw = dict(J1=1.0, alpha=0.1, dt=0.01)
-    with asd.Context(asd.Params.make(N, nfile, **kw), modes=["fp64"]) as ctx:
+    grids = {}
+    with asd.Context(asd.Params.make(N, nfile, **kw)) as ctx:
         ctx.set_spins(s0, as_origin=True)
         ctx.step(2)
         st = ctx.get_spins()
-        g1 = ctx.sqt_grid("fp64")
-        g2 = ctx.sqt_grid("fp64")
-    assert np.array_equal(g1, g2)
+        for mode in ("fp64", "tf32x3", "bf16x3"):
+            g1 = ctx.sqt_grid(mode)
+            g2 = ctx.sqt_grid(mode)
+            assert np.array_equal(g1, g2), mode
+            grids[mode] = g1
     rng = np.random.default_rng(N)
     qs = [(0, 0), (N // 10, N // 10), (N - 1, 1), (1, N - 1), (N // 2, N // 3)]
     qs += [tuple(int(x) for x in rng.integers(0, N, size=2)) for _ in range(7)]
     want = {q: oracle.sqt_factorized(N, nfile, q[0], q[1], st, s0) for q in qs}
     scale = max(abs(v) for v in want.values())
-    for q, w in want.items():
-        assert abs(g1[q] - w) <= 1e-12 * scale, (q, g1[q], w)
+    for mode, tol in (("fp64", 1e-12), ("tf32x3", 1e-5), ("bf16x3", 1e-5)):
+        for q, w in want.items():
+            assert abs(grids[mode][q] - w) <= tol * scale, (mode, q, grids[mode][q], w)

@@ -1,0 +1,70 @@
+"""Split-precision S(q,t) along whole trajectories, not only near t = 0.
+
+S(q,t) is the phase-weighted sum of the connected terms C_ij - m_i . z_j; as
+the dynamics decorrelate the state from the origin it shrinks while the
+terms do not, so a fixed arithmetic error grows relative to |S|.  These
+tests step the 128 x 128, 500-replica antiferromagnet (J = -1,
+h = (0, 0, 0.5), alpha = 0.05, dt = 0.005) for 4000 steps and the
+256 x 256, 1000-replica lattice with J2 = -0.3 for 400 steps, evaluate
+S(q,t) in TF32x3 and BF16x3 at times spread over the run, and compare each
+with the FP64 path on the same state (itself checked against the oracle's
+factorised FP64 value at three of the times).  Errors are taken relative to
+|S| and to the magnitude of the summed terms, (1/M) sum_ij |C_ij - m_i . z_j|;
+the worst of each is printed.
+
+Bound: 1e-5 of |S| at every sampled time (the terms' magnitude is about
+0.03 M here, thousands of times |S|, so the bound relative to it is far
+tighter: 1e-9)."""
+from __future__ import annotations
+
+import pytest
+
+import asd_b200 as asd
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def run_trajectory(oracle, N, nf, kw, steps, every, oracle_at):
+    s0 = asd.random_spins(N, nf, seed=11)
+    rows = []
+    with asd.Context(asd.Params.make(N, nf, **kw)) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        done = 0
+        for t in range(0, steps + 1, every):
+            ctx.step(t - done)
+            done = t
+            ref = ctx.sqt("fp64")
+            mag = ctx.sqt_magnitude()
+            if t in oracle_at:
+                want = oracle.sqt_factorized(N, nf, N // 10, N // 10, ctx.get_spins(), s0)
+                assert rel_err(ref, want) < 1e-12, (t, ref, want)
+            for mode in ("tf32x3", "bf16x3"):
+                v = ctx.sqt(mode)
+                rows.append((t, mode, abs(ref), mag, abs(v - ref) / abs(ref), abs(v - ref) / mag))
+    return rows
+
+
+def check(rows, label):
+    worst_s = max(rows, key=lambda r: r[4])
+    worst_m = max(rows, key=lambda r: r[5])
+    print(f"\n{label}: |S| from {max(r[2] for r in rows):.3e} down to {min(r[2] for r in rows):.3e}"
+          f" (terms' magnitude {rows[0][3]:.3e} .. {rows[-1][3]:.3e})")
+    print(f"  worst error / |S|: {worst_s[4]:.3e} ({worst_s[1]}, step {worst_s[0]}, |S| = "
+          f"{worst_s[2]:.3e})")
+    print(f"  worst error / magnitude: {worst_m[5]:.3e} ({worst_m[1]}, step {worst_m[0]})")
+    for t, mode, s, mag, e_s, e_m in rows:
+        assert e_s <= 1e-5, (label, t, mode, s, e_s)
+        assert e_m <= 1e-9, (label, t, mode, e_m)
+
+
+def test_split_modes_over_4000_steps_128(oracle):
+    kw = dict(J1=-1.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005)
+    rows = run_trajectory(oracle, 128, 500, kw, 4000, 250, {0, 2000, 4000})
+    check(rows, "128x128x500, 4000 steps")
+
+
+def test_split_modes_over_400_steps_256(oracle):
+    kw = dict(J1=1.0, J2=-0.3, alpha=0.02, dt=0.005)
+    rows = run_trajectory(oracle, 256, 1000, kw, 400, 100, {400})
+    check(rows, "256x256x1000, 400 steps")

@@ -40,7 +40,7 @@ def test_grid_vs_oracle(oracle, N, nfile, steps):
             assert rel_err(got[vx, vx], ctx.sqt(mode)) < max(tol, 1e-11), mode
 
 
-def test_grid_largest_and_too_large():
+def test_grid_q0_and_past_64():
     N, nf = 64, 4
     s0 = asd.random_spins(N, nf, seed=3)
     with asd.Context(asd.Params.make(N, nf)) as ctx:
@@ -52,13 +52,14 @@ def test_grid_largest_and_too_large():
     with asd.Context(asd.Params.make(N, nf, vx=0, vy=0)) as ctx:
         ctx.set_spins(s0, as_origin=True)
         assert rel_err(g[0, 0], ctx.sqt("fp64")) < 1e-11
-    with asd.Context(asd.Params.make(65, 1)) as ctx:
-        ctx.set_spins(asd.random_spins(65, 1, seed=1), as_origin=True)
-        assert np.all(np.isfinite(ctx.sqt_grid("fp64")))  # no size limit in FP64
-        for mode in ("tf32x3", "bf16x3"):
-            with pytest.raises(asd.AsdError) as e:
-                ctx.sqt_grid(mode)
-            assert e.value.code == asd.ASD_ERR_UNSUPPORTED
+    # no size limit: 65 x 65 (past the former shared-memory bins) in every mode
+    with asd.Context(asd.Params.make(65, 2)) as ctx:
+        s65 = asd.random_spins(65, 2, seed=1)
+        ctx.set_spins(s65, as_origin=True)
+        ctx.step(1)
+        grids = {m: ctx.sqt_grid(m) for m in TOL}
+    for m, tol in TOL.items():
+        assert grid_err(grids[m], grids["fp64"]) < tol, m
 
 
 def test_fp64_configuration_32x32_full_run(oracle):
