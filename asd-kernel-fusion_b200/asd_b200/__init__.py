@@ -42,7 +42,7 @@ MODES = {v: k for k, v in MODE_NAMES.items()}
 EXPORTED_SYMBOLS = (
     "asd_version", "asd_last_error", "asd_params_default", "asd_set_device",
     "asd_ctx_create", "asd_ctx_destroy", "asd_ctx_set_stream", "asd_ctx_get_params",
-    "asd_ctx_set_params", "asd_ctx_loss_grad",
+    "asd_ctx_set_params", "asd_ctx_loss_grad", "asd_ctx_loss_forward", "asd_ctx_loss_backward",
     "asd_ctx_set_spins", "asd_ctx_set_spins_device", "asd_ctx_get_spins",
     "asd_ctx_get_spins_device", "asd_ctx_step", "asd_ctx_sqt", "asd_ctx_sqt_async",
     "asd_ctx_sqt_magnitude",
@@ -126,6 +126,8 @@ def load() -> C.CDLL:
         "asd_ctx_get_params": ([vp, P], C.c_int),
         "asd_ctx_set_params": ([vp, P], C.c_int),
         "asd_ctx_loss_grad": ([vp, C.c_int, C.c_int, C.c_int, vp, dp, vp, vp], C.c_int),
+        "asd_ctx_loss_forward": ([vp, C.c_int, C.c_int, C.c_int, vp, dp, vp], C.c_int),
+        "asd_ctx_loss_backward": ([vp, vp, vp, vp], C.c_int),
         "asd_ctx_set_spins": ([vp, vp, C.c_int], C.c_int),
         "asd_ctx_set_spins_device": ([vp, vp, C.c_int], C.c_int),
         "asd_ctx_get_spins": ([vp, vp], C.c_int),
@@ -283,6 +285,39 @@ class Context:
                                         C.byref(loss), C.c_void_p(_ptr(grad)),
                                         C.c_void_p(_ptr(sq))))
         return loss.value, grad, sq[0::2] + 1j * sq[1::2]
+
+    @staticmethod
+    def _target(target, E):
+        t = np.asarray(target)
+        tgt = np.ascontiguousarray(np.stack([t.real, t.imag], axis=-1).reshape(-1)
+                                   if np.iscomplexobj(t) else t, dtype=np.float64)
+        if tgt.size != 2 * E:
+            raise ValueError(f"target has {tgt.size} values, expected {2 * E}")
+        return tgt
+
+    def loss_forward(self, nsteps: int, stride: int, checkpoint: int = 50, target=None):
+        """asd_ctx_loss_forward: (loss, S(q,t_e) as a complex array); keeps the
+        tape for loss_backward."""
+        E = nsteps // stride
+        sq = np.zeros(2 * E)
+        loss = C.c_double(0.0)
+        tgt = None if target is None else self._target(target, E)
+        _check(load().asd_ctx_loss_forward(self._h, int(nsteps), int(stride), int(checkpoint),
+                                           None if tgt is None else C.c_void_p(_ptr(tgt)),
+                                           C.byref(loss), C.c_void_p(_ptr(sq))))
+        self._tape_E = E
+        return loss.value, sq[0::2] + 1j * sq[1::2]
+
+    def loss_backward(self, target):
+        """asd_ctx_loss_backward: (grad[6] = dL/d(J1, J2, alpha, hx, hy, hz),
+        dL/dtarget as a complex array d/dRe + i d/dIm)."""
+        E = getattr(self, "_tape_E", 0)
+        tgt = self._target(target, E)
+        grad = np.zeros(6)
+        dt = np.zeros(2 * E)
+        _check(load().asd_ctx_loss_backward(self._h, C.c_void_p(_ptr(tgt)), C.c_void_p(_ptr(grad)),
+                                            C.c_void_p(_ptr(dt))))
+        return grad, dt[0::2] + 1j * dt[1::2]
 
     def set_stream(self, stream_ptr: int) -> None:
         _check(load().asd_ctx_set_stream(self._h, C.c_void_p(stream_ptr)))

@@ -88,6 +88,13 @@ struct asd_ctx {
     // adjoint work space (allocated on the first asd_ctx_loss_grad)
     std::vector<double *> adj_bufs;
     long adj_states = 0;
+    // the tape of the last loss forward pass: its S(q,t) values and sizes,
+    // valid while the parameters and the origin stay those it ran with
+    bool tape_valid = false;
+    int tape_nsteps = 0, tape_stride = 0, tape_ckpt = 0;
+    long tape_params = -1, tape_origin = -1;
+    std::vector<double2> tape_S;
+    long params_version = 0;
     // asd_ctx_step_host: copy stream and event for the overlapped read-back
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t spins_ready = nullptr;
@@ -482,11 +489,9 @@ int step_into(asd_ctx *c, const double *y_in, double *s2, double *s3, double *s4
     return ASD_OK;
 }
 
-int loss_grad(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target, double *loss,
-              double *grad, double *sqt_out) {
-    if (!c->has_origin) return fail(ASD_ERR_STATE, "set the origin (t = 0 spins) first");
-    if (nsteps < 1 || stride < 1 || stride > nsteps || ckpt < 1)
-        return fail(ASD_ERR_INVALID, "nsteps=%d stride=%d checkpoint=%d", nsteps, stride, ckpt);
+// Work space of the adjoint: state-sized buffers (stage states, adjoint
+// variables, checkpoints, one recomputed segment) and small reduction buffers.
+int ensure_adjoint(asd_ctx *c, int nsteps, int stride, int ckpt) {
     const long M = c->M;
     const int K = c->K, E = nsteps / stride;
     const size_t sb = (size_t)M * K * sizeof(double);
@@ -494,6 +499,7 @@ int loss_grad(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target
     const long need = 10 + nck + (ckpt + 1);
     int rc;
     if (c->adj_states < need) {
+        c->tape_valid = false;
         for (double *q : c->adj_bufs)
             if (q) cudaFree(q);
         c->adj_bufs.assign(need + 2, nullptr);
@@ -509,106 +515,194 @@ int loss_grad(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target
         c->adj_states = need;
     } else {
         // the S(q,t) buffer depends on E
+        c->tape_valid = false;
         if (c->adj_bufs[c->adj_states + 1]) cudaFree(c->adj_bufs[c->adj_states + 1]);
         c->adj_bufs[c->adj_states + 1] = nullptr;
         if ((rc = dalloc(&c->adj_bufs[c->adj_states + 1], (size_t)(E + 8) * sizeof(double2))) !=
             ASD_OK)
             return rc;
     }
+    return ASD_OK;
+}
+
+// The adjoint's buffers by role.
+struct AdjBufs {
+    double *s2, *s3, *s4, *acc, *lam, *lam_v, *lam_y, *mu, *P, *loc;
+    double **ck, **seg;
+    double *bacc, *dgrad;
+    double2 *Fpart, *G, *Z, *Sv;
+    int nb;
+};
+
+AdjBufs adj_bufs(asd_ctx *c, int nck) {
     double **B = c->adj_bufs.data();
-    double *s2 = B[0], *s3 = B[1], *s4 = B[2], *acc = B[3], *lam = B[4], *lam_v = B[5],
-           *lam_y = B[6], *mu = B[7], *P = B[8], *loc = B[9];
-    double **ck = B + 10;               // nck checkpoints
-    double **seg = B + 10 + nck;        // ckpt + 1 recomputed states
-    const int nb = adjoint_blocks(c->a);
-    double *bacc = B[c->adj_states];
-    double2 *Fpart = reinterpret_cast<double2 *>(bacc + (size_t)nb * 6);
-    double2 *G = Fpart + (size_t)fsum_chunks(M) * K;
-    double2 *Z = G + K;
-    double *dgrad = reinterpret_cast<double *>(Z + 4);
-    double2 *Sv = reinterpret_cast<double2 *>(B[c->adj_states + 1]);
+    AdjBufs b;
+    b.s2 = B[0], b.s3 = B[1], b.s4 = B[2], b.acc = B[3], b.lam = B[4], b.lam_v = B[5];
+    b.lam_y = B[6], b.mu = B[7], b.P = B[8], b.loc = B[9];
+    b.ck = B + 10;        // nck checkpoints
+    b.seg = B + 10 + nck; // ckpt + 1 recomputed states
+    b.nb = adjoint_blocks(c->a);
+    b.bacc = B[c->adj_states];
+    b.Fpart = reinterpret_cast<double2 *>(b.bacc + (size_t)b.nb * 6);
+    b.G = b.Fpart + (size_t)fsum_chunks(c->M) * c->K;
+    b.Z = b.G + c->K;
+    b.dgrad = reinterpret_cast<double *>(b.Z + 4);
+    b.Sv = reinterpret_cast<double2 *>(B[c->adj_states + 1]);
+    return b;
+}
+
+// Forward pass of the loss: nsteps RK4 steps from the origin with the
+// checkpoints kept for the adjoint, S(q,t) at every stride-th step (host copy
+// in c->tape_S), and L against target if given.  Leaves the tape valid for
+// loss_backward while the parameters and the origin stay as they are.
+int loss_forward(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target, double *loss,
+                 double *sqt_out) {
+    if (!c->has_origin) return fail(ASD_ERR_STATE, "set the origin (t = 0 spins) first");
+    if (nsteps < 1 || stride < 1 || stride > nsteps || ckpt < 1)
+        return fail(ASD_ERR_INVALID, "nsteps=%d stride=%d checkpoint=%d", nsteps, stride, ckpt);
+    int rc = ensure_adjoint(c, nsteps, stride, ckpt);
+    if (rc != ASD_OK) return rc;
+    const long M = c->M;
+    const int K = c->K, E = nsteps / stride;
+    const size_t sb = (size_t)M * K * sizeof(double);
+    const int nck = (nsteps + ckpt - 1) / ckpt;
+    AdjBufs b = adj_bufs(c, nck);
     cudaStream_t st = c->stream;
     c->last_launches = 0;
-
+    c->tape_valid = false;
     // G_k and Z_c of the origin
-    ASD_CUDA_TRY(launch_fsum(c->origin, M, K, c->wphase, Fpart, st));
-    ASD_CUDA_TRY(launch_gz(Fpart, M, K, c->p.nfile, G, Z, st));
+    ASD_CUDA_TRY(launch_fsum(c->origin, M, K, c->wphase, b.Fpart, st));
+    ASD_CUDA_TRY(launch_gz(b.Fpart, M, K, c->p.nfile, b.G, b.Z, st));
+    c->last_launches += 2;
     // forward: checkpoints and S(q,t) at every stride-th step
-    ASD_CUDA_TRY(cudaMemcpyAsync(ck[0], c->origin, sb, cudaMemcpyDeviceToDevice, st));
-    double *cur = seg[0], *nxt = seg[1];
+    ASD_CUDA_TRY(cudaMemcpyAsync(b.ck[0], c->origin, sb, cudaMemcpyDeviceToDevice, st));
+    double *cur = b.seg[0], *nxt = b.seg[1];
     ASD_CUDA_TRY(cudaMemcpyAsync(cur, c->origin, sb, cudaMemcpyDeviceToDevice, st));
     // Only states are kept on the way forward: one launch per step where
     // that fills the GPU.
     const bool fwd_fused = use_fused(c, c->a);
     for (int n = 1; n <= nsteps; ++n) {
-        if (fwd_fused) ASD_CUDA_TRY(launch_llg_step_fused(c->a, cur, nxt, st));
-        else if ((rc = step_into(c, cur, s2, s3, s4, acc, nxt)) != ASD_OK) return rc;
+        if (fwd_fused) {
+            ASD_CUDA_TRY(launch_llg_step_fused(c->a, cur, nxt, st));
+            c->last_launches += 1;
+        } else {
+            if ((rc = step_into(c, cur, b.s2, b.s3, b.s4, b.acc, nxt)) != ASD_OK) return rc;
+            c->last_launches += 4;
+        }
         double *t = cur;
         cur = nxt;
         nxt = t;
         if (n % ckpt == 0 && n / ckpt < nck)
-            ASD_CUDA_TRY(cudaMemcpyAsync(ck[n / ckpt], cur, sb, cudaMemcpyDeviceToDevice, st));
+            ASD_CUDA_TRY(cudaMemcpyAsync(b.ck[n / ckpt], cur, sb, cudaMemcpyDeviceToDevice, st));
         if (n % stride == 0 && n / stride <= E) {
-            ASD_CUDA_TRY(launch_fsum(cur, M, K, c->uphase, Fpart, st));
-            ASD_CUDA_TRY(launch_sqt_value(Fpart, M, K, c->p.nfile, G, Z, Sv + (n / stride - 1), st));
+            ASD_CUDA_TRY(launch_fsum(cur, M, K, c->uphase, b.Fpart, st));
+            ASD_CUDA_TRY(launch_sqt_value(b.Fpart, M, K, c->p.nfile, b.G, b.Z, b.Sv + (n / stride - 1), st));
+            c->last_launches += 2;
         }
     }
-    std::vector<double2> S((size_t)E);
-    ASD_CUDA_TRY(cudaMemcpyAsync(S.data(), Sv, (size_t)E * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    c->tape_S.assign((size_t)E, make_double2(0.0, 0.0));
+    ASD_CUDA_TRY(cudaMemcpyAsync(c->tape_S.data(), b.Sv, (size_t)E * sizeof(double2),
+                                 cudaMemcpyDeviceToHost, st));
     ASD_CUDA_TRY(cudaStreamSynchronize(st));
     if (sqt_out)
-        for (int e = 0; e < E; ++e) sqt_out[2 * e] = S[e].x, sqt_out[2 * e + 1] = S[e].y;
+        for (int e = 0; e < E; ++e) sqt_out[2 * e] = c->tape_S[e].x, sqt_out[2 * e + 1] = c->tape_S[e].y;
     double L = 0.0;
-    std::vector<double2> coef((size_t)E, make_double2(0.0, 0.0));
     if (target) {
-        const double scale = 2.0 / ((double)E * (double)M * c->p.nfile);
         for (int e = 0; e < E; ++e) {
-            const double dr = S[e].x - target[2 * e], di = S[e].y - target[2 * e + 1];
+            const double dr = c->tape_S[e].x - target[2 * e], di = c->tape_S[e].y - target[2 * e + 1];
             L += dr * dr + di * di;
-            coef[e] = make_double2(scale * dr, -scale * di);  // 2 conj(S - T) / (E M nfile)
         }
         L /= E;
     }
     if (loss) *loss = L;
-    if (!grad) return ASD_OK;
-    for (int q = 0; q < 6; ++q) grad[q] = 0.0;
-    if (!target) return ASD_OK;
+    c->tape_valid = true;
+    c->tape_nsteps = nsteps;
+    c->tape_stride = stride;
+    c->tape_ckpt = ckpt;
+    c->tape_params = c->params_version;
+    c->tape_origin = c->origin_version;
+    return ASD_OK;
+}
 
+// Backward pass of the loss from the tape of the last loss_forward:
+// dL/d(J1, J2, alpha, hx, hy, hz) by the adjoint of the RK4 step and the
+// renormalisation, segment by segment from the checkpoints; and, with
+// dtarget, dL/dtarget = -2 (S - target) / E.
+int loss_backward(asd_ctx *c, const double *target, double *grad, double *dtarget) {
+    if (!target) return fail(ASD_ERR_INVALID, "target is NULL");
+    if (!c->tape_valid || c->tape_params != c->params_version || c->tape_origin != c->origin_version)
+        return fail(ASD_ERR_STATE, "no forward pass of the loss with the current parameters and origin");
+    const long M = c->M;
+    const int K = c->K, nsteps = c->tape_nsteps, stride = c->tape_stride, ckpt = c->tape_ckpt;
+    const int E = nsteps / stride;
+    const size_t sb = (size_t)M * K * sizeof(double);
+    const int nck = (nsteps + ckpt - 1) / ckpt;
+    AdjBufs b = adj_bufs(c, nck);
+    cudaStream_t st = c->stream;
+    int rc;
+    c->last_launches = 0;
+    std::vector<double2> coef((size_t)E, make_double2(0.0, 0.0));
+    const double scale = 2.0 / ((double)E * (double)M * c->p.nfile);
+    for (int e = 0; e < E; ++e) {
+        const double dr = c->tape_S[e].x - target[2 * e], di = c->tape_S[e].y - target[2 * e + 1];
+        coef[e] = make_double2(scale * dr, -scale * di);  // 2 conj(S - T) / (E M nfile)
+        if (dtarget) {
+            dtarget[2 * e] = -2.0 * dr / E;
+            dtarget[2 * e + 1] = -2.0 * di / E;
+        }
+    }
+    if (!grad) return ASD_OK;
+    const bool fwd_fused = use_fused(c, c->a);
     // backward through the segments, last first
-    ASD_CUDA_TRY(cudaMemsetAsync(lam, 0, sb, st));
-    ASD_CUDA_TRY(cudaMemsetAsync(bacc, 0, (size_t)nb * 6 * sizeof(double), st));
+    ASD_CUDA_TRY(cudaMemsetAsync(b.lam, 0, sb, st));
+    ASD_CUDA_TRY(cudaMemsetAsync(b.bacc, 0, (size_t)b.nb * 6 * sizeof(double), st));
+    double **seg = b.seg;
     for (int cidx = nck - 1; cidx >= 0; --cidx) {
         const int base = cidx * ckpt;
         const int len = (nsteps - base < ckpt) ? nsteps - base : ckpt;
-        ASD_CUDA_TRY(cudaMemcpyAsync(seg[0], ck[cidx], sb, cudaMemcpyDeviceToDevice, st));
+        ASD_CUDA_TRY(cudaMemcpyAsync(seg[0], b.ck[cidx], sb, cudaMemcpyDeviceToDevice, st));
         for (int j = 1; j <= len; ++j) {
             if (fwd_fused) ASD_CUDA_TRY(launch_llg_step_fused(c->a, seg[j - 1], seg[j], st));
-            else if ((rc = step_into(c, seg[j - 1], s2, s3, s4, acc, seg[j])) != ASD_OK) return rc;
+            else if ((rc = step_into(c, seg[j - 1], b.s2, b.s3, b.s4, b.acc, seg[j])) != ASD_OK) return rc;
+            c->last_launches += fwd_fused ? 1 : 4;
         }
         for (int n = base + len; n > base; --n) {
             const int j = n - base;
             if (n % stride == 0 && n / stride <= E) {
                 const double2 cf = coef[n / stride - 1];
-                ASD_CUDA_TRY(launch_loss_grad(lam, M, K, c->uphase, G, Z, cf.x, cf.y, st));
+                ASD_CUDA_TRY(launch_loss_grad(b.lam, M, K, c->uphase, b.G, b.Z, cf.x, cf.y, st));
+                c->last_launches += 1;
             }
             // y_{n-1} = seg[j-1]: recompute the stage states, then the adjoint
-            if ((rc = step_into(c, seg[j - 1], s2, s3, s4, acc, nullptr)) != ASD_OK) return rc;
+            if ((rc = step_into(c, seg[j - 1], b.s2, b.s3, b.s4, b.acc, nullptr)) != ASD_OK) return rc;
             const LLGArgs &a = c->a;
-            ASD_CUDA_TRY(launch_adj_renorm(a, s4, acc, lam, lam_v, mu, st));
-            ASD_CUDA_TRY(launch_vjp_p(a, s4, mu, P, loc, bacc, st));
-            ASD_CUDA_TRY(launch_vjp_gather(a, P, loc, lam_v, lam_v, lam_y, mu, 1.0 / 3.0, 1.0, 1, st));
-            ASD_CUDA_TRY(launch_vjp_p(a, s3, mu, P, loc, bacc, st));
-            ASD_CUDA_TRY(launch_vjp_gather(a, P, loc, lam_v, lam_y, lam_y, mu, 1.0 / 3.0, 0.5, 1, st));
-            ASD_CUDA_TRY(launch_vjp_p(a, s2, mu, P, loc, bacc, st));
-            ASD_CUDA_TRY(launch_vjp_gather(a, P, loc, lam_v, lam_y, lam_y, mu, 1.0 / 6.0, 0.5, 1, st));
-            ASD_CUDA_TRY(launch_vjp_p(a, seg[j - 1], mu, P, loc, bacc, st));
-            ASD_CUDA_TRY(launch_vjp_gather(a, P, loc, lam_v, lam_y, lam, mu, 0.0, 0.0, 0, st));
+            ASD_CUDA_TRY(launch_adj_renorm(a, b.s4, b.acc, b.lam, b.lam_v, b.mu, st));
+            ASD_CUDA_TRY(launch_vjp_p(a, b.s4, b.mu, b.P, b.loc, b.bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_v, b.lam_y, b.mu, 1.0 / 3.0, 1.0, 1, st));
+            ASD_CUDA_TRY(launch_vjp_p(a, b.s3, b.mu, b.P, b.loc, b.bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_y, b.lam_y, b.mu, 1.0 / 3.0, 0.5, 1, st));
+            ASD_CUDA_TRY(launch_vjp_p(a, b.s2, b.mu, b.P, b.loc, b.bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_y, b.lam_y, b.mu, 1.0 / 6.0, 0.5, 1, st));
+            ASD_CUDA_TRY(launch_vjp_p(a, seg[j - 1], b.mu, b.P, b.loc, b.bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_y, b.lam, b.mu, 0.0, 0.0, 0, st));
+            c->last_launches += 4 + 9;
         }
     }
-    ASD_CUDA_TRY(launch_param_reduce(bacc, nb, dgrad, st));
-    ASD_CUDA_TRY(cudaMemcpyAsync(grad, dgrad, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ASD_CUDA_TRY(launch_param_reduce(b.bacc, b.nb, b.dgrad, st));
+    c->last_launches += 1;
+    ASD_CUDA_TRY(cudaMemcpyAsync(grad, b.dgrad, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
     ASD_CUDA_TRY(cudaStreamSynchronize(st));
     return ASD_OK;
+}
+
+int loss_grad(asd_ctx *c, int nsteps, int stride, int ckpt, const double *target, double *loss,
+              double *grad, double *sqt_out) {
+    int rc = loss_forward(c, nsteps, stride, ckpt, target, loss, sqt_out);
+    if (rc != ASD_OK) return rc;
+    if (!grad) return ASD_OK;
+    for (int q = 0; q < 6; ++q) grad[q] = 0.0;
+    if (!target) return ASD_OK;
+    return loss_backward(c, target, grad, nullptr);
 }
 
 // Work space of the q grid's diagonal partials, grown on demand.
@@ -1275,6 +1369,19 @@ int asd_ctx_loss_grad(asd_ctx *c, int nsteps, int stride, int checkpoint, const 
     return loss_grad(c, nsteps, stride, checkpoint, target, loss, grad, sqt_out);
 }
 
+int asd_ctx_loss_forward(asd_ctx *c, int nsteps, int stride, int checkpoint, const double *target,
+                         double *loss, double *sqt_out) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    ASD_CUDA_TRY(enter(c));
+    return loss_forward(c, nsteps, stride, checkpoint, target, loss, sqt_out);
+}
+
+int asd_ctx_loss_backward(asd_ctx *c, const double *target, double *grad, double *dtarget) {
+    if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
+    ASD_CUDA_TRY(enter(c));
+    return loss_backward(c, target, grad, dtarget);
+}
+
 int asd_ctx_set_params(asd_ctx *c, const asd_params *p) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
     int rc = check_params(p);
@@ -1283,6 +1390,7 @@ int asd_ctx_set_params(asd_ctx *c, const asd_params *p) {
         return fail(ASD_ERR_INVALID, "N and nfile are fixed at create");
     const bool q_changed = (p->vx != c->p.vx || p->vy != c->p.vy);
     c->p = *p;
+    c->params_version++;
     c->a = make_llg_args(*p);
     if (q_changed) {
         const double qx = 2.0 * M_PI * p->vx / (double)p->N, qy = 2.0 * M_PI * p->vy / (double)p->N;
@@ -1562,6 +1670,7 @@ int asd_debug_fail_alloc(long n) {
 int asd_ctx_debug_poison(asd_ctx *c) {
     if (!c) return fail(ASD_ERR_INVALID, "ctx is NULL");
     ASD_CUDA_TRY(enter(c));
+    c->tape_valid = false;  // the checkpoints are among the poisoned buffers
     const cudaStream_t streams[] = {c->stream, c->llg_stream, c->gemm_stream, c->copy_stream,
                                     c->h2d_stream};
     for (cudaStream_t s : streams)

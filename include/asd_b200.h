@@ -156,6 +156,22 @@ int asd_ctx_sqt_grid(asd_ctx *ctx, asd_sqt_mode mode, double *out);
  * current state is not changed.  No counterpart in the reference. */
 int asd_ctx_loss_grad(asd_ctx *ctx, int nsteps, int stride, int checkpoint, const double *target,
                       double *loss, double *grad, double *sqt_out);
+/* asd_ctx_loss_grad in two calls, so that a caller that does not need the
+ * gradient (a forward-only evaluation) does not pay for the adjoint.
+ * asd_ctx_loss_forward runs the forward pass -- the nsteps RK4 steps with the
+ * checkpoints kept on the device, S(q,t_e) into sqt_out (2E doubles, may be
+ * NULL) and, with target, the loss into *loss -- and leaves a tape.
+ * asd_ctx_loss_backward then runs the adjoint from that tape: grad (6
+ * doubles, may be NULL) = dL/d(J1, J2, alpha, hx, hy, hz) and dtarget (2E
+ * doubles, may be NULL) = dL/dtarget = -2 (S - target) / E; target (2E
+ * doubles) is required.  The tape holds while the parameters and the origin
+ * are unchanged (else ASD_ERR_STATE) and until the next forward pass or
+ * asd_ctx_loss_grad; backward may run more than once.  Forward + backward
+ * give asd_ctx_loss_grad's results bit for bit.  Host buffers; synchronous.
+ * No counterpart in the reference. */
+int asd_ctx_loss_forward(asd_ctx *ctx, int nsteps, int stride, int checkpoint, const double *target,
+                         double *loss, double *sqt_out);
+int asd_ctx_loss_backward(asd_ctx *ctx, const double *target, double *grad, double *dtarget);
 
 /* One full step through host buffers, the reference's own contract: spins
  * (AoS) come from host memory, one RK4 step runs, the new spins go back to

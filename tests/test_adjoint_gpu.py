@@ -177,3 +177,62 @@ def test_autograd_wrapper_and_descent():
             opt.step()
             losses.append(l.item())
         assert losses[-1] < losses[0]
+
+
+def test_forward_pays_no_adjoint_and_backward_matches():
+    """asd_ctx_loss_forward runs the forward pass only (its launch count is
+    that of the steps and the S(q,t) evaluations); asd_ctx_loss_backward from
+    its tape gives asd_ctx_loss_grad's gradient bit for bit and
+    dL/dtarget = -2 (S - target) / E; a parameter change invalidates the tape."""
+    N, nf, nsteps, stride, ck = 16, 8, 60, 6, 20
+    s0 = asd.random_spins(N, nf, seed=4)
+    p = asd.Params.make(N, nf, J1=1.0, alpha=0.1, h=(0.0, 0.0, 0.2), dt=0.01)
+    with asd.Context(p, modes=["fp64"]) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        _, _, target = ctx.loss_grad(nsteps, stride, ck, None)
+        target = target * (1.0 + 0.01j)
+        loss_ref, grad_ref, S_ref = ctx.loss_grad(nsteps, stride, ck, target)
+        loss, S = ctx.loss_forward(nsteps, stride, ck, target)
+        fwd_launches = ctx.last_launches()
+        assert loss == loss_ref
+        assert np.array_equal(S, S_ref)
+        E = nsteps // stride
+        # one launch per step (the one-launch RK4 step or 4 stage kernels) and
+        # two per S(q,t) evaluation, plus the origin's sums: no adjoint
+        assert fwd_launches <= 4 * nsteps + 2 * E + 2
+        grad, dtarget = ctx.loss_backward(target)
+        assert ctx.last_launches() > 13 * nsteps  # the adjoint's launches come here
+        np.testing.assert_array_equal(grad, grad_ref)
+        np.testing.assert_allclose(dtarget, -2.0 * (S - target) / E, rtol=1e-15, atol=0)
+        grad2, _ = ctx.loss_backward(target)  # the tape stays until the next forward pass
+        np.testing.assert_array_equal(grad2, grad_ref)
+        ctx.set_params(asd.Params.make(N, nf, J1=1.1, alpha=0.1, h=(0.0, 0.0, 0.2), dt=0.01))
+        with pytest.raises(asd.AsdError) as e:
+            ctx.loss_backward(target)
+        assert e.value.code == asd.ASD_ERR_STATE
+
+
+def test_autograd_target_gradient():
+    """With a target tensor that requires grad, backward gives dL/dtarget too."""
+    import torch
+
+    from asd_b200.autograd import sqt_loss
+
+    N, nf, nsteps, stride, ck = 12, 6, 40, 5, 20
+    s0 = asd.random_spins(N, nf, seed=5)
+    p = asd.Params.make(N, nf, J1=1.0, alpha=0.1, dt=0.01)
+    with asd.Context(p, modes=["fp64"]) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        _, _, tgt = ctx.loss_grad(nsteps, stride, ck, None)
+        target = torch.tensor(tgt * 0.9, dtype=torch.complex128, requires_grad=True)
+        theta = torch.tensor([1.0, 0.0, 0.1, 0.0, 0.0, 0.0], dtype=torch.float64,
+                             requires_grad=True)
+        loss = sqt_loss(theta, ctx, nsteps, stride, ck, target)
+        loss.backward()
+        S = torch.tensor(tgt, dtype=torch.complex128)
+        want = -2.0 * (S - target.detach()) / (nsteps // stride)
+        torch.testing.assert_close(target.grad, want, rtol=1e-14, atol=1e-16)
+        # torch's own autograd of the same loss on the same S gives the same
+        t2 = target.detach().clone().requires_grad_(True)
+        ((S - t2).abs() ** 2).mean().backward()
+        torch.testing.assert_close(target.grad, t2.grad, rtol=1e-14, atol=1e-16)
