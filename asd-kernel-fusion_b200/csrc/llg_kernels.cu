@@ -230,12 +230,12 @@ __global__ void __launch_bounds__(stream::NT_MAX, 2)
         }
         const long row_stride = (long)N * K;
         // y row R0 - 4 + j (periodic) of this band and replica group -> y ring
-        auto load_row = [&](int j) {
+        auto load_row = [&](int j, int slot) {  // slot = j % YR
             int gr = R0 - 4 + j;  // in [-4, N + 4): at most two wraps for N >= 3
             while (gr < 0) gr += N;
             while (gr >= N) gr -= N;
             const double *src = y + (long)gr * row_stride;
-            double *dst = ybuf + (j % YR) * rw;
+            double *dst = ybuf + slot * rw;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const int x = tid + k * (int)blockDim.x;
@@ -248,19 +248,20 @@ __global__ void __launch_bounds__(stream::NT_MAX, 2)
         // Stage bodies on relative row r (in y slot r % 5, ring slot r % 3),
         // each split into its shared-memory loads (ld) and its arithmetic and
         // stores (st*), so that the two stages of a phase can issue all their
-        // loads before either computes.
-        auto ld = [&](const double *ring, int nrows, int r, bool with_base) {
+        // loads before either computes.  The callers pass the ring slots of
+        // rows r - 1, r, r + 1 (and of the base row in the y ring, or -1):
+        // the y slots are compile-time constants of the unrolled iteration,
+        // the 3-row ring slots one of three rotations of a running j % 3.
+        auto ld = [&](const double *ring, int su, int sm, int sd, int sb) {
             SIn in;
-            const double *up = ring + ((r - 1) % nrows) * rw, *mid = ring + (r % nrows) * rw,
-                         *dn = ring + ((r + 1) % nrows) * rw;
-            load_in<J2>(up, mid, dn, me, in);
-            if (with_base) in.yb = ld3(ybuf + (r % YR) * rw + me);
+            load_in<J2>(ring + su * rw, ring + sm * rw, ring + sd * rw, me, in);
+            if (sb >= 0) in.yb = ld3(ybuf + sb * rw + me);
             return in;
         };
-        auto st1 = [&](const SIn &in, int r, double *ac) {  // s1 = y + k/2, acc = y + k/6
+        auto st1 = [&](const SIn &in, int r3, double *ac) {  // s1 = y + k/2, acc = y + k/6
             const V3 d = llg_rhs_vals<J2, H, DAMP>(in.s, in.nb, in.n2, a);
             const double k0 = dm(d.x, dt), k1 = dm(d.y, dt), k2 = dm(d.z, dt);
-            double *o = s1 + (r % 3) * rw + me;
+            double *o = s1 + r3 * rw + me;
             o[0] = da(in.s.x, half(k0));
             o[1] = da(in.s.y, half(k1));
             o[2] = da(in.s.z, half(k2));
@@ -268,10 +269,10 @@ __global__ void __launch_bounds__(stream::NT_MAX, 2)
             ac[1] = da(in.s.y, div6(k1));
             ac[2] = da(in.s.z, div6(k2));
         };
-        auto st2 = [&](const SIn &in, int r, double *ac) {  // s2 = y + k/2, acc += k/3
+        auto st2 = [&](const SIn &in, int r3, double *ac) {  // s2 = y + k/2, acc += k/3
             const V3 d = llg_rhs_vals<J2, H, DAMP>(in.s, in.nb, in.n2, a);
             const double k0 = dm(d.x, dt), k1 = dm(d.y, dt), k2 = dm(d.z, dt);
-            double *o = s2 + (r % 3) * rw + me;
+            double *o = s2 + r3 * rw + me;
             o[0] = da(in.yb.x, half(k0));
             o[1] = da(in.yb.y, half(k1));
             o[2] = da(in.yb.z, half(k2));
@@ -279,10 +280,10 @@ __global__ void __launch_bounds__(stream::NT_MAX, 2)
             ac[1] = da(ac[1], div3(k1));
             ac[2] = da(ac[2], div3(k2));
         };
-        auto st3 = [&](const SIn &in, int r, double *ac) {  // s3 = y + k, acc += k/3
+        auto st3 = [&](const SIn &in, int r3, double *ac) {  // s3 = y + k, acc += k/3
             const V3 d = llg_rhs_vals<J2, H, DAMP>(in.s, in.nb, in.n2, a);
             const double k0 = dm(d.x, dt), k1 = dm(d.y, dt), k2 = dm(d.z, dt);
-            double *o = s3 + (r % 3) * rw + me;
+            double *o = s3 + r3 * rw + me;
             o[0] = da(in.yb.x, k0);
             o[1] = da(in.yb.y, k1);
             o[2] = da(in.yb.z, k2);
@@ -307,40 +308,48 @@ __global__ void __launch_bounds__(stream::NT_MAX, 2)
 
         double acc[5][3];  // row r's combination in acc[r % 5]
         __syncthreads();   // the previous piece is done with every buffer
-        load_row(0);
+        load_row(0, 0);
         cp_async_commit();
-        // Iteration j with R = j % 5 known at compile time, so acc[] is
-        // indexed statically.  Valid rows: stage s on relative rows s..rs+7-s.
+        // Iteration j with R = j % 5 known at compile time, so acc[] and the y
+        // ring slots are static; m3 = j % 3 runs along, and the 3-row ring
+        // slots of rows j - 1 .. j - 6 are its rotations (j-3, j-6: m3;
+        // j-2, j-5: m3 + 1; j-1, j-4: m3 + 2, mod 3).  Valid rows: stage s on
+        // relative rows s..rs+7-s.
+        int m3 = 0;
         auto iter = [&](auto rc, int j) {
             constexpr int R = decltype(rc)::value;
             if (j >= J) return;  // uniform over the CTA
+            const int a0 = m3, a1 = (m3 == 2) ? 0 : m3 + 1, a2 = (m3 == 0) ? 2 : m3 - 1;
+            m3 = a1;
             cp_async_wait_all();
             __syncthreads();  // phase A: stage 1 on row j-1, stage 3 on row j-4
             if (comp) {
                 const bool d1 = j >= 2 && j <= rs + 7, d3 = j >= 7;
+                const int y_m2 = (j + 3) % 5, y_m1 = (j + 4) % 5, y_0 = j % 5, y_m4 = (j + 1) % 5;
                 if (d1 && d3) {
-                    const SIn i1 = ld(ybuf, YR, j - 1, false), i3 = ld(s2, 3, j - 4, true);
-                    st1(i1, j - 1, acc[(R + 4) % 5]);
-                    st3(i3, j - 4, acc[(R + 1) % 5]);
+                    const SIn i1 = ld(ybuf, y_m2, y_m1, y_0, -1), i3 = ld(s2, a1, a2, a0, y_m4);
+                    st1(i1, a2, acc[(R + 4) % 5]);
+                    st3(i3, a2, acc[(R + 1) % 5]);
                 } else if (d1) {
-                    st1(ld(ybuf, YR, j - 1, false), j - 1, acc[(R + 4) % 5]);
+                    st1(ld(ybuf, y_m2, y_m1, y_0, -1), a2, acc[(R + 4) % 5]);
                 } else if (d3) {
-                    st3(ld(s2, 3, j - 4, true), j - 4, acc[(R + 1) % 5]);
+                    st3(ld(s2, a1, a2, a0, y_m4), a2, acc[(R + 1) % 5]);
                 }
             }
             __syncthreads();  // phase B: prefetch, stage 2 on row j-2, stage 4 on row j-5
-            if (j + 1 <= rs + 7) load_row(j + 1);
+            if (j + 1 <= rs + 7) load_row(j + 1, (R + 1) % 5);
             cp_async_commit();
             if (comp) {
                 const bool d2 = j >= 4 && j <= rs + 7, d4 = j >= 9;
+                const int y_m2 = (j + 3) % 5;
                 if (d2 && d4) {
-                    const SIn i2 = ld(s1, 3, j - 2, true), i4 = ld(s3, 3, j - 5, false);
-                    st2(i2, j - 2, acc[(R + 3) % 5]);
+                    const SIn i2 = ld(s1, a0, a1, a2, y_m2), i4 = ld(s3, a0, a1, a2, -1);
+                    st2(i2, a1, acc[(R + 3) % 5]);
                     st4(i4, j - 5, acc[R]);
                 } else if (d2) {
-                    st2(ld(s1, 3, j - 2, true), j - 2, acc[(R + 3) % 5]);
+                    st2(ld(s1, a0, a1, a2, y_m2), a1, acc[(R + 3) % 5]);
                 } else if (d4) {
-                    st4(ld(s3, 3, j - 5, false), j - 5, acc[R]);
+                    st4(ld(s3, a0, a1, a2, -1), j - 5, acc[R]);
                 }
             }
         };
