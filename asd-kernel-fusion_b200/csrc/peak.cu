@@ -13,8 +13,8 @@ namespace {
 
 constexpr int kChains = 8;     // independent FMA chains per thread
 constexpr int kFmaIters = 16384;
-constexpr int kMmaTiles = 4;   // independent accumulator tiles per warp
-constexpr int kMmaIters = 1024;
+constexpr int kMmaTiles = 16;  // independent accumulator tiles per warp
+constexpr int kMmaIters = 256;
 
 // Where the peak kernels would store a result that cannot occur: the stores
 // keep the compiler from dropping the arithmetic.

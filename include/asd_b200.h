@@ -326,8 +326,8 @@ int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, const void 
 /* Diagnostic: measured FP64 throughput of the current device, the
  * denominators of the FP64 roofline fractions.  which = 0: independent
  * __fma_rn chains on the CUDA cores (an FMA counts 2 flops); which = 1:
- * independent mma.sync m16n8k8 .f64 tensor-core products (2*16*8*8 flops
- * each).  32 warps per SM, about a millisecond; *tflops and *ms of the second
+ * 16 independent mma.sync m16n8k8 .f64 accumulators per warp (2*16*8*8 flops
+ * per product).  32 warps per SM, about a millisecond; *tflops and *ms of the second
  * of two launches.  Synchronous.  No counterpart in the reference. */
 int asd_measure_fp64_peak(int which, double *tflops, double *ms, void *stream);
 /* Diagnostic: one warp computes D[16][8] = A[16][8] B[8][8] (row-major device

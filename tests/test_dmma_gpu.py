@@ -43,10 +43,10 @@ def test_fp64_peak_is_plausible(which):
     assert 5.0 < tf < 200.0, tf
 
 
-@pytest.mark.parametrize("N,nfile,steps", [(20, 8, 2), (20, 7, 2), (37, 33, 1), (12, 1, 3),
+@pytest.mark.parametrize("N,nfile,steps", [(20, 8, 2), (20, 7, 2), (37, 33, 1), (12, 3, 3),
                                            (24, 40, 1)])
 def test_fp64_sqt_vs_oracle(oracle, N, nfile, steps):
-    """K = 3 nfile even (24, 120) and odd (21, 99, 3); N*N = 400, 1369, 144,
+    """K = 3 nfile even (24, 120) and odd (21, 99, 9); N*N = 400, 1369, 144,
     576 sites: every lattice has a partial tile."""
     s0 = asd.random_spins(N, nfile, seed=N * 31 + nfile)
     kw = dict(J1=-1.0, J2=0.2, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005)
@@ -60,6 +60,20 @@ def test_fp64_sqt_vs_oracle(oracle, N, nfile, steps):
     want = oracle.sqt_factorized(N, nfile, vx, vy, st, s0)
     assert rel_err(a, want) < 1e-12, (a, want)
     assert a == b
+
+
+def test_fp64_single_replica_is_zero():
+    """With one replica the connected part is identically zero (m_i = S_i):
+    the FP64 path gives zero up to rounding of the O(1) terms it cancels."""
+    N = 12
+    s0 = asd.random_spins(N, 1, seed=5)
+    with asd.Context(asd.Params.make(N, 1, J1=1.0, dt=0.01), modes=["fp64"]) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        ctx.step(3)
+        v = ctx.sqt("fp64")
+        mag = ctx.sqt_magnitude()
+    assert abs(v) < 1e-15
+    assert mag < 1e-13
 
 
 def test_fp64_kernel_is_timed():
