@@ -71,17 +71,137 @@ __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double 
     }
 }
 
+// The same stage with the stage input staged through a shared-memory halo
+// tile: a block takes TR x TC sites of the lattice (plus a one-site periodic
+// halo, corners only with J2) for 32 replicas, one per lane, so each input
+// vector crosses L2 -> SM (TR+2)(TC+2)/(TR*TC) = 1.9 times instead of once
+// per neighbour (5 times, 9 with J2).  Global reads of a site's 32 replicas
+// are 768 contiguous bytes; in shared memory lane r reads word 3r + c of a
+// site, conflict-free within each half warp.  The arithmetic is llg_rhs_vals
+// on the same values in the same order: the results are bit-identical to
+// llg_stage_kernel's.
+__device__ __forceinline__ V3 ld3(const double *p) { return V3{p[0], p[1], p[2]}; }
+
+constexpr int kTiledMinReplicas = 64;  // below: the per-(site, replica) kernel
+
+namespace tiled {
+constexpr int FG = 32;          // replicas per block, one per lane
+constexpr int TR = 4, TC = 8;   // sites per block
+constexpr int HR = TR + 2, HC = TC + 2;
+constexpr int SD = FG * 3;      // doubles per site slot
+}  // namespace tiled
+
+template <int STAGE, bool J2, bool H, bool DAMP>
+__global__ void __launch_bounds__(256) llg_stage_tiled_kernel(LLGArgs a, const double *__restrict__ y,
+                                                              const double *__restrict__ ys,
+                                                              double *__restrict__ acc,
+                                                              double *__restrict__ out, int tiles_c,
+                                                              int tiles_r) {
+    using namespace tiled;
+    __shared__ double sm[HR * HC * SD];  // 46 080 bytes
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int b = blockIdx.x;
+    const int tc = b % tiles_c;
+    b /= tiles_c;
+    const int tr = b % tiles_r;
+    const int grp = b / tiles_r;
+    const int N = a.N;
+    const long K = 3L * a.nfile;
+    const int fbase = a.f0 + grp * FG;
+    const int nvalid = min(FG, a.f0 + a.nc - fbase);
+    const int r0 = tr * TR, c0 = tc * TC;
+    // halo tile -> shared memory, one site per warp at a time
+    for (int sidx = warp; sidx < HR * HC; sidx += 8) {
+        const int hr = sidx / HC, hc = sidx - hr * HC;
+        if (!J2 && (hr == 0 || hr == HR - 1) && (hc == 0 || hc == HC - 1)) continue;
+        int gr = (r0 - 1 + hr) % N, gc = (c0 - 1 + hc) % N;
+        if (gr < 0) gr += N;
+        if (gc < 0) gc += N;
+        const double *src = ys + ((long)gr * N + gc) * K + 3L * fbase;
+        double *dst = sm + sidx * SD;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int x = lane + 32 * k;
+            dst[x] = (x < 3 * nvalid) ? src[x] : 0.0;
+        }
+    }
+    __syncthreads();
+    if (lane >= nvalid) return;
+    const int f = fbase + lane;
+    const long off = 3L * f;
+    for (int sidx = warp; sidx < TR * TC; sidx += 8) {
+        const int lr = sidx / TC, lc = sidx - lr * TC;
+        const int row = r0 + lr, col = c0 + lc;
+        if (row >= N || col >= N) continue;
+        const double *c = sm + ((lr + 1) * HC + (lc + 1)) * SD + 3 * lane;
+        const V3 sc = ld3(c);
+        // neighbours in llg_rhs's order: (row+1), (row-1), (col-1), (col+1);
+        // diagonals (+1,+1), (+1,-1), (-1,+1), (-1,-1)
+        const V3 nb[4] = {ld3(c + HC * SD), ld3(c - HC * SD), ld3(c - SD), ld3(c + SD)};
+        V3 n2[4];
+        if (J2) {
+            n2[0] = ld3(c + (HC + 1) * SD);
+            n2[1] = ld3(c + (HC - 1) * SD);
+            n2[2] = ld3(c - (HC - 1) * SD);
+            n2[3] = ld3(c - (HC + 1) * SD);
+        }
+        const V3 d = llg_rhs_vals<J2, H, DAMP>(sc, nb, n2, a);
+        const long e = ((long)row * N + col) * K + off;
+        const double k0 = dm(d.x, a.dt), k1 = dm(d.y, a.dt), k2 = dm(d.z, a.dt);
+        if (STAGE == 1) {
+            const double y0 = y[e], y1 = y[e + 1], y2 = y[e + 2];
+            out[e] = da(y0, half(k0));
+            out[e + 1] = da(y1, half(k1));
+            out[e + 2] = da(y2, half(k2));
+            acc[e] = da(y0, div6(k0));
+            acc[e + 1] = da(y1, div6(k1));
+            acc[e + 2] = da(y2, div6(k2));
+        } else if (STAGE == 2 || STAGE == 3) {
+            const double y0 = y[e], y1 = y[e + 1], y2 = y[e + 2];
+            if (STAGE == 2) {
+                out[e] = da(y0, half(k0));
+                out[e + 1] = da(y1, half(k1));
+                out[e + 2] = da(y2, half(k2));
+            } else {
+                out[e] = da(y0, k0);
+                out[e + 1] = da(y1, k1);
+                out[e + 2] = da(y2, k2);
+            }
+            acc[e] = da(acc[e], div3(k0));
+            acc[e + 1] = da(acc[e + 1], div3(k1));
+            acc[e + 2] = da(acc[e + 2], div3(k2));
+        } else {
+            const double o0 = da(acc[e], div6(k0));
+            const double o1 = da(acc[e + 1], div6(k1));
+            const double o2 = da(acc[e + 2], div6(k2));
+            const double nrm = __dsqrt_rn(da(da(dm(o0, o0), dm(o1, o1)), dm(o2, o2)));
+            out[e] = dq(dm(a.spin_len, o0), nrm);
+            out[e + 1] = dq(dm(a.spin_len, o1), nrm);
+            out[e + 2] = dq(dm(a.spin_len, o2), nrm);
+        }
+    }
+}
+
 template <int STAGE>
 cudaError_t launch_stage_t(const LLGArgs &a, const double *y, const double *ys, double *acc,
                            double *out, cudaStream_t st) {
     if (a.f0 < 0 || a.nc < 1 || a.f0 + a.nc > a.nfile) return cudaErrorInvalidValue;
     const long total = a.M * a.nc;
     const int threads = 256;
-    const unsigned blocks = (unsigned)((total + threads - 1) / threads);
     const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
+    // the halo-tiled kernel when the replica groups of 32 are mostly full
+    const bool use_tiled = a.nc >= kTiledMinReplicas;
+    const int tiles_c = (a.N + tiled::TC - 1) / tiled::TC, tiles_r = (a.N + tiled::TR - 1) / tiled::TR;
+    const long tblocks = (long)tiles_c * tiles_r * ((a.nc + tiled::FG - 1) / tiled::FG);
+    if (use_tiled && tblocks > 0x7fffffffL) return cudaErrorInvalidConfiguration;
+    const unsigned blocks = use_tiled ? (unsigned)tblocks : (unsigned)((total + threads - 1) / threads);
 #define ASD_STAGE_CASE(S, J, Hh, D)                                                            \
     case S:                                                                                    \
-        llg_stage_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(a, y, ys, acc, out);     \
+        if (use_tiled)                                                                         \
+            llg_stage_tiled_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(               \
+                a, y, ys, acc, out, tiles_c, tiles_r);                                         \
+        else                                                                                   \
+            llg_stage_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(a, y, ys, acc, out); \
         break;
     switch (sel) {
         ASD_STAGE_CASE(0, false, false, false)
@@ -148,7 +268,6 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-__device__ __forceinline__ V3 ld3(const double *p) { return V3{p[0], p[1], p[2]}; }
 
 // Inputs of one stage at one (site, replica): the centre value, its
 // neighbours in llg_rhs's order -- (row+1), (row-1), (col-1), (col+1), then
