@@ -71,81 +71,52 @@ __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double 
     }
 }
 
-// The same stage with the stage input staged through a shared-memory halo
-// tile: a block takes TR x TC sites of the lattice (plus a one-site periodic
-// halo, corners only with J2) for 32 replicas, one per lane, so each input
-// vector crosses L2 -> SM (TR+2)(TC+2)/(TR*TC) = 1.9 times instead of once
-// per neighbour (5 times, 9 with J2).  Global reads of a site's 32 replicas
-// are 768 contiguous bytes; in shared memory lane r reads word 3r + c of a
-// site, conflict-free within each half warp.  The arithmetic is llg_rhs_vals
-// on the same values in the same order: the results are bit-identical to
-// llg_stage_kernel's.
+// The same stage walked down the lattice: a warp takes a strip of SR rows of
+// one column for 32 replicas (one per lane) and keeps the 3 x 3 window of
+// stage inputs around the current site in registers, so each row costs three
+// new input vectors (the next row at columns c-1, c, c+1) instead of one per
+// neighbour (5, or 9 with J2).  A site's 32 replicas are 768 contiguous bytes
+// of every array.  The arithmetic is llg_rhs_vals on the same values in the
+// same order: the results are bit-identical to llg_stage_kernel's.
 __device__ __forceinline__ V3 ld3(const double *p) { return V3{p[0], p[1], p[2]}; }
 
-constexpr int kTiledMinReplicas = 64;  // below: the per-(site, replica) kernel
-
-namespace tiled {
-constexpr int FG = 32;          // replicas per block, one per lane
-constexpr int TR = 4, TC = 8;   // sites per block
-constexpr int HR = TR + 2, HC = TC + 2;
-constexpr int SD = FG * 3;      // doubles per site slot
-}  // namespace tiled
+constexpr int kStripMinReplicas = 64;  // below: the per-(site, replica) kernel
+constexpr int kStripRows = 16;          // rows per strip
 
 template <int STAGE, bool J2, bool H, bool DAMP>
-__global__ void __launch_bounds__(256) llg_stage_tiled_kernel(LLGArgs a, const double *__restrict__ y,
+__global__ void __launch_bounds__(256) llg_stage_strip_kernel(LLGArgs a, const double *__restrict__ y,
                                                               const double *__restrict__ ys,
                                                               double *__restrict__ acc,
-                                                              double *__restrict__ out, int tiles_c,
-                                                              int tiles_r) {
-    using namespace tiled;
-    __shared__ double sm[HR * HC * SD];  // 46 080 bytes
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int b = blockIdx.x;
-    const int tc = b % tiles_c;
-    b /= tiles_c;
-    const int tr = b % tiles_r;
-    const int grp = b / tiles_r;
+                                                              double *__restrict__ out, int ngroups) {
+    const int lane = threadIdx.x & 31;
+    const long w = (long)blockIdx.x * 8 + (threadIdx.x >> 5);
     const int N = a.N;
+    const int nstrips = (N + kStripRows - 1) / kStripRows;
+    const long nwarps = (long)ngroups * N * nstrips;
+    if (w >= nwarps) return;
+    const int grp = (int)(w % ngroups);
+    const long rest = w / ngroups;
+    const int col = (int)(rest % N);
+    const int strip = (int)(rest / N);
+    const int f = a.f0 + grp * 32 + lane;
+    if (f >= a.f0 + a.nc) return;
     const long K = 3L * a.nfile;
-    const int fbase = a.f0 + grp * FG;
-    const int nvalid = min(FG, a.f0 + a.nc - fbase);
-    const int r0 = tr * TR, c0 = tc * TC;
-    // halo tile -> shared memory, one site per warp at a time
-    for (int sidx = warp; sidx < HR * HC; sidx += 8) {
-        const int hr = sidx / HC, hc = sidx - hr * HC;
-        if (!J2 && (hr == 0 || hr == HR - 1) && (hc == 0 || hc == HC - 1)) continue;
-        int gr = (r0 - 1 + hr) % N, gc = (c0 - 1 + hc) % N;
-        if (gr < 0) gr += N;
-        if (gc < 0) gc += N;
-        const double *src = ys + ((long)gr * N + gc) * K + 3L * fbase;
-        double *dst = sm + sidx * SD;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const int x = lane + 32 * k;
-            dst[x] = (x < 3 * nvalid) ? src[x] : 0.0;
-        }
-    }
-    __syncthreads();
-    if (lane >= nvalid) return;
-    const int f = fbase + lane;
     const long off = 3L * f;
-    for (int sidx = warp; sidx < TR * TC; sidx += 8) {
-        const int lr = sidx / TC, lc = sidx - lr * TC;
-        const int row = r0 + lr, col = c0 + lc;
-        if (row >= N || col >= N) continue;
-        const double *c = sm + ((lr + 1) * HC + (lc + 1)) * SD + 3 * lane;
-        const V3 sc = ld3(c);
+    const int cm = (col == 0) ? N - 1 : col - 1, cp = (col + 1 == N) ? 0 : col + 1;
+    const int r0 = strip * kStripRows, r1 = min(N, r0 + kStripRows);
+    auto at = [&](int row, int c) { return ys + ((long)row * N + c) * K + off; };
+    // window rows: u = row - 1, m = row, d = row + 1; columns l = c-1, c, r = c+1
+    int ru = (r0 == 0) ? N - 1 : r0 - 1;
+    V3 ul = ld3(at(ru, cm)), uc = ld3(at(ru, col)), ur = ld3(at(ru, cp));
+    V3 ml = ld3(at(r0, cm)), mc = ld3(at(r0, col)), mr = ld3(at(r0, cp));
+    for (int row = r0; row < r1; ++row) {
+        const int rd = (row + 1 == N) ? 0 : row + 1;
+        const V3 dl = ld3(at(rd, cm)), dc = ld3(at(rd, col)), dr = ld3(at(rd, cp));
         // neighbours in llg_rhs's order: (row+1), (row-1), (col-1), (col+1);
         // diagonals (+1,+1), (+1,-1), (-1,+1), (-1,-1)
-        const V3 nb[4] = {ld3(c + HC * SD), ld3(c - HC * SD), ld3(c - SD), ld3(c + SD)};
-        V3 n2[4];
-        if (J2) {
-            n2[0] = ld3(c + (HC + 1) * SD);
-            n2[1] = ld3(c + (HC - 1) * SD);
-            n2[2] = ld3(c - (HC - 1) * SD);
-            n2[3] = ld3(c - (HC + 1) * SD);
-        }
-        const V3 d = llg_rhs_vals<J2, H, DAMP>(sc, nb, n2, a);
+        const V3 nb[4] = {dc, uc, ml, mr};
+        const V3 n2[4] = {dr, dl, ur, ul};
+        const V3 d = llg_rhs_vals<J2, H, DAMP>(mc, nb, n2, a);
         const long e = ((long)row * N + col) * K + off;
         const double k0 = dm(d.x, a.dt), k1 = dm(d.y, a.dt), k2 = dm(d.z, a.dt);
         if (STAGE == 1) {
@@ -179,6 +150,8 @@ __global__ void __launch_bounds__(256) llg_stage_tiled_kernel(LLGArgs a, const d
             out[e + 1] = dq(dm(a.spin_len, o1), nrm);
             out[e + 2] = dq(dm(a.spin_len, o2), nrm);
         }
+        ul = ml, uc = mc, ur = mr;
+        ml = dl, mc = dc, mr = dr;
     }
 }
 
@@ -189,17 +162,18 @@ cudaError_t launch_stage_t(const LLGArgs &a, const double *y, const double *ys, 
     const long total = a.M * a.nc;
     const int threads = 256;
     const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
-    // the halo-tiled kernel when the replica groups of 32 are mostly full
-    const bool use_tiled = a.nc >= kTiledMinReplicas;
-    const int tiles_c = (a.N + tiled::TC - 1) / tiled::TC, tiles_r = (a.N + tiled::TR - 1) / tiled::TR;
-    const long tblocks = (long)tiles_c * tiles_r * ((a.nc + tiled::FG - 1) / tiled::FG);
-    if (use_tiled && tblocks > 0x7fffffffL) return cudaErrorInvalidConfiguration;
-    const unsigned blocks = use_tiled ? (unsigned)tblocks : (unsigned)((total + threads - 1) / threads);
+    // the strip kernel when the replica groups of 32 are mostly full
+    const bool use_strip = a.nc >= kStripMinReplicas;
+    const int ngroups = (a.nc + 31) / 32;
+    const long swarps = (long)ngroups * a.N * ((a.N + kStripRows - 1) / kStripRows);
+    if (use_strip && (swarps + 7) / 8 > 0x7fffffffL) return cudaErrorInvalidConfiguration;
+    const unsigned blocks = use_strip ? (unsigned)((swarps + 7) / 8)
+                                      : (unsigned)((total + threads - 1) / threads);
 #define ASD_STAGE_CASE(S, J, Hh, D)                                                            \
     case S:                                                                                    \
-        if (use_tiled)                                                                         \
-            llg_stage_tiled_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(               \
-                a, y, ys, acc, out, tiles_c, tiles_r);                                         \
+        if (use_strip)                                                                         \
+            llg_stage_strip_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(               \
+                a, y, ys, acc, out, ngroups);                                                  \
         else                                                                                   \
             llg_stage_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(a, y, ys, acc, out); \
         break;

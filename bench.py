@@ -662,14 +662,41 @@ def run_secondary(args):
     adjoint64  64x64 lattice, 100 replicas, 1000 steps, S(q,t) every 10 steps,
              checkpoints every 50: loss + gradient wrt (J1, J2, alpha, h)
     batch48  48 lattices of sizes in {48,64,96,128,160}^2, noise amplitude in
-             [0, 0.5], alpha in [0.01, 0.2]: 2000 steps in one persistent launch"""
+             [0, 0.5], alpha in [0.01, 0.2]: 2000 steps in one persistent launch
+    llg128j2 the LLG kernels alone on the 128x128 lattice with 500 replicas and
+             the 256x256 workload's model (J=1, J2=-0.3, alpha=0.02): stage
+             kernels against HBM, the one-launch step against FP64 issue"""
     import torch
 
     import asd_b200 as asd
 
     torch.cuda.set_device(0)
     out = {"impl": "ours", "workload": args.workload, "n_gpus": 1, "data": "synthetic"}
-    if args.workload == "grid32":
+    if args.workload == "llg128j2":
+        N, nf = 128, 500
+        M = N * N
+        ctx = asd.Context(asd.Params.make(N, nf, J1=1.0, J2=-0.3, alpha=0.02, dt=0.005),
+                          modes=["fp64"])
+        stream = torch.cuda.current_stream()
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_spins(asd.random_spins(N, nf, seed=0), as_origin=True)
+        fma_tf, _ = asd.measure_fp64_peak("fma", stream.cuda_stream)
+        llg_ms = {}
+        for kern in ("stages", "fused"):
+            ctx.set_llg_kernel(kern)
+            ctx.step(3)
+            llg_ms[kern] = timed(torch, lambda: ctx.step(1), max(args.steps, 10))
+        out.update({
+            "metric": "LLG site-steps/s (RK4 step alone)", "unit": "site-steps/s",
+            "value": M * nf / (llg_ms["fused"] / 1e3), "higher_is_better": True,
+            "dtype": "f64",
+            "config": {"workload": "128x128 lattice, 500 replicas, J=1, J2=-0.3, alpha=0.02, "
+                                   "dt=0.005, RK4 step only", "sites": M, "replicas": nf},
+            "llg": llg_report(llg_ms, M * nf, llg_fp64_ops(True, False, True),
+                              measured_peaks()["hbm_gbs"], fma_tf / 2.0),
+        })
+        ctx.close()
+    elif args.workload == "grid32":
         # 32x32 lattice, 200 replicas, J=1, alpha=0.1, dt=0.01, 2000 RK4 steps, S(q,t) on the
         # whole 32x32 q grid after every step (FP64 GEMM + displacement bins + 2-D DFT)
         N, nf, nsteps = 32, 200, 2000
@@ -858,7 +885,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sqt256", "sqt128", "grid32", "adjoint64", "batch48"],
+    ap.add_argument("--workload", choices=["sqt256", "sqt128", "grid32", "adjoint64", "batch48",
+                                           "llg128j2"],
                     default="sqt256",
                     help="sqt256 (default) and sqt128 print the full line; the others a line of "
                          "their own")

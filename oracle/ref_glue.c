@@ -266,7 +266,10 @@ int ref_gemm_sqt_band(const double *spin_all, const double *spin_0, long rows, d
         free(spin_zero), free(spint), free(zerot), free(fint), free(cmat);
         return -2;
     }
-    memset(cmat, 0, (size_t)mm * M * sizeof(double)); /* first touch outside the timing */
+    /* first touch of the work arrays outside the timing (the reference's
+     * program allocates them once and reuses them every step) */
+    memset(cmat, 0, (size_t)mm * M * sizeof(double));
+    memset(spint, 0, (size_t)M * K * sizeof(double));
     /* the program's one-time set-up (spin_zero and zerot before the time loop) */
 #pragma omp parallel for
     for (long i = 0; i < M; i++)
