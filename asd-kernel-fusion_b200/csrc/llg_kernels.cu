@@ -21,16 +21,32 @@ namespace {
 // records (768 contiguous bytes) of each operand.  The combination order
 // reproduces runge_kutta's final sum spin + k1/6 + k2/3 + k3/3 + k4/6
 // evaluated left to right (llg_sqt_baseline.c:138), carried in acc.
+//
+// Thread mapping.  With fewer than 64 replicas, thread t is (site t / nc,
+// replica t % nc).  With 64 or more (ngroups = ceil(nc / 32) groups of 32),
+// block b takes 8 consecutive sites (one per warp) of replica group
+// b % ngroups, lane = replica within the group: the warps of a block are
+// horizontal neighbours, so each reads the others' centre vectors as its left
+// and right neighbours and those loads hit in L1 instead of L2.
 template <int STAGE, bool J2, bool H, bool DAMP>
 __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double *__restrict__ y,
                                                         const double *__restrict__ ys,
                                                         double *__restrict__ acc,
-                                                        double *__restrict__ out) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long total = a.M * a.nc;
-    if (t >= total) return;
-    const long site = t / a.nc;
-    const int f = a.f0 + (int)(t - site * a.nc);
+                                                        double *__restrict__ out, int ngroups) {
+    long site;
+    int f;
+    if (ngroups > 0) {
+        const int g = (int)(blockIdx.x % ngroups);
+        site = (long)(blockIdx.x / ngroups) * 8 + (threadIdx.x >> 5);
+        const int lf = g * 32 + (threadIdx.x & 31);
+        if (site >= a.M || lf >= a.nc) return;
+        f = a.f0 + lf;
+    } else {
+        const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= a.M * a.nc) return;
+        site = t / a.nc;
+        f = a.f0 + (int)(t - site * a.nc);
+    }
     const int row = (int)(site / a.N), col = (int)(site - (long)row * a.N);
     const long sstride = 3L * a.nfile;
     const long off = 3L * f;
@@ -71,89 +87,9 @@ __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double 
     }
 }
 
-// The same stage walked down the lattice: a warp takes a strip of SR rows of
-// one column for 32 replicas (one per lane) and keeps the 3 x 3 window of
-// stage inputs around the current site in registers, so each row costs three
-// new input vectors (the next row at columns c-1, c, c+1) instead of one per
-// neighbour (5, or 9 with J2).  A site's 32 replicas are 768 contiguous bytes
-// of every array.  The arithmetic is llg_rhs_vals on the same values in the
-// same order: the results are bit-identical to llg_stage_kernel's.
 __device__ __forceinline__ V3 ld3(const double *p) { return V3{p[0], p[1], p[2]}; }
 
-constexpr int kStripMinReplicas = 64;  // below: the per-(site, replica) kernel
-constexpr int kStripRows = 16;          // rows per strip
-
-template <int STAGE, bool J2, bool H, bool DAMP>
-__global__ void __launch_bounds__(256) llg_stage_strip_kernel(LLGArgs a, const double *__restrict__ y,
-                                                              const double *__restrict__ ys,
-                                                              double *__restrict__ acc,
-                                                              double *__restrict__ out, int ngroups) {
-    const int lane = threadIdx.x & 31;
-    const long w = (long)blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int N = a.N;
-    const int nstrips = (N + kStripRows - 1) / kStripRows;
-    const long nwarps = (long)ngroups * N * nstrips;
-    if (w >= nwarps) return;
-    const int grp = (int)(w % ngroups);
-    const long rest = w / ngroups;
-    const int col = (int)(rest % N);
-    const int strip = (int)(rest / N);
-    const int f = a.f0 + grp * 32 + lane;
-    if (f >= a.f0 + a.nc) return;
-    const long K = 3L * a.nfile;
-    const long off = 3L * f;
-    const int cm = (col == 0) ? N - 1 : col - 1, cp = (col + 1 == N) ? 0 : col + 1;
-    const int r0 = strip * kStripRows, r1 = min(N, r0 + kStripRows);
-    auto at = [&](int row, int c) { return ys + ((long)row * N + c) * K + off; };
-    // window rows: u = row - 1, m = row, d = row + 1; columns l = c-1, c, r = c+1
-    int ru = (r0 == 0) ? N - 1 : r0 - 1;
-    V3 ul = ld3(at(ru, cm)), uc = ld3(at(ru, col)), ur = ld3(at(ru, cp));
-    V3 ml = ld3(at(r0, cm)), mc = ld3(at(r0, col)), mr = ld3(at(r0, cp));
-    for (int row = r0; row < r1; ++row) {
-        const int rd = (row + 1 == N) ? 0 : row + 1;
-        const V3 dl = ld3(at(rd, cm)), dc = ld3(at(rd, col)), dr = ld3(at(rd, cp));
-        // neighbours in llg_rhs's order: (row+1), (row-1), (col-1), (col+1);
-        // diagonals (+1,+1), (+1,-1), (-1,+1), (-1,-1)
-        const V3 nb[4] = {dc, uc, ml, mr};
-        const V3 n2[4] = {dr, dl, ur, ul};
-        const V3 d = llg_rhs_vals<J2, H, DAMP>(mc, nb, n2, a);
-        const long e = ((long)row * N + col) * K + off;
-        const double k0 = dm(d.x, a.dt), k1 = dm(d.y, a.dt), k2 = dm(d.z, a.dt);
-        if (STAGE == 1) {
-            const double y0 = y[e], y1 = y[e + 1], y2 = y[e + 2];
-            out[e] = da(y0, half(k0));
-            out[e + 1] = da(y1, half(k1));
-            out[e + 2] = da(y2, half(k2));
-            acc[e] = da(y0, div6(k0));
-            acc[e + 1] = da(y1, div6(k1));
-            acc[e + 2] = da(y2, div6(k2));
-        } else if (STAGE == 2 || STAGE == 3) {
-            const double y0 = y[e], y1 = y[e + 1], y2 = y[e + 2];
-            if (STAGE == 2) {
-                out[e] = da(y0, half(k0));
-                out[e + 1] = da(y1, half(k1));
-                out[e + 2] = da(y2, half(k2));
-            } else {
-                out[e] = da(y0, k0);
-                out[e + 1] = da(y1, k1);
-                out[e + 2] = da(y2, k2);
-            }
-            acc[e] = da(acc[e], div3(k0));
-            acc[e + 1] = da(acc[e + 1], div3(k1));
-            acc[e + 2] = da(acc[e + 2], div3(k2));
-        } else {
-            const double o0 = da(acc[e], div6(k0));
-            const double o1 = da(acc[e + 1], div6(k1));
-            const double o2 = da(acc[e + 2], div6(k2));
-            const double nrm = __dsqrt_rn(da(da(dm(o0, o0), dm(o1, o1)), dm(o2, o2)));
-            out[e] = dq(dm(a.spin_len, o0), nrm);
-            out[e + 1] = dq(dm(a.spin_len, o1), nrm);
-            out[e + 2] = dq(dm(a.spin_len, o2), nrm);
-        }
-        ul = ml, uc = mc, ur = mr;
-        ml = dl, mc = dc, mr = dr;
-    }
-}
+constexpr int kGroupedMinReplicas = 64;  // below: one thread per (site, replica) in order
 
 template <int STAGE>
 cudaError_t launch_stage_t(const LLGArgs &a, const double *y, const double *ys, double *acc,
@@ -162,20 +98,16 @@ cudaError_t launch_stage_t(const LLGArgs &a, const double *y, const double *ys, 
     const long total = a.M * a.nc;
     const int threads = 256;
     const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
-    // the strip kernel when the replica groups of 32 are mostly full
-    const bool use_strip = a.nc >= kStripMinReplicas;
-    const int ngroups = (a.nc + 31) / 32;
-    const long swarps = (long)ngroups * a.N * ((a.N + kStripRows - 1) / kStripRows);
-    if (use_strip && (swarps + 7) / 8 > 0x7fffffffL) return cudaErrorInvalidConfiguration;
-    const unsigned blocks = use_strip ? (unsigned)((swarps + 7) / 8)
-                                      : (unsigned)((total + threads - 1) / threads);
+    // site-grouped mapping when the replica groups of 32 are mostly full
+    const int ngroups = (a.nc >= kGroupedMinReplicas) ? (a.nc + 31) / 32 : 0;
+    const long gblocks = (long)ngroups * ((a.M + 7) / 8);
+    if (gblocks > 0x7fffffffL) return cudaErrorInvalidConfiguration;
+    const unsigned blocks = ngroups > 0 ? (unsigned)gblocks
+                                        : (unsigned)((total + threads - 1) / threads);
 #define ASD_STAGE_CASE(S, J, Hh, D)                                                            \
     case S:                                                                                    \
-        if (use_strip)                                                                         \
-            llg_stage_strip_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(               \
-                a, y, ys, acc, out, ngroups);                                                  \
-        else                                                                                   \
-            llg_stage_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(a, y, ys, acc, out); \
+        llg_stage_kernel<STAGE, J, Hh, D><<<blocks, threads, 0, st>>>(a, y, ys, acc, out,      \
+                                                                       ngroups);               \
         break;
     switch (sel) {
         ASD_STAGE_CASE(0, false, false, false)
