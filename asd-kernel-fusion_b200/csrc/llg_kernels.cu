@@ -24,10 +24,13 @@ namespace {
 //
 // Thread mapping.  With fewer than 64 replicas, thread t is (site t / nc,
 // replica t % nc).  With 64 or more (ngroups = ceil(nc / 32) groups of 32),
-// block b takes 8 consecutive sites (one per warp) of replica group
+// block b takes a 2 x 4 patch of sites (one per warp) of replica group
 // b % ngroups, lane = replica within the group: the warps of a block are
-// horizontal neighbours, so each reads the others' centre vectors as its left
-// and right neighbours and those loads hit in L1 instead of L2.
+// lattice neighbours, so many of the input vectors a warp reads as
+// neighbours are other warps' centres and hit in L1 instead of L2 (the block
+// reads 20 distinct site vectors for 8 sites, 24 with J2, instead of 40 / 72).
+// Measured on B200 against one thread per (site, replica) in order:
+// 256x256x1000 with J2 5.21 vs 6.12-6.21 ms per step of four stages.
 template <int STAGE, bool J2, bool H, bool DAMP>
 __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double *__restrict__ y,
                                                         const double *__restrict__ ys,
@@ -37,9 +40,13 @@ __global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double 
     int f;
     if (ngroups > 0) {
         const int g = (int)(blockIdx.x % ngroups);
-        site = (long)(blockIdx.x / ngroups) * 8 + (threadIdx.x >> 5);
+        const long tile = blockIdx.x / ngroups;
+        const int tcols = (a.N + 3) / 4;
+        const int w = threadIdx.x >> 5;
+        const int trow = (int)(tile / tcols) * 2 + (w >> 2), tcol = (int)(tile % tcols) * 4 + (w & 3);
         const int lf = g * 32 + (threadIdx.x & 31);
-        if (site >= a.M || lf >= a.nc) return;
+        if (trow >= a.N || tcol >= a.N || lf >= a.nc) return;
+        site = (long)trow * a.N + tcol;
         f = a.f0 + lf;
     } else {
         const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -100,7 +107,7 @@ cudaError_t launch_stage_t(const LLGArgs &a, const double *y, const double *ys, 
     const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
     // site-grouped mapping when the replica groups of 32 are mostly full
     const int ngroups = (a.nc >= kGroupedMinReplicas) ? (a.nc + 31) / 32 : 0;
-    const long gblocks = (long)ngroups * ((a.M + 7) / 8);
+    const long gblocks = (long)ngroups * ((a.N + 1) / 2) * ((a.N + 3) / 4);
     if (gblocks > 0x7fffffffL) return cudaErrorInvalidConfiguration;
     const unsigned blocks = ngroups > 0 ? (unsigned)gblocks
                                         : (unsigned)((total + threads - 1) / threads);
