@@ -17,13 +17,15 @@
 //
 // Operands: A = the state at t, B = the origin, both site-major [M][K] FP64
 // (K = 3 * nfile contiguous), i.e. the GEMM is C = A B^T with both operands
-// K-major.  Tiles of 128 x 128, K staged 16 at a time through a 4-deep
+// K-major.  Tiles of 128 x 128, K staged 32 at a time through a 3-deep
 // cp.async pipeline (16-byte copies when K is even, 8-byte ones otherwise;
 // zero fill past M and K); 8 warps of 64 x 32, each a 4 x 4 grid of
-// m16n8k8 accumulators (64 FP64 registers).  Shared-memory rows are 128 bytes
-// (16 doubles) with the 16-byte chunks of odd rows rotated by half a row, so
-// that the 16-byte fragment loads of a quarter warp (two rows) fall into
-// different banks.
+// m16n8k8 accumulators (64 FP64 registers).  Shared-memory rows are 256 bytes
+// (32 doubles) with the 16-byte chunks of odd rows XOR-ed by 4 (a 64-byte
+// shift), so that the 16-byte fragment loads of a quarter warp (two rows) fall
+// into different banks.  (K stages of 16 in a 4-deep pipeline took 1.6 %
+// longer at 256x256x1000; the k order of every accumulator, and so the result,
+// is the same bit for bit.)
 #include <cuda_runtime.h>
 
 #include "asd_internal.h"
@@ -32,15 +34,17 @@
 namespace asd {
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4, THREADS = 256;
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 256;
 constexpr int GROUP_M = 16;  // row tiles per raster group (A bands stay in L2)
 constexpr int TILE_DOUBLES = BM * BK;          // one operand tile of one stage
-constexpr int STAGE_DOUBLES = (BM + BN) * BK;  // 4096 doubles = 32 KB
+constexpr int STAGE_DOUBLES = (BM + BN) * BK;  // 8192 doubles = 64 KB
 constexpr int PIPE_BYTES = STAGES * STAGE_DOUBLES * 8;
 constexpr int TSTRIDE = BN + 1;  // q grid: epilogue tile row stride (doubles)
 constexpr int GRID_SMEM = BM * TSTRIDE * 8;
 constexpr int EPI_PHASE = 0, EPI_GRID = 1;
-static_assert(GRID_SMEM > PIPE_BYTES, "grid smem covers the pipeline");
+constexpr int KCH = BK / 2;  // 16-byte chunks per shared-memory row
+constexpr int LOG_KCH = 4;
+static_assert(KCH == (1 << LOG_KCH), "chunks per row");
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -83,7 +87,7 @@ __device__ __forceinline__ void load_tile(double *dst, const double *__restrict_
 #pragma unroll
         for (int q = 0; q < (BM * BK / 2) / THREADS; ++q) {
             const int idx = threadIdx.x + q * THREADS;
-            const int r = idx >> 3, ch = idx & 7;
+            const int r = idx >> LOG_KCH, ch = idx & (KCH - 1);
             const long gi = row0 + r;
             const int gk = k0 + 2 * ch;
             const bool ok = (gi < M) && (gk < K);
@@ -94,7 +98,7 @@ __device__ __forceinline__ void load_tile(double *dst, const double *__restrict_
 #pragma unroll
         for (int q = 0; q < (BM * BK) / THREADS; ++q) {
             const int idx = threadIdx.x + q * THREADS;
-            const int r = idx >> 4, k = idx & 15;
+            const int r = idx >> (LOG_KCH + 1), k = idx & (BK - 1);
             const long gi = row0 + r;
             const int gk = k0 + k;
             const bool ok = (gi < M) && (gk < K);
@@ -318,7 +322,7 @@ int launch_dmma_sqt(const DmmaSqtArgs &p, cudaStream_t st) {
     if (grid && (p.lat_n < 1 || (long)p.lat_n * p.lat_n != p.M))
         return fail(ASD_ERR_INVALID, "q grid needs M = N*N");
     const bool vec2 = (p.K % 2 == 0) && (((uintptr_t)p.A | (uintptr_t)p.B) & 15) == 0;
-    const int smem = grid ? GRID_SMEM : PIPE_BYTES;
+    const int smem = (grid && GRID_SMEM > PIPE_BYTES) ? GRID_SMEM : PIPE_BYTES;
     auto go = [&](auto kern) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;

@@ -663,6 +663,8 @@ def run_secondary(args):
              checkpoints every 50: loss + gradient wrt (J1, J2, alpha, h)
     batch48  48 lattices of sizes in {48,64,96,128,160}^2, noise amplitude in
              [0, 0.5], alpha in [0.01, 0.2]: 2000 steps in one persistent launch
+    grid128, grid256  S(q,t) on the whole q grid after one step of the 128x128x500
+             and 256x256x1000 workloads, every mode, against one q of the same mode
     llg128j2 the LLG kernels alone on the 128x128 lattice with 500 replicas and
              the 256x256 workload's model (J=1, J2=-0.3, alpha=0.02): stage
              kernels against HBM, the one-launch step against FP64 issue"""
@@ -672,7 +674,40 @@ def run_secondary(args):
 
     torch.cuda.set_device(0)
     out = {"impl": "ours", "workload": args.workload, "n_gpus": 1, "data": "synthetic"}
-    if args.workload == "llg128j2":
+    if args.workload in ("grid128", "grid256"):
+        w = WORKLOADS["sqt128" if args.workload == "grid128" else "sqt256"]
+        N, nf = w["N"], w["nfile"]
+        M, K = N * N, 3 * nf
+        ctx = asd.Context(asd.Params.make(N, nf, J1=w["J1"], J2=w["J2"], alpha=w["alpha"],
+                                          h=w["h"], dt=w["dt"]))
+        stream = torch.cuda.current_stream()
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_spins(asd.random_spins(N, nf, seed=0), as_origin=True)
+        ctx.step(1)
+        grid = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
+        one = torch.zeros(2, dtype=torch.float64, device="cuda")
+        res = {}
+        for mode in ("bf16x3", "tf32x3", "fp64"):
+            reps = 1 if mode == "fp64" else 3
+            ctx.sqt_grid_async(mode, grid.data_ptr())  # work space, warm
+            g_ms = timed(torch, lambda: ctx.sqt_grid_async(mode, grid.data_ptr()), reps)
+            ctx.sqt_async(mode, one.data_ptr())
+            q_ms = timed(torch, lambda: ctx.sqt_async(mode, one.data_ptr()), reps)
+            g = grid.view(N, N, 2)
+            vx = N // 10
+            res[mode] = {"grid_ms": g_ms, "single_q_ms": q_ms, "grid_over_single": g_ms / q_ms,
+                         "gemm_tflops": 2.0 * M * M * K / (g_ms / 1e3) / 1e12,
+                         "grid_at_vx_vy": [float(g[vx, vx, 0]), float(g[vx, vx, 1])],
+                         "single_q": one.tolist()}
+        out.update({
+            "metric": "S(q,t) on the whole N x N q grid, ms per evaluation", "unit": "ms",
+            "value": res[w["mode"]]["grid_ms"], "higher_is_better": False,
+            "dtype": w["mode"] + " GEMM, f64 bins and DFT",
+            "config": {"workload": w["desc"] + ", S(q,t) at all N*N q", "sites": M, "replicas": nf},
+            "modes": res,
+        })
+        ctx.close()
+    elif args.workload == "llg128j2":
         N, nf = 128, 500
         M = N * N
         ctx = asd.Context(asd.Params.make(N, nf, J1=1.0, J2=-0.3, alpha=0.02, dt=0.005),
@@ -885,8 +920,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sqt256", "sqt128", "grid32", "adjoint64", "batch48",
-                                           "llg128j2"],
+    ap.add_argument("--workload", choices=["sqt256", "sqt128", "grid32", "grid128", "grid256",
+                                           "adjoint64", "batch48", "llg128j2"],
                     default="sqt256",
                     help="sqt256 (default) and sqt128 print the full line; the others a line of "
                          "their own")
