@@ -174,7 +174,6 @@ int do_fused_dgemm(int m, int n, int k, double alpha, const double *a, int lda, 
     ASD_CUDA_TRY(cudaMemcpy(g_buf.g[2], c, nc * sizeof(double), cudaMemcpyHostToDevice));
     ASD_CUDA_TRY(cudaMemcpy(g_buf.g[3], q, nc * sizeof(double), cudaMemcpyHostToDevice));
     Fp64GemmArgs g{};
-    g.dropin = 1;
     g.m = m;
     g.n = n;
     g.k = k;

@@ -1,14 +1,13 @@
-// fp64_gemm.cu -- FP64 CUDA-core GEMM with two fused epilogues.
+// fp64_gemm.cu -- the reference's fused_dgemm on the GPU (FP64 CUDA cores),
+// for the drop-in entry point (dropin.cu).
 //
-//  * DROPIN: the reference's fused_dgemm semantics (kernel_fusion/
-//    gemm_kernel.h:355-422): alpha folded into A, K in blocks of 240, per
-//    element a sequential FMA chain over k (the AVX2 micro-kernel's order,
-//    :9-35), then C = fma(q, acc, C) on the interleaved re/im layout and the
-//    updated values summed once per K block (:39-88).  Because the per-element
-//    arithmetic is the same chain of correctly rounded FMAs, C is
-//    bit-identical to the reference's.
-//  * PHASE: S(q,t) in FP64 without storing C: per element
-//    v = alpha*acc - m_i . z_j, accumulated as u_i * sum_j w_j v.
+// Semantics of kernel_fusion/gemm_kernel.h:355-422: alpha folded into A, K in
+// blocks of 240, per element a sequential FMA chain over k (the AVX2
+// micro-kernel's order, :9-35), then C = fma(q, acc, C) on the interleaved
+// re/im layout and the updated values summed once per K block (:39-88).
+// Because the per-element arithmetic is the same chain of correctly rounded
+// FMAs, C is bit-identical to the reference's.  (S(q,t) in FP64 does not come
+// here: it runs on the FP64 tensor cores, dmma_sqt.cu.)
 //
 // Tile 64 x 64, 256 threads, 4 x 4 results per thread, k staged through
 // shared memory 16 at a time (240 = 15 * 16, so K blocks never straddle a
@@ -25,15 +24,13 @@ constexpr int TK = 16;
 __device__ __forceinline__ long row_re(long i) { return (i / 4) * 8 + (i % 4); }
 
 // A(i,k) = a[i*sai + k*sak], B(k,j) = b[k*sbk + j*sbj].
-template <bool DROPIN>
 __global__ void __launch_bounds__(256) fp64_gemm_kernel(Fp64GemmArgs p) {
     __shared__ double As[TK][TB + 1];
     __shared__ double Bs[TK][TB + 1];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const long i0 = (long)blockIdx.y * TB, j0 = (long)blockIdx.x * TB;
     double acc[4][4];
-    double part_re = 0.0, part_im = 0.0;
-    const long kblk = DROPIN ? 240 : p.k;
+    const long kblk = 240;
     int kb_index = 0;
     for (long kbeg = 0; kbeg < p.k; kbeg += kblk, ++kb_index) {
         const long kend = min(kbeg + kblk, (long)p.k);
@@ -54,7 +51,7 @@ __global__ void __launch_bounds__(256) fp64_gemm_kernel(Fp64GemmArgs p) {
                 double v = 0.0;
                 if (gi < p.m && kk < kcnt) {
                     v = p.a[gi * p.sai + gk * p.sak];
-                    if (DROPIN) v = __dmul_rn(v, p.alpha);  // dgemm_tcopy_4 (:238)
+                    v = __dmul_rn(v, p.alpha);  // dgemm_tcopy_4 (:238)
                 }
                 As[kk][ii] = v;
                 int jj, kk2;
@@ -79,82 +76,43 @@ __global__ void __launch_bounds__(256) fp64_gemm_kernel(Fp64GemmArgs p) {
             }
             __syncthreads();
         }
-        if (DROPIN) {
-            // C = fma(q, acc, C) and the K-block sum, rows < m4, cols < n2 only
-            double bre = 0.0, bim = 0.0;
+        // C = fma(q, acc, C) and the K-block sum, rows < m4, cols < n2 only
+        double bre = 0.0, bim = 0.0;
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const long i = i0 + ty + 16 * r;
-                if (i >= p.m4) continue;
+        for (int r = 0; r < 4; ++r) {
+            const long i = i0 + ty + 16 * r;
+            if (i >= p.m4) continue;
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    const long j = j0 + tx + 16 * c;
-                    if (j >= p.n2) continue;
-                    const long ir = row_re(i) + j * p.ldc;
-                    const double cr = __fma_rn(p.q[ir], acc[r][c], p.c[ir]);
-                    const double ci = __fma_rn(p.q[ir + 4], acc[r][c], p.c[ir + 4]);
-                    p.c[ir] = cr;
-                    p.c[ir + 4] = ci;
-                    bre += cr;
-                    bim += ci;
-                }
-            }
-            // per-block reduction of this K block's sum
-            __shared__ double red[2][256];
-            red[0][threadIdx.x] = bre;
-            red[1][threadIdx.x] = bim;
-            __syncthreads();
-            for (int s = 128; s > 0; s >>= 1) {
-                if (threadIdx.x < s) {
-                    red[0][threadIdx.x] += red[0][threadIdx.x + s];
-                    red[1][threadIdx.x] += red[1][threadIdx.x + s];
-                }
-                __syncthreads();
-            }
-            if (threadIdx.x == 0) {
-                const long nblk = (long)gridDim.x * gridDim.y;
-                const long b = (long)blockIdx.y * gridDim.x + blockIdx.x;
-                p.part[(long)kb_index * nblk + b] = make_double2(red[0][0], red[1][0]);
-            }
-            __syncthreads();
-        } else {
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const long i = i0 + ty + 16 * r;
-                if (i >= p.m) continue;
-                const double mx = p.mrow[i * 3], my = p.mrow[i * 3 + 1], mz = p.mrow[i * 3 + 2];
-                double sre = 0.0, sim = 0.0;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    const long j = j0 + tx + 16 * c;
-                    if (j >= p.n) continue;
-                    const double outer = mx * p.zcol[j * 3] + my * p.zcol[j * 3 + 1] +
-                                         mz * p.zcol[j * 3 + 2];
-                    const double v = p.alpha * acc[r][c] - outer;
-                    const double2 w = p.wphase[j];
-                    sre += w.x * v;
-                    sim += w.y * v;
-                }
-                const double2 u = p.uphase[i];
-                part_re += u.x * sre - u.y * sim;
-                part_im += u.x * sim + u.y * sre;
+            for (int c = 0; c < 4; ++c) {
+                const long j = j0 + tx + 16 * c;
+                if (j >= p.n2) continue;
+                const long ir = row_re(i) + j * p.ldc;
+                const double cr = __fma_rn(p.q[ir], acc[r][c], p.c[ir]);
+                const double ci = __fma_rn(p.q[ir + 4], acc[r][c], p.c[ir + 4]);
+                p.c[ir] = cr;
+                p.c[ir + 4] = ci;
+                bre += cr;
+                bim += ci;
             }
         }
-    }
-    if (!DROPIN) {
-        __shared__ double red2[2][256];
-        red2[0][threadIdx.x] = part_re;
-        red2[1][threadIdx.x] = part_im;
+        // per-block reduction of this K block's sum
+        __shared__ double red[2][256];
+        red[0][threadIdx.x] = bre;
+        red[1][threadIdx.x] = bim;
         __syncthreads();
         for (int s = 128; s > 0; s >>= 1) {
             if (threadIdx.x < s) {
-                red2[0][threadIdx.x] += red2[0][threadIdx.x + s];
-                red2[1][threadIdx.x] += red2[1][threadIdx.x + s];
+                red[0][threadIdx.x] += red[0][threadIdx.x + s];
+                red[1][threadIdx.x] += red[1][threadIdx.x + s];
             }
             __syncthreads();
         }
-        if (threadIdx.x == 0)
-            p.part[(long)blockIdx.y * gridDim.x + blockIdx.x] = make_double2(red2[0][0], red2[1][0]);
+        if (threadIdx.x == 0) {
+            const long nblk = (long)gridDim.x * gridDim.y;
+            const long b = (long)blockIdx.y * gridDim.x + blockIdx.x;
+            p.part[(long)kb_index * nblk + b] = make_double2(red[0][0], red[1][0]);
+        }
+        __syncthreads();
     }
 }
 
@@ -162,17 +120,14 @@ __global__ void __launch_bounds__(256) fp64_gemm_kernel(Fp64GemmArgs p) {
 
 long fp64_gemm_num_parts(const Fp64GemmArgs &p) {
     const long nbx = (p.n + TB - 1) / TB, nby = (p.m + TB - 1) / TB;
-    const long nkb = p.dropin ? (p.k + 239) / 240 : 1;
+    const long nkb = (p.k + 239) / 240;
     return nbx * nby * nkb;
 }
 
 cudaError_t launch_fp64_gemm(const Fp64GemmArgs &p, cudaStream_t st) {
     dim3 grid((unsigned)((p.n + TB - 1) / TB), (unsigned)((p.m + TB - 1) / TB));
     if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
-    if (p.dropin)
-        fp64_gemm_kernel<true><<<grid, 256, 0, st>>>(p);
-    else
-        fp64_gemm_kernel<false><<<grid, 256, 0, st>>>(p);
+    fp64_gemm_kernel<<<grid, 256, 0, st>>>(p);
     return cudaGetLastError();
 }
 
