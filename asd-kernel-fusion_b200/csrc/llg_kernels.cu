@@ -31,8 +31,10 @@ namespace {
 // reads 20 distinct site vectors for 8 sites, 24 with J2, instead of 40 / 72).
 // Measured on B200 against one thread per (site, replica) in order:
 // 256x256x1000 with J2 5.21 vs 6.12-6.21 ms per step of four stages.
+// At most 32 registers (8 blocks of 256 threads per SM): stage 4 with J2
+// otherwise takes 34 and only 6 blocks fit.
 template <int STAGE, bool J2, bool H, bool DAMP>
-__global__ void __launch_bounds__(256) llg_stage_kernel(LLGArgs a, const double *__restrict__ y,
+__global__ void __launch_bounds__(256, 8) llg_stage_kernel(LLGArgs a, const double *__restrict__ y,
                                                         const double *__restrict__ ys,
                                                         double *__restrict__ acc,
                                                         double *__restrict__ out, int ngroups) {

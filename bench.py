@@ -665,9 +665,10 @@ def run_secondary(args):
              [0, 0.5], alpha in [0.01, 0.2]: 2000 steps in one persistent launch
     grid128, grid256  S(q,t) on the whole q grid after one step of the 128x128x500
              and 256x256x1000 workloads, every mode, against one q of the same mode
-    llg128j2 the LLG kernels alone on the 128x128 lattice with 500 replicas and
-             the 256x256 workload's model (J=1, J2=-0.3, alpha=0.02): stage
-             kernels against HBM, the one-launch step against FP64 issue"""
+    llg128j2, llg256j2  the LLG kernels alone on the 128x128 lattice with 500
+             replicas or the 256x256 lattice with 1000, with the 256x256
+             workload's model (J=1, J2=-0.3, alpha=0.02): stage kernels against
+             HBM, the one-launch step against FP64 issue"""
     import torch
 
     import asd_b200 as asd
@@ -707,8 +708,8 @@ def run_secondary(args):
             "modes": res,
         })
         ctx.close()
-    elif args.workload == "llg128j2":
-        N, nf = 128, 500
+    elif args.workload in ("llg128j2", "llg256j2"):
+        N, nf = (128, 500) if args.workload == "llg128j2" else (256, 1000)
         M = N * N
         ctx = asd.Context(asd.Params.make(N, nf, J1=1.0, J2=-0.3, alpha=0.02, dt=0.005),
                           modes=["fp64"])
@@ -725,7 +726,7 @@ def run_secondary(args):
             "metric": "LLG site-steps/s (RK4 step alone)", "unit": "site-steps/s",
             "value": M * nf / (llg_ms["fused"] / 1e3), "higher_is_better": True,
             "dtype": "f64",
-            "config": {"workload": "128x128 lattice, 500 replicas, J=1, J2=-0.3, alpha=0.02, "
+            "config": {"workload": f"{N}x{N} lattice, {nf} replicas, J=1, J2=-0.3, alpha=0.02, "
                                    "dt=0.005, RK4 step only", "sites": M, "replicas": nf},
             "llg": llg_report(llg_ms, M * nf, llg_fp64_ops(True, False, True),
                               measured_peaks()["hbm_gbs"], fma_tf / 2.0),
@@ -921,7 +922,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["sqt256", "sqt128", "grid32", "grid128", "grid256",
-                                           "adjoint64", "batch48", "llg128j2"],
+                                           "adjoint64", "batch48", "llg128j2", "llg256j2"],
                     default="sqt256",
                     help="sqt256 (default) and sqt128 print the full line; the others a line of "
                          "their own")

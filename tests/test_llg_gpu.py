@@ -33,6 +33,17 @@ CASES = [
     (70, 13, dict(J1=1.0, J2=-0.3, alpha=0.02, dt=0.005)),
     (130, 5, dict(J1=-1.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005)),
     (256, 3, dict(J1=1.0, J2=-0.3, h=(0.2, 0.0, 0.1), alpha=0.02, dt=0.005)),
+    # 64 or more replicas: the stage kernels' blocks of 2 x 4 sites x 32
+    # replicas.  Odd replica count with a last group of 1 and ragged blocks;
+    # with and without J2; N = 3, narrower than one block, so neighbours wrap
+    # onto the block's own sites; a last group of 6 with every extension;
+    # N = 70, ragged in both directions, with a last group of 2.
+    (9, 65, dict(J1=0.7, J2=0.4, dt=0.03)),
+    (6, 96, dict(J1=-1.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005)),
+    (3, 64, dict(J1=1.0, J2=-0.3, alpha=0.1, dt=0.01)),
+    (13, 70, dict(J1=1.0, J2=-0.3, h=(0.1, 0.2, 0.0), alpha=0.02, dt=0.005, spin_len=1.5)),
+    (5, 67, dict(J1=1.0, dt=0.02)),
+    (70, 66, dict(J1=-1.0, J2=0.2, alpha=0.05, dt=0.005)),
 ]
 
 
