@@ -515,21 +515,23 @@ def pre_measurements(ctx, asd, torch, stream, name, args):
     dmma_tf, _ = asd.measure_fp64_peak("dmma", stream.cuda_stream)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = 10
-    llg = {}
+    llg, llg_clocks = {}, {}
     for kern in ("stages", "fused"):
         ctx.set_llg_kernel(kern)
         ctx.step(2)
         ts = []
-        for _ in range(3):
-            torch.cuda.synchronize()
-            ev0.record(stream)
-            ctx.step(reps)
-            ev1.record(stream)
-            torch.cuda.synchronize()
-            ts.append(ev0.elapsed_time(ev1) / reps)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            for _ in range(3):
+                torch.cuda.synchronize()
+                ev0.record(stream)
+                ctx.step(reps)
+                ev1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(ev0.elapsed_time(ev1) / reps)
         llg[kern] = sorted(ts)[1]
+        llg_clocks[kern] = clk.summary()
     ctx.set_llg_kernel(args.llg_kernel)
-    return {"fma_tf": fma_tf, "dmma_tf": dmma_tf, "llg": llg}
+    return {"fma_tf": fma_tf, "dmma_tf": dmma_tf, "llg": llg, "llg_clocks": llg_clocks}
 
 
 def component_measurements(ctx, asd, torch, stream, name, mode, args, pre):
@@ -585,6 +587,7 @@ def component_measurements(ctx, asd, torch, stream, name, mode, args, pre):
         "llg": llg_report(llg, M * nf, llg_fp64_ops(w["J2"] != 0.0, any(w["h"]), w["alpha"] != 0.0),
                           peaks["hbm_gbs"], fma_tf / 2.0),
         "llg_note": "each LLG kernel alone before the timed region (median of 3 x 10 steps)",
+        "llg_clocks": pre.get("llg_clocks"),
         "sqt": sqt,
         "sqt_term_magnitude": mag,
         "sqt_speedup_vs_fp64": {m: sqt_ms["fp64"] / sqt_ms[m] for m in ("tf32x3", "bf16x3")},

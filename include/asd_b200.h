@@ -232,7 +232,7 @@ int asd_ctx_shard_sqt_finish(asd_ctx *ctx, const double *d_part, const double *d
  * bit-identical spins. */
 #define ASD_LLG_STAGES 0     /* four launches, one fused kernel per RK4 stage,
                                 HBM-bound (384 B of DRAM traffic per
-                                site-step; 75-85% of the measured HBM copy
+                                site-step; 70-85% of the measured HBM copy
                                 bandwidth on B200)                           */
 #define ASD_LLG_FUSED_STEP 1 /* one launch per step, the four stages
                                 streamed down the lattice through shared
