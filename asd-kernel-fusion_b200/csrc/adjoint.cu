@@ -85,78 +85,83 @@ __device__ __forceinline__ void block_add(double (&v)[NPAR], double *acc) {
     if (threadIdx.x < NPAR) acc[(long)blockIdx.x * NPAR + threadIdx.x] += red[threadIdx.x][0];
 }
 
-// P = S x nu and the local part of the vector-Jacobian product of f at stage
-// state S for the adjoint mu; the parameter derivatives are added to this
-// block's running slot bacc[blockIdx.x][6] (same sites every launch, so the
-// sum is deterministic).
-__global__ void __launch_bounds__(TPB) vjp_p_kernel(LLGArgs a, const double *__restrict__ S,
-                                                    const double *__restrict__ mu,
-                                                    double *__restrict__ P,
-                                                    double *__restrict__ loc,
-                                                    double *__restrict__ bacc) {
+// The vector-Jacobian product of f at stage state S for the adjoint m of one
+// (site, replica): P = S x nu (to be gathered by the neighbours), the local
+// part loc, and the parameter derivatives added to part[].
+__device__ __forceinline__ void vjp_local(const LLGArgs &a, const Site &s,
+                                          const double *__restrict__ S, const V3 &m, double *P,
+                                          double *loc, double (&part)[NPAR]) {
+    const V3 sv = vload(S + s.e);
+    V3 nn, nnn;
+    neighbour_sums(S, s, a.N, nn, nnn);
+    const V3 H = vadd(vadd(vmul(a.J1, nn), vmul(a.J2, nnn)), v3(a.hx, a.hy, a.hz));
+    const V3 tau = vcross(H, sv);
+    const V3 nu = vmul(a.g, vadd(m, vmul(a.alpha, vcross(m, sv))));
+    const V3 p = vcross(sv, nu);
+    const V3 l = vadd(vmul(a.g * a.alpha, vcross(tau, m)), vcross(nu, H));
+    vstore(P + s.e, p);
+    vstore(loc + s.e, l);
+    const V3 sxt = vcross(sv, tau);
+    const V3 f = vmul(a.g, vadd(tau, vmul(a.alpha, sxt)));
+    part[0] = vdot(p, nn);
+    part[1] = vdot(p, nnn);
+    part[2] = vdot(m, vadd(vmul(-2.0 * a.alpha * a.g, f), vmul(a.g, sxt)));
+    part[3] = p.x;
+    part[4] = p.y;
+    part[5] = p.z;
+}
+
+// Adjoint of the renormalisation, then the vector-Jacobian product at the
+// stage-4 state.  v = acc + k4/6 with k4 = dt f(s4) (the forward stage 4),
+// lam_v = (l/|v|)(lam - v^ (v^ . lam)), mu4 = dt lam_v / 6 (kept in
+// registers: only this element's vector-Jacobian product uses it).  The
+// parameter derivatives are added to this block's running slot
+// bacc[blockIdx.x][6]; the blocks cover the same sites in every launch, so
+// the sums are deterministic.
+template <bool J2, bool H, bool DAMP>
+__global__ void __launch_bounds__(TPB) adj_renorm_vjp_kernel(
+    LLGArgs a, const double *__restrict__ s4, const double *__restrict__ acc,
+    const double *__restrict__ lam, double *__restrict__ lam_v, double *__restrict__ P,
+    double *__restrict__ loc, double *__restrict__ bacc) {
     double part[NPAR] = {0, 0, 0, 0, 0, 0};
     Site s;
     if (site_of(a, s)) {
-        const V3 sv = vload(S + s.e), m = vload(mu + s.e);
-        V3 nn, nnn;
-        neighbour_sums(S, s, a.N, nn, nnn);
-        const V3 H = vadd(vadd(vmul(a.J1, nn), vmul(a.J2, nnn)), v3(a.hx, a.hy, a.hz));
-        const V3 tau = vcross(H, sv);
-        const V3 nu = vmul(a.g, vadd(m, vmul(a.alpha, vcross(m, sv))));
-        const V3 p = vcross(sv, nu);
-        const V3 l = vadd(vmul(a.g * a.alpha, vcross(tau, m)), vcross(nu, H));
-        vstore(P + s.e, p);
-        vstore(loc + s.e, l);
-        const V3 sxt = vcross(sv, tau);
-        const V3 f = vmul(a.g, vadd(tau, vmul(a.alpha, sxt)));
-        part[0] = vdot(p, nn);
-        part[1] = vdot(p, nnn);
-        part[2] = vdot(m, vadd(vmul(-2.0 * a.alpha * a.g, f), vmul(a.g, sxt)));
-        part[3] = p.x;
-        part[4] = p.y;
-        part[5] = p.z;
+        const V3 d = llg_rhs<J2, H, DAMP>(s4, s.sstride, s.off, a.N, s.row, s.col, a);
+        const V3 v = v3(da(acc[s.e], div6(dm(d.x, a.dt))), da(acc[s.e + 1], div6(dm(d.y, a.dt))),
+                        da(acc[s.e + 2], div6(dm(d.z, a.dt))));
+        const double r = sqrt(vdot(v, v));
+        const V3 vh = vmul(1.0 / r, v);
+        const V3 l = vload(lam + s.e);
+        const V3 lv = vmul(a.spin_len / r, vsub(l, vmul(vdot(vh, l), vh)));
+        vstore(lam_v + s.e, lv);
+        vjp_local(a, s, s4, vmul(a.dt / 6.0, lv), P, loc, part);
     }
     block_add(part, bacc);
 }
 
-// lam_s = loc + J1 sum_nn P + J2 sum_nnn P;  lam_y_out = lam_y_in + lam_s;
-// mu_out = dt (cv lam_v + cs lam_s) when has_next.  lam_y_in may equal
-// lam_y_out (each thread reads and writes its own element).
-__global__ void __launch_bounds__(TPB) vjp_gather_kernel(LLGArgs a, const double *__restrict__ P,
-                                                         const double *__restrict__ loc,
-                                                         const double *__restrict__ lam_v,
-                                                         const double *lam_y_in, double *lam_y_out,
-                                                         double *__restrict__ mu_out, double cv,
-                                                         double cs, int has_next) {
+// lam_s = loc + J1 sum_nn P_in + J2 sum_nnn P_in;  lam_y_out = lam_y_in +
+// lam_s.  With a next stage state S: mu = dt (cv lam_v + cs lam_s) and its
+// vector-Jacobian product at S, written to P_out (P_in is still being read by
+// the neighbours) and loc (read above by this thread only), derivatives to
+// bacc.  lam_y_in may equal lam_y_out (each thread reads and writes its own
+// element).
+__global__ void __launch_bounds__(TPB) vjp_gather_kernel(
+    LLGArgs a, const double *__restrict__ P_in, double *loc, const double *__restrict__ lam_v,
+    const double *lam_y_in, double *lam_y_out, double cv, double cs,
+    const double *__restrict__ S, double *__restrict__ P_out, double *__restrict__ bacc) {
+    double part[NPAR] = {0, 0, 0, 0, 0, 0};
     Site s;
-    if (!site_of(a, s)) return;
-    V3 nn, nnn;
-    neighbour_sums(P, s, a.N, nn, nnn);
-    const V3 lam_s = vadd(vload(loc + s.e), vadd(vmul(a.J1, nn), vmul(a.J2, nnn)));
-    vstore(lam_y_out + s.e, vadd(vload(lam_y_in + s.e), lam_s));
-    if (has_next)
-        vstore(mu_out + s.e, vmul(a.dt, vadd(vmul(cv, vload(lam_v + s.e)), vmul(cs, lam_s))));
-}
-
-// Adjoint of the renormalisation: v = acc + k4/6 with k4 = dt f(s4) (the
-// forward stage 4), lam_v = (l/|v|)(lam - v^ (v^ . lam)), mu4 = dt lam_v / 6.
-template <bool J2, bool H, bool DAMP>
-__global__ void __launch_bounds__(TPB) adj_renorm_kernel(LLGArgs a, const double *__restrict__ s4,
-                                                         const double *__restrict__ acc,
-                                                         const double *__restrict__ lam,
-                                                         double *__restrict__ lam_v,
-                                                         double *__restrict__ mu) {
-    Site s;
-    if (!site_of(a, s)) return;
-    const V3 d = llg_rhs<J2, H, DAMP>(s4, s.sstride, s.off, a.N, s.row, s.col, a);
-    const V3 v = v3(da(acc[s.e], div6(dm(d.x, a.dt))), da(acc[s.e + 1], div6(dm(d.y, a.dt))),
-                    da(acc[s.e + 2], div6(dm(d.z, a.dt))));
-    const double r = sqrt(vdot(v, v));
-    const V3 vh = vmul(1.0 / r, v);
-    const V3 l = vload(lam + s.e);
-    const V3 lv = vmul(a.spin_len / r, vsub(l, vmul(vdot(vh, l), vh)));
-    vstore(lam_v + s.e, lv);
-    vstore(mu + s.e, vmul(a.dt / 6.0, lv));
+    if (site_of(a, s)) {
+        V3 nn, nnn;
+        neighbour_sums(P_in, s, a.N, nn, nnn);
+        const V3 lam_s = vadd(vload(loc + s.e), vadd(vmul(a.J1, nn), vmul(a.J2, nnn)));
+        vstore(lam_y_out + s.e, vadd(vload(lam_y_in + s.e), lam_s));
+        if (S) {
+            const V3 m = vmul(a.dt, vadd(vmul(cv, vload(lam_v + s.e)), vmul(cs, lam_s)));
+            vjp_local(a, s, S, m, P_out, loc, part);
+        }
+    }
+    if (S) block_add(part, bacc);  // uniform over the grid
 }
 
 // Column sums over sites for each k: Fpart[chunk][k] = sum_i ph_i A[i][k].
@@ -273,28 +278,15 @@ __global__ void param_reduce_kernel(const double *__restrict__ bacc, int nblocks
 
 int adjoint_blocks(const LLGArgs &a) { return (int)((a.M * a.nfile + TPB - 1) / TPB); }
 
-cudaError_t launch_vjp_p(const LLGArgs &a, const double *S, const double *mu, double *P,
-                         double *loc, double *bacc, cudaStream_t st) {
-    vjp_p_kernel<<<adjoint_blocks(a), TPB, 0, st>>>(a, S, mu, P, loc, bacc);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_vjp_gather(const LLGArgs &a, const double *P, const double *loc,
-                              const double *lam_v, const double *lam_y_in, double *lam_y_out,
-                              double *mu_out, double cv, double cs, int has_next,
-                              cudaStream_t st) {
-    vjp_gather_kernel<<<adjoint_blocks(a), TPB, 0, st>>>(a, P, loc, lam_v, lam_y_in, lam_y_out,
-                                                         mu_out, cv, cs, has_next);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_adj_renorm(const LLGArgs &a, const double *s4, const double *acc,
-                              const double *lam, double *lam_v, double *mu, cudaStream_t st) {
+cudaError_t launch_adj_renorm_vjp(const LLGArgs &a, const double *s4, const double *acc,
+                                  const double *lam, double *lam_v, double *P, double *loc,
+                                  double *bacc, cudaStream_t st) {
     const int sel = (a.use_j2 ? 4 : 0) | (a.use_h ? 2 : 0) | (a.use_damp ? 1 : 0);
     const int nb = adjoint_blocks(a);
 #define ASD_ADJ_CASE(S, J, Hh, D)                                                          \
     case S:                                                                                \
-        adj_renorm_kernel<J, Hh, D><<<nb, TPB, 0, st>>>(a, s4, acc, lam, lam_v, mu);       \
+        adj_renorm_vjp_kernel<J, Hh, D><<<nb, TPB, 0, st>>>(a, s4, acc, lam, lam_v, P, loc, \
+                                                            bacc);                         \
         break;
     switch (sel) {
         ASD_ADJ_CASE(0, false, false, false)
@@ -307,6 +299,15 @@ cudaError_t launch_adj_renorm(const LLGArgs &a, const double *s4, const double *
         ASD_ADJ_CASE(7, true, true, true)
     }
 #undef ASD_ADJ_CASE
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vjp_gather(const LLGArgs &a, const double *P_in, double *loc,
+                              const double *lam_v, const double *lam_y_in, double *lam_y_out,
+                              double cv, double cs, const double *S, double *P_out, double *bacc,
+                              cudaStream_t st) {
+    vjp_gather_kernel<<<adjoint_blocks(a), TPB, 0, st>>>(a, P_in, loc, lam_v, lam_y_in, lam_y_out,
+                                                         cv, cs, S, P_out, bacc);
     return cudaGetLastError();
 }
 

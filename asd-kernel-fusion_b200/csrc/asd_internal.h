@@ -147,14 +147,18 @@ cudaError_t launch_finalize(const double2 *part, int nparts, double scale, doubl
 
 // ------------------------------------------------ adjoint (adjoint.cu)
 int adjoint_blocks(const LLGArgs &a);
-cudaError_t launch_vjp_p(const LLGArgs &a, const double *S, const double *mu, double *P,
-                         double *loc, double *bacc, cudaStream_t st);
-cudaError_t launch_vjp_gather(const LLGArgs &a, const double *P, const double *loc,
+// Adjoint of the renormalisation, then the vector-Jacobian product at s4
+// (P, loc, parameter derivatives into bacc).
+cudaError_t launch_adj_renorm_vjp(const LLGArgs &a, const double *s4, const double *acc,
+                                  const double *lam, double *lam_v, double *P, double *loc,
+                                  double *bacc, cudaStream_t st);
+// Gather of P_in into lam_y_out = lam_y_in + lam_s; with S != NULL, the
+// vector-Jacobian product at S for mu = dt (cv lam_v + cs lam_s) into P_out
+// (a buffer other than P_in) and loc.
+cudaError_t launch_vjp_gather(const LLGArgs &a, const double *P_in, double *loc,
                               const double *lam_v, const double *lam_y_in, double *lam_y_out,
-                              double *mu_out, double cv, double cs, int has_next,
+                              double cv, double cs, const double *S, double *P_out, double *bacc,
                               cudaStream_t st);
-cudaError_t launch_adj_renorm(const LLGArgs &a, const double *s4, const double *acc,
-                              const double *lam, double *lam_v, double *mu, cudaStream_t st);
 int fsum_chunks(long M);
 cudaError_t launch_fsum(const double *A, long M, int K, const double2 *ph, double2 *Fpart,
                         cudaStream_t st);

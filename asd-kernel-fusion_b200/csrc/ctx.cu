@@ -527,7 +527,7 @@ int ensure_adjoint(asd_ctx *c, int nsteps, int stride, int ckpt) {
 
 // The adjoint's buffers by role.
 struct AdjBufs {
-    double *s2, *s3, *s4, *acc, *lam, *lam_v, *lam_y, *mu, *P, *loc;
+    double *s2, *s3, *s4, *acc, *lam, *lam_v, *lam_y, *P2, *P, *loc;
     double **ck, **seg;
     double *bacc, *dgrad;
     double2 *Fpart, *G, *Z, *Sv;
@@ -538,7 +538,7 @@ AdjBufs adj_bufs(asd_ctx *c, int nck) {
     double **B = c->adj_bufs.data();
     AdjBufs b;
     b.s2 = B[0], b.s3 = B[1], b.s4 = B[2], b.acc = B[3], b.lam = B[4], b.lam_v = B[5];
-    b.lam_y = B[6], b.mu = B[7], b.P = B[8], b.loc = B[9];
+    b.lam_y = B[6], b.P2 = B[7], b.P = B[8], b.loc = B[9];
     b.ck = B + 10;        // nck checkpoints
     b.seg = B + 10 + nck; // ckpt + 1 recomputed states
     b.nb = adjoint_blocks(c->a);
@@ -675,17 +675,20 @@ int loss_backward(asd_ctx *c, const double *target, double *grad, double *dtarge
             }
             // y_{n-1} = seg[j-1]: recompute the stage states, then the adjoint
             if ((rc = step_into(c, seg[j - 1], b.s2, b.s3, b.s4, b.acc, nullptr)) != ASD_OK) return rc;
+            // stage 4 (through the renormalisation), 3, 2, 1: each launch
+            // gathers the previous stage's P and forms the next stage's
+            // product, so P alternates between two buffers
             const LLGArgs &a = c->a;
-            ASD_CUDA_TRY(launch_adj_renorm(a, b.s4, b.acc, b.lam, b.lam_v, b.mu, st));
-            ASD_CUDA_TRY(launch_vjp_p(a, b.s4, b.mu, b.P, b.loc, b.bacc, st));
-            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_v, b.lam_y, b.mu, 1.0 / 3.0, 1.0, 1, st));
-            ASD_CUDA_TRY(launch_vjp_p(a, b.s3, b.mu, b.P, b.loc, b.bacc, st));
-            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_y, b.lam_y, b.mu, 1.0 / 3.0, 0.5, 1, st));
-            ASD_CUDA_TRY(launch_vjp_p(a, b.s2, b.mu, b.P, b.loc, b.bacc, st));
-            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_y, b.lam_y, b.mu, 1.0 / 6.0, 0.5, 1, st));
-            ASD_CUDA_TRY(launch_vjp_p(a, seg[j - 1], b.mu, b.P, b.loc, b.bacc, st));
-            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_y, b.lam, b.mu, 0.0, 0.0, 0, st));
-            c->last_launches += 4 + 9;
+            ASD_CUDA_TRY(launch_adj_renorm_vjp(a, b.s4, b.acc, b.lam, b.lam_v, b.P, b.loc, b.bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_v, b.lam_y, 1.0 / 3.0, 1.0,
+                                           b.s3, b.P2, b.bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, b.P2, b.loc, b.lam_v, b.lam_y, b.lam_y, 1.0 / 3.0, 0.5,
+                                           b.s2, b.P, b.bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_y, b.lam_y, 1.0 / 6.0, 0.5,
+                                           seg[j - 1], b.P2, b.bacc, st));
+            ASD_CUDA_TRY(launch_vjp_gather(a, b.P2, b.loc, b.lam_v, b.lam_y, b.lam, 0.0, 0.0, nullptr,
+                                           nullptr, b.bacc, st));
+            c->last_launches += 4 + 5;
         }
     }
     ASD_CUDA_TRY(launch_param_reduce(b.bacc, b.nb, b.dgrad, st));
