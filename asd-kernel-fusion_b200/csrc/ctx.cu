@@ -88,9 +88,11 @@ struct asd_ctx {
     // adjoint work space (allocated on the first asd_ctx_loss_grad)
     std::vector<double *> adj_bufs;
     long adj_states = 0;
+    bool adj_keep = false;  // the work space holds every stage state of a segment
     // the tape of the last loss forward pass: its S(q,t) values and sizes,
     // valid while the parameters and the origin stay those it ran with
     bool tape_valid = false;
+    bool tape_keep = false;  // the backward pass keeps a segment's stage states
     int tape_nsteps = 0, tape_stride = 0, tape_ckpt = 0;
     long tape_params = -1, tape_origin = -1;
     std::vector<double2> tape_S;
@@ -491,12 +493,32 @@ int step_into(asd_ctx *c, const double *y_in, double *s2, double *s3, double *s4
 
 // Work space of the adjoint: state-sized buffers (stage states, adjoint
 // variables, checkpoints, one recomputed segment) and small reduction buffers.
+// Where the RK4 step runs as four stage kernels and half of the free device
+// memory holds them, also the stage states (s2, s3, s4, acc) of every step of
+// a segment, so that the backward pass reads them instead of recomputing
+// each step's stages a second time (c->adj_keep).
 int ensure_adjoint(asd_ctx *c, int nsteps, int stride, int ckpt) {
     const long M = c->M;
     const int K = c->K, E = nsteps / stride;
     const size_t sb = (size_t)M * K * sizeof(double);
     const int nck = (nsteps + ckpt - 1) / ckpt;  // checkpoints at 0, ckpt, 2 ckpt, ...
-    const long need = 10 + nck + (ckpt + 1);
+    long need = 10 + nck + (ckpt + 1);
+    const long need_keep = need + 4L * ckpt;
+    bool keep = false;
+    if (!use_fused(c, c->a)) {
+        size_t free_b = 0, total_b = 0;
+        if (c->adj_states >= need_keep) {
+            keep = true;
+        } else if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            // the buffers held now are freed before the new set is allocated
+            const double avail = (double)free_b + (double)c->adj_states * (double)sb;
+            keep = (double)need_keep * (double)sb <= 0.5 * avail;
+        } else {
+            cudaGetLastError();
+        }
+    }
+    if (keep) need = need_keep;
+    c->adj_keep = keep;
     int rc;
     if (c->adj_states < need) {
         c->tape_valid = false;
@@ -529,18 +551,20 @@ int ensure_adjoint(asd_ctx *c, int nsteps, int stride, int ckpt) {
 struct AdjBufs {
     double *s2, *s3, *s4, *acc, *lam, *lam_v, *lam_y, *P2, *P, *loc;
     double **ck, **seg;
+    double **stg;  // with a kept segment: stg[4 (j - 1) + q] = s2, s3, s4, acc of step j
     double *bacc, *dgrad;
     double2 *Fpart, *G, *Z, *Sv;
     int nb;
 };
 
-AdjBufs adj_bufs(asd_ctx *c, int nck) {
+AdjBufs adj_bufs(asd_ctx *c, int nck, int ckpt) {
     double **B = c->adj_bufs.data();
     AdjBufs b;
     b.s2 = B[0], b.s3 = B[1], b.s4 = B[2], b.acc = B[3], b.lam = B[4], b.lam_v = B[5];
     b.lam_y = B[6], b.P2 = B[7], b.P = B[8], b.loc = B[9];
     b.ck = B + 10;        // nck checkpoints
     b.seg = B + 10 + nck; // ckpt + 1 recomputed states
+    b.stg = b.seg + ckpt + 1;
     b.nb = adjoint_blocks(c->a);
     b.bacc = B[c->adj_states];
     b.Fpart = reinterpret_cast<double2 *>(b.bacc + (size_t)b.nb * 6);
@@ -566,7 +590,7 @@ int loss_forward(asd_ctx *c, int nsteps, int stride, int ckpt, const double *tar
     const int K = c->K, E = nsteps / stride;
     const size_t sb = (size_t)M * K * sizeof(double);
     const int nck = (nsteps + ckpt - 1) / ckpt;
-    AdjBufs b = adj_bufs(c, nck);
+    AdjBufs b = adj_bufs(c, nck, ckpt);
     cudaStream_t st = c->stream;
     c->last_launches = 0;
     c->tape_valid = false;
@@ -616,6 +640,7 @@ int loss_forward(asd_ctx *c, int nsteps, int stride, int ckpt, const double *tar
     }
     if (loss) *loss = L;
     c->tape_valid = true;
+    c->tape_keep = c->adj_keep;
     c->tape_nsteps = nsteps;
     c->tape_stride = stride;
     c->tape_ckpt = ckpt;
@@ -637,7 +662,7 @@ int loss_backward(asd_ctx *c, const double *target, double *grad, double *dtarge
     const int E = nsteps / stride;
     const size_t sb = (size_t)M * K * sizeof(double);
     const int nck = (nsteps + ckpt - 1) / ckpt;
-    AdjBufs b = adj_bufs(c, nck);
+    AdjBufs b = adj_bufs(c, nck, ckpt);
     cudaStream_t st = c->stream;
     int rc;
     c->last_launches = 0;
@@ -653,6 +678,7 @@ int loss_backward(asd_ctx *c, const double *target, double *grad, double *dtarge
     }
     if (!grad) return ASD_OK;
     const bool fwd_fused = use_fused(c, c->a);
+    const bool keep = c->tape_keep && !fwd_fused;
     // backward through the segments, last first
     ASD_CUDA_TRY(cudaMemsetAsync(b.lam, 0, sb, st));
     ASD_CUDA_TRY(cudaMemsetAsync(b.bacc, 0, (size_t)b.nb * 6 * sizeof(double), st));
@@ -662,8 +688,11 @@ int loss_backward(asd_ctx *c, const double *target, double *grad, double *dtarge
         const int len = (nsteps - base < ckpt) ? nsteps - base : ckpt;
         ASD_CUDA_TRY(cudaMemcpyAsync(seg[0], b.ck[cidx], sb, cudaMemcpyDeviceToDevice, st));
         for (int j = 1; j <= len; ++j) {
+            double **sj = keep ? b.stg + 4 * (j - 1) : nullptr;
             if (fwd_fused) ASD_CUDA_TRY(launch_llg_step_fused(c->a, seg[j - 1], seg[j], st));
-            else if ((rc = step_into(c, seg[j - 1], b.s2, b.s3, b.s4, b.acc, seg[j])) != ASD_OK) return rc;
+            else if ((rc = keep ? step_into(c, seg[j - 1], sj[0], sj[1], sj[2], sj[3], seg[j])
+                                : step_into(c, seg[j - 1], b.s2, b.s3, b.s4, b.acc, seg[j])) != ASD_OK)
+                return rc;
             c->last_launches += fwd_fused ? 1 : 4;
         }
         for (int n = base + len; n > base; --n) {
@@ -673,22 +702,30 @@ int loss_backward(asd_ctx *c, const double *target, double *grad, double *dtarge
                 ASD_CUDA_TRY(launch_loss_grad(b.lam, M, K, c->uphase, b.G, b.Z, cf.x, cf.y, st));
                 c->last_launches += 1;
             }
-            // y_{n-1} = seg[j-1]: recompute the stage states, then the adjoint
-            if ((rc = step_into(c, seg[j - 1], b.s2, b.s3, b.s4, b.acc, nullptr)) != ASD_OK) return rc;
+            // y_{n-1} = seg[j-1]: its stage states (kept from the segment's
+            // forward pass, or recomputed), then the adjoint
+            double *s2 = b.s2, *s3 = b.s3, *s4 = b.s4, *acc = b.acc;
+            if (keep) {
+                double **sj = b.stg + 4 * (j - 1);
+                s2 = sj[0], s3 = sj[1], s4 = sj[2], acc = sj[3];
+            } else {
+                if ((rc = step_into(c, seg[j - 1], s2, s3, s4, acc, nullptr)) != ASD_OK) return rc;
+                c->last_launches += 4;
+            }
             // stage 4 (through the renormalisation), 3, 2, 1: each launch
             // gathers the previous stage's P and forms the next stage's
             // product, so P alternates between two buffers
             const LLGArgs &a = c->a;
-            ASD_CUDA_TRY(launch_adj_renorm_vjp(a, b.s4, b.acc, b.lam, b.lam_v, b.P, b.loc, b.bacc, st));
+            ASD_CUDA_TRY(launch_adj_renorm_vjp(a, s4, acc, b.lam, b.lam_v, b.P, b.loc, b.bacc, st));
             ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_v, b.lam_y, 1.0 / 3.0, 1.0,
-                                           b.s3, b.P2, b.bacc, st));
+                                           s3, b.P2, b.bacc, st));
             ASD_CUDA_TRY(launch_vjp_gather(a, b.P2, b.loc, b.lam_v, b.lam_y, b.lam_y, 1.0 / 3.0, 0.5,
-                                           b.s2, b.P, b.bacc, st));
+                                           s2, b.P, b.bacc, st));
             ASD_CUDA_TRY(launch_vjp_gather(a, b.P, b.loc, b.lam_v, b.lam_y, b.lam_y, 1.0 / 6.0, 0.5,
                                            seg[j - 1], b.P2, b.bacc, st));
             ASD_CUDA_TRY(launch_vjp_gather(a, b.P2, b.loc, b.lam_v, b.lam_y, b.lam, 0.0, 0.0, nullptr,
                                            nullptr, b.bacc, st));
-            c->last_launches += 4 + 5;
+            c->last_launches += 5;
         }
     }
     ASD_CUDA_TRY(launch_param_reduce(b.bacc, b.nb, b.dgrad, st));

@@ -201,7 +201,9 @@ def test_forward_pays_no_adjoint_and_backward_matches():
         # two per S(q,t) evaluation, plus the origin's sums: no adjoint
         assert fwd_launches <= 4 * nsteps + 2 * E + 2
         grad, dtarget = ctx.loss_backward(target)
-        assert ctx.last_launches() > 13 * nsteps  # the adjoint's launches come here
+        # the adjoint's launches come here: per step at least the segment's
+        # recomputed forward step (4 stage kernels) and 5 adjoint launches
+        assert ctx.last_launches() >= 9 * nsteps
         np.testing.assert_array_equal(grad, grad_ref)
         np.testing.assert_allclose(dtarget, -2.0 * (S - target) / E, rtol=1e-15, atol=0)
         grad2, _ = ctx.loss_backward(target)  # the tape stays until the next forward pass

@@ -112,8 +112,8 @@ def test_failed_work_space_allocation_leaves_the_context_usable(call):
     With the 1st, 2nd, ... of those allocations failing, the call returns
     ASD_ERR_NOMEM each time, until it makes fewer allocations than the
     injection counts and succeeds; then, with the spins set again, it gives
-    what a context that never failed gives, bit for bit (the q grid within
-    the run-to-run variation of its atomic bin sums)."""
+    what a context that never failed gives, bit for bit (the q grid
+    included: its sums run in a fixed order)."""
     import torch
 
     N, nf = 16, 72
