@@ -1,0 +1,74 @@
+"""bench.py's output contract, on the CPU: the reference arm (the reference's
+own programs on the host cores) prints one JSON line with the keys the
+driver reads and the same `config` as the GPU arm; ranks other than 0 exit
+without work; the whole-job aggregation takes the slowest rank."""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import types
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _bench():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    return bench
+
+
+def _run(*extra, env=None):
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference", *extra]
+    e = dict(os.environ, **(env or {}))
+    p = subprocess.run(cmd, cwd=ROOT, env=e, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-3000:]
+    return [json.loads(l) for l in p.stdout.splitlines() if l.startswith("{")]
+
+
+def test_reference_arm_line():
+    lines = _run("--steps", "1", "--warmup", "0", "--ref-target-s", "0.02")
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference"
+    if "unavailable" in d:  # the reference was not compiled in this checkout
+        assert isinstance(d["unavailable"], str) and d["unavailable"]
+        pytest.skip(d["unavailable"])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["unit"] == "site-steps/s" and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["ms_per_step"] > 0
+    assert d["steps"] == 1 and d["warmup"] == 0 and d["n_gpus"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
+    assert cb["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": "site-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+    # the same workload description as the GPU arm, key for key
+    bench = _bench()
+    args = types.SimpleNamespace(mode=None, llg_kernel="auto", chunk_k=-1)
+    assert d["config"] == bench.bench_config("sqt256", args)
+    # the fused program's S(q,t) is invalid at K = 3000 > 240: timed, labelled
+    fused = d["paths"]["fused_avx2"]
+    assert fused["value_valid"] is False and fused["value"] > 0
+
+
+def test_reference_arm_other_ranks_do_no_work():
+    lines = _run("--steps", "1", "--warmup", "0",
+                 env={"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
+    assert lines == []
+
+
+def test_aggregate_takes_the_slowest_rank():
+    bench = _bench()
+    ms, value = bench.aggregate(50.0, 1e6, 1)
+    assert ms == 50.0 and value == pytest.approx(2e7)
+    # weak scaling: every rank did units_per_rank in its own time
+    ms, value = bench.aggregate(50.0, 1e6, 4)
+    assert value == pytest.approx(8e7)
