@@ -153,7 +153,13 @@ int asd_ctx_sqt_grid(asd_ctx *ctx, asd_sqt_mode mode, double *out);
  * adjoint of the RK4 step and of the renormalisation, with checkpoints every
  * `checkpoint` steps and recomputation of each segment.  sqt_out (2E
  * doubles) receives the S(q,t_e) values.  Host buffers; synchronous.  The
- * current state is not changed.  No counterpart in the reference. */
+ * current state is not changed.  Device work space, allocated on the first
+ * call and kept by the context: about (nsteps / checkpoint + checkpoint + 13)
+ * spin-state arrays; where the RK4 step runs as four stage kernels (small
+ * lattices) and half of the free device memory holds them, 4 * checkpoint
+ * more, so that the backward pass reads each segment's stage states instead
+ * of recomputing them (the results are the same bits either way).  No
+ * counterpart in the reference. */
 int asd_ctx_loss_grad(asd_ctx *ctx, int nsteps, int stride, int checkpoint, const double *target,
                       double *loss, double *grad, double *sqt_out);
 /* asd_ctx_loss_grad in two calls, so that a caller that does not need the
