@@ -311,24 +311,37 @@ cudaError_t launch_vjp_gather(const LLGArgs &a, const double *P_in, double *loc,
     return cudaGetLastError();
 }
 
-int fsum_chunks(long M) { return (int)((M + 255) / 256); }
+// Rows per chunk of the site sums: 256, halved (down to 16) until the grid
+// of (K / 128) x chunks has at least four blocks per SM of a B200, so that
+// small lattices (64 x 64 x 100: 48 blocks of 256 rows) still fill the GPU;
+// doubled where the chunks would exceed the grid's y extent (N = 4096).
+int fsum_rows(long M, int K) {
+    constexpr long kMinBlocks = 4 * 148;
+    const long kb = (K + 127) / 128;
+    int rows = 256;
+    while (rows > 16 && kb * ((M + rows - 1) / rows) < kMinBlocks) rows >>= 1;
+    while ((M + rows - 1) / rows > 65535) rows <<= 1;  // the grid's y extent
+    return rows;
+}
+
+int fsum_chunks(long M, int K) { return (int)((M + fsum_rows(M, K) - 1) / fsum_rows(M, K)); }
 
 cudaError_t launch_fsum(const double *A, long M, int K, const double2 *ph, double2 *Fpart,
                         cudaStream_t st) {
-    dim3 grid((unsigned)((K + 127) / 128), (unsigned)fsum_chunks(M));
-    fsum_kernel<<<grid, 128, 0, st>>>(A, M, K, ph, 256, Fpart);
+    dim3 grid((unsigned)((K + 127) / 128), (unsigned)fsum_chunks(M, K));
+    fsum_kernel<<<grid, 128, 0, st>>>(A, M, K, ph, fsum_rows(M, K), Fpart);
     return cudaGetLastError();
 }
 
 cudaError_t launch_gz(const double2 *Fpart, long M, int K, int nfile, double2 *G, double2 *Z,
                       cudaStream_t st) {
-    gz_kernel<<<1, 256, 0, st>>>(Fpart, fsum_chunks(M), K, nfile, G, Z);
+    gz_kernel<<<1, 256, 0, st>>>(Fpart, fsum_chunks(M, K), K, nfile, G, Z);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sqt_value(const double2 *Fpart, long M, int K, int nfile, const double2 *G,
                              const double2 *Z, double2 *out, cudaStream_t st) {
-    sqt_value_kernel<<<1, 256, 0, st>>>(Fpart, fsum_chunks(M), K, nfile, M, G, Z, out);
+    sqt_value_kernel<<<1, 256, 0, st>>>(Fpart, fsum_chunks(M, K), K, nfile, M, G, Z, out);
     return cudaGetLastError();
 }
 

@@ -159,7 +159,8 @@ cudaError_t launch_vjp_gather(const LLGArgs &a, const double *P_in, double *loc,
                               const double *lam_v, const double *lam_y_in, double *lam_y_out,
                               double cv, double cs, const double *S, double *P_out, double *bacc,
                               cudaStream_t st);
-int fsum_chunks(long M);
+int fsum_rows(long M, int K);
+int fsum_chunks(long M, int K);
 cudaError_t launch_fsum(const double *A, long M, int K, const double2 *ph, double2 *Fpart,
                         cudaStream_t st);
 cudaError_t launch_gz(const double2 *Fpart, long M, int K, int nfile, double2 *G, double2 *Z,

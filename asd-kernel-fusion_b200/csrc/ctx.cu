@@ -530,7 +530,7 @@ int ensure_adjoint(asd_ctx *c, int nsteps, int stride, int ckpt) {
             if ((rc = dalloc(&c->adj_bufs[i], sb)) != ASD_OK) return rc;
         const int nb = adjoint_blocks(c->a);
         const size_t small = (size_t)nb * 6 * sizeof(double) +
-                             ((size_t)fsum_chunks(M) * K + 2 * K + 8 + 2) * sizeof(double2);
+                             ((size_t)fsum_chunks(M, K) * K + 2 * K + 8 + 2) * sizeof(double2);
         if ((rc = dalloc(&c->adj_bufs[need], small)) != ASD_OK) return rc;
         if ((rc = dalloc(&c->adj_bufs[need + 1], (size_t)(E + 8) * sizeof(double2))) != ASD_OK)
             return rc;
@@ -568,7 +568,7 @@ AdjBufs adj_bufs(asd_ctx *c, int nck, int ckpt) {
     b.nb = adjoint_blocks(c->a);
     b.bacc = B[c->adj_states];
     b.Fpart = reinterpret_cast<double2 *>(b.bacc + (size_t)b.nb * 6);
-    b.G = b.Fpart + (size_t)fsum_chunks(c->M) * c->K;
+    b.G = b.Fpart + (size_t)fsum_chunks(c->M, c->K) * c->K;
     b.Z = b.G + c->K;
     b.dgrad = reinterpret_cast<double *>(b.Z + 4);
     b.Sv = reinterpret_cast<double2 *>(B[c->adj_states + 1]);
