@@ -1472,6 +1472,7 @@ int asd_ctx_sqt_magnitude(asd_ctx *c, double *out) {
                                   c->stream));
     c->rows_ready = true;
     const long tiles = dmma_sqt_tiles(c->M);
+    if (tiles > 0x7fffffffL) return fail(ASD_ERR_UNSUPPORTED, "lattice too large for the FP64 GEMM");
     int rc = ensure_part(c, tiles);
     if (rc != ASD_OK) return rc;
     DmmaSqtArgs g = dmma_args(c, false);

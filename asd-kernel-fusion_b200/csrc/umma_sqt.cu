@@ -82,15 +82,17 @@ constexpr int smem_bytes() {
 // Tile raster: groups of group_m row tiles, each walked over all column tiles
 // with the row index fastest, so the concurrent tiles share a few B bands and
 // the group's A bands stay in L2 while B streams past once per group.
-__device__ __forceinline__ void tile_coords(int tile, int num_m, int num_n, int group_m, int &mb,
+// The tile index is 64-bit: above N = 2896 (M = N^2 sites) there are more
+// than 2^31 tiles of 128 x 256.
+__device__ __forceinline__ void tile_coords(long tile, int num_m, int num_n, int group_m, int &mb,
                                             int &nb) {
-    const int per_group = group_m * num_n;
-    const int group = tile / per_group;
+    const long per_group = (long)group_m * num_n;
+    const int group = (int)(tile / per_group);
     const int first_m = group * group_m;
     const int gsz = min(group_m, num_m - first_m);
-    const int r = tile - group * per_group;
-    mb = first_m + r % gsz;
-    nb = r / gsz;
+    const long r = tile - group * per_group;
+    mb = first_m + (int)(r % gsz);
+    nb = (int)(r / gsz);
 }
 
 __device__ __forceinline__ void raise_abort(SmemTail *t, unsigned *status) {
@@ -204,7 +206,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     uint8_t *gscr = smem + G::PIPE_BYTES + G::TABLE_BYTES + ((sizeof(SmemTail) + 15) & ~size_t(15));
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
-    const int num_tiles = num_m * num_n;
+    const long num_tiles = (long)num_m * num_n;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < G::STAGES; ++s) {
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             bool issued[G::STAGES] = {};
             uint32_t issued_parity[G::STAGES] = {};
             bool ok = true;
-            for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+            for (long tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
                 int mb, nb;
                 tile_coords(tile, num_m, num_n, group_m, mb, nb);
                 const int arow = mb * BM;
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             uint32_t aphase = 0;
             bool ok = true;
             const uint32_t smem_base = ptx::smem_u32(smem);
-            for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+            for (long tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
                 // K is accumulated in chunks of kb_per_chunk k blocks, each
                 // into a fresh TMEM buffer: the tensor core's FP32
                 // accumulation loses precision with the number of
@@ -370,7 +372,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         uint32_t ephase = 0;
         float *xpose = reinterpret_cast<float *>(gscr) + quarter * 32 * 32;  // [32][32]
         double *wdiag = reinterpret_cast<double *>(gscr);                       // [4][9][32][2]
-        for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++tcount) {
+        for (long tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++tcount) {
             int mb, nb;
             tile_coords(tile, num_m, num_n, group_m, mb, nb);
             const long i = (long)mb * BM + rloc;
@@ -616,7 +618,7 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
         return fail(ASD_ERR_INVALID, "K range [%d, %d) is not whole k blocks of %d in [0, %d)",
                     a.k_begin, k_end, ke, a.Kp);
     const int kb_begin = a.k_begin / ke, kb_end = k_end / ke;
-    const int tiles = num_m * num_n;
+    const long tiles = (long)num_m * num_n;
     // k blocks per accumulation chunk: chunk_k elements of K (0 = all of K)
     int kpc = a.chunk_k > 0 ? (a.chunk_k + ke - 1) / ke : num_kb;
     if (kpc < 1) kpc = 1;
@@ -624,7 +626,7 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     // One persistent CTA per SM (or per tile, if fewer); every CTA strides
     // over the tiles, so any grid size is correct and a caller's cap (the
     // partials it has room for) only lengthens each CTA's tile list.
-    int grid = tiles < a.num_sms ? tiles : a.num_sms;
+    int grid = tiles < a.num_sms ? (int)tiles : a.num_sms;
     if (a.max_grid > 0 && grid > a.max_grid) grid = a.max_grid;
     if (grid < 1) return fail(ASD_ERR_INVALID, "no tiles to launch");
     const int epi = a.dbg_c ? EPI_STORE : (a.tdiag ? EPI_GRID : EPI_PHASE);

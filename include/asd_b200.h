@@ -56,7 +56,9 @@ extern "C" {
 /* Arithmetic of the S(q,t) correlation GEMM. */
 typedef enum {
     ASD_SQT_FP64 = 0,   /* the plain path: FP64 tensor-core GEMM (mma.sync .f64) with
-                           the phase, connected-part and reduction epilogue fused */
+                           the phase, connected-part and reduction epilogue fused;
+                           one block per 128 x 128 tile, so up to N = 2435
+                           (ASD_ERR_UNSUPPORTED beyond) */
     ASD_SQT_TF32X3 = 1, /* tcgen05 kind::tf32, hi*hi + hi*lo + lo*hi, FP32 accumulate   */
     ASD_SQT_BF16X3 = 2  /* tcgen05 kind::f16 (bf16), hi*hi + hi*lo + lo*hi, FP32 accum. */
 } asd_sqt_mode;

@@ -92,3 +92,29 @@ def test_sqt_fp64_against_oracle_and_split_modes_within_tolerance(case, oracle):
     for m in modes:
         if m != "fp64":
             assert abs(got[m] - got["fp64"]) <= 1e-5 * abs(got["fp64"]), m
+
+
+def test_more_tiles_than_a_32_bit_index(oracle):
+    """N = 2900 (8.41 M sites): the split GEMM walks (M/128) x (M/256) =
+    2.16e9 tiles, more than a 32-bit index holds.  Two replicas keep it to a
+    few seconds.  One RK4 step bit for bit against the oracle; BF16x3 S(q,t)
+    against the oracle's factorised FP64 value (1e-5 of |S| plus 4 times the
+    operands' precision floor 2^-17 sqrt(K) / (3 nfile)); the FP64 path, one
+    block per 128 x 128 tile (4.3e9 blocks), refuses with ASD_ERR_UNSUPPORTED.
+    About 90 s on a B200: K = 6 pads to one k block of 64, so the GEMM is
+    bound by streaming its operands, not by the tensor cores."""
+    N, nf = 2900, 2
+    kw = dict(J1=1.0, alpha=0.05, h=(0.0, 0.0, 0.3), dt=0.01)
+    s0 = asd.random_spins(N, nf, seed=29)
+    with asd.Context(asd.Params.make(N, nf, **kw), modes=["fp64", "bf16x3"]) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        ctx.step(1)
+        st = ctx.get_spins()
+        assert np.array_equal(st, oracle.steps(orc.make_params(N, nf, **kw), s0, 1))
+        got = ctx.sqt("bf16x3")
+        with pytest.raises(asd.AsdError) as e:
+            ctx.sqt("fp64")
+        assert e.value.code == asd.ASD_ERR_UNSUPPORTED
+    want = oracle.sqt_factorized(N, nf, N // 10, N // 10, st, s0)
+    floor = 2.0 ** -17 * (3 * nf) ** 0.5 / (3 * nf)
+    assert abs(got - want) <= 1e-5 * abs(want) + 4 * floor, (got, want)
