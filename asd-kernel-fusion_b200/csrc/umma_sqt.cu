@@ -112,21 +112,62 @@ __device__ __forceinline__ bool epilogue_sync(uint64_t *bar, uint32_t &phase,
     return ok;
 }
 
+// q grid: bits l = 0..31 of the rows 32 q + l whose lattice column
+// x(l) = (x0 + l) mod N lies below thr, i.e. the rows in class 1 of a
+// diagonal whose column displacement is thr.  For N >= 32 the 32 rows wrap
+// at most once (at l = N - x0), so the set is at most two runs of bits.
+__device__ __forceinline__ uint32_t grid_below_mask(int x0, int thr, int N) {
+    auto low = [](int k) -> uint32_t {
+        return k >= 32 ? 0xffffffffu : (k <= 0 ? 0u : (1u << k) - 1u);
+    };
+    if (N >= 32) {
+        const int nw = min(32, N - x0);  // rows before the wrap: x = x0 + l
+        return low(min(nw, thr - x0)) | (low(thr + N - x0) & ~low(nw));
+    }
+    uint32_t m = 0;
+    int x = x0;
+    for (int l = 0; l < 32; ++l) {
+        if (x < thr) m |= 1u << l;
+        if (++x == N) x = 0;
+    }
+    return m;
+}
+
+// val added to exactly one of the four sums, chosen by (b, c): predicated
+// adds, so no lane branches and each sum sees its values in step order.
+__device__ __forceinline__ void grid_add4(float &pa0, float &pa1, float &pb0, float &pb1,
+                                          float val, uint32_t b, uint32_t c) {
+    asm("{\n\t.reg .pred pb, q0, q1, q2, q3;\n\t"
+        "setp.ne.u32 pb, %5, 0;\n\t"
+        "setp.eq.and.u32 q0, %6, 0, !pb;\n\t"
+        "setp.ne.and.u32 q1, %6, 0, !pb;\n\t"
+        "setp.eq.and.u32 q2, %6, 0, pb;\n\t"
+        "setp.ne.and.u32 q3, %6, 0, pb;\n\t"
+        "@q0 add.rn.f32 %0, %0, %4;\n\t"
+        "@q1 add.rn.f32 %1, %1, %4;\n\t"
+        "@q2 add.rn.f32 %2, %2, %4;\n\t"
+        "@q3 add.rn.f32 %3, %3, %4;\n\t}"
+        : "+f"(pa0), "+f"(pa1), "+f"(pb0), "+f"(pb1)
+        : "f"(val), "r"(b), "r"(c));
+}
+
 // q grid: one 32 x 32 block (column group c) of a warp's accumulator rows.
 // Lane l holds v[jj] = acc(row 32 q + l, column 32 c + jj).  The block's
 // diagonals are lambda = l - jj in [-31, 31]; lane L owns lambda = L (tile
 // diagonal 32 (q - c) + L, register gd[8 - c]) and lambda = L - 32 (tile
 // diagonal 32 (q - c - 1) + L, gd[7 - c]).  Lane l writes v[jj] to row
 // (l - jj) mod 32, column l of the warp's buffer; lane L then reads its row,
-// from column L onwards (conflict-free both ways), and adds each value to
-// its diagonal and class.  a_first is (i - j) mod N on lambda = L of block 0;
-// the column displacement a of a diagonal decides the class of an element of
-// row x (its lattice column): class 0 iff x >= a.
+// from column L onwards (conflict-free both ways): step s reads column
+// l = (L + s) mod 32, which is on lambda = L - 32 iff s >= 32 - L.  The class
+// of a step (class 0 iff the row's lattice column x >= a, a = (i - j) mod N
+// of the diagonal) comes from two 32-bit masks formed once per block, so a
+// step is a shared load and one predicated add to one of four sums.
 __device__ __forceinline__ void grid_block(const uint32_t (&v)[32], int c, int lane,
                                            const float4 &r4, const float4 *z_tab, float alpha,
                                            bool last, int x_row, int a_first, int N, float *xp,
                                            double (&gd)[9][2]) {
     const float4 *zq = z_tab + c * 32;
+    const int wbase = lane * 33;  // row (lane - jj) mod 32, column lane: (wbase - 32 jj) mod 1024
 #pragma unroll
     for (int jj = 0; jj < 32; ++jj) {
         float val = alpha * __uint_as_float(v[jj]);
@@ -137,7 +178,7 @@ __device__ __forceinline__ void grid_block(const uint32_t (&v)[32], int c, int l
             o = fmaf(r4.z, z.z, o);
             val -= o;
         }
-        xp[((lane - jj) & 31) * 32 + lane] = val;
+        xp[(wbase - 32 * jj) & 1023] = val;
     }
     __syncwarp();
     // diagonal lambda = L of block c: i - j shifted by -32 c from block 0
@@ -145,21 +186,21 @@ __device__ __forceinline__ void grid_block(const uint32_t (&v)[32], int c, int l
     if (aa < 0) aa += N;
     int ab = (aa - (32 % N)) % N;  // lambda = L - 32
     if (ab < 0) ab += N;
-    // column of source row l = lane + s (mod 32): x_row of lane l
     const int x0 = __shfl_sync(0xffffffffu, x_row, 0);  // row 32 q + 0
+    // class-1 rows: lambda = L on rows l >= L, lambda = L - 32 on rows l < L;
+    // rotated right by L so that bit s is the row read at step s
+    const uint32_t lowL = (1u << lane) - 1u;
+    const uint32_t cm = (grid_below_mask(x0, aa, N) & ~lowL) | (grid_below_mask(x0, ab, N) & lowL);
+    uint32_t cbits = __funnelshift_r(cm, cm, lane);
+    uint32_t bbits = __funnelshift_r(lowL, lowL, lane);  // steps on lambda = L - 32
+    const float *row = xp + lane * 32;
     float pa0 = 0.f, pa1 = 0.f, pb0 = 0.f, pb1 = 0.f;
 #pragma unroll 8
     for (int s = 0; s < 32; ++s) {
-        const int l = (lane + s) & 31;
-        const float val = xp[lane * 32 + l];
-        int x = x0 + l;
-        if (x >= N) x = (N >= 32) ? x - N : x % N;
-        const bool b = s >= 32 - lane;  // l < lane: lambda = L - 32
-        const bool c1 = x < (b ? ab : aa);
-        pa0 += (!b && !c1) ? val : 0.f;
-        pa1 += (!b && c1) ? val : 0.f;
-        pb0 += (b && !c1) ? val : 0.f;
-        pb1 += (b && c1) ? val : 0.f;
+        const float val = row[(lane + s) & 31];
+        grid_add4(pa0, pa1, pb0, pb1, val, bbits & 1u, cbits & 1u);
+        bbits >>= 1;
+        cbits >>= 1;
     }
     __syncwarp();  // the buffer is free for the next block
     gd[8 - c][0] += (double)pa0;
