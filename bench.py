@@ -95,10 +95,37 @@ def split_ceiling(mode, frac):
     return {"split_ceiling_frac": ceil, "frac_of_split_ceiling": frac / ceil}
 
 
-def llg_report(ms_by_kernel, sites_replicas, ops, hbm, fma_tops):
+def sustained_fma_peak(asd, stream, device, seconds=0.3):
+    """The FP64 FMA issue rate held for `seconds` back to back (the one-launch
+    LLG step runs long enough for the power cap to lower the SM clock, as a
+    ~1 ms burst does not): median TFLOP/s of the repeated peak kernel and the
+    SM clock sampled meanwhile."""
+    tfs = []
+    with ClockSampler(device) as clk:
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < seconds:
+            tfs.append(asd.measure_fp64_peak("fma", stream.cuda_stream)[0])
+    return statistics.median(tfs), clk.summary()
+
+
+def add_per_clock(llg, llg_clocks, fma_clocks):
+    """Per LLG kernel, the FP64 fraction at equal SM clocks: the fraction of
+    the sustained FMA rate times (FMA clock / the kernel's clock), where both
+    median clocks were sampled (ops per cycle against FMAs per cycle)."""
+    fmhz = (fma_clocks or {}).get("sm_mhz")
+    for k, e in llg.items():
+        kmhz = ((llg_clocks or {}).get(k) or {}).get("sm_mhz")
+        if fmhz and kmhz and e.get("fp64_frac_sustained") is not None:
+            e["sm_mhz"] = kmhz
+            e["fp64_frac_per_clock"] = e["fp64_frac_sustained"] * fmhz / kmhz
+    return llg
+
+
+def llg_report(ms_by_kernel, sites_replicas, ops, hbm, fma_tops, fma_sustained_tops=None):
     """Per LLG kernel: site-steps/s, DRAM bytes against the HBM peak (the
     bound of the stage kernels) and FP64 operations against the measured FP64
-    FMA issue rate (the bound of the one-launch step)."""
+    FMA issue rate (the bound of the one-launch step): the burst figure and,
+    where given, the rate the same GPU holds under its power cap."""
     out = {}
     for k, ms in ms_by_kernel.items():
         bps = LLG_BYTES_PER_SITE_STEP if k == "stages" else LLG_FUSED_BYTES_PER_SITE_STEP
@@ -110,6 +137,9 @@ def llg_report(ms_by_kernel, sites_replicas, ops, hbm, fma_tops):
                   "fp64_fma_peak_tops": fma_tops,
                   "fp64_frac": ops * rate / 1e12 / fma_tops if fma_tops else None,
                   "bound": "hbm" if k == "stages" else "fp64"}
+        if fma_sustained_tops:
+            out[k]["fp64_fma_sustained_tops"] = fma_sustained_tops
+            out[k]["fp64_frac_sustained"] = ops * rate / 1e12 / fma_sustained_tops
     return out
 
 
@@ -513,6 +543,7 @@ def pre_measurements(ctx, asd, torch, stream, name, args):
     kernel alone (median of 3 runs of 10 steps), timed by CUDA events."""
     fma_tf, _ = asd.measure_fp64_peak("fma", stream.cuda_stream)
     dmma_tf, _ = asd.measure_fp64_peak("dmma", stream.cuda_stream)
+    fma_sus, fma_clk = sustained_fma_peak(asd, stream, torch.cuda.current_device())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = 10
     llg, llg_clocks = {}, {}
@@ -531,7 +562,8 @@ def pre_measurements(ctx, asd, torch, stream, name, args):
         llg[kern] = sorted(ts)[1]
         llg_clocks[kern] = clk.summary()
     ctx.set_llg_kernel(args.llg_kernel)
-    return {"fma_tf": fma_tf, "dmma_tf": dmma_tf, "llg": llg, "llg_clocks": llg_clocks}
+    return {"fma_tf": fma_tf, "dmma_tf": dmma_tf, "fma_sustained_tf": fma_sus,
+            "fma_sustained_clocks": fma_clk, "llg": llg, "llg_clocks": llg_clocks}
 
 
 def component_measurements(ctx, asd, torch, stream, name, mode, args, pre):
@@ -583,9 +615,15 @@ def component_measurements(ctx, asd, torch, stream, name, mode, args, pre):
     return {
         "fp64_peaks": {"fma_tflops": fma_tf, "fma_tops": fma_tf / 2.0, "dmma_tflops": dmma_tf,
                        "source": "asd_measure_fp64_peak on this GPU before the timed region "
-                                 "(burst, ~1 ms each)"},
-        "llg": llg_report(llg, M * nf, llg_fp64_ops(w["J2"] != 0.0, any(w["h"]), w["alpha"] != 0.0),
-                          peaks["hbm_gbs"], fma_tf / 2.0),
+                                 "(burst, ~1 ms each)",
+                       "fma_sustained_tflops": pre.get("fma_sustained_tf"),
+                       "fma_sustained_clocks": pre.get("fma_sustained_clocks"),
+                       "sustained_source": "the FMA peak kernel back to back for 0.3 s"},
+        "llg": add_per_clock(
+            llg_report(llg, M * nf, llg_fp64_ops(w["J2"] != 0.0, any(w["h"]), w["alpha"] != 0.0),
+                       peaks["hbm_gbs"], fma_tf / 2.0,
+                       (pre["fma_sustained_tf"] / 2.0) if pre.get("fma_sustained_tf") else None),
+            pre.get("llg_clocks"), pre.get("fma_sustained_clocks")),
         "llg_note": "each LLG kernel alone before the timed region (median of 3 x 10 steps)",
         "llg_clocks": pre.get("llg_clocks"),
         "sqt": sqt,
@@ -720,19 +758,24 @@ def run_secondary(args):
         ctx.set_stream(stream.cuda_stream)
         ctx.set_spins(asd.random_spins(N, nf, seed=0), as_origin=True)
         fma_tf, _ = asd.measure_fp64_peak("fma", stream.cuda_stream)
-        llg_ms = {}
+        fma_sus, fma_clk = sustained_fma_peak(asd, stream, 0)
+        llg_ms, llg_clk = {}, {}
         for kern in ("stages", "fused"):
             ctx.set_llg_kernel(kern)
             ctx.step(3)
-            llg_ms[kern] = timed(torch, lambda: ctx.step(1), max(args.steps, 10))
+            with ClockSampler(0) as clk:
+                llg_ms[kern] = timed(torch, lambda: ctx.step(1), max(args.steps, 10))
+            llg_clk[kern] = clk.summary()
         out.update({
             "metric": "LLG site-steps/s (RK4 step alone)", "unit": "site-steps/s",
             "value": M * nf / (llg_ms["fused"] / 1e3), "higher_is_better": True,
             "dtype": "f64",
             "config": {"workload": f"{N}x{N} lattice, {nf} replicas, J=1, J2=-0.3, alpha=0.02, "
                                    "dt=0.005, RK4 step only", "sites": M, "replicas": nf},
-            "llg": llg_report(llg_ms, M * nf, llg_fp64_ops(True, False, True),
-                              measured_peaks()["hbm_gbs"], fma_tf / 2.0),
+            "llg": add_per_clock(llg_report(llg_ms, M * nf, llg_fp64_ops(True, False, True),
+                                            measured_peaks()["hbm_gbs"], fma_tf / 2.0,
+                                            fma_sus / 2.0), llg_clk, fma_clk),
+            "llg_clocks": llg_clk, "fma_sustained_clocks": fma_clk,
         })
         ctx.close()
     elif args.workload == "grid32":

@@ -72,3 +72,17 @@ def test_aggregate_takes_the_slowest_rank():
     # weak scaling: every rank did units_per_rank in its own time
     ms, value = bench.aggregate(50.0, 1e6, 4)
     assert value == pytest.approx(8e7)
+
+
+def test_llg_fraction_per_clock():
+    """The FP64 fraction at equal clocks scales the sustained fraction by the
+    FMA kernel's clock over the LLG kernel's; without both clocks it is not
+    reported."""
+    bench = _bench()
+    llg = bench.llg_report({"fused": 4.0}, 6.5536e7, 387, 6538.0, 16.9, 16.9)
+    frac = llg["fused"]["fp64_frac_sustained"]
+    bench.add_per_clock(llg, {"fused": {"sm_mhz": 1500}}, {"sm_mhz": 1965})
+    assert llg["fused"]["fp64_frac_per_clock"] == pytest.approx(frac * 1965 / 1500)
+    llg2 = bench.llg_report({"fused": 4.0}, 6.5536e7, 387, 6538.0, 16.9, 16.9)
+    bench.add_per_clock(llg2, None, {"sm_mhz": 1965})
+    assert "fp64_frac_per_clock" not in llg2["fused"]
