@@ -11,6 +11,9 @@ alpha = 0.02, dt = 0.005; S(q,t) in BF16x3 and FP64).
   and the renormalised spins have the set length.
 * S(q,t): the FP64 GEMM path against the oracle's factorised form (1e-12),
   the split modes within 1e-5 of the FP64 path.
+* Known answers at 256 x 256 x 1000: a uniform ferromagnet is stationary and
+  identical replicas have no connected correlation.
+* A lattice whose GEMM has more than 2^31 tiles (N = 2900).
 """
 from __future__ import annotations
 
@@ -118,3 +121,27 @@ def test_more_tiles_than_a_32_bit_index(oracle):
     want = oracle.sqt_factorized(N, nf, N // 10, N // 10, st, s0)
     floor = 2.0 ** -17 * (3 * nf) ** 0.5 / (3 * nf)
     assert abs(got - want) <= 1e-5 * abs(want) + 4 * floor, (got, want)
+
+
+def test_known_answers_at_full_size():
+    """At 256 x 256 x 1000 with the headline model (J = 1, J2 = -0.3, alpha =
+    0.02): a uniform ferromagnet, every spin along z, is stationary (H is
+    parallel to S, the torque is exactly zero) through both LLG kernels, bit
+    for bit; with every replica the same configuration the connected S(q,t)
+    vanishes (C_ij = m_i . z_j), here through the FP64 path."""
+    N, nf = 256, 1000
+    kw = dict(J1=1.0, J2=-0.3, alpha=0.02, dt=0.005)
+    up = np.zeros((nf, N * N, 3))
+    up[..., 2] = 1.0
+    with asd.Context(asd.Params.make(N, nf, **kw), modes=["fp64"]) as ctx:
+        for kern in ("fused", "stages"):
+            ctx.set_llg_kernel(kern)
+            ctx.set_spins(up, as_origin=True)
+            ctx.step(3)
+            assert np.array_equal(ctx.get_spins(), up), kern
+        del up
+        same = np.repeat(asd.random_spins(N, 1, seed=7), nf, axis=0)
+        ctx.set_llg_kernel("auto")
+        ctx.set_spins(same, as_origin=True)
+        ctx.step(2)
+        assert abs(ctx.sqt("fp64")) < 1e-9
