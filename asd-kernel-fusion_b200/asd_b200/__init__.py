@@ -35,7 +35,9 @@ LLG_AUTO = 2
 SQT_FP64 = 0
 SQT_TF32X3 = 1
 SQT_BF16X3 = 2
-MODE_NAMES = {SQT_FP64: "fp64", SQT_TF32X3: "tf32x3", SQT_BF16X3: "bf16x3"}
+SQT_FP16X3 = 3
+MODE_NAMES = {SQT_FP64: "fp64", SQT_TF32X3: "tf32x3", SQT_BF16X3: "bf16x3",
+              SQT_FP16X3: "fp16x3"}
 MODES = {v: k for k, v in MODE_NAMES.items()}
 
 # every symbol include/asd_b200.h declares

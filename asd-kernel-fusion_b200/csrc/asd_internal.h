@@ -94,8 +94,6 @@ cudaError_t launch_rk_pass(int pass, long n, double dt, const double *spin, doub
 cudaError_t launch_site_mean(const double *state, long M, int nfile, const double2 *phase,
                              double *mean, float4 *vec4, float *vec1, cudaStream_t st);
 
-// FP64 state [M][K] -> split operands hi/lo [M][Kp] (zero for k >= K).
-// kind 1 = TF32 (stored as fp32 bit patterns), 2 = BF16.
 // Per-site sums over the context's replicas ([M][3]), and the S(q,t) of a
 // replica-sharded ensemble from its all-reduced partial and site sums.
 cudaError_t launch_site_sum(const double *state, long M, int nfile, double *sums,
@@ -103,11 +101,22 @@ cudaError_t launch_site_sum(const double *state, long M, int nfile, double *sums
 cudaError_t launch_shard_finish(long M, int nfile_total, const double *part, const double *sums,
                                 const double *zsums, const double2 *u, const double2 *w,
                                 double *out, cudaStream_t st);
-// Columns [kbeg, kend) of every row only (both even, kend <= Kp).
+// FP64 state [M][K] -> split operands hi/lo [M][Kp] (zero for k >= K):
+// kind 1 = TF32 (stored as fp32 bit patterns), 2 = BF16, 3 = FP16 of
+// scale * x (scale a power of two; ignored by kinds 1 and 2).
+// launch_split_range: columns [kbeg, kend) of every row only (both even,
+// kend <= Kp).
 cudaError_t launch_split_range(int kind, const double *state, long M, int K, int Kp, int kbeg,
-                               int kend, void *hi, void *lo, cudaStream_t st);
+                               int kend, void *hi, void *lo, double scale, cudaStream_t st);
 cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, void *hi,
-                         void *lo, cudaStream_t st);
+                         void *lo, double scale, cudaStream_t st);
+// Bytes per split operand element and K elements per 128-byte k block.
+inline int split_esize(int kind) { return kind == 1 ? 4 : 2; }
+// The power of two FP16x3 scales the spins by: spin_len * scale in
+// [2^12, 2^13), so components up to 7.9 * spin_len stay below FP16's
+// largest finite value (65504) and the lo parts of all components above
+// 2^-15 * spin_len are normal numbers.  1 for the other kinds.
+double split_scale(int kind, double spin_len);
 
 // ------------------------------------------ FP64 tensor-core GEMM S(q,t)
 // (dmma_sqt.cu) C = alpha A B^T over site-major [M][K] FP64 operands, never
@@ -173,14 +182,14 @@ cudaError_t launch_param_reduce(const double *bacc, int nblocks, double *grad, c
 
 // ------------------------------------------------ tcgen05 split GEMM S(q,t)
 struct UmmaSqtArgs {
-    int kind;             // 1 = TF32x3, 2 = BF16x3
+    int kind;             // 1 = TF32x3, 2 = BF16x3, 3 = FP16x3
     long M;               // rows (sites at t)   -- also the column count
     int Kp;               // padded K (multiple of the 128-byte k block)
     const void *a_hi, *a_lo;   // [M][Kp]
     const void *b_hi, *b_lo;   // [M][Kp]
     const float4 *row4; const float *row1;   // padded to the tile multiple
     const float4 *col4; const float *col1;
-    float alpha;          // 1/nfile
+    float alpha;          // 1/nfile (FP16x3: divided by the operands' scale squared)
     double2 *part;        // one partial per CTA
     unsigned *status;     // device status word
     int num_sms;

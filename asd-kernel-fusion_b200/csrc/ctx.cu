@@ -64,11 +64,14 @@ struct asd_ctx {
     double2 *uphase = nullptr, *wphase = nullptr;
     float4 *row4 = nullptr, *col4 = nullptr;
     float *row1 = nullptr, *col1 = nullptr;
-    // split operands per kind (index 1 = TF32, 2 = BF16)
-    void *a_hi[3] = {}, *a_lo[3] = {}, *b_hi[3] = {}, *b_lo[3] = {};
-    int Kp[3] = {};
-    long a_version[3] = {-1, -1, -1};
-    long b_version[3] = {-1, -1, -1};
+    // split operands per kind (index 1 = TF32, 2 = BF16, 3 = FP16), the
+    // state / origin version each was split from, and the scale it was split
+    // with (FP16: a power of two that follows spin_len)
+    void *a_hi[4] = {}, *a_lo[4] = {}, *b_hi[4] = {}, *b_lo[4] = {};
+    int Kp[4] = {};
+    long a_version[4] = {-1, -1, -1, -1};
+    long b_version[4] = {-1, -1, -1, -1};
+    double a_scale[4] = {}, b_scale[4] = {};
     double2 *part = nullptr;
     long part_cap = 0;
     double *d_out = nullptr;
@@ -77,7 +80,7 @@ struct asd_ctx {
     long state_version = 0, origin_version = -1;
     bool has_state = false, has_origin = false;
     int last_launches = 0;
-    int chunk_k = -1;  // < 0: per mode, 512 for TF32x3 and 1024 for BF16x3
+    int chunk_k = -1;  // < 0: per mode, 512 for TF32x3, 1024 for BF16x3 and FP16x3
     double *grid_g = nullptr;     // q grid: N*N displacement bins (FP64)
     double2 *grid_t = nullptr;    // q grid: DFT intermediate
     double *grid_out = nullptr;   // q grid: device result for the host-buffer form
@@ -209,8 +212,20 @@ int ensure_part(asd_ctx *c, long n) {
 }
 
 int kp_for(int kind, int K) {
-    const int ke = (kind == 2) ? 64 : 32;
+    const int ke = 128 / split_esize(kind);  // K elements per 128-byte k block
     return (K + ke - 1) / ke * ke;
+}
+
+// The split kind of an S(q,t) mode (0: the FP64 path).
+int mode_kind(int mode) {
+    return mode == ASD_SQT_TF32X3 ? 1 : mode == ASD_SQT_BF16X3 ? 2 : mode == ASD_SQT_FP16X3 ? 3 : 0;
+}
+
+// K elements per TMEM accumulation chunk: the context's setting, else the
+// same number of tensor-core accumulation steps for every kind (TF32 MMAs
+// take 8 K elements per step, 16-bit ones 16).
+int chunk_for(const asd_ctx *c, int kind) {
+    return c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
 }
 
 // Prologue of every entry point that may enqueue work: select the device and
@@ -312,7 +327,7 @@ int refresh_origin(asd_ctx *c) {
                                   c->col1, c->stream));
     c->last_launches += 1;
     c->origin_version = c->state_version;
-    for (int k = 1; k <= 2; ++k) c->b_version[k] = -1;
+    for (int k = 1; k <= 3; ++k) c->b_version[k] = -1;
     return ASD_OK;
 }
 
@@ -410,25 +425,40 @@ int sqt_plain(asd_ctx *c, double *d_out, bool shard) {
     return ASD_OK;
 }
 
-int sqt_split(asd_ctx *c, int kind, double *d_out, bool shard) {
+// Splits the origin (B) for `kind` where its operands are out of date: after
+// a new origin and, for FP16x3, after a change of spin_len (which changes
+// the operands' scale).
+int ensure_split_origin(asd_ctx *c, int kind) {
+    const double sc = split_scale(kind, c->p.spin_len);
+    if (c->b_version[kind] == c->origin_version && c->b_scale[kind] == sc) return ASD_OK;
+    ASD_CUDA_TRY(launch_split(kind, c->origin, c->M, c->K, c->Kp[kind], c->b_hi[kind],
+                              c->b_lo[kind], sc, c->stream));
+    c->b_version[kind] = c->origin_version;
+    c->b_scale[kind] = sc;
+    c->last_launches += 1;
+    return ASD_OK;
+}
+
+// Both operands of `kind` up to date: the current state (A) after a step or
+// set_spins, and the origin (B).
+int ensure_split(asd_ctx *c, int kind) {
     if (!c->a_hi[kind]) return fail(ASD_ERR_STATE, "split mode %d not enabled at create", kind);
-    if (c->a_version[kind] != c->state_version) {
+    const double sc = split_scale(kind, c->p.spin_len);
+    if (c->a_version[kind] != c->state_version || c->a_scale[kind] != sc) {
         ASD_CUDA_TRY(launch_split(kind, c->y, c->M, c->K, c->Kp[kind], c->a_hi[kind],
-                                  c->a_lo[kind], c->stream));
+                                  c->a_lo[kind], sc, c->stream));
         c->a_version[kind] = c->state_version;
+        c->a_scale[kind] = sc;
         c->last_launches += 1;
     }
-    if (c->b_version[kind] != c->origin_version) {
-        ASD_CUDA_TRY(launch_split(kind, c->origin, c->M, c->K, c->Kp[kind], c->b_hi[kind],
-                                  c->b_lo[kind], c->stream));
-        c->b_version[kind] = c->origin_version;
-        c->last_launches += 1;
-    }
-    int rc = ensure_part(c, c->num_sms);
-    if (rc != ASD_OK) return rc;
-    cudaStream_t gemm = c->stream;
-    rc = arm_y_free(c, &gemm);
-    if (rc != ASD_OK) return rc;
+    return ensure_split_origin(c, kind);
+}
+
+// The GEMM arguments every split-mode launch shares.  alpha is the product's
+// scale; the FP16 operands carry the factor scale^2, which alpha takes out
+// (a power of two: the same FP32 roundings as unscaled operands).
+UmmaSqtArgs split_args(const asd_ctx *c, int kind, double alpha) {
+    const double sc = split_scale(kind, c->p.spin_len);
     UmmaSqtArgs u{};
     u.kind = kind;
     u.M = c->M;
@@ -441,14 +471,24 @@ int sqt_split(asd_ctx *c, int kind, double *d_out, bool shard) {
     u.row1 = c->row1;
     u.col4 = c->col4;
     u.col1 = c->col1;
-    u.alpha = (float)gemm_alpha(c, shard);
-    u.outer = shard ? 0 : 1;
+    u.alpha = (float)(alpha / (sc * sc));
     u.part = c->part;
     u.status = c->status;
     u.num_sms = c->num_sms;
-    // Same number of tensor-core accumulation steps per chunk for both kinds
-    // (TF32 MMAs take 8 K elements per step, BF16 ones 16).
-    u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
+    u.chunk_k = chunk_for(c, kind);
+    return u;
+}
+
+int sqt_split(asd_ctx *c, int kind, double *d_out, bool shard) {
+    int rc = ensure_split(c, kind);
+    if (rc != ASD_OK) return rc;
+    rc = ensure_part(c, c->num_sms);
+    if (rc != ASD_OK) return rc;
+    cudaStream_t gemm = c->stream;
+    rc = arm_y_free(c, &gemm);
+    if (rc != ASD_OK) return rc;
+    UmmaSqtArgs u = split_args(c, kind, gemm_alpha(c, shard));
+    u.outer = shard ? 0 : 1;
     cudaEvent_t t0 = time_begin(c, gemm);
     const int grid = launch_umma_sqt(u, gemm);
     time_end(c, 1, 1, gemm, t0);
@@ -466,7 +506,7 @@ int sqt_split(asd_ctx *c, int kind, double *d_out, bool shard) {
 int sqt_async(asd_ctx *c, int mode, double *d_out, bool shard = false) {
     if (!c->has_state || !c->has_origin)
         return fail(ASD_ERR_STATE, "set the spins and the origin before S(q,t)");
-    if (mode < 0 || mode > 2) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
+    if (mode < 0 || mode > 3) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
     if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
     ASD_CUDA_TRY(launch_site_mean(c->y, c->M, c->p.nfile, c->uphase, c->mean_t, c->row4, c->row1,
                                   c->stream));
@@ -476,6 +516,7 @@ int sqt_async(asd_ctx *c, int mode, double *d_out, bool shard = false) {
         case ASD_SQT_FP64: return sqt_plain(c, d_out, shard);
         case ASD_SQT_TF32X3: return sqt_split(c, 1, d_out, shard);
         case ASD_SQT_BF16X3: return sqt_split(c, 2, d_out, shard);
+        case ASD_SQT_FP16X3: return sqt_split(c, 3, d_out, shard);
     }
     return ASD_ERR_INVALID;
 }
@@ -770,7 +811,7 @@ int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
         return fail(ASD_ERR_STATE, "set the spins and the origin before S(q,t)");
     const int N = c->p.N;
     const long M = c->M;
-    if (mode != ASD_SQT_FP64 && mode != ASD_SQT_TF32X3 && mode != ASD_SQT_BF16X3)
+    if (mode < 0 || mode > 3)
         return fail(ASD_ERR_UNSUPPORTED, "q-grid S(q,t): mode %d not supported", mode);
     if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
     int rc;
@@ -799,42 +840,14 @@ int sqt_grid_async(asd_ctx *c, int mode, double *d_out) {
         c->last_launches += 5;
         return ASD_OK;
     }
-    const int kind = (mode == ASD_SQT_TF32X3) ? 1 : 2;
-    if (!c->a_hi[kind]) return fail(ASD_ERR_STATE, "split mode %d not enabled at create", kind);
-    if (c->a_version[kind] != c->state_version) {
-        ASD_CUDA_TRY(launch_split(kind, c->y, c->M, c->K, c->Kp[kind], c->a_hi[kind],
-                                  c->a_lo[kind], c->stream));
-        c->a_version[kind] = c->state_version;
-        c->last_launches += 1;
-    }
-    if (c->b_version[kind] != c->origin_version) {
-        ASD_CUDA_TRY(launch_split(kind, c->origin, c->M, c->K, c->Kp[kind], c->b_hi[kind],
-                                  c->b_lo[kind], c->stream));
-        c->b_version[kind] = c->origin_version;
-        c->last_launches += 1;
-    }
+    const int kind = mode_kind(mode);
+    if ((rc = ensure_split(c, kind)) != ASD_OK) return rc;
     const int bm = umma_tile_rows(), bn = umma_tile_cols();
     const int num_m = (int)(c->Mp / bm), num_n = (int)(c->Mp / bn);
     const size_t nd2 = 2 * (size_t)(bm + bn - 1);
     rc = ensure_grid_work(c, (size_t)num_m * num_n * nd2, (size_t)qgrid_keys(num_m, num_n, bm, bn) * nd2);
     if (rc != ASD_OK) return rc;
-    UmmaSqtArgs u{};
-    u.kind = kind;
-    u.M = c->M;
-    u.Kp = c->Kp[kind];
-    u.a_hi = c->a_hi[kind];
-    u.a_lo = c->a_lo[kind];
-    u.b_hi = c->b_hi[kind];
-    u.b_lo = c->b_lo[kind];
-    u.row4 = c->row4;
-    u.row1 = c->row1;
-    u.col4 = c->col4;
-    u.col1 = c->col1;
-    u.alpha = (float)(1.0 / (double)c->p.nfile);
-    u.part = c->part;
-    u.status = c->status;
-    u.num_sms = c->num_sms;
-    u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
+    UmmaSqtArgs u = split_args(c, kind, 1.0 / (double)c->p.nfile);
     u.tdiag = c->grid_tdiag;
     u.lat_n = N;
     const int grid = launch_umma_sqt(u, c->stream);
@@ -917,19 +930,15 @@ int ensure_host_pipeline(asd_ctx *c, int cr) {
 int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int mode, int cr) {
     const int nf = c->p.nfile;
     const long M = c->M;
-    const int kind = (mode == ASD_SQT_TF32X3) ? 1 : (mode == ASD_SQT_BF16X3) ? 2 : 0;
-    if (mode < 0 || mode > 2) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
+    const int kind = mode_kind(mode);
+    if (mode < 0 || mode > 3) return fail(ASD_ERR_INVALID, "unknown S(q,t) mode %d", mode);
     if (!(c->modes & (1u << mode))) return fail(ASD_ERR_STATE, "mode %d not enabled at create", mode);
     int rc = ensure_host_pipeline(c, cr);
     if (rc != ASD_OK) return rc;
     const int nchunks = (nf + cr - 1) / cr;
     if (kind) {
-        if (c->b_version[kind] != c->origin_version) {
-            ASD_CUDA_TRY(launch_split(kind, c->origin, M, c->K, c->Kp[kind], c->b_hi[kind],
-                                      c->b_lo[kind], c->stream));
-            c->b_version[kind] = c->origin_version;
-            c->last_launches += 1;
-        }
+        if (!c->a_hi[kind]) return fail(ASD_ERR_STATE, "split mode %d not enabled at create", kind);
+        if ((rc = ensure_split_origin(c, kind)) != ASD_OK) return rc;
         if (!c->rows_ready) {  // the early chunks' epilogues read the phase u_i
             ASD_CUDA_TRY(launch_site_mean(c->y, M, nf, c->uphase, c->mean_t, c->row4, c->row1,
                                           c->stream));
@@ -979,30 +988,16 @@ int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int m
         if (!kind) continue;
         const int kbeg = 3 * f0, kend = last ? c->Kp[kind] : 3 * (f0 + nc);
         ASD_CUDA_TRY(launch_split_range(kind, ynew, M, c->K, c->Kp[kind], kbeg, kend,
-                                        c->a_hi[kind], c->a_lo[kind], comp));
+                                        c->a_hi[kind], c->a_lo[kind],
+                                        split_scale(kind, c->p.spin_len), comp));
         c->last_launches += 1;
         if (last) {
             ASD_CUDA_TRY(launch_site_mean(ynew, M, nf, c->uphase, c->mean_t, c->row4, c->row1,
                                           comp));
             c->last_launches += 1;
         }
-        UmmaSqtArgs u{};
-        u.kind = kind;
-        u.M = M;
-        u.Kp = c->Kp[kind];
-        u.a_hi = c->a_hi[kind];
-        u.a_lo = c->a_lo[kind];
-        u.b_hi = c->b_hi[kind];
-        u.b_lo = c->b_lo[kind];
-        u.row4 = c->row4;
-        u.row1 = c->row1;
-        u.col4 = c->col4;
-        u.col1 = c->col1;
-        u.alpha = (float)(1.0 / (double)nf);
+        UmmaSqtArgs u = split_args(c, kind, 1.0 / (double)nf);
         u.part = c->part + nparts;
-        u.status = c->status;
-        u.num_sms = c->num_sms;
-        u.chunk_k = c->chunk_k >= 0 ? c->chunk_k : (kind == 1 ? 512 : 1024);
         u.k_begin = kbeg;
         u.k_end = kend;
         u.outer = last ? 1 : 0;
@@ -1019,6 +1014,7 @@ int step_host_chunked(asd_ctx *c, const double *spin_in, double *spin_out, int m
     c->has_state = true;
     if (kind) {
         c->a_version[kind] = c->state_version;
+        c->a_scale[kind] = split_scale(kind, c->p.spin_len);
         ASD_CUDA_TRY(launch_finalize(c->part, (int)nparts, 1.0 / (double)M, c->d_out, comp));
         c->last_launches += 1;
         return ASD_OK;
@@ -1133,7 +1129,7 @@ void destroy(asd_ctx *c) {
                     c->status, c->grid_g, c->grid_t, c->grid_out};
     for (void *q : ptrs)
         if (q) cudaFree(q);
-    for (int k = 1; k <= 2; ++k) {
+    for (int k = 1; k <= 3; ++k) {
         void *ops[] = {c->a_hi[k], c->a_lo[k], c->b_hi[k], c->b_lo[k]};
         for (void *q : ops)
             if (q) cudaFree(q);
@@ -1236,11 +1232,11 @@ int asd_ctx_create(const asd_params *p, unsigned mode_mask, asd_ctx **out) {
     c->M = (long)p->N * p->N;
     c->Mp = umma_row_pad(c->M);
     c->K = 3 * p->nfile;
-    if (mode_mask & ~0x7u) {
+    if (mode_mask & ~0xFu) {
         delete c;
-        return fail(ASD_ERR_INVALID, "mode_mask 0x%x has bits beyond the three S(q,t) modes", mode_mask);
+        return fail(ASD_ERR_INVALID, "mode_mask 0x%x has bits beyond the four S(q,t) modes", mode_mask);
     }
-    c->modes = mode_mask ? mode_mask : 0x7u;
+    c->modes = mode_mask ? mode_mask : 0xFu;
     const size_t sbytes = (size_t)c->M * c->K * sizeof(double);
 #define ASD_ALLOC(ptr, bytes)                 \
     do {                                      \
@@ -1262,11 +1258,11 @@ int asd_ctx_create(const asd_params *p, unsigned mode_mask, asd_ctx **out) {
     ASD_ALLOC(c->col1, (size_t)c->Mp * sizeof(float));
     ASD_ALLOC(c->d_out, 2 * sizeof(double));
     ASD_ALLOC(c->status, sizeof(unsigned));
-    for (int kind = 1; kind <= 2; ++kind) {
-        const int mode = (kind == 1) ? ASD_SQT_TF32X3 : ASD_SQT_BF16X3;
+    for (int mode = ASD_SQT_TF32X3; mode <= ASD_SQT_FP16X3; ++mode) {
+        const int kind = mode_kind(mode);
         if (!(c->modes & (1u << mode))) continue;
         c->Kp[kind] = kp_for(kind, c->K);
-        const size_t ob = (size_t)c->Mp * c->Kp[kind] * (kind == 2 ? 2 : 4);
+        const size_t ob = (size_t)c->Mp * c->Kp[kind] * split_esize(kind);
         ASD_ALLOC(c->a_hi[kind], ob);
         ASD_ALLOC(c->a_lo[kind], ob);
         ASD_ALLOC(c->b_hi[kind], ob);

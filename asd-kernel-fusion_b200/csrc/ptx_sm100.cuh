@@ -164,7 +164,8 @@ __device__ __forceinline__ uint64_t umma_desc_kmajor(uint32_t smem_addr) {
 
 // Instruction descriptor for kind::f16 / kind::tf32 with FP32 accumulation,
 // both operands K-major: D format F32 [4,6), A format [7,10), B format
-// [10,13), N >> 3 [17,23), M >> 4 [24,29).  fmt: 1 = BF16, 2 = TF32.
+// [10,13), N >> 3 [17,23), M >> 4 [24,29).  fmt: 0 = FP16, 1 = BF16 (kind::f16),
+// 2 = TF32 (kind::tf32).
 __host__ __device__ constexpr uint32_t umma_idesc(uint32_t fmt, uint32_t M, uint32_t N) {
     return (1u << 4) | (fmt << 7) | (fmt << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
 }

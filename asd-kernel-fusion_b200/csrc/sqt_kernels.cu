@@ -8,6 +8,9 @@
 // replica mean at t (fint_avg, :349-366) and z_j the mean at t = 0
 // (zerot_avg, llg_sqt_baseline.c:240-259).
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cmath>
 
 #include "asd_internal.h"
 
@@ -171,6 +174,29 @@ __global__ void __launch_bounds__(256) split_bf16_kernel(const double *__restric
     lo[o] = __halves2bfloat162(l0, l1);
 }
 
+// FP16 split of scale * x (scale a power of two, so the product is exact):
+// hi and lo each round to nearest even, and lo is formed from the exact FP64
+// difference.  FP16 has TF32's 11-bit significand, so hi + lo carry 22 bits.
+__global__ void __launch_bounds__(256) split_f16_kernel(const double *__restrict__ s, long M,
+                                                        int K, int Kp, int kbeg, int kend,
+                                                        double scale, __half2 *__restrict__ hi,
+                                                        __half2 *__restrict__ lo) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pairs = (kend - kbeg) / 2;
+    if (t >= M * pairs) return;
+    const long row = t / pairs;
+    const int k = kbeg + (int)(t - row * pairs) * 2;
+    double x0 = 0.0, x1 = 0.0;
+    if (k < K) x0 = s[row * K + k] * scale;
+    if (k + 1 < K) x1 = s[row * K + k + 1] * scale;
+    const __half h0 = __double2half(x0), h1 = __double2half(x1);
+    const __half l0 = __double2half(x0 - (double)__half2float(h0));
+    const __half l1 = __double2half(x1 - (double)__half2float(h1));
+    const long o = row * (Kp / 2) + k / 2;
+    hi[o] = __halves2half2(h0, h1);
+    lo[o] = __halves2half2(l0, l1);
+}
+
 
 // Separable 2-D DFT of the displacement histogram: T[dr][b] = sum_dc G[dr][dc]
 // e^{-2 pi i b dc / N}, then S[a][b] = scale * sum_dr T[dr][b] e^{-2 pi i a dr / N}.
@@ -259,23 +285,31 @@ cudaError_t launch_shard_finish(long M, int nfile_total, const double *part, con
 }
 
 cudaError_t launch_split_range(int kind, const double *state, long M, int K, int Kp, int kbeg,
-                               int kend, void *hi, void *lo, cudaStream_t st) {
-    if (kbeg < 0 || kend > Kp || kbeg >= kend || (kbeg | kend | Kp) & 1)
+                               int kend, void *hi, void *lo, double scale, cudaStream_t st) {
+    if (kbeg < 0 || kend > Kp || kbeg >= kend || (kbeg | kend | Kp) & 1 || kind < 1 || kind > 3)
         return cudaErrorInvalidValue;
     const long total = M * ((kend - kbeg) / 2);
     const unsigned blocks = (unsigned)((total + 255) / 256);
     if (kind == 1)
         split_tf32_kernel<<<blocks, 256, 0, st>>>(state, M, K, Kp, kbeg, kend, (float2 *)hi,
                                                   (float2 *)lo);
-    else
+    else if (kind == 2)
         split_bf16_kernel<<<blocks, 256, 0, st>>>(state, M, K, Kp, kbeg, kend,
                                                   (__nv_bfloat162 *)hi, (__nv_bfloat162 *)lo);
+    else
+        split_f16_kernel<<<blocks, 256, 0, st>>>(state, M, K, Kp, kbeg, kend, scale,
+                                                 (__half2 *)hi, (__half2 *)lo);
     return cudaGetLastError();
 }
 
 cudaError_t launch_split(int kind, const double *state, long M, int K, int Kp, void *hi, void *lo,
-                         cudaStream_t st) {
-    return launch_split_range(kind, state, M, K, Kp, 0, Kp, hi, lo, st);
+                         double scale, cudaStream_t st) {
+    return launch_split_range(kind, state, M, K, Kp, 0, Kp, hi, lo, scale, st);
+}
+
+double split_scale(int kind, double spin_len) {
+    if (kind != 3 || !(spin_len > 0.0) || !(spin_len < 1e300)) return 1.0;
+    return ldexp(1.0, 12 - ilogb(spin_len));
 }
 
 

@@ -8,7 +8,7 @@
 // outer term as m_i . z_j, so the epilogue needs only per-row and per-column
 // vectors, and each CTA leaves one complex partial sum.
 //
-// Precision (3-term split): A = Ah + Al, B = Bh + Bl in TF32 or BF16, the
+// Precision (3-term split): A = Ah + Al, B = Bh + Bl in TF32, BF16 or FP16, the
 // tensor cores accumulate Ah Bh + Ah Bl + Al Bh in FP32 in TMEM; the epilogue
 // works in FP32 per 32-column chunk and accumulates in FP64 across chunks,
 // tiles and CTAs.
@@ -209,7 +209,7 @@ __device__ __forceinline__ void grid_block(const uint32_t (&v)[32], int c, int l
     gd[7 - c][1] += (double)pb1;
 }
 
-// KIND: 1 = TF32x3, 2 = BF16x3.  EPI selects the epilogue:
+// KIND: 1 = TF32x3, 2 = BF16x3, 3 = FP16x3.  EPI selects the epilogue:
 //   EPI_PHASE  S(q,t) at one q: per-CTA partial sum of u_i w_j (alpha C - m.z)
 //   EPI_STORE  the raw FP32 accumulator to dbg_c[i * dbg_ldc + j] (diagnostic)
 //   EPI_GRID   the whole q grid: per tile, the sums of alpha C_ij - m_i.z_j
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             ptx::tma_prefetch_desc(&tm_al);
             ptx::tma_prefetch_desc(&tm_bh);
             ptx::tma_prefetch_desc(&tm_bl);
-            constexpr int KE = G::ROWB / ((KIND == 2) ? 2 : 4);  // elements per stage row
+            constexpr int KE = G::ROWB / ((KIND == 1) ? 4 : 2);  // elements per stage row
             int stage = 0;
             uint32_t phase = 0;
             bool issued[G::STAGES] = {};
@@ -328,7 +328,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            constexpr uint32_t IDESC = ptx::umma_idesc(KIND == 2 ? 1u : 2u, BM, BN);
+            // A/B format: TF32 2 (kind::tf32); BF16 1, FP16 0 (kind::f16)
+            constexpr uint32_t FMT = KIND == 1 ? 2u : KIND == 2 ? 1u : 0u;
+            constexpr uint32_t IDESC = ptx::umma_idesc(FMT, BM, BN);
             int stage = 0;
             uint32_t phase = 0;
             int abuf = 0;
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         for (int kk = 0; kk < G::KSTEPS; ++kk) {
                             const uint64_t adv = (uint64_t)(2 * kk);  // 32 bytes per k step
                             const uint32_t accum = (kb > kb0 || kk > 0) ? 1u : 0u;
-                            if (KIND == 2) {
+                            if (KIND != 1) {
                                 ptx::umma_f16(d_tmem, dah + adv, dbh + adv, IDESC, accum);
                                 ptx::umma_f16(d_tmem, dah + adv, dbl + adv, IDESC, 1u);
                                 ptx::umma_f16(d_tmem, dal + adv, dbh + adv, IDESC, 1u);
@@ -610,9 +612,10 @@ int make_tmap(CUtensorMap *m, const void *base, int kind, long rows, int Kp, int
               int rowb) {
     auto enc = get_encode_fn();
     if (!enc) return fail(ASD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
-    const int esize = (kind == 2) ? 2 : 4;
-    const CUtensorMapDataType dt =
-        (kind == 2) ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const int esize = split_esize(kind);
+    const CUtensorMapDataType dt = kind == 1   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : kind == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                               : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
     cuuint64_t gdim[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
     cuuint64_t gstride[1] = {(cuuint64_t)Kp * esize};
     cuuint32_t box[2] = {(cuuint32_t)(rowb / esize), (cuuint32_t)box_rows};
@@ -640,7 +643,8 @@ long umma_max_grid_for(long M, int num_sms) {
 
 int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
     const long Mp = umma_row_pad(a.M);
-    const int esize = (a.kind == 2) ? 2 : 4;
+    if (a.kind < 1 || a.kind > 3) return fail(ASD_ERR_INVALID, "split kind %d", a.kind);
+    const int esize = split_esize(a.kind);
     if (a.Kp <= 0 || (a.Kp * esize) % Geo::ROWB != 0)
         return fail(ASD_ERR_INVALID, "Kp=%d: rows must be a multiple of 128 bytes", a.Kp);
     if (((uintptr_t)a.a_hi | (uintptr_t)a.a_lo | (uintptr_t)a.b_hi | (uintptr_t)a.b_lo) & 15)
@@ -686,7 +690,11 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
         return cudaGetLastError();
     };
     cudaError_t e;
-    if (a.kind == 2)
+    if (a.kind == 3)
+        e = epi == EPI_STORE  ? go(umma_sqt_kernel<3, EPI_STORE>)
+            : epi == EPI_GRID ? go(umma_sqt_kernel<3, EPI_GRID>)
+                              : go(umma_sqt_kernel<3, EPI_PHASE>);
+    else if (a.kind == 2)
         e = epi == EPI_STORE  ? go(umma_sqt_kernel<2, EPI_STORE>)
             : epi == EPI_GRID ? go(umma_sqt_kernel<2, EPI_GRID>)
                               : go(umma_sqt_kernel<2, EPI_PHASE>);
@@ -729,7 +737,8 @@ extern "C" int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, 
                                  const void *b_hi, const void *b_lo, float *c, long ldc,
                                  int chunk_k, void *stream) {
     using namespace asd;
-    if (kind != 1 && kind != 2) return fail(ASD_ERR_INVALID, "kind must be 1 (TF32) or 2 (BF16)");
+    if (kind < 1 || kind > 3)
+        return fail(ASD_ERR_INVALID, "kind must be 1 (TF32), 2 (BF16) or 3 (FP16)");
     if (rows <= 0 || rows % 256 != 0) return fail(ASD_ERR_INVALID, "rows must be a multiple of 256");
     if (!a_hi || !a_lo || !b_hi || !b_lo || !c || ldc < rows)
         return fail(ASD_ERR_INVALID, "bad pointer or ldc");

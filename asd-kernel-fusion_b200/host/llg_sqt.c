@@ -11,7 +11,7 @@
  * appended to the timing file, like the reference's amd_gcc_11.2_*_sqt.txt.
  *
  * Extensions: -J J1, -K J2, -a alpha, -H hx,hy,hz, -S spin length, -s seed,
- * -q fp64|tf32x3|bf16x3, -i/-o spin files (asd_spins_load/save
+ * -q fp64|tf32x3|bf16x3|fp16x3, -i/-o spin files (asd_spins_load/save
  * format), -w warm-up steps (default 20), -r timing file, -p print S(q,t)
  * every step, -g print S(q,t) on the whole q grid at the end (N*N <= 4096).
  *
@@ -49,7 +49,7 @@ static void usage(const char *prog) {
     fprintf(stderr,
             "usage: %s [-n N] [-m steps] [-f Nfile] [-e dt] [-t threads] [-x vx] [-y vy]\n"
             "          [-J J1] [-K J2] [-a alpha] [-H hx,hy,hz] [-S spin_len] [-s seed]\n"
-            "          [-q fp64|tf32x3|bf16x3] [-i in.spins] [-o out.spins]\n"
+            "          [-q fp64|tf32x3|bf16x3|fp16x3] [-i in.spins] [-o out.spins]\n"
             "          [-w warmup] [-r timing_file] [-p] [-g]\n",
             prog);
 }
@@ -58,6 +58,7 @@ static int parse_mode(const char *s, asd_sqt_mode *m) {
     if (!strcmp(s, "fp64")) *m = ASD_SQT_FP64;
     else if (!strcmp(s, "tf32x3")) *m = ASD_SQT_TF32X3;
     else if (!strcmp(s, "bf16x3")) *m = ASD_SQT_BF16X3;
+    else if (!strcmp(s, "fp16x3")) *m = ASD_SQT_FP16X3;
     else return -1;
     return 0;
 }

@@ -57,7 +57,7 @@ WORKLOADS = {
 }
 LLG_BYTES_PER_SITE_STEP = 384  # 4 fused stage kernels: 3+5+5+3 FP64 3-vectors
 LLG_FUSED_BYTES_PER_SITE_STEP = 48  # one streamed step: read y, write y
-DEFAULT_CHUNK_K = {"tf32x3": 512, "bf16x3": 1024}
+DEFAULT_CHUNK_K = {"tf32x3": 512, "bf16x3": 1024, "fp16x3": 1024}
 
 
 def llg_fp64_ops(J2: bool, H: bool, damp: bool) -> int:
@@ -86,10 +86,10 @@ def measured_peaks():
 
 def split_ceiling(mode, frac):
     """The highest useful-flop fraction of the dense BF16 peak a 3-term split
-    GEMM can reach: three tensor-core products per useful one, and TF32
-    products run at half the BF16 rate on B200.  frac_of_ceiling is how close
+    GEMM can reach: three tensor-core products per useful one, FP16 products
+    run at the BF16 rate and TF32 ones at half of it on B200.  frac_of_ceiling is how close
     the kernel is to that bound."""
-    ceil = {"tf32x3": 1.0 / 6.0, "bf16x3": 1.0 / 3.0}.get(mode)
+    ceil = {"tf32x3": 1.0 / 6.0, "bf16x3": 1.0 / 3.0, "fp16x3": 1.0 / 3.0}.get(mode)
     if ceil is None or frac is None:
         return {}
     return {"split_ceiling_frac": ceil, "frac_of_split_ceiling": frac / ceil}
@@ -431,7 +431,7 @@ def run_ours(args):
     params = asd.Params.make(N, nf, J1=w["J1"], J2=w["J2"], alpha=w["alpha"], h=w["h"], dt=w["dt"])
     asd.load().asd_set_device(local)
     extras = not args.no_extras
-    ctx = asd.Context(params, modes=(["fp64", "tf32x3", "bf16x3"] if extras else [mode]))
+    ctx = asd.Context(params, modes=(["fp64", "tf32x3", "bf16x3", "fp16x3"] if extras else [mode]))
     ctx.set_llg_kernel(args.llg_kernel)
     if args.chunk_k >= 0:
         ctx.set_chunk_k(args.chunk_k)
@@ -580,7 +580,7 @@ def component_measurements(ctx, asd, torch, stream, name, mode, args, pre):
     d = torch.zeros(2, dtype=torch.float64, device="cuda")
     sqt_ms, kern_ms, vals = {}, {}, {}
     ctx.time_kernels(True)
-    for m in ("fp64", "tf32x3", "bf16x3"):
+    for m in ("fp64", "tf32x3", "bf16x3", "fp16x3"):
         n = 1 if m == "fp64" else 3
         ctx.sqt_async(m, d.data_ptr())  # operands split, warm
         torch.cuda.synchronize()
@@ -628,7 +628,8 @@ def component_measurements(ctx, asd, torch, stream, name, mode, args, pre):
         "llg_clocks": pre.get("llg_clocks"),
         "sqt": sqt,
         "sqt_term_magnitude": mag,
-        "sqt_speedup_vs_fp64": {m: sqt_ms["fp64"] / sqt_ms[m] for m in ("tf32x3", "bf16x3")},
+        "sqt_speedup_vs_fp64": {m: sqt_ms["fp64"] / sqt_ms[m]
+                                for m in ("tf32x3", "bf16x3", "fp16x3")},
     }
 
 
@@ -729,7 +730,7 @@ def run_secondary(args):
         grid = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
         one = torch.zeros(2, dtype=torch.float64, device="cuda")
         res = {}
-        for mode in ("bf16x3", "tf32x3", "fp64"):
+        for mode in ("bf16x3", "fp16x3", "tf32x3", "fp64"):
             reps = 1 if mode == "fp64" else 3
             ctx.sqt_grid_async(mode, grid.data_ptr())  # work space, warm
             g_ms = timed(torch, lambda: ctx.sqt_grid_async(mode, grid.data_ptr()), reps)
@@ -972,7 +973,7 @@ def main():
                     default="sqt256",
                     help="sqt256 (default) and sqt128 print the full line; the others a line of "
                          "their own")
-    ap.add_argument("--mode", choices=["tf32x3", "bf16x3", "fp64"], default=None,
+    ap.add_argument("--mode", choices=["tf32x3", "bf16x3", "fp16x3", "fp64"], default=None,
                     help="S(q,t) arithmetic (default: the workload's)")
     ap.add_argument("--batch-cluster", type=int, default=0,
                     help="batch48: clusters of this many CTAs instead of the autotuner's choice")

@@ -21,8 +21,8 @@
  *  2. A context API (asd_ctx_*) that keeps the replicas' spins resident in
  *     HBM and runs a whole step on one CUDA stream: the RK4 step with its
  *     renormalisation (one launch, or one kernel per stage), then S(q,t)
- *     through a tcgen05 tensor-core GEMM in split precision (TF32x3 or
- *     BF16x3) whose epilogue applies the phase, the connected-part
+ *     through a tcgen05 tensor-core GEMM in split precision (TF32x3,
+ *     BF16x3 or FP16x3) whose epilogue applies the phase, the connected-part
  *     subtraction and the reduction, or through the FP64 path.  It replaces
  *     the per-step body of main() (llg_sqt_baseline.c:289-426,
  *     llg_sqt_fusion.c:340-449); host-buffer forms keep the reference's data
@@ -60,7 +60,13 @@ typedef enum {
                            one block per 128 x 128 tile, so up to N = 2435
                            (ASD_ERR_UNSUPPORTED beyond) */
     ASD_SQT_TF32X3 = 1, /* tcgen05 kind::tf32, hi*hi + hi*lo + lo*hi, FP32 accumulate   */
-    ASD_SQT_BF16X3 = 2  /* tcgen05 kind::f16 (bf16), hi*hi + hi*lo + lo*hi, FP32 accum. */
+    ASD_SQT_BF16X3 = 2, /* tcgen05 kind::f16 (bf16), hi*hi + hi*lo + lo*hi, FP32 accum. */
+    ASD_SQT_FP16X3 = 3  /* tcgen05 kind::f16 (fp16), hi*hi + hi*lo + lo*hi, FP32 accum.:
+                           the operands are scaled by 2^e (spin_len * 2^e in [2^12, 2^13))
+                           before the split, so hi + lo keep 22 bits like TF32's while the
+                           products run at the 16-bit rate; components up to
+                           7.9 * spin_len always fit, larger ones can overflow FP16
+                           and then make S(q,t) non-finite */
 } asd_sqt_mode;
 
 /* Model parameters.  The reference hard-wires alpha = J2 = h = 0,
@@ -133,7 +139,7 @@ int asd_ctx_sqt_magnitude(asd_ctx *ctx, double *out);
 
 /* S(q,t) for every q = 2*pi*(a, b)/N of the N x N grid, into d_out[2*(a*N+b)]
  * (real) and d_out[2*(a*N+b)+1] (imaginary), a device buffer of 2*N*N
- * doubles; asynchronous.  The same correlation GEMM (FP64, TF32x3 or BF16x3),
+ * doubles; asynchronous.  The same correlation GEMM (any asd_sqt_mode),
  * with an epilogue that sums every connected C_ij - m_i . z_j along the
  * diagonals i - j of each tile; the diagonal sums are binned by displacement
  * r_i - r_j (mod N) and a 2-D DFT of the N*N bins gives S at every q.
@@ -258,10 +264,10 @@ int asd_ctx_set_llg_kernel(asd_ctx *ctx, int kernel);
  * up to the pipeline's k block; 0 = all of K in one accumulator; negative =
  * the default).  The tensor cores' FP32 accumulation loses precision with
  * every accumulation step, so K is cut into chunks whose partial products the
- * epilogue adds in FP64.  Default: 512 for TF32x3 and 1024 for BF16x3, the
- * same number of accumulation steps (TF32 MMAs take 8 K elements per step,
- * BF16 ones 16); measured relative error of S(q,t) about 5e-6 and 4e-6 at
- * K = 3000. */
+ * epilogue adds in FP64.  Default: 512 for TF32x3 and 1024 for BF16x3 and
+ * FP16x3, the same number of accumulation steps (TF32 MMAs take 8 K elements
+ * per step, 16-bit ones 16); measured relative error of S(q,t) about 5e-6 and
+ * 4e-6 at K = 3000. */
 int asd_ctx_set_chunk_k(asd_ctx *ctx, int chunk_k);
 
 /* Number of kernels the last asd_ctx_step / asd_ctx_sqt* call launched. */
@@ -323,8 +329,8 @@ int asd_check_const_division_f32(unsigned long long *bad, void *stream);
 /* Diagnostic: the bare tensor-core product of the split S(q,t) GEMM,
  * C[i*ldc + j] = sum_k Ah[i][k]Bh[j][k] + Ah[i][k]Bl[j][k] + Al[i][k]Bh[j][k]
  * in FP32, for device operands [rows][Kp] (kind 1: TF32 bit patterns in
- * float, kind 2: bf16), rows a multiple of 256, Kp a multiple of 32 (TF32)
- * or 64 (BF16); chunk_k as for asd_ctx_set_chunk_k (the chunk partials are
+ * float, kind 2: bf16, kind 3: fp16), rows a multiple of 256, Kp a multiple
+ * of 32 (TF32) or 64 (16-bit kinds); chunk_k as for asd_ctx_set_chunk_k (the chunk partials are
  * added in FP32 here).  Asynchronous on stream.  It has no counterpart in the
  * reference; tests use it to check the tcgen05 core apart from the epilogue. */
 int asd_umma_gemm_f32(int kind, long rows, int Kp, const void *a_hi, const void *a_lo,

@@ -108,7 +108,7 @@ def test_qgrid_large_lattices(oracle, N, nfile):
         ctx.set_spins(s0, as_origin=True)
         ctx.step(2)
         st = ctx.get_spins()
-        for mode in ("fp64", "tf32x3", "bf16x3"):
+        for mode in ("fp64", "tf32x3", "bf16x3", "fp16x3"):
             g1 = ctx.sqt_grid(mode)
             g2 = ctx.sqt_grid(mode)
             assert np.array_equal(g1, g2), mode
@@ -118,6 +118,6 @@ def test_qgrid_large_lattices(oracle, N, nfile):
     qs += [tuple(int(x) for x in rng.integers(0, N, size=2)) for _ in range(7)]
     want = {q: oracle.sqt_factorized(N, nfile, q[0], q[1], st, s0) for q in qs}
     scale = max(abs(v) for v in want.values())
-    for mode, tol in (("fp64", 1e-12), ("tf32x3", 1e-5), ("bf16x3", 1e-5)):
+    for mode, tol in (("fp64", 1e-12), ("tf32x3", 1e-5), ("bf16x3", 1e-5), ("fp16x3", 1e-5)):
         for q, w in want.items():
             assert abs(grids[mode][q] - w) <= tol * scale, (mode, q, grids[mode][q], w)

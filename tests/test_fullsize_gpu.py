@@ -27,9 +27,9 @@ pytestmark = pytest.mark.gpu
 
 CONFIGS = {
     "128x128x500": (128, 500, dict(J1=-1.0, alpha=0.05, h=(0.0, 0.0, 0.5), dt=0.005),
-                    ["fp64", "tf32x3", "bf16x3"]),
+                    ["fp64", "tf32x3", "bf16x3", "fp16x3"]),
     "256x256x1000": (256, 1000, dict(J1=1.0, J2=-0.3, alpha=0.02, dt=0.005),
-                     ["fp64", "bf16x3", "tf32x3"]),
+                     ["fp64", "bf16x3", "tf32x3", "fp16x3"]),
 }
 
 

@@ -94,7 +94,7 @@ class Grid:
                     np.abs(self.v - other.v).max() <= self.rtol * np.abs(other.v).max())
 
 
-GRID_RTOL = {"fp64": 1e-12, "tf32x3": 1e-6, "bf16x3": 1e-6}
+GRID_RTOL = {"fp64": 1e-12, "tf32x3": 1e-6, "bf16x3": 1e-6, "fp16x3": 1e-6}
 
 
 def _same(x, y):
@@ -167,12 +167,12 @@ def test_scratch_poisoning_changes_nothing(kernel):
         ctx.set_llg_kernel(kernel)
         P()
         ctx.set_spins(s0, as_origin=True)
-        for mode in ("fp64", "tf32x3", "bf16x3"):
+        for mode in ("fp64", "tf32x3", "bf16x3", "fp16x3"):
             P()
             ctx.step(1)
             P()
             out.append(ctx.sqt(mode))
-        for mode in ("fp64", "tf32x3", "bf16x3"):
+        for mode in ("fp64", "tf32x3", "bf16x3", "fp16x3"):
             P()
             out.append(Grid(ctx.sqt_grid(mode), GRID_RTOL[mode]))
         P()

@@ -2,7 +2,7 @@
 reference fixtures.
 
 Tolerances: FP64 paths 1e-12 relative; the split-precision tensor-core paths
-(TF32x3, BF16x3) 1e-5 relative, the bound the design targets."""
+(TF32x3, BF16x3, FP16x3) 1e-5 relative, the bound the design targets."""
 from __future__ import annotations
 
 import numpy as np
@@ -14,7 +14,7 @@ from conftest import rel_err
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp64": 1e-12, "tf32x3": 1e-5, "bf16x3": 1e-5}
+TOL = {"fp64": 1e-12, "tf32x3": 1e-5, "bf16x3": 1e-5, "fp16x3": 1e-5}
 
 
 @pytest.mark.parametrize("name", ["llg_n12_f4", "llg_n20_f6"])
@@ -140,7 +140,7 @@ def test_step_host_matches_the_device_path(pinned):
             assert got == want
 
 
-@pytest.mark.parametrize("mode", ["tf32x3", "bf16x3"])
+@pytest.mark.parametrize("mode", ["tf32x3", "bf16x3", "fp16x3"])
 @pytest.mark.parametrize("kernel", ["stages", "fused"])
 def test_step_pipelined_behind_the_split_gemm(oracle, mode, kernel):
     """asd_ctx_step after a split-mode asd_ctx_sqt_async runs the next RK4 step
@@ -182,7 +182,7 @@ def test_step_pipelined_behind_the_split_gemm(oracle, mode, kernel):
                                           ("fused", "device")])
 @pytest.mark.parametrize("nf", [200, 40, 7])
 def test_step_host_async_consecutive_steps(oracle, nf, kernel, where):
-    """asd_ctx_step_host_async: five steps enqueued back to back on one pinned
+    """asd_ctx_step_host_async: six steps enqueued back to back on one pinned
     buffer (each call's output is the next call's input, so every chunk's
     upload must wait for the previous call's download of that chunk), then
     one asd_ctx_synchronize.  200 replicas make chunks of 32 (six) and 8; 40
@@ -196,7 +196,7 @@ def test_step_host_async_consecutive_steps(oracle, nf, kernel, where):
     s0 = asd.random_spins(N, nf, seed=21)
     kw = dict(J1=-1.0, J2=0.2, alpha=0.05, h=(0, 0, 0.5), dt=0.005)
     p = asd.Params.make(N, nf, vx=3, vy=2, **kw)
-    modes = ["tf32x3", "fp64", "bf16x3", "fp64", "tf32x3"]
+    modes = ["tf32x3", "fp64", "bf16x3", "fp16x3", "fp64", "tf32x3"]
     with asd.Context(p) as a, asd.Context(p) as b:
         a.set_llg_kernel(kernel)
         a.set_spins(s0, as_origin=True)
@@ -270,7 +270,7 @@ def test_step_host_in_replica_chunks(oracle, nf, pinned, kernel):
         if pinned:
             buf = buf.pin_memory()
         want_spins = s0
-        for step, mode in enumerate(["tf32x3", "fp64", "bf16x3", "fp64", "tf32x3"]):
+        for step, mode in enumerate(["tf32x3", "fp64", "bf16x3", "fp16x3", "fp64", "tf32x3"]):
             got = a.step_host(buf.data_ptr(), buf.data_ptr(), mode)
             b.step(1)
             ref = b.sqt("fp64")
@@ -284,3 +284,38 @@ def test_step_host_in_replica_chunks(oracle, nf, pinned, kernel):
                 # shorter K ranges in FP32 and is usually the closer of the two
                 assert abs(got - ref) <= 1e-5 * abs(ref), (step, mode, got, ref)
                 assert abs(b.sqt(mode) - ref) <= 1e-5 * abs(ref), (step, mode)
+
+
+@pytest.mark.parametrize("spin_len", [1e-3, 1.5, 3e4])
+def test_fp16x3_scale_follows_spin_len(oracle, spin_len):
+    """FP16x3 scales the spins by a power of two (spin_len * scale in
+    [2^12, 2^13)) before the split, so spins of any length keep the FP16
+    pair's 22 bits: 1e-3 would leave the lo parts subnormal and 3e4 would
+    come close to FP16's largest value without it.  A change of spin_len
+    through asd_ctx_set_params changes the scale, and the origin is split
+    again with it.  A component beyond FP16's range after scaling gives a
+    non-finite S(q,t), not a wrong finite one.  The exchange torque grows as
+    spin_len^2, so dt = 0.005 / spin_len keeps the same dynamics at every
+    length (without a field, which would not scale)."""
+    N, nf = 32, 40
+    kw = dict(J1=-1.0, alpha=0.05, dt=0.005 / spin_len)
+    s0 = asd.random_spins(N, nf, seed=5, spin_len=spin_len)
+    p = asd.Params.make(N, nf, spin_len=spin_len, **kw)
+    with asd.Context(p, modes=["fp64", "fp16x3"]) as ctx:
+        ctx.set_spins(s0, as_origin=True)
+        ctx.step(3)
+        st = ctx.get_spins()
+        ref = oracle.sqt_factorized(N, nf, N // 10, N // 10, st, s0)
+        assert rel_err(ctx.sqt("fp16x3"), ref) < 1e-5
+        assert rel_err(ctx.sqt("fp64"), ref) < 1e-12
+        # a new length: the next step renormalises to it, the origin keeps the
+        # old one, and both operands take the new scale
+        ctx.set_params(asd.Params.make(N, nf, spin_len=spin_len * 300.0, **kw))
+        ctx.step(1)
+        ref = ctx.sqt("fp64")
+        assert rel_err(ctx.sqt("fp16x3"), ref) < 1e-5
+    big = s0.copy()
+    big[0, 0, 0] = spin_len * 2.0 ** 5  # at least 2^17 > 65504 after scaling
+    with asd.Context(p, modes=["fp16x3"]) as ctx:
+        ctx.set_spins(big, as_origin=True)
+        assert not np.isfinite(ctx.sqt("fp16x3"))

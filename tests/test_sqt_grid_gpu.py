@@ -16,7 +16,7 @@ from conftest import rel_err
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp64": 1e-12, "tf32x3": 1e-5, "bf16x3": 1e-5}
+TOL = {"fp64": 1e-12, "tf32x3": 1e-5, "bf16x3": 1e-5, "fp16x3": 1e-5}
 
 
 def grid_err(got, want):
