@@ -13,10 +13,15 @@
 // works in FP32 per 32-column chunk and accumulates in FP64 across chunks,
 // tiles and CTAs.
 //
-// Roles (192 threads, one CTA per SM, persistent over 128 x 256 tiles):
+// Roles (one CTA per SM, persistent over 128 x 256 tiles):
 //   warp 0      TMA producer (one thread): 4 tiles per k block (Ah, Al, Bh, Bl)
 //   warp 1      MMA issuer (one thread): 3 x 4 tcgen05.mma per k block
-//   warps 2..5  epilogue: TMEM -> registers, phase/outer/reduction
+//   warps 2..   epilogue: TMEM -> registers, phase/outer/reduction.  Eight
+//               warps (two per TMEM lane quarter, each taking half of the
+//               tile's columns) for the phase epilogue, so that its pass over
+//               an accumulation chunk stays shorter than the chunk's MMAs even
+//               for small chunks; four for the q-grid epilogue, whose
+//               per-warp transposition buffers fill the shared memory.
 // TMEM holds two 128 x 256 FP32 accumulators (all 512 columns), so the
 // epilogue of one tile overlaps the MMAs of the next.
 #include <cuda.h>
@@ -32,7 +37,11 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BN = 256;
-constexpr int NUM_THREADS = 192;
+// Epilogue warps of each epilogue kind (EPI_GRID: 4, the others 8) and the
+// CTA's threads: the TMA and MMA warps plus those.
+__host__ __device__ constexpr int epi_warps(int epi) { return epi == 2 ? 4 : 8; }
+__host__ __device__ constexpr int cta_threads(int epi) { return 64 + 32 * epi_warps(epi); }
+constexpr int MAX_EPI_WARPS = 8;
 constexpr int TMEM_COLS = 512;
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
 // Row tiles per raster group.  Measured on B200 at 128x128x500 and
@@ -71,7 +80,7 @@ struct SmemTail {
     uint64_t ebar;  // epilogue warps' barrier
     uint32_t tmem_base;
     int abort_flag;
-    double red[2][4];
+    double red[2][MAX_EPI_WARPS];
 };
 
 constexpr int smem_bytes() {
@@ -100,9 +109,9 @@ __device__ __forceinline__ void raise_abort(SmemTail *t, unsigned *status) {
     if (status) atomicOr(status, (unsigned)kStatusTimeout);
 }
 
-// Barrier among the four epilogue warps on an mbarrier (count 4, one arrival
-// per warp), so that the wait is bounded like every other wait here: a warp
-// that gives up, or sees the abort flag, leaves instead of hanging.
+// Barrier among the epilogue warps on an mbarrier (one arrival per warp), so
+// that the wait is bounded like every other wait here: a warp that gives up,
+// or sees the abort flag, leaves instead of hanging.
 __device__ __forceinline__ bool epilogue_sync(uint64_t *bar, uint32_t &phase,
                                               volatile int *abort) {
     __syncwarp();
@@ -225,8 +234,9 @@ __device__ __forceinline__ void grid_block(const uint32_t (&v)[32], int c, int l
 //              warps' registers are combined per tile in warp order.  No
 //              atomics: the bins repeat bit for bit.
 constexpr int EPI_PHASE = 0, EPI_STORE = 1, EPI_GRID = 2;
+static_assert(epi_warps(EPI_GRID) == 4 && epi_warps(EPI_PHASE) == MAX_EPI_WARPS, "warp counts");
 template <int KIND, int EPI>
-__global__ void __launch_bounds__(NUM_THREADS, 1)
+__global__ void __launch_bounds__(cta_threads(EPI), 1)
     umma_sqt_kernel(const __grid_constant__ CUtensorMap tm_ah,
                     const __grid_constant__ CUtensorMap tm_al,
                     const __grid_constant__ CUtensorMap tm_bh,
@@ -238,6 +248,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     int lat_n, double *__restrict__ tdiag, int group_m) {
     using G = Geo;
     constexpr bool STORE = (EPI == EPI_STORE);
+    constexpr int EW = epi_warps(EPI);         // epilogue warps
+    constexpr int NHALF = EW / 4;              // warps per TMEM lane quarter
+    constexpr int GPH = BN / 32 / NHALF;       // 32-column groups per warp
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -256,10 +269,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             ptx::mbar_init(&tail->tfull[b], 1);
-            ptx::mbar_init(&tail->tempty[b], 4);  // one arrival per epilogue warp
+            ptx::mbar_init(&tail->tempty[b], EW);  // one arrival per epilogue warp
         }
         ptx::mbar_init(&tail->drain, 1);
-        ptx::mbar_init(&tail->ebar, 4);
+        ptx::mbar_init(&tail->ebar, EW);
         tail->abort_flag = 0;
         ptx::fence_mbar_init();
     }
@@ -404,10 +417,13 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             if (i >= WAIT_LIMIT && status) atomicOr(status, (unsigned)kStatusTimeout);
         }
     } else {
-        // Epilogue warps 2..5 own TMEM lane quarters (warp % 4) * 32.
+        // Epilogue warps 2.. own TMEM lane quarters (warp % 4) * 32; with
+        // eight, warps 2..5 take the column groups [0, 4) and warps 6..9
+        // the groups [4, 8) of every chunk.
         const int quarter = warp & 3;
         const int rloc = quarter * 32 + lane;
-        const int etid = threadIdx.x - 64;  // 0..127 among the epilogue threads
+        const int etid = threadIdx.x - 64;  // 0 .. 32 EW - 1 among the epilogue threads
+        const int c_first = ((warp - 2) / 4) * GPH;
         int abuf = 0;
         uint32_t aphase = 0;
         double tot_re = 0.0, tot_im = 0.0;
@@ -428,8 +444,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 // epilogue warp finished tile - 2 before it passed the
                 // barrier of tile - 1).
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int jl = etid + 128 * h;
+                for (int h = 0; h < BN / (32 * EW); ++h) {
+                    const int jl = etid + 32 * EW * h;
                     const float4 cz = __ldg(&col4[j0 + jl]);
                     w_tab[jl] = make_float2(cz.w, __ldg(&col1[j0 + jl]));
                     z_tab[jl] = make_float4(cz.x, cz.y, cz.z, 0.f);
@@ -474,7 +490,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 // the groups: its per-lane diagonal registers are indexed by c.)
                 constexpr int CU = (EPI == EPI_GRID) ? BN / 32 : 1;
 #pragma unroll CU
-                for (int c = 0; c < BN / 32; ++c) {
+                for (int cc = 0; cc < GPH; ++cc) {
+                    const int c = (EPI == EPI_GRID) ? cc : c_first + cc;  // a constant for the grid
                     uint32_t v[32];
                     const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) +
                                            (uint32_t)(abuf * BN + c * 32);
@@ -549,7 +566,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     break;
                 }
                 double *td = tdiag + ((long)mb * num_n + nb) * GRID_ND * 2;
-                for (int idx = etid; idx < GRID_ND * 2; idx += 128) {
+                for (int idx = etid; idx < GRID_ND * 2; idx += 32 * EW) {
                     const int d = idx / 2 - (BN - 1), cls = idx & 1;
                     const int L = (d + 256) & 31, m = (d - L) / 32;
                     double sum = 0.0;
@@ -585,8 +602,12 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     __syncthreads();
     ptx::tc_fence_after();
     if (threadIdx.x == 0 && EPI == EPI_PHASE) {
-        const double re = (tail->red[0][0] + tail->red[0][1]) + (tail->red[0][2] + tail->red[0][3]);
-        const double im = (tail->red[1][0] + tail->red[1][1]) + (tail->red[1][2] + tail->red[1][3]);
+        double re = 0.0, im = 0.0;  // fixed order: the results repeat bit for bit
+#pragma unroll
+        for (int w = 0; w < EW; ++w) {
+            re += tail->red[0][w];
+            im += tail->red[1][w];
+        }
         part[blockIdx.x] = make_double2(re, im);
     }
     if (warp == 0) ptx::tmem_dealloc(tmem_base, TMEM_COLS);
@@ -683,7 +704,7 @@ int launch_umma_sqt(const UmmaSqtArgs &a, cudaStream_t st) {
         cudaError_t r =
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (r != cudaSuccess) return r;
-        kern<<<grid, NUM_THREADS, smem, st>>>(tah, tal, tbh, tbl, num_m, num_n, kb_begin, kb_end,
+        kern<<<grid, cta_threads(epi), smem, st>>>(tah, tal, tbh, tbl, num_m, num_n, kb_begin, kb_end,
                                               kpc, a.outer, a.row4, a.row1, a.col4, a.col1,
                                               a.alpha, a.part, a.status, a.dbg_c, a.dbg_ldc,
                                               a.lat_n, a.tdiag, GROUP_M);
