@@ -173,7 +173,9 @@ def bench_config(name: str, args) -> dict:
     M, K = N * N, 3 * nf
     mode = args.mode or w["mode"]
     state_mb = M * K * 8 / 1e6
-    return {"workload": w["desc"], "sites": M, "replicas": nf, "gemm_m": M, "gemm_n": M,
+    label = {"fp64": "FP64", "tf32x3": "TF32x3", "bf16x3": "BF16x3", "fp16x3": "FP16x3"}
+    desc = w["desc"].replace(f"S(q,t) in {label[w['mode']]}", f"S(q,t) in {label[mode]}")
+    return {"workload": desc, "sites": M, "replicas": nf, "gemm_m": M, "gemm_n": M,
             "gemm_k": K, "sqt_mode": mode, "llg_kernel": args.llg_kernel,
             "chunk_k": args.chunk_k if args.chunk_k >= 0 else DEFAULT_CHUNK_K.get(mode, 0),
             "l2": f"inputs larger than L2 (spin state {state_mb:.0f} MB per array)"}
