@@ -60,7 +60,7 @@ EXPORTED_SYMBOLS = (
     "asd_batch_set_stream", "asd_batch_set_spins", "asd_batch_get_spins", "asd_batch_run",
     "asd_batch_configure", "asd_batch_configure_cluster", "asd_batch_autotune",
     "asd_batch_plan_clusters", "asd_set_params", "euler", "runge_kutta",
-    "fused_dgemm",
+    "fused_dgemm", "asd_cblas_dgemm",
 )
 
 
@@ -187,6 +187,8 @@ def load() -> C.CDLL:
         "fused_dgemm": ([C.POINTER(C.c_int)] * 3 + [dp, vp, C.POINTER(C.c_int), vp,
                                                    C.POINTER(C.c_int), vp, C.POINTER(C.c_int),
                                                    vp, vp], None),
+        "asd_cblas_dgemm": ([C.c_int] * 6 + [C.c_double, vp, C.c_int, vp, C.c_int, C.c_double,
+                                             vp, C.c_int], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -479,6 +481,23 @@ def fused_dgemm(m, n, k, alpha, a, lda, b, ldb, c, ldc, q, sum_):
             raise ValueError("fused_dgemm arrays must be C-contiguous float64")
     load().fused_dgemm(ci(m), ci(n), ci(k), C.byref(al), _ptr(a), ci(lda), _ptr(b), ci(ldb),
                        _ptr(c), ci(ldc), _ptr(q), _ptr(sum_))
+
+
+CBLAS_ROW_MAJOR, CBLAS_COL_MAJOR = 101, 102
+CBLAS_NO_TRANS, CBLAS_TRANS, CBLAS_CONJ_TRANS = 111, 112, 113
+
+
+def cblas_dgemm(order, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> None:
+    """asd_cblas_dgemm, the reference's cblas_dgemm (gemm/llg_sqt_mkl.c:378) on the GPU,
+    on host float64 arrays (a and b may be None where BLAS reads neither); c is updated
+    in place."""
+    for arr in (a, b, c):
+        if arr is not None and not (arr.dtype == np.float64 and arr.flags.c_contiguous):
+            raise ValueError("cblas_dgemm arrays must be C-contiguous float64")
+    ptr = lambda arr: None if arr is None else C.c_void_p(arr.ctypes.data)
+    _check(load().asd_cblas_dgemm(int(order), int(transa), int(transb), int(m), int(n), int(k),
+                                  float(alpha), ptr(a), int(lda), ptr(b), int(ldb), float(beta),
+                                  ptr(c), int(ldc)))
 
 
 def umma_gemm_f32(kind: int, rows: int, Kp: int, a_hi: int, a_lo: int, b_hi: int, b_lo: int,

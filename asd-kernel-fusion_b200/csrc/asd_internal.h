@@ -134,10 +134,22 @@ struct DmmaSqtArgs {
     int lat_n = 0;        // q grid: lattice side
     double *tdiag = nullptr;  // q grid: [tiles][dmma_sqt_tile() * 2 - 1][2]
     int abs_sum = 0;      // sum |alpha C_ij - m_i . z_j| instead (no phase)
+    // Plain product (the cblas_dgemm drop-in): with C set, B has MB rows and
+    // the kernel stores C[i + j ldc] = alpha sum_k A_ik B_jk (+ beta C[..] when
+    // beta != 0; C is not read when beta == 0) for i < M, j < MB.
+    long MB = 0;
+    double *C = nullptr;
+    long ldc = 0;
+    double beta = 0.0;
 };
 constexpr int kDmmaTile = 128;  // tile rows = tile columns
 long dmma_sqt_tiles(long M);
 int launch_dmma_sqt(const DmmaSqtArgs &p, cudaStream_t st);
+// Device transpose of a dense [rows][cols] FP64 matrix into [cols][rows].
+cudaError_t launch_transpose_f64(const double *in, long rows, long cols, double *out,
+                                 cudaStream_t st);
+// C[i + j ldc] *= beta for i < m, j < n (beta == 0: set to +0).
+cudaError_t launch_scale_f64(double *c, long m, long n, long ldc, double beta, cudaStream_t st);
 
 // q grid (qgrid.cu): from per-tile diagonal partials tdiag[mb][nb][bm+bn-1][2]
 // of num_m x num_n tiles of bm x bn sites (bn a multiple of bm) to the N*N

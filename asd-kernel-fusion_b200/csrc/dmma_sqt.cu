@@ -15,6 +15,9 @@
 // whether the lattice column of j wraps around (qgrid.cu bins them by
 // displacement).  Every sum runs in a fixed order: results repeat bit for bit.
 //
+// The same main loop with a store epilogue is the plain product behind the
+// cblas_dgemm drop-in (C = alpha A B^T + beta C, A [M][K], B [MB][K]).
+//
 // Operands: A = the state at t, B = the origin, both site-major [M][K] FP64
 // (K = 3 * nfile contiguous), i.e. the GEMM is C = A B^T with both operands
 // K-major.  Tiles of 128 x 128, K staged 32 at a time through a 3-deep
@@ -41,7 +44,7 @@ constexpr int STAGE_DOUBLES = (BM + BN) * BK;  // 8192 doubles = 64 KB
 constexpr int PIPE_BYTES = STAGES * STAGE_DOUBLES * 8;
 constexpr int TSTRIDE = BN + 1;  // q grid: epilogue tile row stride (doubles)
 constexpr int GRID_SMEM = BM * TSTRIDE * 8;
-constexpr int EPI_PHASE = 0, EPI_GRID = 1;
+constexpr int EPI_PHASE = 0, EPI_GRID = 1, EPI_STORE = 2;
 constexpr int KCH = BK / 2;  // 16-byte chunks per shared-memory row
 constexpr int LOG_KCH = 4;
 static_assert(KCH == (1 << LOG_KCH), "chunks per row");
@@ -115,7 +118,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const double *__restrict__ mrow, const double *__restrict__ zcol,
                     const double2 *__restrict__ uphase, const double2 *__restrict__ wphase,
                     double2 *__restrict__ part, int lat_n, double *__restrict__ tdiag,
-                    int abs_sum) {
+                    int abs_sum, long MB, double *__restrict__ Cst, long ldc, double beta) {
     extern __shared__ __align__(16) double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
@@ -124,6 +127,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     tile_coords(blockIdx.x, num_m, num_n, mb, nb);
     const long m0 = (long)mb * BM, n0 = (long)nb * BN;
     const int nkb = (K + BK - 1) / BK;
+    const long MBr = (EPI == EPI_STORE) ? MB : M;  // rows of B (M for S(q,t))
 
     double acc[4][4][4];
 #pragma unroll
@@ -137,7 +141,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     for (int s = 0; s < STAGES - 1; ++s) {
         if (s < nkb) {
             load_tile<VEC>(smem + s * STAGE_DOUBLES, A, M, K, m0, s * BK);
-            load_tile<VEC>(smem + s * STAGE_DOUBLES + TILE_DOUBLES, B, M, K, n0, s * BK);
+            load_tile<VEC>(smem + s * STAGE_DOUBLES + TILE_DOUBLES, B, MBr, K, n0, s * BK);
         }
         cp_commit();
     }
@@ -150,7 +154,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             if (kn < nkb) {
                 double *st = smem + (kn % STAGES) * STAGE_DOUBLES;
                 load_tile<VEC>(st, A, M, K, m0, kn * BK);
-                load_tile<VEC>(st + TILE_DOUBLES, B, M, K, n0, kn * BK);
+                load_tile<VEC>(st + TILE_DOUBLES, B, MBr, K, n0, kn * BK);
             }
             cp_commit();
         }
@@ -185,7 +189,25 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     cp_wait<0>();
 
-    if (EPI == EPI_PHASE) {
+    if (EPI == EPI_STORE) {
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const long i = m0 + wm * 64 + mt * 16 + g + 8 * h;
+                if (i >= M) continue;
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const long j = n0 + wn * 32 + nt * 8 + 2 * t + e;
+                        if (j >= MBr) continue;
+                        double *cp = Cst + i + j * ldc;
+                        const double v = alpha * acc[mt][nt][2 * h + e];
+                        *cp = (beta != 0.0) ? v + beta * *cp : v;
+                    }
+            }
+    } else if (EPI == EPI_PHASE) {
         // sum over the thread's 8 rows x 8 columns of u_i w_j (alpha C_ij - m_i . z_j)
         double tot_re = 0.0, tot_im = 0.0;
 #pragma unroll
@@ -304,7 +326,50 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
 }
 
+// 32 x 32 tiles through shared memory (a padded column avoids bank conflicts).
+__global__ void __launch_bounds__(256) transpose_f64_kernel(const double *__restrict__ in,
+                                                            long rows, long cols,
+                                                            double *__restrict__ out) {
+    __shared__ double tile[32][33];
+    const long r0 = (long)blockIdx.y * 32, c0 = (long)blockIdx.x * 32;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const long r = r0 + y, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) tile[y][threadIdx.x] = in[r * cols + c];
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const long c = c0 + y, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) out[c * rows + r] = tile[threadIdx.x][y];
+    }
+}
+
+__global__ void scale_f64_kernel(double *c, long m, long n, long ldc, double beta) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m * n) return;
+    const long j = t / m, i = t - j * m;
+    double *p = c + i + j * ldc;
+    *p = (beta == 0.0) ? 0.0 : beta * *p;
+}
+
 }  // namespace
+
+cudaError_t launch_transpose_f64(const double *in, long rows, long cols, double *out,
+                                 cudaStream_t st) {
+    if (rows <= 0 || cols <= 0) return cudaSuccess;
+    const long gx = (cols + 31) / 32, gy = (rows + 31) / 32;
+    if (gx > 0x7fffffffL || gy > 65535) return cudaErrorInvalidConfiguration;
+    transpose_f64_kernel<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(in, rows, cols,
+                                                                                   out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale_f64(double *c, long m, long n, long ldc, double beta, cudaStream_t st) {
+    if (m <= 0 || n <= 0) return cudaSuccess;
+    const long blocks = (m * n + 255) / 256;
+    if (blocks > 0x7fffffffL) return cudaErrorInvalidConfiguration;
+    scale_f64_kernel<<<(unsigned)blocks, 256, 0, st>>>(c, m, n, ldc, beta);
+    return cudaGetLastError();
+}
 
 long dmma_sqt_tiles(long M) {
     const long nm = (M + BM - 1) / BM;
@@ -314,10 +379,13 @@ long dmma_sqt_tiles(long M) {
 int dmma_sqt_diagonals() { return BM + BN - 1; }
 
 int launch_dmma_sqt(const DmmaSqtArgs &p, cudaStream_t st) {
-    if (p.M <= 0 || p.K <= 0) return fail(ASD_ERR_INVALID, "empty GEMM");
-    const long nm = (p.M + BM - 1) / BM;
-    if (nm * nm > 0x7fffffffL) return fail(ASD_ERR_UNSUPPORTED, "too many tiles");
-    const int num_m = (int)nm, num_n = (int)nm;
+    const bool store = (p.C != nullptr);
+    const long MB = store ? p.MB : p.M;
+    if (p.M <= 0 || MB <= 0 || p.K <= 0) return fail(ASD_ERR_INVALID, "empty GEMM");
+    if (store && (p.tdiag || p.ldc < p.M)) return fail(ASD_ERR_INVALID, "store: bad ldc or q grid");
+    const long nm = (p.M + BM - 1) / BM, nn = (MB + BN - 1) / BN;
+    if (nm * nn > 0x7fffffffL) return fail(ASD_ERR_UNSUPPORTED, "too many tiles");
+    const int num_m = (int)nm, num_n = (int)nn;
     const bool grid = (p.tdiag != nullptr);
     if (grid && (p.lat_n < 1 || (long)p.lat_n * p.lat_n != p.M))
         return fail(ASD_ERR_INVALID, "q grid needs M = N*N");
@@ -326,14 +394,16 @@ int launch_dmma_sqt(const DmmaSqtArgs &p, cudaStream_t st) {
     auto go = [&](auto kern) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
-        kern<<<(unsigned)(nm * nm), THREADS, smem, st>>>(p.A, p.B, p.M, p.K, num_m, num_n, p.alpha,
+        kern<<<(unsigned)(nm * nn), THREADS, smem, st>>>(p.A, p.B, p.M, p.K, num_m, num_n, p.alpha,
                                                           p.outer, p.mrow, p.zcol, p.uphase,
                                                           p.wphase, p.part, p.lat_n, p.tdiag,
-                                                          p.abs_sum);
+                                                          p.abs_sum, MB, p.C, p.ldc, p.beta);
         return cudaGetLastError();
     };
     cudaError_t e;
-    if (grid)
+    if (store)
+        e = vec2 ? go(dmma_sqt_kernel<2, EPI_STORE>) : go(dmma_sqt_kernel<1, EPI_STORE>);
+    else if (grid)
         e = vec2 ? go(dmma_sqt_kernel<2, EPI_GRID>) : go(dmma_sqt_kernel<1, EPI_GRID>);
     else
         e = vec2 ? go(dmma_sqt_kernel<2, EPI_PHASE>) : go(dmma_sqt_kernel<1, EPI_PHASE>);

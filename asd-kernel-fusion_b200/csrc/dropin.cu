@@ -3,6 +3,9 @@
 //   euler        baseline/llg_sqt_baseline.c:29
 //   runge_kutta  baseline/llg_sqt_baseline.c:95
 //   fused_dgemm  kernel_fusion/gemm_kernel.h:355
+// and the BLAS product of the reference's plain path, cblas_dgemm
+// (gemm/llg_sqt_mkl.c:378), as asd_cblas_dgemm (exported under the BLAS name
+// by the separate libasd_cblas.so, csrc/cblas_shim.c).
 // They take host pointers and return when the results are back in host
 // memory, like the originals.  Device buffers are cached between calls on the
 // current device and grow on demand.  The functions return void, as in the
@@ -10,6 +13,7 @@
 // and leaves the outputs unchanged.
 #include <cstdio>
 #include <mutex>
+#include <utility>
 
 #include "asd_internal.h"
 #include "fp64_gemm.h"
@@ -43,6 +47,8 @@ struct Buffers {
     double *g[4] = {};  // a, b, c, q
     double2 *part = nullptr;
     size_t part_cap = 0;
+    size_t blas_cap[4] = {};
+    double *blas[4] = {};  // A [m][k], B [n][k], C [n][m], transpose staging
 };
 Buffers g_buf;
 
@@ -220,6 +226,90 @@ int do_fused_dgemm(int m, int n, int k, double alpha, const double *a, int lda, 
     return ASD_OK;
 }
 
+// cblas_dgemm with the CBLAS constants (CblasRowMajor 101, CblasColMajor 102,
+// CblasNoTrans 111, CblasTrans 112, CblasConjTrans 113 = CblasTrans for real
+// data) and the BLAS argument rules.  A row-major product is the column-major
+// product of the transposes with the operands swapped.  Column-major
+// C (m x n) = alpha op(A) op(B) + beta C runs on the FP64 tensor-core GEMM
+// with K-contiguous operands [m][k] and [n][k]: op(A) with transa = T and
+// op(B) with transb = N are already K-contiguous in host memory (strided
+// copies), the other two are uploaded as they lie and transposed on the
+// device.  C is read only when beta != 0, as BLAS specifies.
+int do_cblas_dgemm(int order, int transa, int transb, int m, int n, int k, double alpha,
+                   const double *a, int lda, const double *b, int ldb, double beta, double *c,
+                   int ldc) {
+    auto is_trans = [](int t) { return t == 112 || t == 113; };
+    if (order != 101 && order != 102) return fail(ASD_ERR_INVALID, "order %d (parameter 1)", order);
+    if (transa != 111 && !is_trans(transa))
+        return fail(ASD_ERR_INVALID, "transa %d (parameter 2)", transa);
+    if (transb != 111 && !is_trans(transb))
+        return fail(ASD_ERR_INVALID, "transb %d (parameter 3)", transb);
+    if (m < 0 || n < 0 || k < 0) return fail(ASD_ERR_INVALID, "negative dimension");
+    if (order == 101) {  // row major: C^T = op(B)^T op(A)^T in column-major terms
+        std::swap(transa, transb);
+        std::swap(m, n);
+        std::swap(a, b);
+        std::swap(lda, ldb);
+    }
+    const bool ta = is_trans(transa), tb = is_trans(transb);
+    const int arows = ta ? k : m, brows = tb ? n : k;
+    if (lda < (arows > 1 ? arows : 1) || ldb < (brows > 1 ? brows : 1) || ldc < (m > 1 ? m : 1))
+        return fail(ASD_ERR_INVALID, "leading dimension too small (lda=%d ldb=%d ldc=%d)", lda, ldb,
+                    ldc);
+    if (m == 0 || n == 0) return ASD_OK;
+    const bool product = (k > 0 && alpha != 0.0);
+    if (!product && beta == 1.0) return ASD_OK;
+    if (!c || (product && (!a || !b))) return fail(ASD_ERR_INVALID, "NULL matrix");
+    int dev = 0;
+    ASD_CUDA_TRY(cudaGetDevice(&dev));
+    if (g_buf.device != dev) {
+        g_buf = Buffers();
+        g_buf.device = dev;
+    }
+    const size_t mk = (size_t)m * k, nk = (size_t)n * k, mn = (size_t)m * n;
+    int rc;
+    if ((rc = reserve(&g_buf.blas[2], &g_buf.blas_cap[2], mn)) != ASD_OK) return rc;
+    double *dC = g_buf.blas[2];  // column-major m x n, leading dimension m
+    const size_t D = sizeof(double);
+    if (beta != 0.0)
+        ASD_CUDA_TRY(cudaMemcpy2D(dC, m * D, c, (size_t)ldc * D, m * D, n, cudaMemcpyHostToDevice));
+    if (!product) {
+        ASD_CUDA_TRY(launch_scale_f64(dC, m, n, m, beta, 0));
+    } else {
+        if ((rc = reserve(&g_buf.blas[0], &g_buf.blas_cap[0], mk)) != ASD_OK) return rc;
+        if ((rc = reserve(&g_buf.blas[1], &g_buf.blas_cap[1], nk)) != ASD_OK) return rc;
+        if ((!ta || tb) &&
+            (rc = reserve(&g_buf.blas[3], &g_buf.blas_cap[3], mk > nk ? mk : nk)) != ASD_OK)
+            return rc;
+        double *dA = g_buf.blas[0], *dB = g_buf.blas[1], *tmp = g_buf.blas[3];
+        if (ta) {  // op(A)(i, l) = a[l + i lda]: m rows of k
+            ASD_CUDA_TRY(cudaMemcpy2D(dA, k * D, a, (size_t)lda * D, k * D, m, cudaMemcpyHostToDevice));
+        } else {  // A(i, l) = a[i + l lda]: k columns of m, transposed on the device
+            ASD_CUDA_TRY(cudaMemcpy2D(tmp, m * D, a, (size_t)lda * D, m * D, k, cudaMemcpyHostToDevice));
+            ASD_CUDA_TRY(launch_transpose_f64(tmp, k, m, dA, 0));
+        }
+        if (!tb) {  // op(B)(l, j) = b[l + j ldb]: n rows of k
+            ASD_CUDA_TRY(cudaMemcpy2D(dB, k * D, b, (size_t)ldb * D, k * D, n, cudaMemcpyHostToDevice));
+        } else {  // op(B)(l, j) = b[j + l ldb]: k rows of n, transposed on the device
+            ASD_CUDA_TRY(cudaMemcpy2D(tmp, n * D, b, (size_t)ldb * D, n * D, k, cudaMemcpyHostToDevice));
+            ASD_CUDA_TRY(launch_transpose_f64(tmp, k, n, dB, 0));
+        }
+        DmmaSqtArgs g{};
+        g.A = dA;
+        g.B = dB;
+        g.M = m;
+        g.MB = n;
+        g.K = k;
+        g.alpha = alpha;
+        g.C = dC;
+        g.ldc = m;
+        g.beta = beta;
+        if ((rc = launch_dmma_sqt(g, 0)) != ASD_OK) return rc;
+    }
+    ASD_CUDA_TRY(cudaMemcpy2D(c, (size_t)ldc * D, dC, m * D, m * D, n, cudaMemcpyDeviceToHost));
+    return ASD_OK;
+}
+
 }  // namespace
 }  // namespace asd
 
@@ -246,6 +336,13 @@ void euler(double *spin0, double *derivative) {
 void runge_kutta(double *spin, double *cur_input, double *k1, double *k2, double *k3, double *k4) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (do_rk(spin, cur_input, k1, k2, k3, k4) != ASD_OK) report("runge_kutta");
+}
+
+int asd_cblas_dgemm(int order, int transa, int transb, int m, int n, int k, double alpha,
+                    const double *a, int lda, const double *b, int ldb, double beta, double *c,
+                    int ldc) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return do_cblas_dgemm(order, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
 }
 
 void fused_dgemm(int *m, int *n, int *k, double *alpha, double *a, int *lda, double *b, int *ldb,

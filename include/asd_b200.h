@@ -13,6 +13,8 @@
  *        euler            <- baseline/llg_sqt_baseline.c:29
  *        runge_kutta      <- baseline/llg_sqt_baseline.c:95
  *        fused_dgemm      <- kernel_fusion/gemm_kernel.h:355
+ *     and the plain path's BLAS call, cblas_dgemm <- gemm/llg_sqt_mkl.c:378,
+ *     as asd_cblas_dgemm (libasd_cblas.so exports it under the BLAS name).
  *     A C program of the reference links libasd_b200.so instead of defining
  *     these functions itself (deleting their bodies and including this
  *     header; the program's globals N, Nfile, J1, dt are read through weak
@@ -489,6 +491,20 @@ void runge_kutta(double *spin, double *cur_input, double *k1, double *k2, double
  * 4 and a last odd column are left untouched, as in the reference. */
 void fused_dgemm(int *m, int *n, int *k, double *alpha, double *a, int *lda, double *b,
                  int *ldb, double *c, int *ldc, double *fuse_C, double *sum);
+
+/* gemm/llg_sqt_mkl.c:378 -- the plain path's cblas_dgemm on the GPU:
+ * C = alpha * op(A) * op(B) + beta * C with the CBLAS arguments (order
+ * 101 row-major / 102 column-major; trans 111 none, 112 or 113 transpose) and
+ * BLAS rules (C is not read when beta == 0; m or n == 0, or k == 0 / alpha
+ * == 0 with beta == 1, do nothing).  Host pointers, synchronous; the product
+ * runs on the FP64 tensor-core GEMM (mma.sync .f64), so its rounding differs
+ * from a CPU BLAS only in the order of the FP64 sums.  libasd_cblas.so
+ * (include/asd_cblas.h) exports it under the BLAS name, so that the
+ * reference's gemm program links it in place of MKL or OpenBLAS.  Returns
+ * ASD_ERR_INVALID for the arguments BLAS rejects. */
+int asd_cblas_dgemm(int order, int transa, int transb, int m, int n, int k, double alpha,
+                    const double *a, int lda, const double *b, int ldb, double beta, double *c,
+                    int ldc);
 
 #ifdef __cplusplus
 }
