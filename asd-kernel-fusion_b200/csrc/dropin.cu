@@ -67,6 +67,28 @@ void report(const char *fn) {
     fprintf(stderr, "libasd_b200 %s: %s\n", fn, asd_last_error());
 }
 
+// The cached buffers belong to one device.  A call on another device frees
+// them there (with that device current, as cudaFree wants) and starts over.
+int use_current_device() {
+    int dev = 0;
+    ASD_CUDA_TRY(cudaGetDevice(&dev));
+    if (g_buf.device == dev) return ASD_OK;
+    if (g_buf.device >= 0 && cudaSetDevice(g_buf.device) == cudaSuccess) {
+        for (double *q : g_buf.arr)
+            if (q) cudaFree(q);
+        for (double *q : g_buf.g)
+            if (q) cudaFree(q);
+        for (double *q : g_buf.blas)
+            if (q) cudaFree(q);
+        if (g_buf.part) cudaFree(g_buf.part);
+    }
+    cudaGetLastError();
+    ASD_CUDA_TRY(cudaSetDevice(dev));
+    g_buf = Buffers();
+    g_buf.device = dev;
+    return ASD_OK;
+}
+
 int reserve(double **p, size_t *cap, size_t n) {
     if (n <= *cap && *p) return ASD_OK;
     if (*p) cudaFree(*p);
@@ -82,13 +104,8 @@ int reserve(double **p, size_t *cap, size_t n) {
 }
 
 int prepare(int ndouble_arrays, size_t n) {
-    int dev = 0;
-    ASD_CUDA_TRY(cudaGetDevice(&dev));
-    if (g_buf.device != dev) {
-        // buffers of another device are abandoned to that device's context
-        g_buf = Buffers();
-        g_buf.device = dev;
-    }
+    int rc0 = use_current_device();
+    if (rc0 != ASD_OK) return rc0;
     if (n > g_buf.cap) {
         for (int i = 0; i < 6; ++i) {
             if (g_buf.arr[i]) cudaFree(g_buf.arr[i]);
@@ -163,12 +180,7 @@ int do_fused_dgemm(int m, int n, int k, double alpha, const double *a, int lda, 
     if (lda < m || ldb < k || ldc < 2 * ((m + 3) / 4) * 4)
         return fail(ASD_ERR_INVALID, "leading dimension too small (lda=%d ldb=%d ldc=%d)", lda,
                     ldb, ldc);
-    int dev = 0;
-    ASD_CUDA_TRY(cudaGetDevice(&dev));
-    if (g_buf.device != dev) {
-        g_buf = Buffers();
-        g_buf.device = dev;
-    }
+    if (int rc0 = use_current_device()) return rc0;
     const size_t na = (size_t)lda * k, nb = (size_t)ldb * n, nc = (size_t)ldc * n;
     int rc;
     if ((rc = reserve(&g_buf.g[0], &g_buf.gemm_cap[0], na)) != ASD_OK) return rc;
@@ -260,12 +272,7 @@ int do_cblas_dgemm(int order, int transa, int transb, int m, int n, int k, doubl
     const bool product = (k > 0 && alpha != 0.0);
     if (!product && beta == 1.0) return ASD_OK;
     if (!c || (product && (!a || !b))) return fail(ASD_ERR_INVALID, "NULL matrix");
-    int dev = 0;
-    ASD_CUDA_TRY(cudaGetDevice(&dev));
-    if (g_buf.device != dev) {
-        g_buf = Buffers();
-        g_buf.device = dev;
-    }
+    if (int rc0 = use_current_device()) return rc0;
     const size_t mk = (size_t)m * k, nk = (size_t)n * k, mn = (size_t)m * n;
     int rc;
     if ((rc = reserve(&g_buf.blas[2], &g_buf.blas_cap[2], mn)) != ASD_OK) return rc;
