@@ -86,3 +86,17 @@ def test_llg_fraction_per_clock():
     llg2 = bench.llg_report({"fused": 4.0}, 6.5536e7, 387, 6538.0, 16.9, 16.9)
     bench.add_per_clock(llg2, None, {"sm_mhz": 1965})
     assert "fp64_frac_per_clock" not in llg2["fused"]
+
+
+@pytest.mark.parametrize("name,mode,label", [("sqt256", None, "BF16x3"), ("sqt128", None, "TF32x3"),
+                                             ("sqt128", "bf16x3", "BF16x3"),
+                                             ("sqt256", "fp16x3", "FP16x3")])
+def test_config_names_the_mode_it_runs(name, mode, label):
+    """The workload string and sqt_mode name the S(q,t) mode a run uses,
+    also when --mode overrides the workload's own."""
+    bench = _bench()
+    args = types.SimpleNamespace(mode=mode, llg_kernel="auto", chunk_k=-1)
+    cfg = bench.bench_config(name, args)
+    assert cfg["workload"].endswith(f"S(q,t) in {label}")
+    assert cfg["sqt_mode"] == label.lower()
+    assert cfg["chunk_k"] == (512 if label == "TF32x3" else 1024)
