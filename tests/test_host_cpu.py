@@ -58,6 +58,10 @@ def test_host_has_no_cpu_fallback(host_bin):
     r = subprocess.run([str(host_bin), "-n", "8", "-f", "2", "-m", "2"], capture_output=True,
                        text=True)
     assert r.returncode == 1 and "CUDA" in r.stderr
+    for mode in ("fp64", "tf32x3", "bf16x3", "fp16x3"):  # every mode parses; none runs on the CPU
+        r = subprocess.run([str(host_bin), "-n", "8", "-f", "2", "-m", "2", "-q", mode],
+                           capture_output=True, text=True)
+        assert r.returncode == 1 and "CUDA" in r.stderr, mode
 
 
 def test_dropin_program_links_against_the_library(tmp_path):
